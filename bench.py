@@ -1,0 +1,376 @@
+"""Benchmark: Newton-step linear solve on one B200.
+
+One step = one Newton linear solve of the workload: triplet assembly, MAS
+preconditioner build, PCG to a relative residual of 1e-4 verified in FP64.
+The workload is 8 jittered Kuhn-split tet cubes of 40^3 cells stacked with
+1 mm gaps (551,368 vertices, 1.65 M DoF, 31.8 M raw triplets, ~4.3 M unique
+upper blocks incl. point-triangle / edge-edge contact blocks), synthetic
+(seeded) data generated on the host.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
+
+Prints ONE JSON line (rank 0). With N > 1 every rank solves its own replica
+(the solve does not shard; replicas only) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # plain vs mixed precision, 8 stacked 40^3-cell cubes
+    "stack8x40": dict(cells=40, n_cubes=8, seed=0),
+    # the reference's CPU-runnable small case
+    "cube10": dict(cells=10, n_cubes=1, seed=0),
+}
+METRIC = "Newton linear-solve ms & PCG iters to 1e-4 rel-res: mixed+learned vs plain, 1 B200"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def spmv_bytes(U: int, nb: int) -> int:
+    """Algorithmic bytes of one FP64 symmetric SpMV from the block-upper
+    minimal format: blocks (4 B column index + 72 B values), row pointers,
+    x read and y written once."""
+    return U * (4 + 72) + 4 * (nb + 1) + 3 * nb * (8 + 8)
+
+
+def build_workload(name: str):
+    from libuipc_b200 import scene
+
+    w = WORKLOADS[name]
+    t = time.time()
+    s = scene.generate(scene=1, cells_x=w["cells"], cells_y=w["cells"], cells_z=w["cells"], n_cubes=w["n_cubes"],
+                       seed=w["seed"])
+    return s, time.time() - t
+
+
+def cpu_baseline(s, budget_s: float = 20.0) -> dict:
+    """Host-core FP64 3x3 block-Jacobi PCG (the oracle port, OpenMP over all
+    cores) on the same system: assembly + PCG to rel-res 1e-4. Bounded: the
+    PCG runs at most as many iterations as fit in the budget, and the time
+    per solve is extrapolated from the measured per-iteration time when it
+    stops early."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    t0 = time.time()
+    A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals)
+    t_asm = time.time() - t0
+    # probe the iteration cost, then run a bounded solve
+    t1 = time.time()
+    _, probe = O.pcg(A, s.b, precond=O.ORC_PRECOND_JACOBI, tol=1e-30, stop_rule=O.ORC_STOP_RELRES, max_iter=6,
+                     threads=threads)
+    per_it = (time.time() - t1) / 6.0
+    cap = int(max(10, min(20000, (budget_s - t_asm) / max(per_it, 1e-6))))
+    t2 = time.time()
+    _, info = O.pcg(A, s.b, precond=O.ORC_PRECOND_JACOBI, tol=1e-4, stop_rule=O.ORC_STOP_RELRES, max_iter=cap,
+                    threads=threads)
+    t_pcg = time.time() - t2
+    if info["converged"]:
+        ms = (t_asm + t_pcg) * 1e3
+        sample = f"full solve: assembly + block-Jacobi PCG to rel-res 1e-4 ({info['iterations']} iterations)"
+    else:
+        its_needed = None
+        ms = None
+        sample = f"bounded: assembly + {cap} block-Jacobi PCG iterations (not converged to 1e-4)"
+        ms = (t_asm + t_pcg) * 1e3
+    return {"value": ms, "unit": "ms/solve", "cores": threads, "kind": "port", "sample": sample,
+            "iterations": int(info["iterations"]), "converged": bool(info["converged"]),
+            "rel_res": float(info["rel_res_true"]), "assembly_ms": t_asm * 1e3}
+
+
+def run_reference(args, rank: int) -> None:
+    """The reference's algorithm on the host cores (the oracle port of
+    libuipc's FP64 MAS-PCG; the CUDA reference cannot be built here)."""
+    if rank != 0:
+        return
+    import numpy as np
+
+    from libuipc_b200.linear_system import partition_maps, partition_rcb
+    from oracle import oracle as O
+
+    s, _ = build_workload(args.workload)
+    threads = os.cpu_count() or 1
+    pid = partition_rcb(s.positions)
+    p2r, r2p = partition_maps(pid)
+    M = O.OracleMAS(s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
+    times, iters = [], []
+    for k in range(args.warmup + args.steps):
+        t0 = time.time()
+        A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals)
+        M.assemble(A, 0, 0)
+        _, info = O.pcg(A, s.b, precond=O.ORC_PRECOND_MAS, mas=M, tol=1e-4, stop_rule=O.ORC_STOP_RELRES,
+                        check_interval=5, threads=threads)
+        dt = (time.time() - t0) * 1e3
+        if k >= args.warmup:
+            times.append(dt)
+            iters.append(int(info["iterations"]))
+        del A
+    ms = sum(times) / len(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms/solve", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "precision": "fp64", "preconditioner": "mas", "stop": "rel-res 1e-4"},
+        "pcg_iterations": iters[-1] if iters else None,
+        "cpu_baseline": {"value": ms, "unit": "ms/solve", "cores": threads, "kind": "port",
+                         "sample": "full solve per step: assembly + MAS build + MAS-PCG to rel-res 1e-4"},
+        "e2e": {"value": ms, "unit": "ms/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="stack8x40")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    from libuipc_b200 import _abi
+    from libuipc_b200.linear_system import Solver, partition_maps, partition_rcb
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+
+    s, gen_s = build_workload(args.workload)
+    pid = partition_rcb(s.positions)
+    p2r, r2p = partition_maps(pid)
+
+    stream = torch.cuda.Stream(device=dev)
+    solver = Solver(local_rank)
+    solver.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        rows = torch.from_numpy(s.rows).to(dev)
+        cols = torch.from_numpy(s.cols).to(dev)
+        vals = torch.from_numpy(s.vals).to(dev)
+        b = torch.from_numpy(s.b).to(dev)
+        x = torch.zeros_like(b)
+    stream.synchronize()
+    solver.mas_init(0, s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
+
+    def solve_step():
+        solver.assemble(s.n_verts, rows, cols, vals)
+        solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_SWEEP_F32)
+        return solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5)
+
+    for _ in range(args.warmup):
+        st = solve_step()
+    nb, U = solver.matrix_info()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    # ---- timed region: device-resident inputs ------------------------------------
+    solver.set_timing(True)
+    solve_step()  # capture the graph with timing nodes outside the timed region
+    solver.reset_timers()
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    stats = []
+    for _ in range(args.steps):
+        stats.append(solve_step())
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    tm = solver.timers()
+    if pg is not None:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # ---- e2e: host (pinned) inputs through the same public API -------------------
+    h_rows = torch.from_numpy(s.rows).pin_memory()
+    h_cols = torch.from_numpy(s.cols).pin_memory()
+    h_vals = torch.from_numpy(s.vals).pin_memory()
+    h_b = torch.from_numpy(s.b).pin_memory()
+    h_x = torch.empty_like(h_b).pin_memory()
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        with torch.cuda.stream(stream):
+            rows.copy_(h_rows, non_blocking=True)
+            cols.copy_(h_cols, non_blocking=True)
+            vals.copy_(h_vals, non_blocking=True)
+            b.copy_(h_b, non_blocking=True)
+        solve_step()
+        with torch.cuda.stream(stream):
+            h_x.copy_(x, non_blocking=True)
+    ev1.record(stream)
+    ev1.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
+    if pg is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = (h_rows.numel() * 4 + h_cols.numel() * 4 + h_vals.numel() * 8 + h_b.numel() * 8)
+    d2h = h_x.numel() * 8
+
+    # ---- roofline of the dominant kernel (SpMV) --------------------------------------
+    peak, peak_kind = _peaks()
+    spmv_avg_ms = tm["spmv_ms"] / max(tm["spmv_launches"], 1)
+    abytes = spmv_bytes(U, nb)
+    achieved = abytes / (spmv_avg_ms * 1e-3) / 1e9 if spmv_avg_ms > 0 else 0.0
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    if os.path.exists(tr_path):
+        try:
+            tr = json.load(open(tr_path))
+            if tr.get("workload") == args.workload:
+                traffic = tr.get("bytes_per_launch")
+        except Exception:
+            pass
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(s)
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "error": str(e)}
+
+    last = stats[-1]
+    line = {
+        "metric": METRIC,
+        "value": ms,
+        "unit": "ms/solve",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "mode": "plain",
+        "config": {"workload": args.workload, "n_dof": 3 * s.n_verts, "n_triplets": s.n_triplets,
+                   "upper_blocks": U, "contacts": s.n_contacts, "precision": "fp64 (FP32 MAS inverses)",
+                   "preconditioner": "mas", "stop": "FP64-verified rel-res 1e-4", "parallelism": "replicas",
+                   "l2": "inputs larger than L2 (matrix 0.33 GB, triplets 2.5 GB)"},
+        "pcg_iterations": int(last["iterations_exact"]),
+        "rel_res": float(last["rel_res"]),
+        "stages_ms": {"assemble": tm["assemble_ms"] / args.steps, "precond_build": tm["precond_build_ms"] / args.steps,
+                      "pcg": tm["pcg_ms"] / args.steps, "spmv_avg": spmv_avg_ms,
+                      "precond_apply_avg": tm["precond_apply_ms"] / max(tm["precond_apply_launches"], 1)},
+        "gpu_launches": int(tm["kernel_launches"]),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "kernel": "k_spmv_sym_f64", "algorithmic_bytes": abytes, "peak_source": peak_kind},
+        "e2e": {"value": e2e_ms, "unit": "ms/solve", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "clocks": clk,
+        "cpu_baseline": cpu,
+        "generate_s": gen_s,
+    }
+    solver.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

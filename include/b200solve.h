@@ -1,0 +1,192 @@
+/*
+ * b200solve -- B200-native (sm_100a) Newton-step linear solve behind a C ABI.
+ *
+ * Drop-in for the linear-solve path of libuipc's CUDA backend:
+ *   triplet -> block-sparse (3x3) Hessian assembly, symmetric block SpMV,
+ *   MAS (multi-level additive Schwarz) preconditioner build and apply, and
+ *   the PCG loop, plus a mixed-precision mode.
+ *
+ * Conventions (identical to libuipc's GlobalLinearSystem):
+ *   - the matrix is given as raw 3x3 block triplets (row, col, value) in the
+ *     global block numbering; only entries with 0 <= row <= col are kept
+ *     (block-upper storage of a symmetric matrix); duplicates are summed;
+ *   - block values are 9 doubles, column-major (Eigen::Matrix3d layout);
+ *   - vectors are FP64 with 3 * n_block_rows entries;
+ *   - every pointer argument named d_* is a device pointer on the solver's
+ *     device; h_* is host memory; "any" accepts either (copied with
+ *     cudaMemcpyDefault).
+ *
+ * Errors: every entry point returns B2S_OK (0) or a negative status; the
+ * message is available from b2s_last_error(). No exception crosses the ABI.
+ * A solver handle is used by one host thread at a time; all work runs on the
+ * stream set by b2s_set_stream (default: the solver's own stream), and the
+ * entry points return after that stream's work for the call has completed
+ * unless stated otherwise.
+ */
+#ifndef B200SOLVE_H
+#define B200SOLVE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2S_OK 0
+#define B2S_ERR_ARGUMENT -1   /* invalid argument / size / index */
+#define B2S_ERR_CUDA -2       /* CUDA runtime error */
+#define B2S_ERR_STATE -3      /* call out of order (e.g. apply before assemble) */
+#define B2S_ERR_NUMERIC -4    /* non-finite values / breakdown */
+#define B2S_ERR_NOT_CONVERGED -5
+
+typedef struct b2s_solver b2s_solver;
+
+/* ---- lifetime ------------------------------------------------------------
+ * Replaces the construction of GlobalLinearSystem::Impl's buffers and the
+ * solver / preconditioner SimSystems
+ * (src/backends/cuda/linear_system/global_linear_system.h:266-325). */
+int         b2s_create(int device, b2s_solver** out);
+int         b2s_destroy(b2s_solver* s);
+const char* b2s_last_error(const b2s_solver* s); /* s may be NULL: last create error */
+int         b2s_set_stream(b2s_solver* s, void* cuda_stream); /* cudaStream_t; NULL = own stream */
+int         b2s_version(void);
+
+/* ---- assembly --------------------------------------------------------------
+ * Replaces MatrixConverter<Float,3>::convert_sym + convert(BCOO->BSR)
+ * (src/backends/cuda/algorithm/details/matrix_converter.inl:1550-1701,
+ * 1040-1097), called from GlobalLinearSystem::Impl::build_linear_system
+ * (src/backends/cuda/linear_system/global_linear_system.cu:272-319).
+ * Triplets with row < 0 (unwritten slots) or row > col are dropped, the rest
+ * are sorted by (row, col, source index) and summed in source order. The
+ * resulting pattern (block-upper BSR row pointers and column indices) is the
+ * reference's exactly; the sums are deterministic. */
+int b2s_assemble(b2s_solver* s, int32_t n_block_rows, int64_t n_triplets,
+                 const int32_t* d_rows, const int32_t* d_cols, const double* d_vals);
+int b2s_matrix_info(const b2s_solver* s, int32_t* n_block_rows, int64_t* n_upper_blocks);
+/* Copy the block-upper BSR out: rowptr [n_block_rows+1], colidx [nnz],
+ * vals [nnz*9] column-major. Any pointer may be NULL; "any" memory. */
+int b2s_get_upper_bsr(b2s_solver* s, int32_t* rowptr, int32_t* colidx, double* vals);
+
+/* ---- SpMV --------------------------------------------------------------------
+ * y = A x with A = U + U^T - diag(U) at block level, and optionally
+ * d_dot = x . y. Replaces Spmv::rbk_sym_spmv / rbk_sym_spmv_dot
+ * (src/backends/cuda/linear_system/spmv.cu:992-1160) as used by
+ * IterativeSolver::spmv / spmv_dot (src/backends/cuda/linear_system/iterative_solver.h:30-40). */
+int b2s_spmv(b2s_solver* s, const double* d_x, double* d_y, double* h_dot /* may be NULL */);
+
+/* ---- MAS preconditioner ----------------------------------------------------------
+ * Initialisation: replaces FEMMASPreconditioner::do_init ->
+ * MASPreconditionerEngine::init_neighbor + init_matrix
+ * (src/backends/cuda/finite_element/fem_mas_preconditioner.cu:157-404,
+ *  src/backends/cuda/finite_element/mas_preconditioner_engine.h:67-80).
+ * The MAS acts on block rows [block_offset, block_offset + vert_num);
+ * h_adj_start/h_adj_list is the vertex adjacency (CSR, sorted), part_to_real
+ * maps partition slots (parts padded to 16) to vertices (-1 = padding) and
+ * real_to_part is its inverse (-1 = unpartitioned vertex, which then gets the
+ * 3x3 block-Jacobi fallback). */
+int b2s_mas_init(b2s_solver* s, int32_t block_offset, int32_t vert_num,
+                 const int32_t* h_adj_start, const int32_t* h_adj_list,
+                 int32_t part_map_size, const int32_t* h_part_to_real,
+                 const int32_t* h_real_to_part);
+/* MAS hierarchy introspection (for parity checks): level count, node slots
+ * over all levels, per-level begin/count [L+1] and the per-vertex coarse
+ * table [vert_num * (L-1)] (global node of vertex v at levels 1..L-1). */
+int b2s_mas_info(const b2s_solver* s, int32_t* level_num, int32_t* total_nodes);
+int b2s_mas_get_hierarchy(b2s_solver* s, int32_t* h_level_begin, int32_t* h_level_count,
+                          int32_t* h_coarse_table);
+/* Cluster matrices after b2s_precond_assemble: Galerkin matrices (FP64) and
+ * inverses (FP32), 136 column-major 3x3 blocks per 16-node cluster. */
+int b2s_mas_get_clusters(b2s_solver* s, double* h_hess, float* h_inv);
+
+/* Partition utility (the caller-side step of FEMMASPreconditioner::do_init):
+ * recursive coordinate bisection into parts of at most max_part vertices,
+ * each part a multiple of max_part except the remainder, then the padded
+ * part_to_real / real_to_part maps (fem_mas_preconditioner.cu:285-330).
+ * b2s_partition_maps with h_part_to_real == NULL only returns the map size
+ * in *part_map_size (call it first to size h_part_to_real). */
+int b2s_partition_rcb(int32_t n, const double* h_positions, int32_t max_part,
+                      int32_t* h_part_ids);
+int b2s_partition_maps(int32_t n, const int32_t* h_part_ids, int32_t max_part,
+                       int32_t* h_part_to_real, int32_t* h_real_to_part,
+                       int32_t* part_map_size);
+
+#define B2S_PRECOND_NONE 0
+#define B2S_PRECOND_JACOBI 1 /* 3x3 block Jacobi (fem_diag_preconditioner.cu:18-58) */
+#define B2S_PRECOND_MAS 2    /* MAS on its range, 3x3 block Jacobi elsewhere */
+
+#define B2S_INVERT_SWEEP_F32 0 /* FP32 symmetric sweep (mas_preconditioner_engine.cu:1077-1175) */
+#define B2S_INVERT_GJ_F64 1    /* FP64 Gauss-Jordan, stored FP32 */
+
+/* Build the preconditioner from the current assembled matrix. Replaces
+ * GlobalPreconditioner::do_assemble / LocalPreconditioner::do_assemble
+ * (src/backends/cuda/linear_system/global_preconditioner.h:16,
+ *  src/backends/cuda/finite_element/fem_mas_preconditioner.cu:406-439). */
+int b2s_precond_assemble(b2s_solver* s, int kind, int invert_mode);
+/* z = P r (FP64 vectors). Replaces GlobalPreconditioner::do_apply
+ * (global_preconditioner.h:17; mas_preconditioner_engine.cu:2887-2960). */
+int b2s_precond_apply(b2s_solver* s, const double* d_r, double* d_z);
+
+/* ---- PCG ---------------------------------------------------------------------------
+ * Replaces IterativeSolver::do_solve as implemented by LinearFusedPCG
+ * (src/backends/cuda/linear_system/linear_fused_pcg.cu:851-943, 1782-2005) and
+ * LinearPCG (src/backends/cuda/linear_system/linear_pcg.cu:395-438, 558-644). */
+#define B2S_STOP_RZ 0     /* |r.z| <= tol |r0.z0| (the reference's rule) */
+#define B2S_STOP_RELRES 1 /* ||b - A x||_2 <= tol ||b||_2, verified in FP64 */
+
+#define B2S_PRECISION_FP64 0  /* FP64 matrix/vectors, FP32 MAS inverses */
+#define B2S_PRECISION_MIXED 1 /* FP32 matrix/vectors, BF16 MAS inverses, FP64 dots + residual replacement */
+
+typedef struct b2s_pcg_options
+{
+    double  tol;            /* stop tolerance (rule below) */
+    int32_t stop_rule;      /* B2S_STOP_* */
+    int32_t check_interval; /* iterations per host convergence check (graph block) */
+    int64_t max_iter;       /* 0 = 2 * n_dof (the reference's max_iter_ratio = 2) */
+    int32_t precision;      /* B2S_PRECISION_* */
+    int32_t use_graph;      /* capture check_interval iterations in a CUDA graph */
+    int32_t x0_given;       /* 1: d_x holds the initial guess; 0: start from 0 */
+    int32_t replace_every;  /* mixed: FP64 residual replacement period (0 = off) */
+} b2s_pcg_options;
+
+typedef struct b2s_pcg_stats
+{
+    int64_t iterations;   /* as the reference reports them (multiple of check_interval when fused) */
+    int64_t iterations_exact; /* iteration at which the stop rule fired */
+    int32_t converged;
+    int32_t bypassed;     /* preconditioner bypassed: rz0 < 0 or non-finite (PSD guard) */
+    double  rz0;
+    double  rel_res;      /* ||b - A x|| / ||b|| recomputed in FP64 at exit */
+    int64_t replacements; /* residual replacements done */
+} b2s_pcg_stats;
+
+void b2s_pcg_default_options(b2s_pcg_options* o);
+int  b2s_pcg(b2s_solver* s, const double* d_b, double* d_x, const b2s_pcg_options* opt,
+             b2s_pcg_stats* stats);
+
+/* ---- stage timers ------------------------------------------------------------------
+ * Device-time counterparts of the reference's scoped timers "Convert To BCOO",
+ * "Assemble Preconditioner", "FusedPCG", "SpMV" and "Apply Preconditioner"
+ * (src/backends/cuda/linear_system/global_linear_system.cu:274-313,
+ *  linear_fused_pcg.cu:1413,1438,1785): CUDA events on the solver's stream,
+ * accumulated while timing is enabled. kernel_launches counts every kernel
+ * this library launched (graph replays included) since the last reset. */
+typedef struct b2s_timers
+{
+    double  assemble_ms;
+    double  precond_build_ms;
+    double  pcg_ms;
+    double  spmv_ms;
+    int64_t spmv_launches;
+    double  precond_apply_ms;
+    int64_t precond_apply_launches;
+    int64_t kernel_launches;
+} b2s_timers;
+
+int b2s_set_timing(b2s_solver* s, int enable);
+int b2s_get_timers(const b2s_solver* s, b2s_timers* out);
+int b2s_reset_timers(b2s_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200SOLVE_H */

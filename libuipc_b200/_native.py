@@ -1,0 +1,78 @@
+"""Loading of the in-tree native libraries.
+
+``libb200solve.so`` is the product (CUDA kernels for sm_100a behind a C ABI,
+declared in ``include/b200solve.h``); ``libb200scene.so`` is the host-side
+synthetic Newton-system generator. Both are built in-tree by
+``libuipc_b200/build.py``. There is no fallback: a missing or stale library
+raises, so nothing silently runs on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib")
+_lock = threading.Lock()
+_scene = None
+_solve = None
+
+c_int_p = C.POINTER(C.c_int)
+c_i32_p = C.POINTER(C.c_int32)
+c_i64_p = C.POINTER(C.c_int64)
+c_dbl_p = C.POINTER(C.c_double)
+
+
+def lib_path(name: str) -> str:
+    return os.path.join(_LIB_DIR, name)
+
+
+def _load(name: str) -> C.CDLL:
+    path = lib_path(name)
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"native library {path} is missing; build it with `python -m libuipc_b200.build`"
+        )
+    return C.CDLL(path, mode=C.RTLD_GLOBAL)
+
+
+def load_scene_lib() -> C.CDLL:
+    global _scene
+    with _lock:
+        if _scene is not None:
+            return _scene
+        lib = _load("libb200scene.so")
+        vp = C.c_void_p
+        lib.b2g_default_config.argtypes = [C.c_void_p]
+        lib.b2g_default_config.restype = None
+        lib.b2g_generate.argtypes = [C.c_void_p, C.POINTER(vp)]
+        lib.b2g_generate.restype = C.c_int
+        lib.b2g_free.argtypes = [vp]
+        lib.b2g_free.restype = None
+        lib.b2g_last_error.argtypes = []
+        lib.b2g_last_error.restype = C.c_char_p
+        for fn in ("b2g_num_verts", "b2g_num_tets", "b2g_num_triplets", "b2g_num_contacts", "b2g_num_adjacency"):
+            getattr(lib, fn).argtypes = [vp]
+            getattr(lib, fn).restype = C.c_int64
+        for fn in ("b2g_positions", "b2g_rest_positions", "b2g_triplet_vals", "b2g_gradient"):
+            getattr(lib, fn).argtypes = [vp]
+            getattr(lib, fn).restype = c_dbl_p
+        for fn in ("b2g_tets", "b2g_triplet_rows", "b2g_triplet_cols", "b2g_adjacency_start", "b2g_adjacency_list"):
+            getattr(lib, fn).argtypes = [vp]
+            getattr(lib, fn).restype = c_i32_p
+        _scene = lib
+        return lib
+
+
+def load_solve_lib() -> C.CDLL:
+    """Load libb200solve.so and declare every entry point of include/b200solve.h."""
+    global _solve
+    with _lock:
+        if _solve is not None:
+            return _solve
+        lib = _load("libb200solve.so")
+        from ._abi import declare
+
+        declare(lib)
+        _solve = lib
+        return lib

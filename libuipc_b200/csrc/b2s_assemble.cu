@@ -1,0 +1,419 @@
+// Triplet -> block-upper BSR assembly (deterministic), and the device scan.
+//
+// Semantics follow MatrixConverter<Float,3>::convert_sym
+// (src/backends/cuda/algorithm/details/matrix_converter.inl:1550-1701):
+// keep row >= 0 && row <= col, order by (row, col) with ties in source
+// order, sum each run. The reference sorts a 64-bit key with CUB and sums
+// runs with cross-warp FP64 atomics (rounding-nondeterministic). Here the
+// sort is a counting sort on the row followed by an in-warp rank sort of each
+// row's (col, source) pairs, and every run is summed by one lane in source
+// order -- the pattern is identical, the values are bit-reproducible.
+#include "b2s_internal.cuh"
+
+namespace b2s
+{
+namespace
+{
+constexpr int SCAN_BLOCK = 256;
+constexpr int SCAN_ITEMS = 4;  // elements per thread
+constexpr int SCAN_TILE  = SCAN_BLOCK * SCAN_ITEMS;
+
+// block-wide inclusive scan of one int per thread (warp shuffles + smem)
+__device__ __forceinline__ int block_inclusive_scan(int v, int* warp_sums)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for(int o = 1; o < 32; o <<= 1)
+    {
+        int t = __shfl_up_sync(0xffffffffu, v, o);
+        if(lane >= o)
+            v += t;
+    }
+    if(lane == 31)
+        warp_sums[warp] = v;
+    __syncthreads();
+    if(warp == 0)
+    {
+        int w = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1)
+        {
+            int t = __shfl_up_sync(0xffffffffu, w, o);
+            if(lane >= o)
+                w += t;
+        }
+        if(lane < (int)(blockDim.x >> 5))
+            warp_sums[lane] = w;
+    }
+    __syncthreads();
+    if(warp > 0)
+        v += warp_sums[warp - 1];
+    return v;
+}
+
+// tile exclusive scan; writes out[i] (i < n) and the tile total into tile_sums
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_tiles(const int32_t* in, int32_t* out, int64_t n,
+                                                           int32_t* tile_sums)
+{
+    __shared__ int warp_sums[SCAN_BLOCK / 32];
+    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    int           v[SCAN_ITEMS];
+    int           local = 0;
+#pragma unroll
+    for(int k = 0; k < SCAN_ITEMS; ++k)
+    {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        local += v[k];
+    }
+    int incl = block_inclusive_scan(local, warp_sums);
+    int run  = incl - local;
+#pragma unroll
+    for(int k = 0; k < SCAN_ITEMS; ++k)
+    {
+        if(base + k < n)
+            out[base + k] = run;
+        run += v[k];
+    }
+    if(threadIdx.x == blockDim.x - 1)
+        tile_sums[blockIdx.x] = incl;
+}
+
+__global__ void k_scan_add(int32_t* out, int64_t n, const int32_t* tile_offsets)
+{
+    const int64_t i = (int64_t)blockIdx.x * SCAN_TILE + threadIdx.x;
+    const int32_t add = tile_offsets[blockIdx.x];
+#pragma unroll
+    for(int k = 0; k < SCAN_ITEMS; ++k)
+    {
+        int64_t j = i + (int64_t)k * SCAN_BLOCK;
+        if(j < n)
+            out[j] += add;
+    }
+}
+
+__global__ void k_write_total(int32_t* out, int64_t n, const int32_t* in, const int32_t* tile_offsets,
+                              int64_t last_tile)
+{
+    // out[n] = exclusive(out[n-1]) + in[n-1]; computed from the last element
+    if(threadIdx.x == 0 && blockIdx.x == 0)
+        out[n] = (n > 0) ? (out[n - 1] + in[n - 1]) : 0;
+}
+}  // namespace
+
+// Exclusive scan of n int32 into out[0..n] (out[n] = total). `in` may alias
+// `out` only when the caller keeps a copy of in[n-1]; here in != out always.
+void exclusive_scan(b2s_solver* s, const int32_t* in, int32_t* out, int64_t n, DBuf<int32_t>& tmp)
+{
+    cudaStream_t st = s->stream;
+    if(n <= 0)
+    {
+        B2S_CUDA(cudaMemsetAsync(out, 0, sizeof(int32_t), st));
+        return;
+    }
+    const int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    // recursion through a flat list of levels inside one scratch buffer
+    std::vector<int64_t> level_n{n};
+    while(level_n.back() > SCAN_TILE)
+        level_n.push_back((level_n.back() + SCAN_TILE - 1) / SCAN_TILE);
+    // scratch: for each level k >= 1 an array of level_n[k] sums + their scan (+1)
+    int64_t need = 0;
+    std::vector<int64_t> off_sums, off_scan;
+    for(size_t k = 0; k < level_n.size(); ++k)
+    {
+        int64_t t = (level_n[k] + SCAN_TILE - 1) / SCAN_TILE;
+        off_sums.push_back(need);
+        need += t;
+        off_scan.push_back(need);
+        need += t + 1;
+    }
+    tmp.resize(need + 1, 1.5);
+    // up-sweep: scan tiles at every level
+    const int32_t* cur_in  = in;
+    int32_t*       cur_out = out;
+    for(size_t k = 0; k < level_n.size(); ++k)
+    {
+        int64_t nk = level_n[k];
+        int64_t t  = (nk + SCAN_TILE - 1) / SCAN_TILE;
+        k_scan_tiles<<<(unsigned)t, SCAN_BLOCK, 0, st>>>(cur_in, cur_out, nk, tmp.data() + off_sums[k]);
+        B2S_CHECK_LAUNCH();
+        cur_in  = tmp.data() + off_sums[k];
+        cur_out = tmp.data() + off_scan[k];
+        if(t == 1)
+        {
+            // single tile: its exclusive scan is zero
+            B2S_CUDA(cudaMemsetAsync(cur_out, 0, sizeof(int32_t), st));
+            break;
+        }
+    }
+    // down-sweep: add scanned tile offsets
+    for(int k = (int)level_n.size() - 1; k >= 0; --k)
+    {
+        int64_t nk = level_n[k];
+        int64_t t  = (nk + SCAN_TILE - 1) / SCAN_TILE;
+        if(t == 1)
+            continue;
+        int32_t* target = (k == 0) ? out : tmp.data() + off_scan[k - 1];
+        k_scan_add<<<(unsigned)t, SCAN_BLOCK, 0, st>>>(target, nk, tmp.data() + off_scan[k]);
+        B2S_CHECK_LAUNCH();
+    }
+    (void)tiles;
+    k_write_total<<<1, 32, 0, st>>>(out, n, in, nullptr, 0);
+    B2S_CHECK_LAUNCH();
+}
+
+namespace
+{
+constexpr int ASM_BLOCK = 256;
+constexpr int ROW_CAP   = 256;  // (col, src) pairs per row held in shared memory
+
+__global__ void k_count_rows(const int32_t* __restrict__ rows, const int32_t* __restrict__ cols, int64_t T,
+                             int32_t nb, int32_t* __restrict__ row_count, int* err)
+{
+    for(int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int32_t r = rows[t], c = cols[t];
+        if(r < 0 || r > c)
+            continue;
+        if(c >= nb)
+        {
+            atomicOr(err, DERR_TRIPLET_INDEX);
+            continue;
+        }
+        atomicAdd(&row_count[r], 1);
+    }
+}
+
+__global__ void k_scatter_rows(const int32_t* __restrict__ rows, const int32_t* __restrict__ cols, int64_t T,
+                               int32_t nb, const int32_t* __restrict__ row_start, int32_t* __restrict__ row_fill,
+                               int32_t* __restrict__ bucket_col, int32_t* __restrict__ bucket_src, int* err)
+{
+    for(int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int32_t r = rows[t], c = cols[t];
+        if(r < 0 || r > c || c >= nb)
+            continue;
+        const int32_t beg = row_start[r], len = row_start[r + 1] - beg;
+        const int32_t k = atomicAdd(&row_fill[r], 1);
+        if(k >= len)
+        {
+            atomicOr(err, DERR_ROW_OVERFLOW);
+            continue;
+        }
+        bucket_col[beg + k] = c;
+        bucket_src[beg + k] = (int32_t)t;
+    }
+}
+
+__device__ __forceinline__ bool key_less(int32_t ca, int32_t sa, int32_t cb, int32_t sb)
+{
+    return ca < cb || (ca == cb && sa < sb);
+}
+
+// One warp per row: rank every (col, src) pair of the row by counting the
+// pairs that order before it, write the sorted row and its unique-column count.
+__global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32_t* __restrict__ row_start,
+                                                         const int32_t* __restrict__ bucket_col,
+                                                         const int32_t* __restrict__ bucket_src,
+                                                         int32_t* __restrict__ sorted_col,
+                                                         int32_t* __restrict__ sorted_src,
+                                                         int32_t* __restrict__ uniq_count)
+{
+    __shared__ int32_t s_col[ASM_BLOCK / 32][ROW_CAP];
+    __shared__ int32_t s_src[ASM_BLOCK / 32][ROW_CAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int warps_total = gridDim.x * (ASM_BLOCK / 32);
+    for(int32_t r = blockIdx.x * (ASM_BLOCK / 32) + w; r < nb; r += warps_total)
+    {
+        const int32_t beg = row_start[r], L = row_start[r + 1] - beg;
+        int           uniq = 0;
+        if(L <= ROW_CAP)
+        {
+            for(int k = lane; k < L; k += 32)
+            {
+                s_col[w][k] = bucket_col[beg + k];
+                s_src[w][k] = bucket_src[beg + k];
+            }
+            __syncwarp();
+            for(int k = lane; k < L; k += 32)
+            {
+                const int32_t c = s_col[w][k], sr = s_src[w][k];
+                int rank = 0, head = 1;
+                for(int q = 0; q < L; ++q)
+                {
+                    const int32_t cq = s_col[w][q], sq = s_src[w][q];
+                    rank += key_less(cq, sq, c, sr) ? 1 : 0;
+                    if(cq == c && sq < sr)
+                        head = 0;
+                }
+                sorted_col[beg + rank] = c;
+                sorted_src[beg + rank] = sr;
+                uniq += head;
+            }
+            __syncwarp();
+        }
+        else
+        {
+            // long row: same ranking straight from global memory
+            for(int k = lane; k < L; k += 32)
+            {
+                const int32_t c = bucket_col[beg + k], sr = bucket_src[beg + k];
+                int rank = 0, head = 1;
+                for(int q = 0; q < L; ++q)
+                {
+                    const int32_t cq = bucket_col[beg + q], sq = bucket_src[beg + q];
+                    rank += key_less(cq, sq, c, sr) ? 1 : 0;
+                    if(cq == c && sq < sr)
+                        head = 0;
+                }
+                sorted_col[beg + rank] = c;
+                sorted_src[beg + rank] = sr;
+                uniq += head;
+            }
+        }
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            uniq += __shfl_xor_sync(0xffffffffu, uniq, o);
+        if(lane == 0)
+            uniq_count[r] = uniq;
+    }
+}
+
+// One warp per row: each run of equal columns is summed by one lane, in source
+// order, and written to its slot of the block-upper BSR (values in planes).
+__global__ void __launch_bounds__(ASM_BLOCK) k_reduce_rows(int32_t nb, const int32_t* __restrict__ row_start,
+                                                           const int32_t* __restrict__ sorted_col,
+                                                           const int32_t* __restrict__ sorted_src,
+                                                           const double* __restrict__ src_vals,
+                                                           const int32_t* __restrict__ rowptr,
+                                                           int32_t* __restrict__ out_rows,
+                                                           int32_t* __restrict__ out_cols,
+                                                           double* __restrict__ out_vals, int64_t U,
+                                                           int32_t* __restrict__ diag_index)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int warps_total = gridDim.x * (ASM_BLOCK / 32);
+    for(int32_t r = blockIdx.x * (ASM_BLOCK / 32) + w; r < nb; r += warps_total)
+    {
+        const int32_t beg = row_start[r], L = row_start[r + 1] - beg;
+        const int32_t obeg = rowptr[r];
+        int           heads_before = 0;
+        for(int base = 0; base < L; base += 32)
+        {
+            const int k = base + lane;
+            bool head = false;
+            int32_t c = 0;
+            if(k < L)
+            {
+                c    = sorted_col[beg + k];
+                head = (k == 0) || (sorted_col[beg + k - 1] != c);
+            }
+            const unsigned hm   = __ballot_sync(0xffffffffu, head);
+            const int      slot = heads_before + __popc(hm & ((1u << lane) - 1u));
+            if(head)
+            {
+                double acc[9];
+                int32_t s0 = sorted_src[beg + k];
+#pragma unroll
+                for(int q = 0; q < 9; ++q)
+                    acc[q] = src_vals[(int64_t)s0 * 9 + q];
+                for(int e = k + 1; e < L && sorted_col[beg + e] == c; ++e)
+                {
+                    const int32_t se = sorted_src[beg + e];
+#pragma unroll
+                    for(int q = 0; q < 9; ++q)
+                        acc[q] += src_vals[(int64_t)se * 9 + q];
+                }
+                const int64_t o = (int64_t)obeg + slot;
+                out_rows[o] = r;
+                out_cols[o] = c;
+#pragma unroll
+                for(int q = 0; q < 9; ++q)
+                    out_vals[(int64_t)q * U + o] = acc[q];
+            }
+            heads_before += __popc(hm);
+        }
+        if(lane == 0)
+            diag_index[r] = (L > 0 && sorted_col[beg] == r) ? obeg : -1;
+    }
+}
+
+int asm_grid(int64_t work, int block)
+{
+    int64_t g = (work + block - 1) / block;
+    const int64_t cap = (int64_t)NUM_SMS_HINT * 16;
+    if(g > cap)
+        g = cap;
+    if(g < 1)
+        g = 1;
+    return (int)g;
+}
+}  // namespace
+
+void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const int32_t* rows, const int32_t* cols,
+                       const double* vals, bool /*vals_planar*/, int64_t /*plane_stride*/)
+{
+    B2S_REQUIRE(nb >= 0 && T >= 0, B2S_ERR_ARGUMENT, "negative matrix size");
+    B2S_REQUIRE(T < (int64_t)INT32_MAX, B2S_ERR_ARGUMENT, "more than 2^31-1 triplets");
+    cudaStream_t     st = s->stream;
+    AssemblyScratch& w  = s->asmb;
+    M.valid             = false;
+    M.nb                = nb;
+    w.err.resize(1);
+    B2S_CUDA(cudaMemsetAsync(w.err.data(), 0, sizeof(int), st));
+    w.row_count.resize((size_t)nb + 1, 1.25);
+    w.row_start.resize((size_t)nb + 1, 1.25);
+    w.row_fill.resize((size_t)nb + 1, 1.25);
+    w.uniq_count.resize((size_t)nb + 1, 1.25);
+    M.rowptr.resize((size_t)nb + 1, 1.25);
+    M.diag_index.resize((size_t)std::max(nb, 1), 1.25);
+    B2S_CUDA(cudaMemsetAsync(w.row_count.data(), 0, sizeof(int32_t) * ((size_t)nb + 1), st));
+    B2S_CUDA(cudaMemsetAsync(w.row_fill.data(), 0, sizeof(int32_t) * ((size_t)nb + 1), st));
+    if(T > 0)
+    {
+        w.bucket_col.resize(T, 1.25);
+        w.bucket_src.resize(T, 1.25);
+        w.sorted_col.resize(T, 1.25);
+        w.sorted_src.resize(T, 1.25);
+        k_count_rows<<<asm_grid(T, ASM_BLOCK), ASM_BLOCK, 0, st>>>(rows, cols, T, nb, w.row_count.data(),
+                                                                   w.err.data());
+        B2S_CHECK_LAUNCH();
+    }
+    exclusive_scan(s, w.row_count.data(), w.row_start.data(), nb, w.scan_tmp);
+    if(T > 0)
+    {
+        k_scatter_rows<<<asm_grid(T, ASM_BLOCK), ASM_BLOCK, 0, st>>>(rows, cols, T, nb, w.row_start.data(),
+                                                                     w.row_fill.data(), w.bucket_col.data(),
+                                                                     w.bucket_src.data(), w.err.data());
+        B2S_CHECK_LAUNCH();
+    }
+    if(nb > 0)
+    {
+        k_sort_rows<<<asm_grid((int64_t)nb * 32, ASM_BLOCK), ASM_BLOCK, 0, st>>>(
+            nb, w.row_start.data(), w.bucket_col.data(), w.bucket_src.data(), w.sorted_col.data(),
+            w.sorted_src.data(), w.uniq_count.data());
+        B2S_CHECK_LAUNCH();
+    }
+    exclusive_scan(s, w.uniq_count.data(), M.rowptr.data(), nb, w.scan_tmp);
+    int32_t U = 0;
+    int     herr = 0;
+    B2S_CUDA(cudaMemcpyAsync(&U, M.rowptr.data() + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    B2S_CUDA(cudaMemcpyAsync(&herr, w.err.data(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2S_CUDA(cudaStreamSynchronize(st));
+    B2S_REQUIRE(!(herr & DERR_TRIPLET_INDEX), B2S_ERR_ARGUMENT,
+                "triplet column index outside [0, n_block_rows)");
+    B2S_REQUIRE(!(herr & DERR_ROW_OVERFLOW), B2S_ERR_ARGUMENT,
+                "triplet arrays changed during assembly (row bucket overflow)");
+    M.nnz = U;
+    M.rows.resize(std::max<int64_t>(U, 1), 1.2);
+    M.cols.resize(std::max<int64_t>(U, 1), 1.2);
+    M.vals.resize((size_t)9 * std::max<int64_t>(U, 1), 1.2);
+    if(nb > 0)
+    {
+        k_reduce_rows<<<asm_grid((int64_t)nb * 32, ASM_BLOCK), ASM_BLOCK, 0, st>>>(
+            nb, w.row_start.data(), w.sorted_col.data(), w.sorted_src.data(), vals, M.rowptr.data(),
+            M.rows.data(), M.cols.data(), M.vals.data(), U, M.diag_index.data());
+        B2S_CHECK_LAUNCH();
+    }
+    M.valid = true;
+}
+}  // namespace b2s

@@ -1,0 +1,259 @@
+// Internal declarations of libb200solve (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/b200solve.h"
+
+namespace b2s
+{
+constexpr int BANK = 16;                    // nodes per MAS cluster
+constexpr int SYM  = BANK * (BANK + 1) / 2;  // 136 upper 3x3 blocks per cluster
+constexpr int MAX_LEVELS = 6;
+constexpr int NUM_SMS_HINT = 148;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error
+{
+    int code;
+    Error(int c, const std::string& m)
+        : std::runtime_error(m)
+        , code(c)
+    {
+    }
+};
+
+#define B2S_CUDA(call)                                                                       \
+    do                                                                                       \
+    {                                                                                        \
+        cudaError_t e__ = (call);                                                            \
+        if(e__ != cudaSuccess)                                                               \
+            throw ::b2s::Error(B2S_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__) \
+                                                 + " (" + __FILE__ + ":" + std::to_string(__LINE__) + ")"); \
+    } while(0)
+
+// kernels launched by this thread through the library (every launch site
+// goes through B2S_CHECK_LAUNCH; graph replays add their node count)
+extern thread_local long long g_kernel_launches;
+
+#define B2S_CHECK_LAUNCH()                    \
+    do                                        \
+    {                                         \
+        ++::b2s::g_kernel_launches;           \
+        B2S_CUDA(cudaGetLastError());         \
+    } while(0)
+
+#define B2S_REQUIRE(cond, code, msg)          \
+    do                                        \
+    {                                         \
+        if(!(cond))                           \
+            throw ::b2s::Error((code), (msg)); \
+    } while(0)
+
+// device-side error bits (written by kernels with bounds checks)
+enum DeviceError : int
+{
+    DERR_TRIPLET_INDEX = 1,  // triplet row/col outside [0, n_block_rows)
+    DERR_ROW_OVERFLOW  = 2,  // a row's bucket exceeded its counted size
+    DERR_MAS_INDEX     = 4,  // MAS hierarchy index out of range
+};
+
+// ---------------------------------------------------------------------------
+// device buffer with capacity growth (no shrink)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DBuf
+{
+    T*     ptr = nullptr;
+    size_t n   = 0;  // size in elements
+    size_t cap = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release()
+    {
+        if(ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        n = cap = 0;
+    }
+    // resize; contents are NOT preserved when capacity grows
+    void resize(size_t count, double growth = 1.0)
+    {
+        if(count > cap)
+        {
+            release();
+            size_t want = (size_t)((double)count * growth);
+            if(want < count)
+                want = count;
+            if(want == 0)
+                want = 1;
+            B2S_CUDA(cudaMalloc(&ptr, want * sizeof(T)));
+            cap = want;
+        }
+        n = count;
+    }
+    T*       data() { return ptr; }
+    const T* data() const { return ptr; }
+    size_t   size() const { return n; }
+    size_t   bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------------------
+// assembled matrix: block-upper BSR, values in 9 component planes
+// ---------------------------------------------------------------------------
+struct Matrix
+{
+    int32_t        nb  = 0;  // block rows
+    int64_t        nnz = 0;  // unique upper blocks U
+    DBuf<int32_t>  rowptr;   // [nb+1]
+    DBuf<int32_t>  rows;     // [U] block row of each block (BCOO row index)
+    DBuf<int32_t>  cols;     // [U]
+    DBuf<double>   vals;     // [9][U]: component q (column-major index) at vals[q*U + k]
+    DBuf<int32_t>  diag_index;  // [nb] position of block (i,i), -1 if absent
+    bool           valid = false;
+};
+
+// scratch of the assembly pipeline (reused across calls)
+struct AssemblyScratch
+{
+    DBuf<int32_t> row_count, row_start, row_fill, uniq_count;
+    DBuf<int32_t> bucket_col, bucket_src, sorted_col, sorted_src;
+    DBuf<int32_t> scan_tmp;
+    DBuf<int>     err;
+};
+
+// ---------------------------------------------------------------------------
+// MAS
+// ---------------------------------------------------------------------------
+struct MasState
+{
+    bool    initialized = false;
+    int32_t offset      = 0;  // block offset of the MAS vertex range
+    int32_t vn          = 0;  // vertices in the range
+    int32_t N           = 0;  // part map size (level-0 nodes)
+    int32_t L           = 0;  // levels
+    int32_t total       = 0;  // node slots over all levels
+    int32_t clusters    = 0;  // total / 16
+    std::vector<int32_t> level_begin, level_count;  // [L+1]
+    // device hierarchy
+    DBuf<int32_t> p2r, r2p;        // [N], [vn]
+    DBuf<int32_t> ctable;          // [vn * (L-1)] global node at levels 1..L-1
+    DBuf<int32_t> cst;             // [L * vn] local id of vertex v at level l+1
+    DBuf<uint16_t> comp_mask[MAX_LEVELS];  // per level: component lane mask of each node
+    DBuf<int32_t>  new_local[MAX_LEVELS];  // per level: local id of each node at the next level
+    DBuf<int32_t>  level_begin_dev;        // [L+1]
+    // per assembly
+    DBuf<double>  hess;            // [clusters * 136 * 9]
+    DBuf<float>   inv;             // [clusters * 136 * 9]
+    // coarse-level Galerkin matrices (upper BCOO per level, in level-local ids)
+    Matrix        coarse[MAX_LEVELS];
+    DBuf<int32_t> trip_rows, trip_cols;
+    DBuf<double>  trip_vals;
+    // apply buffers (FP32, 3 per node slot)
+    DBuf<float>   R, Z;
+    // host copies for introspection
+    std::vector<int32_t> h_ctable;
+};
+
+// ---------------------------------------------------------------------------
+// PCG state
+// ---------------------------------------------------------------------------
+struct PcgScalars
+{
+    double rz;        // r.z of the current iterate
+    double rz_new;
+    double pAp;
+    double rr;        // r.r (recursive residual)
+    double rz_tol;    // tol * |rz0|
+    double rr_tol;    // (tol * ||b||)^2
+    double alpha;
+    double beta;
+    int    converged;
+    int    stop_rule;
+    long long iter;       // iterations executed
+    long long iter_conv;  // iteration at which the rule fired
+    long long max_iter;
+};
+
+struct Reduction
+{
+    DBuf<double>       partials;  // [2 * grid]
+    DBuf<unsigned int> counter;
+};
+
+struct PcgState
+{
+    DBuf<double> r, z, p, Ap, tmp;
+    DBuf<PcgScalars> sc;
+    Reduction        red;
+    PcgScalars*      h_sc = nullptr;  // pinned mirror
+    cudaGraphExec_t  graph = nullptr;
+    size_t           graph_key = 0;
+    long long        graph_kernels = 0;  // kernel nodes per graph launch
+};
+
+}  // namespace b2s
+
+// the opaque ABI handle
+struct b2s_solver
+{
+    int          device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string  last_error;
+    b2s::Matrix          A;
+    b2s::AssemblyScratch asmb;
+    b2s::MasState        mas;
+    b2s::PcgState        pcg;
+    int                  precond_kind = -1;
+    int                  invert_mode  = 0;
+    b2s::DBuf<double>    dinv;  // [nb*9] row-major inverses of diagonal blocks
+    b2s::DBuf<double>    dot_out;
+    b2s::Reduction       red;
+    // stage timers (CUDA events on `stream`)
+    bool                     timing = false;
+    b2s_timers               timers{};
+    cudaEvent_t              ev_begin = nullptr, ev_end = nullptr;
+    std::vector<cudaEvent_t> iter_events;  // 4 per iteration of a graph block
+};
+
+namespace b2s
+{
+// device-wide exclusive scan of int32 (n elements, out may alias in); returns
+// the total (synchronises when want_total)
+void exclusive_scan(b2s_solver* s, const int32_t* in, int32_t* out, int64_t n, DBuf<int32_t>& tmp);
+
+// assembly of raw triplets into a block-upper matrix (shared by the global
+// matrix and the MAS coarse levels)
+void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const int32_t* rows,
+                       const int32_t* cols, const double* vals, bool vals_planar, int64_t plane_stride);
+
+// y = A x (+ optional pAp into partial reduction slot)
+void spmv_f64(b2s_solver* s, const Matrix& A, const double* x, double* y, double* d_dot);
+
+// reductions
+int  reduction_grid();
+void launch_dot(b2s_solver* s, const double* a, const double* b, int64_t n, double* d_out);
+
+// preconditioners
+void precond_assemble(b2s_solver* s, int kind, int invert_mode);
+void precond_apply(b2s_solver* s, const double* r, double* z);
+void mas_init(b2s_solver* s, int32_t offset, int32_t vn, const int32_t* adj_start,
+              const int32_t* adj_list, int32_t N, const int32_t* p2r, const int32_t* r2p);
+void mas_assemble(b2s_solver* s, int invert_mode);
+void mas_apply(b2s_solver* s, const double* r, double* z);
+
+// PCG
+void pcg_solve(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st);
+
+inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
+}  // namespace b2s

@@ -1,0 +1,848 @@
+// MAS (multi-level additive Schwarz) preconditioner: hierarchy, Galerkin
+// cluster matrices, cluster inversion and apply.
+//
+// Algorithm of libuipc's MASPreconditionerEngine (StiffGIPC MAS, 16-node
+// banks), src/backends/cuda/finite_element/mas_preconditioner_engine.cu:
+//  * hierarchy (:57-460, host :1958-2280): partition slots form 16-lane banks;
+//    connected components of the mesh graph inside a bank become one node of
+//    the next level, numbered by bank then by lowest lane; coarser levels
+//    repeat on the remaining cross-bank edges; levels capped at 6.
+//  * Galerkin matrices (:530-953): the 48x48 matrix of every bank at every
+//    level is R_l A R_l^T restricted to the bank, R_l summing the fine
+//    vertices of each level-l node.
+//  * inversion (:1077-1175): per-cluster symmetric sweep (Gauss-Jordan without
+//    pivoting, zero diagonal -> 1).
+//  * apply (:1604-1955, :2887-2960): z = sum_l P_l^T A_l^{-1} P_l r with
+//    summation restriction and injection prolongation, FP32 inside.
+//
+// Design here: the hierarchy is built by bank-parallel kernels; the coarse
+// Galerkin matrices are built level by level as sparse matrices with the same
+// deterministic triplet assembly as the global matrix (A_{l+1} from A_l), so
+// no FP64 atomics pile onto the few clusters of the top levels; the apply
+// runs one warp per bank and level with the restriction sums of the next
+// level computed in the same pass (no atomics, bit-reproducible).
+#include "b2s_internal.cuh"
+#include "b2s_reduce.cuh"
+
+#include <algorithm>
+
+namespace b2s
+{
+namespace
+{
+inline int bank_align(int n) { return (n + BANK - 1) / BANK * BANK; }
+__host__ __device__ __forceinline__ int sym_index(int row, int col)
+{
+    return BANK * row - row * (row + 1) / 2 + col;
+}
+
+int compute_num_levels(int vert_num)
+{
+    int n_level = 1, sz = bank_align(vert_num);
+    while(sz > BANK)
+    {
+        sz /= BANK;
+        n_level++;
+        sz = bank_align(sz);
+    }
+    n_level++;
+    return std::min(n_level, MAX_LEVELS);
+}
+
+// ---------------------------------------------------------------------------
+// hierarchy kernels
+// ---------------------------------------------------------------------------
+
+// level 0: direct in-bank adjacency mask of every partition slot; cross-bank
+// neighbours stay in the (compacted) list, unpartitioned ones are dropped
+__global__ void k_h_mask_l0(int N, const int32_t* p2r, const int32_t* r2p, const int32_t* nbr_start,
+                            int32_t* nbr_num, int32_t* nbr_list, uint32_t* mask)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= N)
+        return;
+    const int v = p2r[p];
+    if(v < 0)
+    {
+        mask[p] = 0;
+        return;
+    }
+    uint32_t m = 1u << (p % BANK);
+    const int s = nbr_start[v], n = nbr_num[v];
+    int       keep = 0;
+    for(int e = 0; e < n; ++e)
+    {
+        const int u  = nbr_list[s + e];
+        const int pu = r2p[u];
+        if(pu < 0)
+            continue;
+        if(pu / BANK == p / BANK)
+            m |= 1u << (pu % BANK);
+        else
+            nbr_list[s + keep++] = u;
+    }
+    nbr_num[v] = keep;
+    mask[p]    = m;
+}
+
+// level l >= 1: OR the in-bank adjacency of every level-l node from its fine
+// vertices' remaining neighbours
+__global__ void k_h_mask_lx(int N, int vn, const int32_t* p2r, const int32_t* cst_prev, const int32_t* nbr_start,
+                            int32_t* nbr_num, int32_t* nbr_list, uint32_t* next_mask, int cnt)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= N)
+        return;
+    const int v = p2r[p];
+    if(v < 0)
+        return;
+    const int c = cst_prev[v];
+    if(c < 0 || c >= cnt)
+        return;
+    uint32_t  conn = 0;
+    const int s = nbr_start[v], n = nbr_num[v];
+    int       keep = 0;
+    for(int e = 0; e < n; ++e)
+    {
+        const int u  = nbr_list[s + e];
+        const int cu = cst_prev[u];
+        if(cu < 0 || cu >= cnt)
+        {
+            nbr_list[s + keep++] = u;
+            continue;
+        }
+        if(cu / BANK == c / BANK)
+            conn |= 1u << (cu % BANK);
+        else
+            nbr_list[s + keep++] = u;
+    }
+    nbr_num[v] = keep;
+    if(conn)
+        atomicOr(&next_mask[c], conn);
+}
+
+// one thread per bank: components (transitive closure of the lane masks),
+// numbered by lowest lane; writes the component count, each node's rank and
+// each node's component mask
+__global__ void k_h_components(int n_nodes, int n_banks, const uint32_t* mask, const int32_t* valid_p2r,
+                               int level0, int32_t* comp_count, int32_t* rank, uint16_t* comp_mask)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if(b >= n_banks)
+        return;
+    uint32_t m[BANK];
+    bool     valid[BANK];
+    for(int l = 0; l < BANK; ++l)
+    {
+        const int node = b * BANK + l;
+        valid[l]       = node < n_nodes && (!level0 || valid_p2r[node] >= 0);
+        m[l]           = valid[l] ? (mask[node] | (1u << l)) : 0u;
+    }
+    uint32_t closure[BANK];
+    uint32_t elected = 0;
+    for(int l = 0; l < BANK; ++l)
+    {
+        if(!valid[l])
+        {
+            closure[l] = 0;
+            continue;
+        }
+        uint32_t c = m[l], visited = 1u << l;
+        for(int guard = 0; guard < BANK; ++guard)
+        {
+            const uint32_t todo = visited ^ c;
+            if(!todo)
+                break;
+            const int nv = __ffs(todo) - 1;
+            visited |= 1u << nv;
+            c |= m[nv];
+        }
+        closure[l] = c;
+        if((c & ((1u << l) - 1u)) == 0)
+            elected |= 1u << l;
+    }
+    for(int l = 0; l < BANK; ++l)
+    {
+        const int node = b * BANK + l;
+        if(node >= n_nodes)
+            break;
+        if(valid[l])
+        {
+            const int el = __ffs(closure[l]) - 1;
+            rank[node]      = __popc(elected & ((1u << el) - 1u));
+            comp_mask[node] = (uint16_t)closure[l];
+        }
+        else
+        {
+            rank[node]      = -1;
+            comp_mask[node] = 0;
+        }
+    }
+    comp_count[b] = __popc(elected);
+}
+
+// next-level local id of every node (bank offset + component rank)
+__global__ void k_h_assign(int n_nodes, const int32_t* rank, const int32_t* bank_offset, int32_t* new_local)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= n_nodes)
+        return;
+    const int rk = rank[c];
+    new_local[c] = rk >= 0 ? bank_offset[c / BANK] + rk : -1;
+}
+
+// per vertex: local id at level 1 from its partition slot
+__global__ void k_h_cst_l1(int vn, const int32_t* r2p, const int32_t* new_local0, int32_t* cst0)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if(v >= vn)
+        return;
+    const int p = r2p[v];
+    cst0[v]     = p >= 0 ? new_local0[p] : -1;
+}
+
+__global__ void k_h_cst_next(int vn, const int32_t* cst_prev, const int32_t* new_local, int cnt, int32_t* cst_next)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if(v >= vn)
+        return;
+    const int c = cst_prev[v];
+    cst_next[v] = (c >= 0 && c < cnt) ? new_local[c] : -1;
+}
+
+__global__ void k_h_ctable(int vn, int L, const int32_t* cst, const int32_t* level_begin_dev, int32_t* ctable)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if(v >= vn)
+        return;
+    for(int l = 1; l < L; ++l)
+    {
+        const int c = cst[(size_t)(l - 1) * vn + v];
+        ctable[(size_t)v * (L - 1) + (l - 1)] = c >= 0 ? level_begin_dev[l] + c : -1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin matrices
+// ---------------------------------------------------------------------------
+
+// level 0: blocks of A inside one partition bank, stored oriented by slot
+__global__ void k_g_level0(int64_t U, const int32_t* rows, const int32_t* cols, const double* vals, int off, int vn,
+                           const int32_t* r2p, double* hess)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(k >= U)
+        return;
+    const int i = rows[k] - off, j = cols[k] - off;
+    if(i < 0 || i >= vn || j < 0 || j >= vn)
+        return;
+    const int pi = r2p[i], pj = r2p[j];
+    if(pi < 0 || pj < 0 || pi / BANK != pj / BANK)
+        return;
+    const bool swap = pj < pi;
+    const int  a = swap ? pj : pi, b = swap ? pi : pj;
+    double*    dst = hess + ((size_t)(a / BANK) * SYM + sym_index(a % BANK, b % BANK)) * 9;
+#pragma unroll
+    for(int p = 0; p < 3; ++p)
+#pragma unroll
+        for(int q = 0; q < 3; ++q)
+        {
+            // dst(p,q) column-major; source B(p,q) = vals[(q*3+p)*U + k]
+            const double v = swap ? vals[(int64_t)(p * 3 + q) * U + k] : vals[(int64_t)(q * 3 + p) * U + k];
+            dst[q * 3 + p] = v;
+        }
+}
+
+// restriction of a block-upper matrix to the next level as raw triplets:
+// (a, b, B) -> (P a, P b) with B, B^T or (a != b) B + B^T when both map to
+// one node. Entries that leave the MAS range are written with row -1.
+__global__ void k_g_restrict(int64_t U, const int32_t* rows, const int32_t* cols, const double* vals, int off,
+                             int n_in, const int32_t* map, int32_t* out_rows, int32_t* out_cols, double* out_vals)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(k >= U)
+        return;
+    const int a = rows[k] - off, b = cols[k] - off;
+    int       ca = -1, cb = -1;
+    if(a >= 0 && a < n_in && b >= 0 && b < n_in)
+    {
+        ca = map[a];
+        cb = map[b];
+    }
+    if(ca < 0 || cb < 0)
+    {
+        out_rows[k] = -1;
+        out_cols[k] = -1;
+#pragma unroll
+        for(int q = 0; q < 9; ++q)
+            out_vals[k * 9 + q] = 0.0;
+        return;
+    }
+    double B[9];
+#pragma unroll
+    for(int q = 0; q < 9; ++q)
+        B[q] = vals[(int64_t)q * U + k];
+    double o[9];
+    if(ca < cb)
+    {
+#pragma unroll
+        for(int q = 0; q < 9; ++q)
+            o[q] = B[q];
+    }
+    else if(ca > cb)
+    {
+#pragma unroll
+        for(int p = 0; p < 3; ++p)
+#pragma unroll
+            for(int q = 0; q < 3; ++q)
+                o[q * 3 + p] = B[p * 3 + q];
+    }
+    else if(a == b)
+    {
+#pragma unroll
+        for(int q = 0; q < 9; ++q)
+            o[q] = B[q];
+    }
+    else
+    {
+#pragma unroll
+        for(int p = 0; p < 3; ++p)
+#pragma unroll
+            for(int q = 0; q < 3; ++q)
+                o[q * 3 + p] = B[q * 3 + p] + B[p * 3 + q];
+    }
+    out_rows[k] = ca < cb ? ca : cb;
+    out_cols[k] = ca < cb ? cb : ca;
+#pragma unroll
+    for(int q = 0; q < 9; ++q)
+        out_vals[k * 9 + q] = o[q];
+}
+
+// level l >= 1: in-bank blocks of the level-l Galerkin matrix into clusters
+__global__ void k_g_extract(int64_t U, const int32_t* rows, const int32_t* cols, const double* vals,
+                            int level_begin, double* hess)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(k >= U)
+        return;
+    const int a = rows[k], b = cols[k];
+    if(a / BANK != b / BANK)
+        return;
+    const int ga = level_begin + a, gb = level_begin + b;
+    double*   dst = hess + ((size_t)(ga / BANK) * SYM + sym_index(ga % BANK, gb % BANK)) * 9;
+#pragma unroll
+    for(int q = 0; q < 9; ++q)
+        dst[q] = vals[(int64_t)q * U + k];
+}
+
+// ---------------------------------------------------------------------------
+// cluster inversion: symmetric sweep, one thread per column, 4 clusters/CTA
+// ---------------------------------------------------------------------------
+constexpr int INV_DIM      = BANK * 3;  // 48
+constexpr int INV_CLUSTERS = 4;
+constexpr int INV_BLOCK    = INV_DIM * INV_CLUSTERS;
+
+template <typename T>
+__device__ __forceinline__ T fma_t(T a, T b, T c);
+template <>
+__device__ __forceinline__ float fma_t<float>(float a, float b, float c)
+{
+    return __fmaf_rn(a, b, c);
+}
+template <>
+__device__ __forceinline__ double fma_t<double>(double a, double b, double c)
+{
+    return __fma_rn(a, b, c);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(INV_BLOCK) k_invert(int clusters, const double* __restrict__ hess,
+                                                      float* __restrict__ inv)
+{
+    __shared__ T s_row[INV_CLUSTERS][2][INV_DIM];
+    const int local = threadIdx.x / INV_DIM;
+    const int col   = threadIdx.x % INV_DIM;
+    const int cl    = blockIdx.x * INV_CLUSTERS + local;
+    const bool live = cl < clusters;
+    const int a = col % 3, nc = col / 3;
+    T c[INV_DIM];
+    const double* H = hess + (size_t)(live ? cl : 0) * SYM * 9;
+#pragma unroll
+    for(int row = 0; row < INV_DIM; ++row)
+    {
+        const int node_row = row / 3;
+        T         v;
+        if(nc >= node_row)
+            v = (T)H[sym_index(node_row, nc) * 9 + a * 3 + (row % 3)];
+        else
+            v = (T)H[sym_index(nc, node_row) * 9 + (row % 3) * 3 + a];
+        if(row == col && v == (T)0)
+            v = (T)1;
+        c[row] = v;
+    }
+#pragma unroll
+    for(int p = 0; p < INV_DIM; ++p)
+    {
+        T* sr   = s_row[local][p & 1];
+        sr[col] = c[p];
+        __syncthreads();
+        const T akk = sr[p];
+        const T f   = c[p];
+        T       nv;
+        if(col == p)
+        {
+            const T iv = (T)1 / akk;
+#pragma unroll
+            for(int i = 0; i < INV_DIM; ++i)
+                c[i] *= iv;
+            nv = -iv;
+        }
+        else
+        {
+            const T sc = f / akk;
+#pragma unroll
+            for(int i = 0; i < INV_DIM; ++i)
+                c[i] = fma_t<T>(-sr[i], sc, c[i]);
+            nv = sc;
+        }
+        c[p] = nv;
+    }
+    if(!live)
+        return;
+    float* O = inv + (size_t)cl * SYM * 9;
+#pragma unroll
+    for(int row = 0; row < INV_DIM; ++row)
+    {
+        const int   node_row = row / 3, b = row % 3;
+        const float v        = (float)(-c[row]);
+        if(node_row < nc)
+            O[sym_index(node_row, nc) * 9 + a * 3 + b] = v;
+        else if(node_row == nc)
+        {
+            const int si = sym_index(nc, nc);
+            if(b <= a)
+                O[si * 9 + a * 3 + b] = v;
+            if(b < a)
+                O[si * 9 + b * 3 + a] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// apply: one warp per bank. Lanes 0-15 own the bank's nodes; the 48x48
+// product is split over the two half-warps (columns 0-7 / 8-15).
+// ---------------------------------------------------------------------------
+constexpr int APPLY_WARPS = 8;
+
+// stage one cluster's 1224-float inverse in shared memory (coalesced float4)
+__device__ __forceinline__ void stage_inverse(const float* __restrict__ src, float* dst, int lane)
+{
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4*       d4 = reinterpret_cast<float4*>(dst);
+    for(int e = lane; e < SYM * 9 / 4; e += 32)
+        d4[e] = __ldg(s4 + e);
+}
+
+__device__ __forceinline__ void cluster_product(const float* M, const float (*r)[3], int lane, float out[3])
+{
+    // lanes 0..15: row node `lane`, columns 0..7; lanes 16..31: row node lane-16, columns 8..15
+    const int rn = lane & 15, c0 = (lane >> 4) * 8;
+    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
+#pragma unroll
+    for(int cc = 0; cc < 8; ++cc)
+    {
+        const int cn = c0 + cc;
+        const float x0 = r[cn][0], x1 = r[cn][1], x2 = r[cn][2];
+        if(cn >= rn)
+        {
+            const float* B = M + sym_index(rn, cn) * 9;  // column-major
+            acc0 = __fmaf_rn(B[0], x0, acc0); acc0 = __fmaf_rn(B[3], x1, acc0); acc0 = __fmaf_rn(B[6], x2, acc0);
+            acc1 = __fmaf_rn(B[1], x0, acc1); acc1 = __fmaf_rn(B[4], x1, acc1); acc1 = __fmaf_rn(B[7], x2, acc1);
+            acc2 = __fmaf_rn(B[2], x0, acc2); acc2 = __fmaf_rn(B[5], x1, acc2); acc2 = __fmaf_rn(B[8], x2, acc2);
+        }
+        else
+        {
+            const float* B = M + sym_index(cn, rn) * 9;  // use B^T
+            acc0 = __fmaf_rn(B[0], x0, acc0); acc0 = __fmaf_rn(B[1], x1, acc0); acc0 = __fmaf_rn(B[2], x2, acc0);
+            acc1 = __fmaf_rn(B[3], x0, acc1); acc1 = __fmaf_rn(B[4], x1, acc1); acc1 = __fmaf_rn(B[5], x2, acc1);
+            acc2 = __fmaf_rn(B[6], x0, acc2); acc2 = __fmaf_rn(B[7], x1, acc2); acc2 = __fmaf_rn(B[8], x2, acc2);
+        }
+    }
+    acc0 += __shfl_down_sync(0xffffffffu, acc0, 16);
+    acc1 += __shfl_down_sync(0xffffffffu, acc1, 16);
+    acc2 += __shfl_down_sync(0xffffffffu, acc2, 16);
+    out[0] = acc0;
+    out[1] = acc1;
+    out[2] = acc2;
+}
+
+// level-0 banks: gather r, push the level-1 sums, local solve -> Z
+template <typename VT>
+__global__ void __launch_bounds__(APPLY_WARPS * 32) k_apply_fine(int n_banks, const int32_t* __restrict__ p2r,
+                                                                 const uint16_t* __restrict__ comp_mask,
+                                                                 const int32_t* __restrict__ new_local0,
+                                                                 int level1_begin, const VT* __restrict__ r,
+                                                                 int off3, const float* __restrict__ inv,
+                                                                 float* __restrict__ R, float* __restrict__ Z,
+                                                                 const int* converged)
+{
+    if(converged && *converged)
+        return;
+    __shared__ __align__(16) float s_inv[APPLY_WARPS][SYM * 9];
+    __shared__ float s_r[APPLY_WARPS][BANK][3];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int bank = blockIdx.x * APPLY_WARPS + w;
+    if(bank >= n_banks)
+        return;
+    stage_inverse(inv + (size_t)bank * SYM * 9, s_inv[w], lane);
+    const int p = bank * BANK + (lane & 15);
+    float     rv[3] = {0.f, 0.f, 0.f};
+    int       v     = -1;
+    if(lane < 16)
+    {
+        v = p2r[p];
+        if(v >= 0)
+        {
+            rv[0] = (float)r[off3 + 3 * (int64_t)v];
+            rv[1] = (float)r[off3 + 3 * (int64_t)v + 1];
+            rv[2] = (float)r[off3 + 3 * (int64_t)v + 2];
+        }
+        s_r[w][lane][0] = rv[0];
+        s_r[w][lane][1] = rv[1];
+        s_r[w][lane][2] = rv[2];
+    }
+    __syncwarp();
+    // restriction: the lowest lane of each component sums it in lane order
+    if(lane < 16 && v >= 0)
+    {
+        const uint32_t cm = comp_mask[p];
+        if((cm & ((1u << lane) - 1u)) == 0)
+        {
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+            for(uint32_t m = cm; m; m &= m - 1)
+            {
+                const int l = __ffs(m) - 1;
+                s0 += s_r[w][l][0];
+                s1 += s_r[w][l][1];
+                s2 += s_r[w][l][2];
+            }
+            const int64_t g = (int64_t)level1_begin + new_local0[p];
+            R[3 * g]     = s0;
+            R[3 * g + 1] = s1;
+            R[3 * g + 2] = s2;
+        }
+    }
+    float out[3];
+    cluster_product(s_inv[w], s_r[w], lane, out);
+    if(lane < 16)
+    {
+        Z[3 * (int64_t)p]     = out[0];
+        Z[3 * (int64_t)p + 1] = out[1];
+        Z[3 * (int64_t)p + 2] = out[2];
+    }
+}
+
+// level-l banks (l >= 1): R_l from the previous pass, push R_{l+1}, solve -> Z_l
+__global__ void __launch_bounds__(APPLY_WARPS * 32) k_apply_coarse(int n_banks, int cnt, int level_begin,
+                                                                   const uint16_t* __restrict__ comp_mask,
+                                                                   const int32_t* __restrict__ new_local,
+                                                                   int next_begin, int push,
+                                                                   const float* __restrict__ inv, float* R,
+                                                                   float* __restrict__ Z, const int* converged)
+{
+    if(converged && *converged)
+        return;
+    __shared__ __align__(16) float s_inv[APPLY_WARPS][SYM * 9];
+    __shared__ float s_r[APPLY_WARPS][BANK][3];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int bank = blockIdx.x * APPLY_WARPS + w;
+    if(bank >= n_banks)
+        return;
+    const int64_t gbank = level_begin / BANK + bank;
+    stage_inverse(inv + (size_t)gbank * SYM * 9, s_inv[w], lane);
+    const int c = bank * BANK + (lane & 15);
+    if(lane < 16)
+    {
+        const bool live = c < cnt;
+        const int64_t g = (int64_t)level_begin + c;
+        s_r[w][lane][0] = live ? R[3 * g] : 0.f;
+        s_r[w][lane][1] = live ? R[3 * g + 1] : 0.f;
+        s_r[w][lane][2] = live ? R[3 * g + 2] : 0.f;
+    }
+    __syncwarp();
+    if(push && lane < 16 && c < cnt)
+    {
+        const uint32_t cm = comp_mask[c];
+        if((cm & ((1u << lane) - 1u)) == 0)
+        {
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+            for(uint32_t m = cm; m; m &= m - 1)
+            {
+                const int l = __ffs(m) - 1;
+                s0 += s_r[w][l][0];
+                s1 += s_r[w][l][1];
+                s2 += s_r[w][l][2];
+            }
+            const int64_t g = (int64_t)next_begin + new_local[c];
+            R[3 * g]     = s0;
+            R[3 * g + 1] = s1;
+            R[3 * g + 2] = s2;
+        }
+    }
+    float out[3];
+    cluster_product(s_inv[w], s_r[w], lane, out);
+    if(lane < 16)
+    {
+        const int64_t g = (int64_t)level_begin + c;
+        Z[3 * g]     = out[0];
+        Z[3 * g + 1] = out[1];
+        Z[3 * g + 2] = out[2];
+    }
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+void mas_init(b2s_solver* s, int32_t offset, int32_t vn, const int32_t* adj_start, const int32_t* adj_list, int32_t N,
+              const int32_t* p2r, const int32_t* r2p)
+{
+    B2S_REQUIRE(vn > 0 && N > 0 && offset >= 0, B2S_ERR_ARGUMENT, "MAS range must be non-empty");
+    B2S_REQUIRE(N % BANK == 0, B2S_ERR_ARGUMENT, "part_map_size must be a multiple of 16");
+    // validate the maps on the host (the reference asserts the same, fem_mas_preconditioner.cu:331-360)
+    for(int p = 0; p < N; ++p)
+    {
+        B2S_REQUIRE(p2r[p] >= -1 && p2r[p] < vn, B2S_ERR_ARGUMENT, "part_to_real entry out of range");
+        if(p2r[p] >= 0)
+            B2S_REQUIRE(r2p[p2r[p]] == p, B2S_ERR_ARGUMENT, "part_to_real / real_to_part are not inverse");
+    }
+    for(int v = 0; v < vn; ++v)
+    {
+        B2S_REQUIRE(r2p[v] >= -1 && r2p[v] < N, B2S_ERR_ARGUMENT, "real_to_part entry out of range");
+        if(r2p[v] >= 0)
+            B2S_REQUIRE(p2r[r2p[v]] == v, B2S_ERR_ARGUMENT, "part_to_real / real_to_part are not inverse");
+        B2S_REQUIRE(adj_start[v + 1] >= adj_start[v], B2S_ERR_ARGUMENT, "adjacency start not monotone");
+    }
+    const int64_t nnz_adj = adj_start[vn];
+    for(int64_t e = 0; e < nnz_adj; ++e)
+        B2S_REQUIRE(adj_list[e] >= 0 && adj_list[e] < vn, B2S_ERR_ARGUMENT, "adjacency entry out of range");
+
+    cudaStream_t st = s->stream;
+    MasState&    M  = s->mas;
+    MasState&    X  = s->mas;
+    M.initialized   = false;
+    M.offset        = offset;
+    M.vn            = vn;
+    M.N             = N;
+    M.L             = compute_num_levels(std::max(N, vn));
+    const int L     = M.L;
+    M.level_begin.assign(L + 1, 0);
+    M.level_count.assign(L + 1, 0);
+
+    DBuf<int32_t> d_start, d_num, d_list;
+    std::vector<int32_t> h_num(vn);
+    for(int v = 0; v < vn; ++v)
+        h_num[v] = adj_start[v + 1] - adj_start[v];
+    d_start.resize(vn + 1);
+    d_num.resize(vn);
+    d_list.resize(std::max<int64_t>(nnz_adj, 1));
+    M.p2r.resize(N);
+    M.r2p.resize(vn);
+    B2S_CUDA(cudaMemcpyAsync(d_start.data(), adj_start, sizeof(int32_t) * (vn + 1), cudaMemcpyHostToDevice, st));
+    B2S_CUDA(cudaMemcpyAsync(d_num.data(), h_num.data(), sizeof(int32_t) * vn, cudaMemcpyHostToDevice, st));
+    if(nnz_adj > 0)
+        B2S_CUDA(cudaMemcpyAsync(d_list.data(), adj_list, sizeof(int32_t) * nnz_adj, cudaMemcpyHostToDevice, st));
+    B2S_CUDA(cudaMemcpyAsync(M.p2r.data(), p2r, sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
+    B2S_CUDA(cudaMemcpyAsync(M.r2p.data(), r2p, sizeof(int32_t) * vn, cudaMemcpyHostToDevice, st));
+
+    // level-1 node slots start after every level-0 slot and every vertex id
+    // (mas_preconditioner_engine.cu:2162-2184 numbers them the same way)
+    const int level1_begin = bank_align(std::max(bank_align(N), vn));
+    X.cst.resize((size_t)L * vn);
+    B2S_CUDA(cudaMemsetAsync(X.cst.data(), 0xff, sizeof(int32_t) * (size_t)L * vn, st));
+
+    DBuf<uint32_t> mask;
+    DBuf<int32_t>  comp_count, bank_off, rank, scan_tmp;
+    mask.resize(std::max(N, vn) + BANK);
+    rank.resize(std::max(N, vn) + BANK);
+    const int TB = 256;
+
+    // level 0
+    {
+        const int n_banks = N / BANK;
+        comp_count.resize(n_banks + 1);
+        bank_off.resize(n_banks + 1);
+        X.comp_mask[0].resize(N);
+        X.new_local[0].resize(N);
+        k_h_mask_l0<<<grid_for(N, TB), TB, 0, st>>>(N, M.p2r.data(), M.r2p.data(), d_start.data(), d_num.data(),
+                                                    d_list.data(), mask.data());
+        B2S_CHECK_LAUNCH();
+        k_h_components<<<grid_for(n_banks, 128), 128, 0, st>>>(N, n_banks, mask.data(), M.p2r.data(), 1,
+                                                                comp_count.data(), rank.data(),
+                                                                X.comp_mask[0].data());
+        B2S_CHECK_LAUNCH();
+        exclusive_scan(s, comp_count.data(), bank_off.data(), n_banks, scan_tmp);
+        k_h_assign<<<grid_for(N, TB), TB, 0, st>>>(N, rank.data(), bank_off.data(), X.new_local[0].data());
+        B2S_CHECK_LAUNCH();
+        k_h_cst_l1<<<grid_for(vn, TB), TB, 0, st>>>(vn, M.r2p.data(), X.new_local[0].data(), X.cst.data());
+        B2S_CHECK_LAUNCH();
+        int32_t cnt1 = 0;
+        B2S_CUDA(cudaMemcpyAsync(&cnt1, bank_off.data() + n_banks, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        B2S_CUDA(cudaStreamSynchronize(st));
+        M.level_begin[0] = 0;
+        M.level_count[0] = N;
+        M.level_begin[1] = level1_begin;
+        M.level_count[1] = cnt1;
+    }
+    // levels 1 .. L-1
+    for(int level = 1; level < L; ++level)
+    {
+        const int cnt = M.level_count[level], beg = M.level_begin[level];
+        const int n_banks = (cnt + BANK - 1) / BANK;
+        const int next_begin = beg + bank_align(cnt);
+        B2S_CUDA(cudaMemsetAsync(mask.data(), 0, sizeof(uint32_t) * (cnt + BANK), st));
+        const int32_t* cst_prev = X.cst.data() + (size_t)(level - 1) * vn;
+        k_h_mask_lx<<<grid_for(N, TB), TB, 0, st>>>(N, vn, M.p2r.data(), cst_prev, d_start.data(), d_num.data(),
+                                                    d_list.data(), mask.data(), cnt);
+        B2S_CHECK_LAUNCH();
+        comp_count.resize(n_banks + 1);
+        bank_off.resize(n_banks + 1);
+        X.comp_mask[level].resize(std::max(cnt, 1));
+        X.new_local[level].resize(std::max(cnt, 1));
+        k_h_components<<<grid_for(n_banks, 128), 128, 0, st>>>(cnt, n_banks, mask.data(), nullptr, 0,
+                                                                comp_count.data(), rank.data(),
+                                                                X.comp_mask[level].data());
+        B2S_CHECK_LAUNCH();
+        exclusive_scan(s, comp_count.data(), bank_off.data(), n_banks, scan_tmp);
+        k_h_assign<<<grid_for(cnt, TB), TB, 0, st>>>(cnt, rank.data(), bank_off.data(), X.new_local[level].data());
+        B2S_CHECK_LAUNCH();
+        k_h_cst_next<<<grid_for(vn, TB), TB, 0, st>>>(vn, cst_prev, X.new_local[level].data(), cnt,
+                                                      X.cst.data() + (size_t)level * vn);
+        B2S_CHECK_LAUNCH();
+        int32_t cnt_next = 0;
+        B2S_CUDA(cudaMemcpyAsync(&cnt_next, bank_off.data() + n_banks, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        B2S_CUDA(cudaStreamSynchronize(st));
+        if(level + 1 <= L)
+        {
+            if(level + 1 < (int)M.level_begin.size())
+            {
+                M.level_begin[level + 1] = next_begin;
+                M.level_count[level + 1] = cnt_next;
+            }
+        }
+    }
+    M.total    = M.level_begin[L];
+    M.clusters = M.total / BANK;
+    // coarse table
+    X.level_begin_dev.resize(L + 1);
+    B2S_CUDA(cudaMemcpyAsync(X.level_begin_dev.data(), M.level_begin.data(), sizeof(int32_t) * (L + 1),
+                             cudaMemcpyHostToDevice, st));
+    M.ctable.resize((size_t)vn * std::max(L - 1, 1));
+    if(L > 1)
+    {
+        k_h_ctable<<<grid_for(vn, TB), TB, 0, st>>>(vn, L, X.cst.data(), X.level_begin_dev.data(), M.ctable.data());
+        B2S_CHECK_LAUNCH();
+    }
+    M.hess.resize((size_t)M.clusters * SYM * 9);
+    M.inv.resize((size_t)M.clusters * SYM * 9);
+    M.R.resize((size_t)M.total * 3 + 3);
+    M.Z.resize((size_t)M.total * 3 + 3);
+    B2S_CUDA(cudaMemsetAsync(M.R.data(), 0, M.R.bytes(), st));
+    B2S_CUDA(cudaMemsetAsync(M.Z.data(), 0, M.Z.bytes(), st));
+    M.h_ctable.resize((size_t)vn * std::max(L - 1, 1));
+    if(L > 1)
+        B2S_CUDA(cudaMemcpyAsync(M.h_ctable.data(), M.ctable.data(), sizeof(int32_t) * M.h_ctable.size(),
+                                 cudaMemcpyDeviceToHost, st));
+    B2S_CUDA(cudaStreamSynchronize(st));
+    M.initialized = true;
+}
+
+void mas_assemble(b2s_solver* s, int invert_mode)
+{
+    MasState& M = s->mas;
+    MasState& X = s->mas;
+    B2S_REQUIRE(M.initialized, B2S_ERR_STATE, "MAS not initialised");
+    B2S_REQUIRE(s->A.valid, B2S_ERR_STATE, "no assembled matrix");
+    B2S_REQUIRE(M.offset + M.vn <= s->A.nb, B2S_ERR_ARGUMENT, "MAS range exceeds the matrix");
+    cudaStream_t st = s->stream;
+    const int    TB = 256;
+    const Matrix& A = s->A;
+    B2S_CUDA(cudaMemsetAsync(M.hess.data(), 0, M.hess.bytes(), st));
+    if(A.nnz > 0)
+    {
+        k_g_level0<<<grid_for(A.nnz, TB), TB, 0, st>>>(A.nnz, A.rows.data(), A.cols.data(), A.vals.data(), M.offset,
+                                                       M.vn, M.r2p.data(), M.hess.data());
+        B2S_CHECK_LAUNCH();
+    }
+    // coarse levels: A_1 from A (vertex ids -> level-1 ids), A_{l+1} from A_l
+    const Matrix* prev     = &A;
+    int           prev_off = M.offset;
+    int           prev_n   = M.vn;
+    const int32_t* map     = X.cst.data();  // vertex -> level-1 local id
+    for(int level = 1; level < M.L; ++level)
+    {
+        const int64_t T = prev->nnz;
+        Matrix&       C = M.coarse[level];
+        M.trip_rows.resize(std::max<int64_t>(T, 1), 1.2);
+        M.trip_cols.resize(std::max<int64_t>(T, 1), 1.2);
+        M.trip_vals.resize((size_t)9 * std::max<int64_t>(T, 1), 1.2);
+        if(T > 0)
+        {
+            k_g_restrict<<<grid_for(T, TB), TB, 0, st>>>(T, prev->rows.data(), prev->cols.data(), prev->vals.data(),
+                                                         prev_off, prev_n, map, M.trip_rows.data(),
+                                                         M.trip_cols.data(), M.trip_vals.data());
+            B2S_CHECK_LAUNCH();
+        }
+        assemble_triplets(s, C, M.level_count[level], T, M.trip_rows.data(), M.trip_cols.data(), M.trip_vals.data(),
+                          false, 0);
+        if(C.nnz > 0)
+        {
+            k_g_extract<<<grid_for(C.nnz, TB), TB, 0, st>>>(C.nnz, C.rows.data(), C.cols.data(), C.vals.data(),
+                                                            M.level_begin[level], M.hess.data());
+            B2S_CHECK_LAUNCH();
+        }
+        prev     = &C;
+        prev_off = 0;
+        prev_n   = M.level_count[level];
+        map      = X.new_local[level].data();
+    }
+    if(M.clusters > 0)
+    {
+        const int grid = (M.clusters + INV_CLUSTERS - 1) / INV_CLUSTERS;
+        if(invert_mode == B2S_INVERT_GJ_F64)
+            k_invert<double><<<grid, INV_BLOCK, 0, st>>>(M.clusters, M.hess.data(), M.inv.data());
+        else
+            k_invert<float><<<grid, INV_BLOCK, 0, st>>>(M.clusters, M.hess.data(), M.inv.data());
+        B2S_CHECK_LAUNCH();
+    }
+}
+
+// z[off..off+vn) gets the MAS part of z = P r; Jacobi/identity elsewhere is
+// handled by the caller (collect kernel in the PCG, or precond_apply)
+void mas_apply_levels(b2s_solver* s, const double* r, const int* converged)
+{
+    MasState& M = s->mas;
+    MasState& X = s->mas;
+    cudaStream_t st = s->stream;
+    const int n_banks0 = M.N / BANK;
+    const int tb       = APPLY_WARPS * 32;
+    k_apply_fine<double><<<grid_for(n_banks0, APPLY_WARPS), tb, 0, st>>>(
+        n_banks0, M.p2r.data(), X.comp_mask[0].data(), X.new_local[0].data(), M.level_begin[1], r, 3 * M.offset,
+        M.inv.data(), M.R.data(), M.Z.data(), converged);
+    B2S_CHECK_LAUNCH();
+    for(int level = 1; level < M.L; ++level)
+    {
+        const int cnt = M.level_count[level];
+        if(cnt <= 0)
+            break;
+        const int n_banks = (cnt + BANK - 1) / BANK;
+        const int push    = level + 1 < M.L ? 1 : 0;
+        k_apply_coarse<<<grid_for(n_banks, APPLY_WARPS), tb, 0, st>>>(
+            n_banks, cnt, M.level_begin[level], X.comp_mask[level].data(),
+            push ? X.new_local[level].data() : X.new_local[0].data(), push ? M.level_begin[level + 1] : 0, push,
+            M.inv.data(), M.R.data(), M.Z.data(), converged);
+        B2S_CHECK_LAUNCH();
+    }
+}
+
+}  // namespace b2s

@@ -1,0 +1,577 @@
+// Preconditioner build/apply dispatch and the PCG loop (FP64 path).
+//
+// PCG semantics follow LinearFusedPCG::fused_pcg
+// (src/backends/cuda/linear_system/linear_fused_pcg.cu:1782-2005) and
+// LinearPCG::pcg (src/backends/cuda/linear_system/linear_pcg.cu:558-644):
+// x0 = 0 (or the given guess), r = b - A x0, z = P r, p = z; per iteration
+// alpha = rz / pAp, x += alpha p, r -= alpha Ap, z = P r, rz' = r.z,
+// converged when |rz'| <= tol |rz0| (or, with the relative-residual rule,
+// ||r|| <= tol ||b||), beta = rz'/rz, p = z + beta p; max_iter = 2 n; the
+// PSD guard re-runs with the preconditioner bypassed when rz0 < 0 or is not
+// finite (:1819-1877). The scalars live on the device; the convergence flag
+// freezes every kernel once set, so `check_interval` iterations can be
+// replayed from one CUDA graph and checked once by the host, as the
+// reference's graph block replay does (:1923-1998).
+#include "b2s_internal.cuh"
+#include "b2s_reduce.cuh"
+
+#include <cmath>
+#include <cstring>
+
+namespace b2s
+{
+void spmv_f64_launch(cudaStream_t st, const Matrix& A, const double* x, double* y, Reduction& red, double* d_dot,
+                     const int* stop);
+int  spmv_grid(int64_t U);
+void ensure_reduction(Reduction& red, int grid, int nv);
+void mas_apply_levels(b2s_solver* s, const double* r, const int* converged);
+
+namespace
+{
+constexpr int VEC_BLOCK = 256;
+
+int vec_grid(int64_t n)
+{
+    int64_t g = (n + VEC_BLOCK - 1) / VEC_BLOCK;
+    const int64_t cap = (int64_t)NUM_SMS_HINT * 8;
+    if(g > cap)
+        g = cap;
+    return (int)(g < 1 ? 1 : g);
+}
+
+__device__ __forceinline__ bool frozen(const PcgScalars* sc) { return sc && sc->converged != 0; }
+
+// 3x3 block Jacobi inverses (row-major), identity where the diagonal block is
+// missing or singular
+__global__ void k_diag_inverse(int32_t nb, const int32_t* diag_index, const double* vals, int64_t U, double* dinv)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= nb)
+        return;
+    const int k = diag_index[i];
+    double*   o = dinv + (size_t)i * 9;
+    if(k < 0)
+    {
+        for(int q = 0; q < 9; ++q)
+            o[q] = (q % 4 == 0) ? 1.0 : 0.0;
+        return;
+    }
+    double m[9];  // row-major
+#pragma unroll
+    for(int p = 0; p < 3; ++p)
+#pragma unroll
+        for(int q = 0; q < 3; ++q)
+            m[p * 3 + q] = vals[(int64_t)(q * 3 + p) * U + k];
+    const double c0 = m[4] * m[8] - m[5] * m[7], c1 = m[5] * m[6] - m[3] * m[8], c2 = m[3] * m[7] - m[4] * m[6];
+    const double det = m[0] * c0 + m[1] * c1 + m[2] * c2;
+    if(!(det != 0.0) || !isfinite(det))
+    {
+        for(int q = 0; q < 9; ++q)
+            o[q] = (q % 4 == 0) ? 1.0 : 0.0;
+        return;
+    }
+    const double id = 1.0 / det;
+    o[0] = c0 * id;
+    o[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+    o[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+    o[3] = c1 * id;
+    o[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+    o[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    o[6] = c2 * id;
+    o[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+    o[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+}
+
+struct MasView
+{
+    int            active;  // MAS present
+    int            off, vn, L;
+    const int32_t* r2p;
+    const int32_t* ctable;  // [vn * (L-1)]
+    const float*   Z;
+};
+
+// z_i for block row i: MAS (partitioned vertices of its range), else 3x3
+// block Jacobi (kind 1 / 2), else identity (kind 0)
+__device__ __forceinline__ void precond_row(int kind, const MasView& mv, const double* dinv, const double* r, int i,
+                                            double z[3])
+{
+    const double r0 = r[3 * (int64_t)i], r1 = r[3 * (int64_t)i + 1], r2 = r[3 * (int64_t)i + 2];
+    if(kind == B2S_PRECOND_MAS && mv.active)
+    {
+        const int v = i - mv.off;
+        if(v >= 0 && v < mv.vn)
+        {
+            const int p = mv.r2p[v];
+            if(p >= 0)
+            {
+                float c0 = mv.Z[3 * (int64_t)p], c1 = mv.Z[3 * (int64_t)p + 1], c2 = mv.Z[3 * (int64_t)p + 2];
+                for(int l = 1; l < mv.L; ++l)
+                {
+                    const int64_t node = mv.ctable[(int64_t)v * (mv.L - 1) + (l - 1)];
+                    c0 += mv.Z[3 * node];
+                    c1 += mv.Z[3 * node + 1];
+                    c2 += mv.Z[3 * node + 2];
+                }
+                z[0] = (double)c0;
+                z[1] = (double)c1;
+                z[2] = (double)c2;
+                return;
+            }
+        }
+    }
+    if(kind == B2S_PRECOND_NONE)
+    {
+        z[0] = r0;
+        z[1] = r1;
+        z[2] = r2;
+        return;
+    }
+    const double* D = dinv + (size_t)i * 9;
+    z[0] = D[0] * r0 + D[1] * r1 + D[2] * r2;
+    z[1] = D[3] * r0 + D[4] * r1 + D[5] * r2;
+    z[2] = D[6] * r0 + D[7] * r1 + D[8] * r2;
+}
+
+// z = P r for every block row; with `sc`, also r.z and r.r and the scalar
+// update of the iteration (last block)
+__global__ void __launch_bounds__(RED_BLOCK) k_precond_finish(int32_t nb, int kind, MasView mv,
+                                                              const double* __restrict__ dinv,
+                                                              const double* __restrict__ r, double* __restrict__ z,
+                                                              PcgScalars* sc, double* partials,
+                                                              unsigned int* counter)
+{
+    if(frozen(sc))
+        return;
+    double rz = 0.0, rr = 0.0;
+    for(int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < nb; i += gridDim.x * RED_BLOCK)
+    {
+        double zi[3];
+        precond_row(kind, mv, dinv, r, i, zi);
+        z[3 * (int64_t)i]     = zi[0];
+        z[3 * (int64_t)i + 1] = zi[1];
+        z[3 * (int64_t)i + 2] = zi[2];
+        if(sc)
+        {
+            const double r0 = r[3 * (int64_t)i], r1 = r[3 * (int64_t)i + 1], r2 = r[3 * (int64_t)i + 2];
+            rz += r0 * zi[0] + r1 * zi[1] + r2 * zi[2];
+            rr += r0 * r0 + r1 * r1 + r2 * r2;
+        }
+    }
+    if(!sc)
+        return;
+    double v[2] = {rz, rr}, tot[2];
+    if(!grid_sum<2>(v, partials, counter, tot))
+        return;
+    // scalar update of the iteration (one thread)
+    const double rz_new = tot[0];
+    sc->rz_new          = rz_new;
+    sc->rr              = tot[1];
+    sc->iter += 1;
+    const bool hit = (sc->stop_rule == B2S_STOP_RZ) ? (fabs(rz_new) <= sc->rz_tol) : (tot[1] <= sc->rr_tol);
+    if(!isfinite(rz_new))
+        sc->converged = 3;
+    else if(hit)
+    {
+        sc->converged = 1;
+        sc->iter_conv = sc->iter;
+    }
+    else if(sc->iter >= sc->max_iter - 1)
+        sc->converged = 2;
+    else
+    {
+        sc->beta = rz_new / sc->rz;
+        sc->rz   = rz_new;
+    }
+}
+
+__global__ void k_update_xr(int64_t n, PcgScalars* sc, double* __restrict__ x, const double* __restrict__ p,
+                            double* __restrict__ r, double* __restrict__ Ap)
+{
+    if(frozen(sc))
+        return;
+    const double alpha = sc->rz / sc->pAp;
+    if(blockIdx.x == 0 && threadIdx.x == 0)
+        sc->alpha = alpha;
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
+    {
+        const double api = Ap[i];
+        x[i] += alpha * p[i];
+        r[i] -= alpha * api;
+        Ap[i] = 0.0;
+    }
+}
+
+__global__ void k_update_p(int64_t n, const PcgScalars* sc, const double* __restrict__ z, double* __restrict__ p)
+{
+    if(frozen(sc))
+        return;
+    const double beta = sc->beta;
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
+        p[i] = z[i] + beta * p[i];
+}
+
+__global__ void k_residual(int64_t n, const double* __restrict__ b, const double* __restrict__ Ax,
+                           double* __restrict__ r)
+{
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
+        r[i] = b[i] - Ax[i];
+}
+
+// sum (b - Ax)^2 and b.b
+__global__ void __launch_bounds__(RED_BLOCK) k_res_norms(int64_t n, const double* __restrict__ b,
+                                                         const double* __restrict__ Ax, double* partials,
+                                                         unsigned int* counter, double* out)
+{
+    double rr = 0.0, bb = 0.0;
+    for(int64_t i = (int64_t)blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_BLOCK)
+    {
+        const double d = b[i] - Ax[i];
+        rr += d * d;
+        bb += b[i] * b[i];
+    }
+    double v[2] = {rr, bb}, tot[2];
+    if(grid_sum<2>(v, partials, counter, tot))
+    {
+        out[0] = tot[0];
+        out[1] = tot[1];
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+void precond_assemble(b2s_solver* s, int kind, int invert_mode)
+{
+    B2S_REQUIRE(s->A.valid, B2S_ERR_STATE, "precond_assemble before b2s_assemble");
+    B2S_REQUIRE(kind >= B2S_PRECOND_NONE && kind <= B2S_PRECOND_MAS, B2S_ERR_ARGUMENT, "unknown preconditioner");
+    B2S_REQUIRE(invert_mode == B2S_INVERT_SWEEP_F32 || invert_mode == B2S_INVERT_GJ_F64, B2S_ERR_ARGUMENT,
+                "unknown inversion mode");
+    cudaStream_t st = s->stream;
+    const Matrix& A = s->A;
+    s->dinv.resize((size_t)std::max(A.nb, 1) * 9);
+    if(A.nb > 0)
+    {
+        k_diag_inverse<<<grid_for(A.nb, 256), 256, 0, st>>>(A.nb, A.diag_index.data(), A.vals.data(), A.nnz,
+                                                            s->dinv.data());
+        B2S_CHECK_LAUNCH();
+    }
+    if(kind == B2S_PRECOND_MAS)
+    {
+        B2S_REQUIRE(s->mas.initialized, B2S_ERR_STATE, "MAS preconditioner requested before b2s_mas_init");
+        mas_assemble(s, invert_mode);
+    }
+    s->precond_kind = kind;
+    s->invert_mode  = invert_mode;
+    B2S_CUDA(cudaStreamSynchronize(st));
+}
+
+static MasView mas_view(b2s_solver* s)
+{
+    MasView mv{};
+    const MasState& M = s->mas;
+    mv.active = (s->precond_kind == B2S_PRECOND_MAS && M.initialized) ? 1 : 0;
+    mv.off    = M.offset;
+    mv.vn     = M.vn;
+    mv.L      = M.L;
+    mv.r2p    = M.r2p.data();
+    mv.ctable = M.ctable.data();
+    mv.Z      = M.Z.data();
+    return mv;
+}
+
+// z = P r, optionally fused with the dots + scalar update of a PCG iteration
+static void precond_launch(b2s_solver* s, int kind, const double* r, double* z, PcgScalars* sc, Reduction& red)
+{
+    cudaStream_t st = s->stream;
+    const int32_t nb = s->A.nb;
+    if(nb == 0)
+        return;
+    if(kind == B2S_PRECOND_MAS)
+        mas_apply_levels(s, r, sc ? &sc->converged : nullptr);
+    const int grid = reduction_grid();
+    ensure_reduction(red, grid, 2);
+    k_precond_finish<<<grid, RED_BLOCK, 0, st>>>(nb, kind, mas_view(s), s->dinv.data(), r, z, sc,
+                                                 red.partials.data(), red.counter.data());
+    B2S_CHECK_LAUNCH();
+}
+
+void precond_apply(b2s_solver* s, const double* r, double* z)
+{
+    B2S_REQUIRE(s->precond_kind >= 0, B2S_ERR_STATE, "precond_apply before b2s_precond_assemble");
+    precond_launch(s, s->precond_kind, r, z, nullptr, s->red);
+    B2S_CUDA(cudaStreamSynchronize(s->stream));
+}
+
+// ---------------------------------------------------------------------------
+// PCG
+// ---------------------------------------------------------------------------
+namespace
+{
+struct GraphKey
+{
+    const void* ptrs[10];
+    int64_t     ints[6];
+    bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
+};
+}  // namespace
+
+// one PCG iteration; with timing on, `slot` selects the 4 events that
+// bracket its SpMV and its preconditioner apply
+static void pcg_iteration(b2s_solver* s, int kind, double* x, int slot)
+{
+    PcgState&     P  = s->pcg;
+    const Matrix& A  = s->A;
+    cudaStream_t  st = s->stream;
+    const int64_t n  = 3 * (int64_t)A.nb;
+    cudaEvent_t*  ev = s->timing ? &s->iter_events[(size_t)slot * 4] : nullptr;
+    if(ev)
+        B2S_CUDA(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
+    spmv_f64_launch(st, A, P.p.data(), P.Ap.data(), P.red, &P.sc.data()->pAp, &P.sc.data()->converged);
+    if(ev)
+        B2S_CUDA(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
+    k_update_xr<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), x, P.p.data(), P.r.data(), P.Ap.data());
+    B2S_CHECK_LAUNCH();
+    if(ev)
+        B2S_CUDA(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
+    precond_launch(s, kind, P.r.data(), P.z.data(), P.sc.data(), P.red);
+    if(ev)
+        B2S_CUDA(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
+    k_update_p<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), P.z.data(), P.p.data());
+    B2S_CHECK_LAUNCH();
+}
+
+static void ensure_iter_events(b2s_solver* s, int ci)
+{
+    while((int)s->iter_events.size() < 4 * ci)
+    {
+        cudaEvent_t e;
+        B2S_CUDA(cudaEventCreate(&e));
+        s->iter_events.push_back(e);
+    }
+}
+
+void pcg_solve(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st_out)
+{
+    B2S_REQUIRE(s->A.valid, B2S_ERR_STATE, "b2s_pcg before b2s_assemble");
+    B2S_REQUIRE(s->precond_kind >= 0, B2S_ERR_STATE, "b2s_pcg before b2s_precond_assemble");
+    B2S_REQUIRE(o.precision == B2S_PRECISION_FP64, B2S_ERR_ARGUMENT, "this entry point runs the FP64 path");
+    B2S_REQUIRE(o.tol > 0.0 && std::isfinite(o.tol), B2S_ERR_ARGUMENT, "tolerance must be positive");
+    B2S_REQUIRE(o.stop_rule == B2S_STOP_RZ || o.stop_rule == B2S_STOP_RELRES, B2S_ERR_ARGUMENT, "unknown stop rule");
+    cudaStream_t  st = s->stream;
+    const Matrix& A  = s->A;
+    PcgState&     P  = s->pcg;
+    const int64_t n  = 3 * (int64_t)A.nb;
+    std::memset(&st_out, 0, sizeof(st_out));
+    if(n == 0)
+    {
+        st_out.converged = 1;
+        return;
+    }
+    P.r.resize(n, 1.1);
+    P.z.resize(n, 1.1);
+    P.p.resize(n, 1.1);
+    P.Ap.resize(n, 1.1);
+    P.tmp.resize(n, 1.1);
+    P.sc.resize(1);
+    if(!P.h_sc)
+        B2S_CUDA(cudaMallocHost(&P.h_sc, sizeof(PcgScalars)));
+    ensure_reduction(P.red, std::max(spmv_grid(A.nnz), reduction_grid()), 2);
+    s->dot_out.resize(4);
+    const int ci = o.check_interval > 0 ? o.check_interval : 1;
+    const int64_t max_iter = o.max_iter > 0 ? o.max_iter : std::max<int64_t>(2 * n, 1);
+
+    // r = b - A x0
+    if(o.x0_given)
+    {
+        spmv_f64(s, A, x, P.tmp.data(), nullptr);
+        k_residual<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, b, P.tmp.data(), P.r.data());
+        B2S_CHECK_LAUNCH();
+    }
+    else
+    {
+        B2S_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+        B2S_CUDA(cudaMemcpyAsync(P.r.data(), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    }
+    int kind = s->precond_kind;
+    precond_launch(s, kind, P.r.data(), P.z.data(), nullptr, s->red);
+    launch_dot(s, P.r.data(), P.z.data(), n, s->dot_out.data());
+    launch_dot(s, P.r.data(), P.r.data(), n, s->dot_out.data() + 1);
+    launch_dot(s, b, b, n, s->dot_out.data() + 2);
+    double h3[3];
+    B2S_CUDA(cudaMemcpyAsync(h3, s->dot_out.data(), sizeof(h3), cudaMemcpyDeviceToHost, st));
+    B2S_CUDA(cudaStreamSynchronize(st));
+    double rz0 = h3[0];
+    const double rr0 = h3[1], bb = h3[2];
+    B2S_REQUIRE(std::isfinite(rr0) && std::isfinite(bb), B2S_ERR_NUMERIC,
+                "non-finite right-hand side or initial residual");
+    bool bypass = false;
+    if(kind != B2S_PRECOND_NONE && (rz0 < 0.0 || !std::isfinite(rz0)))
+    {
+        // PSD guard: the preconditioner's action is not SPD/finite -> plain CG
+        bypass = true;
+        kind   = B2S_PRECOND_NONE;
+        B2S_CUDA(cudaMemcpyAsync(P.z.data(), P.r.data(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        rz0 = rr0;
+    }
+    st_out.rz0      = rz0;
+    st_out.bypassed = bypass ? 1 : 0;
+    const double bnorm = std::sqrt(bb);
+
+    auto true_residual = [&]() -> double
+    {
+        spmv_f64(s, A, x, P.tmp.data(), nullptr);
+        k_res_norms<<<reduction_grid(), RED_BLOCK, 0, st>>>(n, b, P.tmp.data(), s->red.partials.data(),
+                                                            s->red.counter.data(), s->dot_out.data());
+        B2S_CHECK_LAUNCH();
+        double h2[2];
+        B2S_CUDA(cudaMemcpyAsync(h2, s->dot_out.data(), sizeof(h2), cudaMemcpyDeviceToHost, st));
+        B2S_CUDA(cudaStreamSynchronize(st));
+        return h2[1] > 0 ? std::sqrt(h2[0] / h2[1]) : 0.0;
+    };
+
+    if(rz0 == 0.0 || bb == 0.0)
+    {
+        st_out.converged = 1;
+        st_out.rel_res   = true_residual();
+        return;
+    }
+    ensure_reduction(s->red, reduction_grid(), 2);
+
+    // device scalars
+    PcgScalars h{};
+    h.rz        = rz0;
+    h.rz_tol    = o.tol * std::fabs(rz0);
+    h.rr_tol    = (o.tol * bnorm) * (o.tol * bnorm);
+    h.stop_rule = o.stop_rule;
+    h.max_iter  = max_iter;
+    int64_t iter_total = 0, replacements = 0;
+    bool    done = false;
+    while(!done)
+    {
+        h.converged = 0;
+        h.iter      = iter_total;
+        h.iter_conv = 0;
+        B2S_CUDA(cudaMemcpyAsync(P.sc.data(), &h, sizeof(h), cudaMemcpyHostToDevice, st));
+        B2S_CUDA(cudaMemcpyAsync(P.p.data(), P.z.data(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        B2S_CUDA(cudaMemsetAsync(P.Ap.data(), 0, sizeof(double) * n, st));
+
+        // CUDA graph of `ci` iterations (re-captured when anything it bakes in changes)
+        bool use_graph = o.use_graph && st != nullptr;
+        if(s->timing)
+            ensure_iter_events(s, ci);
+        if(use_graph)
+        {
+            GraphKey key{};
+            key.ptrs[0] = x;
+            key.ptrs[1] = A.vals.data();
+            key.ptrs[2] = A.rows.data();
+            key.ptrs[3] = P.r.data();
+            key.ptrs[4] = s->mas.inv.data();
+            key.ptrs[5] = s->dinv.data();
+            key.ptrs[6] = P.red.partials.data();
+            key.ptrs[7] = s->mas.Z.data();
+            key.ptrs[8] = A.cols.data();
+            key.ptrs[9] = b;
+            key.ints[0] = A.nnz;
+            key.ints[1] = A.nb;
+            key.ints[2] = kind;
+            key.ints[3] = ci;
+            key.ints[4] = s->mas.initialized ? s->mas.total : -1;
+            key.ints[5] = s->mas.L + (s->timing ? 1000 : 0);
+            size_t hk = 1469598103934665603ull;
+            const unsigned char* kb = reinterpret_cast<const unsigned char*>(&key);
+            for(size_t q = 0; q < sizeof(key); ++q)
+                hk = (hk ^ kb[q]) * 1099511628211ull;
+            if(!P.graph || P.graph_key != hk)
+            {
+                if(P.graph)
+                {
+                    cudaGraphExecDestroy(P.graph);
+                    P.graph = nullptr;
+                }
+                cudaGraph_t g = nullptr;
+                const long long before = g_kernel_launches;
+                B2S_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                for(int it = 0; it < ci; ++it)
+                    pcg_iteration(s, kind, x, it);
+                B2S_CUDA(cudaStreamEndCapture(st, &g));
+                P.graph_kernels = g_kernel_launches - before;
+                g_kernel_launches = before;
+                cudaError_t e = cudaGraphInstantiate(&P.graph, g, 0);
+                cudaGraphDestroy(g);
+                if(e != cudaSuccess)
+                {
+                    P.graph   = nullptr;
+                    use_graph = false;
+                    cudaGetLastError();
+                }
+                else
+                    P.graph_key = hk;
+            }
+        }
+        long long iter_before = h.iter;
+        while(true)
+        {
+            if(use_graph)
+            {
+                B2S_CUDA(cudaGraphLaunch(P.graph, st));
+                g_kernel_launches += P.graph_kernels;
+            }
+            else
+                for(int it = 0; it < ci; ++it)
+                    pcg_iteration(s, kind, x, it);
+            B2S_CUDA(cudaMemcpyAsync(P.h_sc, P.sc.data(), sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+            B2S_CUDA(cudaStreamSynchronize(st));
+            if(s->timing)
+            {
+                // the iterations of this block that did work (the rest were frozen)
+                const long long live = std::min<long long>(P.h_sc->iter - iter_before, ci);
+                for(long long it = 0; it < live; ++it)
+                {
+                    float a = 0.f, c = 0.f;
+                    B2S_CUDA(cudaEventElapsedTime(&a, s->iter_events[it * 4 + 0], s->iter_events[it * 4 + 1]));
+                    B2S_CUDA(cudaEventElapsedTime(&c, s->iter_events[it * 4 + 2], s->iter_events[it * 4 + 3]));
+                    s->timers.spmv_ms += a;
+                    s->timers.spmv_launches += 1;
+                    s->timers.precond_apply_ms += c;
+                    s->timers.precond_apply_launches += 1;
+                }
+            }
+            iter_before = P.h_sc->iter;
+            if(P.h_sc->converged != 0)
+                break;
+        }
+        const PcgScalars r = *P.h_sc;
+        iter_total         = r.iter;
+        if(r.converged == 3)
+            throw Error(B2S_ERR_NUMERIC, "PCG breakdown: r.z became non-finite at iteration " + std::to_string(r.iter));
+        st_out.iterations_exact = r.converged == 1 ? r.iter_conv : r.iter;
+        st_out.converged        = r.converged == 1 ? 1 : 0;
+        st_out.rel_res          = true_residual();
+        done = true;
+        if(r.converged == 1 && o.stop_rule == B2S_STOP_RELRES && st_out.rel_res > o.tol && replacements < 8
+           && iter_total < max_iter - 1)
+        {
+            // the recursive residual drifted from b - A x: replace it and continue
+            ++replacements;
+            spmv_f64(s, A, x, P.tmp.data(), nullptr);
+            k_residual<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, b, P.tmp.data(), P.r.data());
+            B2S_CHECK_LAUNCH();
+            precond_launch(s, kind, P.r.data(), P.z.data(), nullptr, s->red);
+            launch_dot(s, P.r.data(), P.z.data(), n, s->dot_out.data());
+            double rz;
+            B2S_CUDA(cudaMemcpyAsync(&rz, s->dot_out.data(), sizeof(double), cudaMemcpyDeviceToHost, st));
+            B2S_CUDA(cudaStreamSynchronize(st));
+            h.rz = rz;
+            done = false;
+        }
+    }
+    st_out.replacements = replacements;
+    if(st_out.converged)
+        st_out.iterations = ci > 1 ? std::min<int64_t>(((st_out.iterations_exact + ci - 1) / ci) * ci, max_iter)
+                                   : st_out.iterations_exact;
+    else
+        st_out.iterations = max_iter;
+}
+}  // namespace b2s

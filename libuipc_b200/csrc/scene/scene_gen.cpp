@@ -1,0 +1,797 @@
+// Synthetic Newton-system generator (host C++, OpenMP). See scene_gen.h.
+//
+// Physics restated from the formulations libuipc uses (own code):
+//  * Stable Neo-Hookean  Psi = lambda/2 (J-1)^2 - mu (J-1) + mu/2 (|F|^2 - 3)
+//    (src/backends/cuda/finite_element/constitutions/sym/simplified_stable_neo_hookean_3d.inl),
+//    element Hessian projected to PSD through the eigen-decomposition of
+//    d2Psi/dF2, scaled by rest volume and dt^2.
+//  * BDF1 kinetic term 1/2 m |x - x_tilde|^2, x_tilde = x + dt v + dt^2 g,
+//    lumped mass rho V / 4 per tet corner
+//    (src/backends/cuda/finite_element/bdf/finite_element_bdf1_kinetic.cu).
+//  * IPC log barrier on squared distance D < dhat^2:
+//        b(D) = -(D - Dhat)^2 log(D / Dhat), energy dt^2 kappa b(D).
+//    Contact Hessians use the barrier curvature along the fixed contact
+//    normal (rank-1 Gauss-Newton form, PSD by construction).
+//  * Fixed vertices: every block touching one is written as 0 (off-diagonal)
+//    or I (diagonal) and its gradient is zeroed
+//    (src/backends/cuda/finite_element/fem_linear_subsystem.cu:23-52).
+#include "scene_gen.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace
+{
+thread_local std::string g_err;
+
+using Vec3 = std::array<double, 3>;
+using Mat3 = std::array<double, 9>;  // column-major
+
+inline Vec3 sub(const Vec3& a, const Vec3& b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
+inline Vec3 add(const Vec3& a, const Vec3& b) { return {a[0] + b[0], a[1] + b[1], a[2] + b[2]}; }
+inline Vec3 scale(const Vec3& a, double s) { return {a[0] * s, a[1] * s, a[2] * s}; }
+inline double dot(const Vec3& a, const Vec3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline Vec3 cross(const Vec3& a, const Vec3& b)
+{
+    return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+inline double norm(const Vec3& a) { return std::sqrt(dot(a, a)); }
+
+inline uint64_t splitmix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+// uniform in [-1, 1) from (seed, stream, index)
+inline double urand(uint64_t seed, uint64_t stream, uint64_t idx)
+{
+    uint64_t r = splitmix64(seed * 0x632BE59BD9B4E019ull + stream * 0x9E3779B97F4A7C15ull + idx);
+    r          = splitmix64(r);
+    return (double)(r >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// Cyclic Jacobi eigen-decomposition of a symmetric n x n matrix (row-major a),
+// eigenvectors in the columns of v (row-major).
+template <int N>
+void jacobi_eigen(double* a, double* w, double* v)
+{
+    for(int i = 0; i < N * N; ++i)
+        v[i] = 0.0;
+    for(int i = 0; i < N; ++i)
+        v[i * N + i] = 1.0;
+    for(int sweep = 0; sweep < 60; ++sweep)
+    {
+        double off = 0.0, diag = 0.0;
+        for(int p = 0; p < N; ++p)
+        {
+            diag += a[p * N + p] * a[p * N + p];
+            for(int q = p + 1; q < N; ++q)
+                off += a[p * N + q] * a[p * N + q];
+        }
+        if(off <= 1e-30 * (diag + 1e-300))
+            break;
+        for(int p = 0; p < N; ++p)
+            for(int q = p + 1; q < N; ++q)
+            {
+                double apq = a[p * N + q];
+                if(std::fabs(apq) < 1e-300)
+                    continue;
+                double app = a[p * N + p], aqq = a[q * N + q];
+                double theta = (aqq - app) / (2.0 * apq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for(int k = 0; k < N; ++k)
+                {
+                    double akp = a[k * N + p], akq = a[k * N + q];
+                    a[k * N + p] = c * akp - s * akq;
+                    a[k * N + q] = s * akp + c * akq;
+                }
+                for(int k = 0; k < N; ++k)
+                {
+                    double apk = a[p * N + k], aqk = a[q * N + k];
+                    a[p * N + k] = c * apk - s * aqk;
+                    a[q * N + k] = s * apk + c * aqk;
+                }
+                for(int k = 0; k < N; ++k)
+                {
+                    double vkp = v[k * N + p], vkq = v[k * N + q];
+                    v[k * N + p] = c * vkp - s * vkq;
+                    v[k * N + q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    for(int i = 0; i < N; ++i)
+        w[i] = a[i * N + i];
+}
+
+// d2Psi/dF2 (9x9, vec(F) column-major) of the stable Neo-Hookean energy,
+// projected to PSD; also dPsi/dF. F column-major.
+void snh_derivatives(const double F[9], double mu, double lambda, double P[9], double H[81])
+{
+    const Vec3 f0{F[0], F[1], F[2]}, f1{F[3], F[4], F[5]}, f2{F[6], F[7], F[8]};
+    const double J = dot(f0, cross(f1, f2));
+    Vec3 g0 = cross(f1, f2), g1 = cross(f2, f0), g2 = cross(f0, f1);
+    double g[9] = {g0[0], g0[1], g0[2], g1[0], g1[1], g1[2], g2[0], g2[1], g2[2]};
+    const double s = lambda * (J - 1.0) - mu;
+    for(int i = 0; i < 9; ++i)
+        P[i] = mu * F[i] + s * g[i];
+    // H = mu I + lambda g g^T + s * d2J/dF2
+    for(int i = 0; i < 9; ++i)
+        for(int j = 0; j < 9; ++j)
+            H[i * 9 + j] = (i == j ? mu : 0.0) + lambda * g[i] * g[j];
+    // d2J/df_a df_b blocks: (0,1) = -[f2]x, (0,2) = [f1]x, (1,2) = -[f0]x (and transposes)
+    auto put_cross = [&](int bi, int bj, const Vec3& a, double sign)
+    {
+        // [a]x = [[0,-a2,a1],[a2,0,-a0],[-a1,a0,0]]
+        const double m[9] = {0, -a[2], a[1], a[2], 0, -a[0], -a[1], a[0], 0};  // row-major
+        for(int r = 0; r < 3; ++r)
+            for(int c = 0; c < 3; ++c)
+            {
+                double v = sign * s * m[r * 3 + c];
+                H[(bi * 3 + r) * 9 + (bj * 3 + c)] += v;
+                H[(bj * 3 + c) * 9 + (bi * 3 + r)] += v;
+            }
+    };
+    put_cross(0, 1, f2, -1.0);
+    put_cross(0, 2, f1, +1.0);
+    put_cross(1, 2, f0, -1.0);
+    // PSD projection
+    double a[81], w[9], v[81];
+    std::memcpy(a, H, sizeof(a));
+    jacobi_eigen<9>(a, w, v);
+    bool neg = false;
+    for(int i = 0; i < 9; ++i)
+        neg |= (w[i] < 0.0);
+    if(!neg)
+        return;
+    for(int i = 0; i < 9; ++i)
+        for(int j = 0; j < 9; ++j)
+        {
+            double acc = 0.0;
+            for(int k = 0; k < 9; ++k)
+                if(w[k] > 0.0)
+                    acc += v[i * 9 + k] * w[k] * v[j * 9 + k];
+            H[i * 9 + j] = acc;
+        }
+}
+
+// barrier b(D) = -(D - Dh)^2 log(D / Dh), derivatives in D
+inline void barrier_d(double D, double Dh, double& b1, double& b2)
+{
+    const double t = D - Dh;
+    const double l = std::log(D / Dh);
+    b1 = -2.0 * t * l - t * t / D;
+    b2 = -2.0 * l - 4.0 * t / D + t * t / (D * D);
+}
+
+struct Triplet
+{
+    int32_t r, c;
+    double  v[9];
+};
+
+struct Builder
+{
+    std::vector<int32_t> rows, cols;
+    std::vector<double>  vals;
+    void reserve(size_t n)
+    {
+        rows.reserve(n);
+        cols.reserve(n);
+        vals.reserve(n * 9);
+    }
+};
+}  // namespace
+
+struct b2g_system
+{
+    std::vector<double>  x, x_rest;
+    std::vector<int32_t> tets;
+    std::vector<int32_t> rows, cols;
+    std::vector<double>  vals;
+    std::vector<double>  grad;
+    std::vector<int32_t> adj_start, adj_list;
+    int64_t              n_contacts = 0;
+};
+
+extern "C" {
+
+void b2g_default_config(b2g_config* c)
+{
+    std::memset(c, 0, sizeof(*c));
+    c->scene         = 1;
+    c->cells_x       = 10;
+    c->cells_y       = 10;
+    c->cells_z       = 10;
+    c->n_cubes       = 1;
+    c->h             = 0.01;
+    c->jitter        = 0.1;
+    c->normal_jitter = 0.45e-3;
+    c->gap           = 1e-3;
+    c->seed          = 0;
+    c->E             = 1e5;
+    c->nu            = 0.45;
+    c->rho           = 1e3;
+    c->dt            = 0.01;
+    c->gravity       = 9.8;
+    c->dhat          = 1e-3;
+    c->kappa         = 1e9;
+    c->ground_offset = 0.1e-3;
+    c->twist_deg     = 2.0;
+    c->n_threads     = 0;
+}
+
+const char* b2g_last_error(void) { return g_err.c_str(); }
+
+int b2g_generate(const b2g_config* cfg, b2g_system** out)
+{
+    try
+    {
+        if(!cfg || !out)
+            throw std::runtime_error("null argument");
+        const b2g_config C = *cfg;
+        if(C.cells_x < 1 || C.cells_y < 1 || C.cells_z < 1 || C.n_cubes < 1 || C.h <= 0 || C.dt <= 0)
+            throw std::runtime_error("invalid configuration sizes");
+        if(C.scene != 1 && C.scene != 2)
+            throw std::runtime_error("unknown scene id");
+#ifdef _OPENMP
+        if(C.n_threads > 0)
+            omp_set_num_threads(C.n_threads);
+#endif
+        auto sys = std::make_unique<b2g_system>();
+        const int nx = C.cells_x, ny = C.cells_y, nz = C.cells_z;
+        const int64_t vx = nx + 1, vy = ny + 1, vz = nz + 1;
+        const int64_t verts_per = vx * vy * vz;
+        const int64_t tets_per  = 6ll * nx * ny * nz;
+        const int n_cubes       = (C.scene == 1) ? C.n_cubes : 1;
+        const int64_t nv        = verts_per * n_cubes;
+        const int64_t nt        = tets_per * n_cubes;
+        if(nv > (int64_t)INT32_MAX / 3)
+            throw std::runtime_error("system too large for 32-bit DoF indices");
+
+        auto vid = [&](int c, int64_t i, int64_t j, int64_t k) -> int64_t
+        { return c * verts_per + i + vx * (j + vy * k); };
+
+        // ---- vertices (rest shape = jittered grid) ----
+        sys->x_rest.resize(nv * 3);
+        const double cube_pitch = ny * C.h + C.gap;
+#pragma omp parallel for schedule(static)
+        for(int64_t g = 0; g < nv; ++g)
+        {
+            int64_t c = g / verts_per, l = g % verts_per;
+            int64_t i = l % vx, j = (l / vx) % vy, k = l / (vx * vy);
+            double  px = i * C.h, py = j * C.h + c * cube_pitch, pz = k * C.h;
+            double  jx = urand(C.seed, 0, g) * C.jitter * C.h;
+            double  jy = urand(C.seed, 1, g) * C.jitter * C.h;
+            double  jz = urand(C.seed, 2, g) * C.jitter * C.h;
+            bool    x_face = (i == 0 || i == nx), z_face = (k == 0 || k == nz);
+            bool    y_face = (j == 0 || j == ny);
+            if(C.scene == 1)
+            {
+                // keep the outer faces planar in their normal direction; the
+                // contact faces (y) get a bounded normal jitter instead
+                if(x_face)
+                    jx = 0.0;
+                if(z_face)
+                    jz = 0.0;
+                if(y_face)
+                    jy = urand(C.seed, 3, g) * C.normal_jitter;
+            }
+            else
+            {
+                if(i == 0 || i == nx)
+                    jx = 0.0;
+            }
+            sys->x_rest[g * 3 + 0] = px + jx;
+            sys->x_rest[g * 3 + 1] = py + jy;
+            sys->x_rest[g * 3 + 2] = pz + jz;
+        }
+
+        // ---- tets: Kuhn 6-tet split of every cell ----
+        sys->tets.resize(nt * 4);
+        static const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+#pragma omp parallel for schedule(static)
+        for(int64_t cell = 0; cell < (int64_t)n_cubes * nx * ny * nz; ++cell)
+        {
+            int64_t c = cell / ((int64_t)nx * ny * nz), l = cell % ((int64_t)nx * ny * nz);
+            int64_t i = l % nx, j = (l / nx) % ny, k = l / ((int64_t)nx * ny);
+            for(int p = 0; p < 6; ++p)
+            {
+                int64_t d[3] = {0, 0, 0};
+                int32_t t[4];
+                t[0] = (int32_t)vid((int)c, i, j, k);
+                for(int s = 0; s < 3; ++s)
+                {
+                    d[perms[p][s]] += 1;
+                    t[s + 1] = (int32_t)vid((int)c, i + d[0], j + d[1], k + d[2]);
+                }
+                // positive orientation in the rest shape
+                Vec3 a{sys->x_rest[t[0] * 3], sys->x_rest[t[0] * 3 + 1], sys->x_rest[t[0] * 3 + 2]};
+                Vec3 b{sys->x_rest[t[1] * 3], sys->x_rest[t[1] * 3 + 1], sys->x_rest[t[1] * 3 + 2]};
+                Vec3 cc{sys->x_rest[t[2] * 3], sys->x_rest[t[2] * 3 + 1], sys->x_rest[t[2] * 3 + 2]};
+                Vec3 dd{sys->x_rest[t[3] * 3], sys->x_rest[t[3] * 3 + 1], sys->x_rest[t[3] * 3 + 2]};
+                if(dot(sub(b, a), cross(sub(cc, a), sub(dd, a))) < 0)
+                    std::swap(t[2], t[3]);
+                int64_t base = (cell * 6 + p) * 4;
+                for(int q = 0; q < 4; ++q)
+                    sys->tets[base + q] = t[q];
+            }
+        }
+
+        // ---- current positions ----
+        sys->x = sys->x_rest;
+        std::vector<uint8_t> fixed(nv, 0);
+        if(C.scene == 2)
+        {
+            // bar along x, ends rotated by +-twist about the x axis through the
+            // cross-section centre; the twist is linear along the bar and both
+            // end layers are fixed (Dirichlet)
+            const double L = nx * C.h, cy = 0.5 * ny * C.h, cz = 0.5 * nz * C.h;
+            const double tw = C.twist_deg * M_PI / 180.0;
+#pragma omp parallel for schedule(static)
+            for(int64_t g = 0; g < nv; ++g)
+            {
+                double px = sys->x_rest[g * 3], py = sys->x_rest[g * 3 + 1] - cy,
+                       pz = sys->x_rest[g * 3 + 2] - cz;
+                double th = tw * (2.0 * px / L - 1.0);
+                double cs = std::cos(th), sn = std::sin(th);
+                sys->x[g * 3 + 1] = cy + cs * py - sn * pz;
+                sys->x[g * 3 + 2] = cz + sn * py + cs * pz;
+                int64_t i = (g % verts_per) % vx;
+                fixed[g] = (i == 0 || i == nx) ? 1 : 0;
+            }
+        }
+
+        const double mu = C.E / (2.0 * (1.0 + C.nu));
+        const double lambda = C.E * C.nu / ((1.0 + C.nu) * (1.0 - 2.0 * C.nu));
+        const double dt2 = C.dt * C.dt;
+
+        // ---- per-tet rest data: volume, shape gradients ----
+        std::vector<double> tet_vol(nt);
+        std::vector<double> tet_grad(nt * 12);  // g_k[b], k = 0..3
+#pragma omp parallel for schedule(static)
+        for(int64_t t = 0; t < nt; ++t)
+        {
+            const int32_t* T = &sys->tets[t * 4];
+            Vec3 X[4];
+            for(int q = 0; q < 4; ++q)
+                X[q] = {sys->x_rest[T[q] * 3], sys->x_rest[T[q] * 3 + 1], sys->x_rest[T[q] * 3 + 2]};
+            Vec3 e1 = sub(X[1], X[0]), e2 = sub(X[2], X[0]), e3 = sub(X[3], X[0]);
+            // Dm column-major: columns e1 e2 e3 ; B = Dm^{-1}
+            double det = dot(e1, cross(e2, e3));
+            tet_vol[t] = det / 6.0;
+            Vec3 r0 = scale(cross(e2, e3), 1.0 / det);  // row 0 of Dm^{-1}
+            Vec3 r1 = scale(cross(e3, e1), 1.0 / det);
+            Vec3 r2 = scale(cross(e1, e2), 1.0 / det);
+            double* G = &tet_grad[t * 12];
+            for(int b = 0; b < 3; ++b)
+            {
+                G[3 + b] = r0[b];
+                G[6 + b] = r1[b];
+                G[9 + b] = r2[b];
+                G[b]     = -(r0[b] + r1[b] + r2[b]);
+            }
+        }
+
+        // ---- lumped masses ----
+        std::vector<double> mass(nv, 0.0);
+        for(int64_t t = 0; t < nt; ++t)
+            for(int q = 0; q < 4; ++q)
+                mass[sys->tets[t * 4 + q]] += C.rho * tet_vol[t] * 0.25;
+
+        // ---- contacts ----
+        struct Pair
+        {
+            int32_t v[4];
+            double  a[12];  // D = (a . x)^2
+            int     nverts;
+        };
+        std::vector<Pair> pairs;
+        std::vector<std::pair<int32_t, double>> ground;  // vertex, distance
+        double ground_y = 0.0;
+        if(C.scene == 1)
+        {
+            double miny = 1e300;
+            for(int64_t k = 0; k < vz; ++k)
+                for(int64_t i = 0; i < vx; ++i)
+                    miny = std::min(miny, sys->x[vid(0, i, 0, k) * 3 + 1]);
+            ground_y = miny - C.ground_offset;
+            for(int64_t k = 0; k < vz; ++k)
+                for(int64_t i = 0; i < vx; ++i)
+                {
+                    int64_t g = vid(0, i, 0, k);
+                    double  d = sys->x[g * 3 + 1] - ground_y;
+                    if(d < C.dhat)
+                        ground.push_back({(int32_t)g, d});
+                }
+            // stacked cube interfaces: top layer of cube c vs bottom layer of c+1.
+            // Each layer is an aligned (nx+1) x (nz+1) grid; cell (i,k) of a
+            // layer holds the two Kuhn face triangles split along (i,k)-(i+1,k+1).
+            for(int c = 0; c + 1 < n_cubes; ++c)
+            {
+                auto P = [&](int cube, int64_t i, int64_t j, int64_t k) -> Vec3
+                {
+                    int64_t g = vid(cube, i, j, k);
+                    return {sys->x[g * 3], sys->x[g * 3 + 1], sys->x[g * 3 + 2]};
+                };
+                // triangles of a layer cell
+                auto cell_tris = [&](int cube, int64_t j, int64_t i, int64_t k, int32_t tri[2][3])
+                {
+                    int32_t v00 = (int32_t)vid(cube, i, j, k), v10 = (int32_t)vid(cube, i + 1, j, k);
+                    int32_t v01 = (int32_t)vid(cube, i, j, k + 1), v11 = (int32_t)vid(cube, i + 1, j, k + 1);
+                    tri[0][0] = v00; tri[0][1] = v10; tri[0][2] = v11;
+                    tri[1][0] = v00; tri[1][1] = v11; tri[1][2] = v01;
+                };
+                auto vpos = [&](int32_t g) -> Vec3 { return {sys->x[g * 3], sys->x[g * 3 + 1], sys->x[g * 3 + 2]}; };
+                // point-triangle: vertices of one layer against triangles of the other
+                for(int side = 0; side < 2; ++side)
+                {
+                    int     pc = side == 0 ? c + 1 : c, tc = side == 0 ? c : c + 1;
+                    int64_t pj = side == 0 ? 0 : ny, tj = side == 0 ? ny : 0;
+                    for(int64_t k = 0; k < vz; ++k)
+                        for(int64_t i = 0; i < vx; ++i)
+                        {
+                            Vec3    p  = P(pc, i, pj, k);
+                            int32_t pv = (int32_t)vid(pc, i, pj, k);
+                            bool    done = false;
+                            for(int64_t ci = i - 1; ci <= i && !done; ++ci)
+                                for(int64_t ck = k - 1; ck <= k && !done; ++ck)
+                                {
+                                    if(ci < 0 || ck < 0 || ci >= nx || ck >= nz)
+                                        continue;
+                                    int32_t tri[2][3];
+                                    cell_tris(tc, tj, ci, ck, tri);
+                                    for(int tt = 0; tt < 2 && !done; ++tt)
+                                    {
+                                        Vec3 t0 = vpos(tri[tt][0]), t1 = vpos(tri[tt][1]), t2 = vpos(tri[tt][2]);
+                                        Vec3 n = cross(sub(t1, t0), sub(t2, t0));
+                                        double nn = norm(n);
+                                        n = scale(n, 1.0 / nn);
+                                        Vec3 q = sub(p, t0);
+                                        double d = dot(q, n);
+                                        Vec3 proj = sub(p, scale(n, d));
+                                        // barycentric of proj
+                                        Vec3 v0 = sub(t1, t0), v1 = sub(t2, t0), v2 = sub(proj, t0);
+                                        double d00 = dot(v0, v0), d01 = dot(v0, v1), d11 = dot(v1, v1);
+                                        double d20 = dot(v2, v0), d21 = dot(v2, v1);
+                                        double den = d00 * d11 - d01 * d01;
+                                        double wb = (d11 * d20 - d01 * d21) / den;
+                                        double wc = (d00 * d21 - d01 * d20) / den;
+                                        double wa = 1.0 - wb - wc;
+                                        if(wa < 0 || wb < 0 || wc < 0)
+                                            continue;
+                                        done = true;
+                                        if(std::fabs(d) >= C.dhat)
+                                            continue;
+                                        Pair pr;
+                                        pr.nverts = 4;
+                                        pr.v[0] = pv; pr.v[1] = tri[tt][0]; pr.v[2] = tri[tt][1]; pr.v[3] = tri[tt][2];
+                                        const double w[4] = {1.0, -wa, -wb, -wc};
+                                        for(int q2 = 0; q2 < 4; ++q2)
+                                            for(int a2 = 0; a2 < 3; ++a2)
+                                                pr.a[q2 * 3 + a2] = w[q2] * n[a2];
+                                        pairs.push_back(pr);
+                                    }
+                                }
+                        }
+                }
+                // edge-edge: axis-aligned layer edges of the upper layer against
+                // face diagonals of the lower layer and vice versa
+                auto layer_edges = [&](int cube, int64_t j, std::vector<std::array<int32_t, 2>>& E)
+                {
+                    for(int64_t k = 0; k < vz; ++k)
+                        for(int64_t i = 0; i < vx; ++i)
+                        {
+                            if(i < nx)
+                                E.push_back({(int32_t)vid(cube, i, j, k), (int32_t)vid(cube, i + 1, j, k)});
+                            if(k < nz)
+                                E.push_back({(int32_t)vid(cube, i, j, k), (int32_t)vid(cube, i, j, k + 1)});
+                            if(i < nx && k < nz)
+                                E.push_back({(int32_t)vid(cube, i, j, k), (int32_t)vid(cube, i + 1, j, k + 1)});
+                        }
+                };
+                std::vector<std::array<int32_t, 2>> Eu, El;
+                layer_edges(c + 1, 0, Eu);
+                layer_edges(c, ny, El);
+                // bucket the lower edges by their first vertex's (i,k)
+                auto ik_of = [&](int32_t g) -> std::pair<int64_t, int64_t>
+                {
+                    int64_t l = g % verts_per;
+                    return {l % vx, l / (vx * vy)};
+                };
+                std::vector<std::vector<int32_t>> bucket(vx * vz);
+                for(size_t e = 0; e < El.size(); ++e)
+                {
+                    auto [i, k] = ik_of(El[e][0]);
+                    bucket[i + vx * k].push_back((int32_t)e);
+                }
+                for(size_t e = 0; e < Eu.size(); ++e)
+                {
+                    auto [i0, k0] = ik_of(Eu[e][0]);
+                    for(int64_t ci = i0 - 1; ci <= i0 + 1; ++ci)
+                        for(int64_t ck = k0 - 1; ck <= k0 + 1; ++ck)
+                        {
+                            if(ci < 0 || ck < 0 || ci >= vx || ck >= vz)
+                                continue;
+                            for(int32_t f : bucket[ci + vx * ck])
+                            {
+                                Vec3 a0 = vpos(Eu[e][0]), a1 = vpos(Eu[e][1]);
+                                Vec3 b0 = vpos(El[f][0]), b1 = vpos(El[f][1]);
+                                Vec3 u = sub(a1, a0), v = sub(b1, b0), w0 = sub(a0, b0);
+                                double A = dot(u, u), B = dot(u, v), Cc = dot(v, v), D = dot(u, w0), Ee = dot(v, w0);
+                                double den = A * Cc - B * B;
+                                if(den < 1e-12 * A * Cc)
+                                    continue;  // (nearly) parallel: covered by point-triangle pairs
+                                double s = (B * Ee - Cc * D) / den, t = (A * Ee - B * D) / den;
+                                if(s <= 0.0 || s >= 1.0 || t <= 0.0 || t >= 1.0)
+                                    continue;
+                                Vec3 pa = add(a0, scale(u, s)), pb = add(b0, scale(v, t));
+                                Vec3 dv = sub(pa, pb);
+                                double d = norm(dv);
+                                if(d >= C.dhat || d <= 0.0)
+                                    continue;
+                                Vec3 n = scale(dv, 1.0 / d);
+                                Pair pr;
+                                pr.nverts = 4;
+                                pr.v[0] = Eu[e][0]; pr.v[1] = Eu[e][1]; pr.v[2] = El[f][0]; pr.v[3] = El[f][1];
+                                const double w[4] = {1.0 - s, s, -(1.0 - t), -t};
+                                for(int q2 = 0; q2 < 4; ++q2)
+                                    for(int a2 = 0; a2 < 3; ++a2)
+                                        pr.a[q2 * 3 + a2] = w[q2] * n[a2];
+                                pairs.push_back(pr);
+                            }
+                        }
+                }
+            }
+        }
+        sys->n_contacts = (int64_t)pairs.size() + (int64_t)ground.size();
+
+        // ---- triplet layout: kinetic | SNH | ground | pairs ----
+        const int64_t n_kin = nv, n_snh = nt * 10, n_gnd = (int64_t)ground.size(),
+                      n_pair = (int64_t)pairs.size() * 10;
+        const int64_t n_trip = n_kin + n_snh + n_gnd + n_pair;
+        sys->rows.assign(n_trip, 0);
+        sys->cols.assign(n_trip, 0);
+        sys->vals.assign(n_trip * 9, 0.0);
+        sys->grad.assign(nv * 3, 0.0);
+
+        auto write_block = [&](int64_t slot, int32_t ra, int32_t rb, const double* Hab /*row-major 3x3 of block (a,b)*/)
+        {
+            bool tp = ra > rb;
+            sys->rows[slot] = tp ? rb : ra;
+            sys->cols[slot] = tp ? ra : rb;
+            double* V = &sys->vals[slot * 9];
+            for(int p = 0; p < 3; ++p)
+                for(int q = 0; q < 3; ++q)
+                {
+                    double v = tp ? Hab[q * 3 + p] : Hab[p * 3 + q];  // value at (p,q) of the written block
+                    V[q * 3 + p] = v;                                  // column-major
+                }
+        };
+
+        // kinetic: x_tilde = x_prev + dt v + dt^2 g with x_prev = rest, v = 0
+#pragma omp parallel for schedule(static)
+        for(int64_t g = 0; g < nv; ++g)
+        {
+            double H[9] = {mass[g], 0, 0, 0, mass[g], 0, 0, 0, mass[g]};
+            write_block(g, (int32_t)g, (int32_t)g, H);
+            double xt[3] = {sys->x_rest[g * 3], sys->x_rest[g * 3 + 1] - dt2 * C.gravity, sys->x_rest[g * 3 + 2]};
+            for(int a = 0; a < 3; ++a)
+                sys->grad[g * 3 + a] += mass[g] * (sys->x[g * 3 + a] - xt[a]);
+        }
+
+        // SNH: the F = I Hessian is shared by every undeformed tet
+        double P_I[9], H_I[81];
+        {
+            const double Fi[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+            snh_derivatives(Fi, mu, lambda, P_I, H_I);
+        }
+        std::vector<double> tet_grad_out(nt * 12);
+#pragma omp parallel for schedule(static)
+        for(int64_t t = 0; t < nt; ++t)
+        {
+            const int32_t* T  = &sys->tets[t * 4];
+            const double*  Gs = &tet_grad[t * 12];
+            double F[9] = {0};
+            for(int q = 0; q < 4; ++q)
+                for(int a = 0; a < 3; ++a)
+                    for(int b = 0; b < 3; ++b)
+                        F[a + 3 * b] += sys->x[T[q] * 3 + a] * Gs[q * 3 + b];
+            double P[9], H[81];
+            bool   ident = true;
+            for(int a = 0; a < 3; ++a)
+                for(int b = 0; b < 3; ++b)
+                    ident &= std::fabs(F[a + 3 * b] - (a == b ? 1.0 : 0.0)) < 1e-12;
+            if(ident)
+            {
+                std::memcpy(H, H_I, sizeof(H));
+                for(int i = 0; i < 9; ++i)
+                    P[i] = 0.0;  // zero stress at rest
+            }
+            else
+                snh_derivatives(F, mu, lambda, P, H);
+            const double s = tet_vol[t] * dt2;
+            // gradient: dE/dx_{q,a} = s * sum_b P[a+3b] g_q[b]
+            for(int q = 0; q < 4; ++q)
+                for(int a = 0; a < 3; ++a)
+                {
+                    double acc = 0.0;
+                    for(int b = 0; b < 3; ++b)
+                        acc += P[a + 3 * b] * Gs[q * 3 + b];
+                    tet_grad_out[t * 12 + q * 3 + a] = s * acc;
+                }
+            // Hessian blocks (q, r), q <= r in local order
+            int slot = 0;
+            for(int q = 0; q < 4; ++q)
+                for(int r = q; r < 4; ++r, ++slot)
+                {
+                    double Hb[9];
+                    for(int a = 0; a < 3; ++a)
+                        for(int c = 0; c < 3; ++c)
+                        {
+                            double acc = 0.0;
+                            for(int b = 0; b < 3; ++b)
+                            {
+                                double gq = Gs[q * 3 + b];
+                                for(int d = 0; d < 3; ++d)
+                                    acc += gq * H[(a + 3 * b) * 9 + (c + 3 * d)] * Gs[r * 3 + d];
+                            }
+                            Hb[a * 3 + c] = s * acc;
+                        }
+                    if(q == r)  // exact symmetry of diagonal blocks
+                        for(int a = 0; a < 3; ++a)
+                            for(int c = a + 1; c < 3; ++c)
+                            {
+                                double m = 0.5 * (Hb[a * 3 + c] + Hb[c * 3 + a]);
+                                Hb[a * 3 + c] = Hb[c * 3 + a] = m;
+                            }
+                    write_block(n_kin + t * 10 + slot, T[q], T[r], Hb);
+                }
+        }
+        for(int64_t t = 0; t < nt; ++t)
+            for(int q = 0; q < 4; ++q)
+                for(int a = 0; a < 3; ++a)
+                    sys->grad[sys->tets[t * 4 + q] * 3 + a] += tet_grad_out[t * 12 + q * 3 + a];
+
+        const double Dh = C.dhat * C.dhat;
+        // ground barrier (normal +y)
+        for(int64_t gi = 0; gi < n_gnd; ++gi)
+        {
+            int32_t g = ground[gi].first;
+            double  d = ground[gi].second, D = d * d, b1, b2;
+            barrier_d(D, Dh, b1, b2);
+            double k = dt2 * C.kappa * (b2 * 4.0 * D + 2.0 * b1);
+            if(k < 0.0)
+                k = 0.0;
+            double H[9] = {0, 0, 0, 0, k, 0, 0, 0, 0};
+            write_block(n_kin + n_snh + gi, g, g, H);
+            sys->grad[g * 3 + 1] += dt2 * C.kappa * b1 * 2.0 * d;
+        }
+        // pair barriers: D = (a.x)^2, H = dt2 kappa (b'' 4 (a.x)^2 + 2 b') a a^T
+#pragma omp parallel for schedule(static)
+        for(int64_t pi = 0; pi < (int64_t)pairs.size(); ++pi)
+        {
+            const Pair& pr = pairs[pi];
+            double ax = 0.0;
+            for(int q = 0; q < 4; ++q)
+                for(int a = 0; a < 3; ++a)
+                    ax += pr.a[q * 3 + a] * sys->x[pr.v[q] * 3 + a];
+            double D = ax * ax, b1, b2;
+            if(D <= 0.0)
+                D = 1e-30;
+            barrier_d(D, Dh, b1, b2);
+            double k = dt2 * C.kappa * (b2 * 4.0 * D + 2.0 * b1);
+            if(k < 0.0)
+                k = 0.0;
+            int slot = 0;
+            for(int q = 0; q < 4; ++q)
+                for(int r = q; r < 4; ++r, ++slot)
+                {
+                    double Hb[9];
+                    for(int a = 0; a < 3; ++a)
+                        for(int c = 0; c < 3; ++c)
+                            Hb[a * 3 + c] = k * pr.a[q * 3 + a] * pr.a[r * 3 + c];
+                    write_block(n_kin + n_snh + n_gnd + pi * 10 + slot, pr.v[q], pr.v[r], Hb);
+                }
+        }
+        for(int64_t pi = 0; pi < (int64_t)pairs.size(); ++pi)
+        {
+            const Pair& pr = pairs[pi];
+            double ax = 0.0;
+            for(int q = 0; q < 4; ++q)
+                for(int a = 0; a < 3; ++a)
+                    ax += pr.a[q * 3 + a] * sys->x[pr.v[q] * 3 + a];
+            double D = std::max(ax * ax, 1e-30), b1, b2;
+            barrier_d(D, Dh, b1, b2);
+            for(int q = 0; q < 4; ++q)
+                for(int a = 0; a < 3; ++a)
+                    sys->grad[pr.v[q] * 3 + a] += dt2 * C.kappa * b1 * 2.0 * ax * pr.a[q * 3 + a];
+        }
+
+        // fixed vertices (Dirichlet)
+        bool any_fixed = false;
+        for(auto f : fixed)
+            any_fixed |= (f != 0);
+        if(any_fixed)
+        {
+#pragma omp parallel for schedule(static)
+            for(int64_t s = 0; s < n_trip; ++s)
+            {
+                int32_t i = sys->rows[s], j = sys->cols[s];
+                if(fixed[i] || fixed[j])
+                {
+                    double* V = &sys->vals[s * 9];
+                    for(int e = 0; e < 9; ++e)
+                        V[e] = 0.0;
+                    if(i == j)
+                        V[0] = V[4] = V[8] = 1.0;
+                }
+            }
+            for(int64_t g = 0; g < nv; ++g)
+                if(fixed[g])
+                    sys->grad[g * 3] = sys->grad[g * 3 + 1] = sys->grad[g * 3 + 2] = 0.0;
+        }
+
+        // ---- MAS neighbour graph (tet edges, sorted unique) ----
+        {
+            std::vector<std::vector<int32_t>> nb(nv);
+            for(int64_t t = 0; t < nt; ++t)
+                for(int q = 0; q < 4; ++q)
+                    for(int r = q + 1; r < 4; ++r)
+                    {
+                        int32_t a = sys->tets[t * 4 + q], b = sys->tets[t * 4 + r];
+                        nb[a].push_back(b);
+                        nb[b].push_back(a);
+                    }
+            sys->adj_start.assign(nv + 1, 0);
+            for(int64_t v = 0; v < nv; ++v)
+            {
+                auto& L = nb[v];
+                std::sort(L.begin(), L.end());
+                L.erase(std::unique(L.begin(), L.end()), L.end());
+                sys->adj_start[v + 1] = sys->adj_start[v] + (int32_t)L.size();
+            }
+            sys->adj_list.resize(sys->adj_start[nv]);
+            for(int64_t v = 0; v < nv; ++v)
+                std::copy(nb[v].begin(), nb[v].end(), sys->adj_list.begin() + sys->adj_start[v]);
+        }
+
+        *out = sys.release();
+        return 0;
+    }
+    catch(const std::exception& e)
+    {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+void b2g_free(b2g_system* s) { delete s; }
+
+int64_t b2g_num_verts(const b2g_system* s) { return (int64_t)s->x.size() / 3; }
+int64_t b2g_num_tets(const b2g_system* s) { return (int64_t)s->tets.size() / 4; }
+int64_t b2g_num_triplets(const b2g_system* s) { return (int64_t)s->rows.size(); }
+int64_t b2g_num_contacts(const b2g_system* s) { return s->n_contacts; }
+const double* b2g_positions(const b2g_system* s) { return s->x.data(); }
+const double* b2g_rest_positions(const b2g_system* s) { return s->x_rest.data(); }
+const int32_t* b2g_tets(const b2g_system* s) { return s->tets.data(); }
+const int32_t* b2g_triplet_rows(const b2g_system* s) { return s->rows.data(); }
+const int32_t* b2g_triplet_cols(const b2g_system* s) { return s->cols.data(); }
+const double* b2g_triplet_vals(const b2g_system* s) { return s->vals.data(); }
+const double* b2g_gradient(const b2g_system* s) { return s->grad.data(); }
+int64_t b2g_num_adjacency(const b2g_system* s) { return (int64_t)s->adj_list.size(); }
+const int32_t* b2g_adjacency_start(const b2g_system* s) { return s->adj_start.data(); }
+const int32_t* b2g_adjacency_list(const b2g_system* s) { return s->adj_list.data(); }
+
+}  // extern "C"

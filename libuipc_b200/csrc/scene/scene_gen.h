@@ -1,0 +1,83 @@
+// Synthetic Newton-system generator for the linear-solve workloads.
+//
+// Produces the raw input of one Newton-step linear solve exactly in the
+// conventions libuipc's CUDA backend hands to GlobalLinearSystem:
+//   * raw 3x3 Hessian triplets (row, col, value) with row <= col in the global
+//     block numbering (producers write only the block-upper half, transposing a
+//     block when its local order is reversed; see
+//     src/backends/cuda/finite_element/constitutions/stable_neo_hookean_3d.cu:252-263
+//     in libuipc),
+//   * values as Eigen::Matrix3d would store them (9 doubles, column-major),
+//   * duplicates NOT summed (one block per element stencil entry),
+//   * the gradient b of E = 1/2|x - x_tilde|_M^2 + dt^2 * (Psi + barrier),
+//     so that the solve is A x = b and the Newton direction is dx = -x
+//     (src/backends/cuda/finite_element/fem_linear_subsystem.cu:119-126).
+//
+// This is input synthesis for tests and benchmarks; it is host C++ only.
+#pragma once
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct b2g_config
+{
+    int    scene;          // 1 = cubes stacked along +y on a ground plane, 2 = twisted bar
+    int    cells_x;        // cells per cube edge (x)
+    int    cells_y;        // (y)
+    int    cells_z;        // (z)
+    int    n_cubes;        // cubes stacked along +y (scene 1)
+    double h;              // cell edge length [m]
+    double jitter;         // vertex jitter amplitude as a fraction of h (uniform +-)
+    double normal_jitter;  // contact-face normal jitter amplitude [m] (scene 1, n_cubes > 1)
+    double gap;            // nominal gap between stacked cubes [m]
+    uint64_t seed;
+    double E;              // Young's modulus [Pa]
+    double nu;             // Poisson ratio
+    double rho;            // density [kg/m^3]
+    double dt;             // time step [s]
+    double gravity;        // gravity along -y [m/s^2]
+    double dhat;           // barrier activation distance [m]
+    double kappa;          // barrier stiffness [Pa]
+    double ground_offset;  // ground plane sits this far below the lowest vertex [m]
+    double twist_deg;      // scene 2: end rotation (+-) about the bar axis [deg]
+    int    n_threads;      // OpenMP threads (0 = default)
+} b2g_config;
+
+typedef struct b2g_system b2g_system;
+
+// Fill `cfg` with the defaults of the 10x10x10 cube-on-ground case.
+void b2g_default_config(b2g_config* cfg);
+
+// Generate one Newton system. Returns 0 on success, non-zero on error
+// (message through b2g_last_error()).
+int b2g_generate(const b2g_config* cfg, b2g_system** out);
+void b2g_free(b2g_system* sys);
+const char* b2g_last_error(void);
+
+// Sizes
+int64_t b2g_num_verts(const b2g_system* s);
+int64_t b2g_num_tets(const b2g_system* s);
+int64_t b2g_num_triplets(const b2g_system* s);
+int64_t b2g_num_contacts(const b2g_system* s);  // PT + EE + ground pairs
+
+// Data (owned by the system; valid until b2g_free)
+const double* b2g_positions(const b2g_system* s);    // [n_verts*3]
+const double* b2g_rest_positions(const b2g_system* s);  // [n_verts*3]
+const int32_t* b2g_tets(const b2g_system* s);         // [n_tets*4]
+const int32_t* b2g_triplet_rows(const b2g_system* s); // [n_triplets]
+const int32_t* b2g_triplet_cols(const b2g_system* s); // [n_triplets]
+const double*  b2g_triplet_vals(const b2g_system* s); // [n_triplets*9] column-major 3x3
+const double*  b2g_gradient(const b2g_system* s);     // [n_verts*3]
+
+// Vertex adjacency from tetrahedra (sorted, unique, CSR) -- the MAS
+// neighbour graph built by FEMMASPreconditioner::do_init
+// (src/backends/cuda/finite_element/fem_mas_preconditioner.cu:157-200).
+int64_t        b2g_num_adjacency(const b2g_system* s);
+const int32_t* b2g_adjacency_start(const b2g_system* s);  // [n_verts+1]
+const int32_t* b2g_adjacency_list(const b2g_system* s);   // [num_adjacency]
+
+#ifdef __cplusplus
+}
+#endif

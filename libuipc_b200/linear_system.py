@@ -1,0 +1,289 @@
+"""Host-side mirror of libuipc's linear-system plug-in interface over the C ABI.
+
+libuipc's CUDA backend solves one Newton step through three sim-system
+interfaces (src/backends/cuda/linear_system/):
+  * GlobalLinearSystem (global_linear_system.h:28-438): owns the triplets,
+    the assembled block matrix, x and b; build_linear_system / solve /
+    distribute_solution;
+  * IterativeSolver (iterative_solver.h:8-62): do_build, do_solve(SolvingInfo)
+    with helpers spmv / spmv_dot / apply_preconditioner;
+  * GlobalPreconditioner (global_preconditioner.h:8-26): do_assemble(A),
+    do_apply(r -> z).
+This module keeps those names and their argument meaning; every call goes to
+libb200solve.so (include/b200solve.h). Device memory is held in torch CUDA
+tensors; PyTorch is only the allocator here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._native import load_solve_lib
+
+
+class B200SolveError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _ptr(t) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Solver:
+    """RAII wrapper of a b2s_solver handle (one CUDA device)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_solve_lib()
+        h = C.c_void_p()
+        rc = self.lib.b2s_create(int(device), C.byref(h))
+        if rc != _abi.B2S_OK:
+            raise B200SolveError(rc, self.lib.b2s_last_error(None).decode())
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.b2s_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != _abi.B2S_OK:
+            raise B200SolveError(rc, self.lib.b2s_last_error(self.h).decode())
+
+    # ---- assembly ----------------------------------------------------------
+    def assemble(self, n_block_rows: int, rows, cols, vals) -> None:
+        """rows/cols: int32 [T], vals: float64 [T, 9] (column-major blocks),
+        device tensors."""
+        T = int(rows.numel())
+        self._check(self.lib.b2s_assemble(self.h, int(n_block_rows), T, _ptr(rows), _ptr(cols), _ptr(vals)))
+
+    def matrix_info(self):
+        nb = C.c_int32()
+        nnz = C.c_int64()
+        self._check(self.lib.b2s_matrix_info(self.h, C.byref(nb), C.byref(nnz)))
+        return nb.value, nnz.value
+
+    def upper_bsr(self):
+        nb, nnz = self.matrix_info()
+        rowptr = np.zeros(nb + 1, np.int32)
+        col = np.zeros(max(nnz, 1), np.int32)
+        vals = np.zeros((max(nnz, 1), 9), np.float64)
+        self._check(self.lib.b2s_get_upper_bsr(self.h, rowptr.ctypes.data, col.ctypes.data, vals.ctypes.data))
+        return rowptr, col[:nnz], vals[:nnz]
+
+    # ---- SpMV ----------------------------------------------------------------
+    def spmv(self, x, y, with_dot: bool = False):
+        d = C.c_double(0.0)
+        self._check(self.lib.b2s_spmv(self.h, _ptr(x), _ptr(y), C.byref(d) if with_dot else None))
+        return d.value if with_dot else None
+
+    # ---- MAS ---------------------------------------------------------------------
+    def mas_init(self, block_offset: int, vert_num: int, adj_start, adj_list, part_to_real, real_to_part):
+        a = [np.ascontiguousarray(v, dtype=np.int32) for v in (adj_start, adj_list, part_to_real, real_to_part)]
+        self._check(
+            self.lib.b2s_mas_init(self.h, int(block_offset), int(vert_num), a[0].ctypes.data,
+                                  a[1].ctypes.data if a[1].size else None, int(a[2].size), a[2].ctypes.data,
+                                  a[3].ctypes.data)
+        )
+
+    def mas_info(self):
+        L = C.c_int32()
+        tot = C.c_int32()
+        self._check(self.lib.b2s_mas_info(self.h, C.byref(L), C.byref(tot)))
+        return L.value, tot.value
+
+    def mas_hierarchy(self, vert_num: int):
+        L, _ = self.mas_info()
+        b = np.zeros(L + 1, np.int32)
+        c = np.zeros(L + 1, np.int32)
+        ct = np.zeros(max(vert_num * (L - 1), 1), np.int32)
+        self._check(self.lib.b2s_mas_get_hierarchy(self.h, b.ctypes.data, c.ctypes.data, ct.ctypes.data))
+        return b, c, ct[: vert_num * (L - 1)].reshape(vert_num, L - 1)
+
+    def mas_clusters(self):
+        L, tot = self.mas_info()
+        ncl = tot // 16
+        hess = np.zeros((ncl, 136, 9), np.float64)
+        inv = np.zeros((ncl, 136, 9), np.float32)
+        self._check(self.lib.b2s_mas_get_clusters(self.h, hess.ctypes.data, inv.ctypes.data))
+        return hess, inv
+
+    # ---- preconditioner ----------------------------------------------------------
+    def precond_assemble(self, kind: int, invert_mode: int = _abi.B2S_INVERT_SWEEP_F32):
+        self._check(self.lib.b2s_precond_assemble(self.h, int(kind), int(invert_mode)))
+
+    def precond_apply(self, r, z):
+        self._check(self.lib.b2s_precond_apply(self.h, _ptr(r), _ptr(z)))
+
+    # ---- PCG -------------------------------------------------------------------------
+    def pcg(self, b, x, tol=1e-3, stop_rule=_abi.B2S_STOP_RZ, check_interval=5, max_iter=0,
+            precision=_abi.B2S_PRECISION_FP64, use_graph=True, x0_given=False, replace_every=0) -> dict:
+        o = _abi.PcgOptions()
+        self.lib.b2s_pcg_default_options(C.byref(o))
+        o.tol = float(tol)
+        o.stop_rule = int(stop_rule)
+        o.check_interval = int(check_interval)
+        o.max_iter = int(max_iter)
+        o.precision = int(precision)
+        o.use_graph = 1 if use_graph else 0
+        o.x0_given = 1 if x0_given else 0
+        o.replace_every = int(replace_every)
+        st = _abi.PcgStats()
+        rc = self.lib.b2s_pcg(self.h, _ptr(b), _ptr(x), C.byref(o), C.byref(st))
+        self._check(rc)
+        return st.as_dict()
+
+
+    # ---- stage timers --------------------------------------------------------------
+    def set_timing(self, enable: bool = True):
+        self._check(self.lib.b2s_set_timing(self.h, 1 if enable else 0))
+
+    def timers(self) -> dict:
+        t = _abi.Timers()
+        self._check(self.lib.b2s_get_timers(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def reset_timers(self):
+        self._check(self.lib.b2s_reset_timers(self.h))
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self.lib.b2s_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None))
+
+
+def partition_rcb(positions: np.ndarray, max_part: int = 16) -> np.ndarray:
+    lib = load_solve_lib()
+    pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros(pos.shape[0], np.int32)
+    rc = lib.b2s_partition_rcb(int(pos.shape[0]), pos.ctypes.data, int(max_part), out.ctypes.data)
+    if rc != 0:
+        raise B200SolveError(rc, "b2s_partition_rcb failed")
+    return out
+
+
+def partition_maps(part_ids: np.ndarray, max_part: int = 16):
+    lib = load_solve_lib()
+    pid = np.ascontiguousarray(part_ids, dtype=np.int32)
+    n = int(pid.size)
+    size = C.c_int32()
+    r2p = np.zeros(max(n, 1), np.int32)
+    rc = lib.b2s_partition_maps(n, pid.ctypes.data, int(max_part), None, r2p.ctypes.data, C.byref(size))
+    if rc != 0:
+        raise B200SolveError(rc, "b2s_partition_maps failed (part larger than max_part?)")
+    p2r = np.zeros(max(size.value, 1), np.int32)
+    rc = lib.b2s_partition_maps(n, pid.ctypes.data, int(max_part), p2r.ctypes.data, r2p.ctypes.data, C.byref(size))
+    if rc != 0:
+        raise B200SolveError(rc, "b2s_partition_maps failed")
+    return p2r[: size.value], r2p[:n]
+
+
+# ---------------------------------------------------------------------------
+# libuipc-shaped plug-in classes
+# ---------------------------------------------------------------------------
+@dataclass
+class SolvingInfo:
+    """GlobalLinearSystem::SolvingInfo (global_linear_system.h:228-246)."""
+
+    x: object  # DenseVectorView<Float> (device tensor)
+    b: object  # CDenseVectorView<Float>
+    iter_count: int = 0
+
+
+class GlobalPreconditioner:
+    """GlobalPreconditioner (global_preconditioner.h:8-26)."""
+
+    def do_assemble(self, system: "GlobalLinearSystem") -> None:
+        raise NotImplementedError
+
+    def do_apply(self, system: "GlobalLinearSystem", r, z) -> None:
+        raise NotImplementedError
+
+
+class IterativeSolver:
+    """IterativeSolver (iterative_solver.h:8-62)."""
+
+    def do_solve(self, system: "GlobalLinearSystem", info: SolvingInfo) -> None:
+        raise NotImplementedError
+
+
+class B200MAS(GlobalPreconditioner):
+    """MAS over the FEM vertex range, 3x3 block Jacobi elsewhere (the role of
+    FEMMASPreconditioner + FEMDiagPreconditioner on this path)."""
+
+    def __init__(self, block_offset, vert_num, adj_start, adj_list, part_to_real, real_to_part,
+                 invert_mode=_abi.B2S_INVERT_SWEEP_F32):
+        self.args = (block_offset, vert_num, adj_start, adj_list, part_to_real, real_to_part)
+        self.invert_mode = invert_mode
+        self._initialised_for = None
+
+    def do_assemble(self, system):
+        if self._initialised_for is not system.solver:
+            system.solver.mas_init(*self.args)
+            self._initialised_for = system.solver
+        system.solver.precond_assemble(_abi.B2S_PRECOND_MAS, self.invert_mode)
+
+    def do_apply(self, system, r, z):
+        system.solver.precond_apply(r, z)
+
+
+class B200Jacobi(GlobalPreconditioner):
+    def do_assemble(self, system):
+        system.solver.precond_assemble(_abi.B2S_PRECOND_JACOBI)
+
+    def do_apply(self, system, r, z):
+        system.solver.precond_apply(r, z)
+
+
+class B200PCG(IterativeSolver):
+    """LinearFusedPCG's role (linear_fused_pcg.cu:851-943) on the B200 path."""
+
+    def __init__(self, tol_rate=1e-3, stop_rule=_abi.B2S_STOP_RZ, check_interval=5,
+                 precision=_abi.B2S_PRECISION_FP64, use_graph=True):
+        self.kw = dict(tol=tol_rate, stop_rule=stop_rule, check_interval=check_interval, precision=precision,
+                       use_graph=use_graph)
+        self.last_stats: dict | None = None
+
+    def do_solve(self, system, info: SolvingInfo):
+        self.last_stats = system.solver.pcg(info.b, info.x, **self.kw)
+        info.iter_count = int(self.last_stats["iterations"])
+
+
+class GlobalLinearSystem:
+    """GlobalLinearSystem::solve (global_linear_system.cu:85-106): assemble the
+    triplets, build the preconditioner, solve A x = b, dx = -x."""
+
+    def __init__(self, solver: Solver, iterative_solver: IterativeSolver,
+                 preconditioner: GlobalPreconditioner | None = None):
+        self.solver = solver
+        self.iterative_solver = iterative_solver
+        self.preconditioner = preconditioner or B200Jacobi()
+        self.last_solve_iterations = 0
+
+    def build_linear_system(self, n_block_rows, rows, cols, vals):
+        self.solver.assemble(n_block_rows, rows, cols, vals)
+        self.preconditioner.do_assemble(self)
+
+    def solve(self, n_block_rows, rows, cols, vals, b):
+        torch = _torch()
+        self.build_linear_system(n_block_rows, rows, cols, vals)
+        x = torch.zeros_like(b)
+        info = SolvingInfo(x=x, b=b)
+        self.iterative_solver.do_solve(self, info)
+        self.last_solve_iterations = info.iter_count
+        return -x  # distribute_solution: dx = -x

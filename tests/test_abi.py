@@ -1,0 +1,90 @@
+"""CPU tests of the C-ABI library: it loads, exports every declared entry
+point, and its host-only utilities (partitioning) behave."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "b200solve.h")
+LIB = os.path.join(ROOT, "libuipc_b200", "_lib", "libb200solve.so")
+
+
+def test_library_exports_every_header_symbol():
+    from libuipc_b200 import _abi
+    from libuipc_b200._native import load_solve_lib
+
+    lib = load_solve_lib()
+    declared = _abi.header_symbols(HEADER)
+    assert declared, "no declarations parsed"
+    for name in declared:
+        assert hasattr(lib, name), f"{name} declared in b200solve.h but not exported"
+    # the ctypes signature table covers the whole header
+    assert sorted(_abi.SIGNATURES) == declared
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l and l.split()[-1].startswith("b2s_")}
+    assert set(declared) <= exported
+
+
+def test_library_is_built_for_sm100a():
+    out = subprocess.run(["cuobjdump", "--list-elf", LIB], capture_output=True, text=True).stdout
+    assert "sm_100a" in out
+
+
+def test_create_without_device_fails_cleanly():
+    import torch
+
+    from libuipc_b200._native import load_solve_lib
+
+    if torch.cuda.is_available():
+        return
+    lib = load_solve_lib()
+    h = C.c_void_p()
+    rc = lib.b2s_create(0, C.byref(h))
+    assert rc != 0 and not h.value
+    assert len(lib.b2s_last_error(None)) > 0
+
+
+def test_null_handle_is_an_argument_error():
+    from libuipc_b200._native import load_solve_lib
+
+    lib = load_solve_lib()
+    assert lib.b2s_assemble(None, 1, 0, None, None, None) == -1
+    assert lib.b2s_pcg(None, None, None, None, None) == -1
+
+
+def test_rcb_partition_and_maps(cube10):
+    from libuipc_b200.linear_system import partition_maps, partition_rcb
+
+    pid = partition_rcb(cube10.positions, 16)
+    counts = np.bincount(pid)
+    assert counts.max() <= 16 and counts.min() >= 1
+    # every part but the last holds exactly 16 vertices
+    assert (counts[:-1] == 16).sum() >= len(counts) - 2
+    p2r, r2p = partition_maps(pid)
+    assert p2r.size % 16 == 0
+    valid = p2r >= 0
+    assert np.array_equal(np.sort(p2r[valid]), np.arange(cube10.n_verts))
+    assert np.all(r2p[p2r[valid]] == np.nonzero(valid)[0])
+
+
+def test_partition_maps_rejects_oversized_parts():
+    from libuipc_b200.linear_system import B200SolveError, partition_maps
+
+    pid = np.zeros(17, np.int32)
+    try:
+        partition_maps(pid)
+    except B200SolveError:
+        return
+    raise AssertionError("a 17-vertex part was accepted")
+
+
+def test_partition_maps_unpartitioned_vertices():
+    from libuipc_b200.linear_system import partition_maps
+
+    pid = np.array([0, -1, 0, 1, -1], np.int32)
+    p2r, r2p = partition_maps(pid)
+    assert p2r.size == 32
+    assert list(r2p) == [0, -1, 1, 16, -1]

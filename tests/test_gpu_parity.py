@@ -1,0 +1,277 @@
+"""GPU parity tests: the CUDA path (through the C ABI) against the oracle.
+
+Tolerances: assembly pattern and sums are bit-exact (integer pattern, FP64
+sums in source order on both sides); SpMV is FP64 with atomics on the
+transposed half, so 1e-13 relative; the MAS cluster matrices are FP64 sums in
+a different association, 1e-12 relative; the FP32 cluster inverses and the
+FP32 MAS apply are compared at 1e-4 relative (FP32 rounding of a 48x48
+elimination); PCG iterates match the oracle's iteration count within one
+check and the solution within 1e-6 relative at a matched tight tolerance.
+"""
+import numpy as np
+import pytest
+
+from conftest import to_dev
+from libuipc_b200 import _abi, scene
+from libuipc_b200.linear_system import partition_maps, partition_rcb
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _upload(s, dev):
+    import torch
+
+    rows = to_dev(s.rows, dev)
+    cols = to_dev(s.cols, dev)
+    vals = to_dev(s.vals, dev)
+    b = to_dev(s.b, dev)
+    return rows, cols, vals, b
+
+
+def _assemble(solver, s, dev):
+    rows, cols, vals, b = _upload(s, dev)
+    solver.assemble(s.n_verts, rows, cols, vals)
+    return b
+
+
+# ---------------------------------------------------------------------------
+# assembly
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("which", ["cube10", "cube5", "stack_small"])
+def test_assembly_bit_exact(request, solver, cuda, which):
+    s = request.getfixturevalue(which)
+    _assemble(solver, s, cuda)
+    A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals)
+    rp, col, val = solver.upper_bsr()
+    orp, orow, ocol, oval = A.bsr()
+    assert np.array_equal(rp, orp)
+    assert np.array_equal(col, ocol)
+    assert np.array_equal(val, oval)  # source-order FP64 sums on both sides
+
+
+def test_assembly_edge_cases(solver, cuda):
+    import torch
+
+    # lower-triangle and unwritten (-1) slots dropped, duplicates summed, an
+    # empty row, a row with many duplicates
+    rng = np.random.default_rng(7)
+    nb = 6
+    rows = [0, 1, 2, -1, 1, 0, 1, 5, 5, 3]
+    cols = [0, 0, 2, 2, 2, 0, 2, 5, 5, 5]
+    rows += [4] * 300
+    cols += list(rng.integers(4, 6, 300))
+    rows = np.array(rows, np.int32)
+    cols = np.array(cols, np.int32)
+    vals = rng.standard_normal((rows.size, 9))
+    solver.assemble(nb, to_dev(rows, cuda), to_dev(cols, cuda), to_dev(vals, cuda))
+    rp, col, val = solver.upper_bsr()
+    orp, _, ocol, oval = O.OracleMatrix(nb, rows, cols, vals).bsr()
+    assert np.array_equal(rp, orp) and np.array_equal(col, ocol) and np.array_equal(val, oval)
+    # empty input
+    e = torch.zeros(0, dtype=torch.int32, device=cuda)
+    solver.assemble(3, e, e, torch.zeros((0, 9), dtype=torch.float64, device=cuda))
+    rp, col, val = solver.upper_bsr()
+    assert list(rp) == [0, 0, 0, 0] and col.size == 0
+
+
+def test_assembly_rejects_out_of_range_column(solver, cuda):
+    from libuipc_b200.linear_system import B200SolveError
+
+    rows = np.array([0, 1], np.int32)
+    cols = np.array([0, 7], np.int32)
+    vals = np.ones((2, 9))
+    with pytest.raises(B200SolveError) as ei:
+        solver.assemble(3, to_dev(rows, cuda), to_dev(cols, cuda), to_dev(vals, cuda))
+    assert ei.value.code == _abi.B2S_ERR_ARGUMENT
+
+
+# ---------------------------------------------------------------------------
+# SpMV
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("which", ["cube10", "stack_small"])
+def test_spmv_parity(request, solver, cuda, which):
+    import torch
+
+    s = request.getfixturevalue(which)
+    _assemble(solver, s, cuda)
+    A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals)
+    x = np.random.default_rng(3).standard_normal(3 * s.n_verts)
+    xd = to_dev(x, cuda)
+    yd = torch.empty_like(xd)
+    dot = solver.spmv(xd, yd, with_dot=True)
+    y = yd.cpu().numpy()
+    ref = A.spmv(x)
+    assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
+    assert abs(dot - x @ ref) <= 1e-12 * abs(x @ ref)
+
+
+# ---------------------------------------------------------------------------
+# MAS
+# ---------------------------------------------------------------------------
+def _mas_setup(solver, s, cuda, part_ids, invert_mode=_abi.B2S_INVERT_SWEEP_F32):
+    p2r, r2p = partition_maps(part_ids)
+    b = _assemble(solver, s, cuda)
+    solver.mas_init(0, s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
+    solver.precond_assemble(_abi.B2S_PRECOND_MAS, invert_mode)
+    A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals)
+    M = O.OracleMAS(s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
+    M.assemble(A, 0, invert_mode)
+    return b, A, M
+
+
+@pytest.mark.parametrize("which", ["cube10", "stack_small"])
+def test_mas_hierarchy_bit_exact(request, solver, cuda, which):
+    s = request.getfixturevalue(which)
+    _, A, M = _mas_setup(solver, s, cuda, partition_rcb(s.positions))
+    L, total = solver.mas_info()
+    assert L == M.L and total == M.total
+    beg, cnt, ct = solver.mas_hierarchy(s.n_verts)
+    obeg, ocnt = M.levels()
+    assert np.array_equal(beg[: L + 1], obeg[: L + 1])
+    assert np.array_equal(cnt[:L], ocnt[:L])
+    assert np.array_equal(ct, M.coarse_table())
+
+
+def test_mas_hierarchy_with_reference_metis(solver, cuda, cube10):
+    if not O.metis_available():
+        pytest.skip("reference METIS not compiled")
+    pid = O.metis_mesh_partition(cube10.adj_start, cube10.adj_list)
+    _, A, M = _mas_setup(solver, cube10, cuda, pid)
+    beg, cnt, ct = solver.mas_hierarchy(cube10.n_verts)
+    assert np.array_equal(ct, M.coarse_table())
+
+
+@pytest.mark.parametrize("invert_mode", [_abi.B2S_INVERT_SWEEP_F32, _abi.B2S_INVERT_GJ_F64])
+def test_mas_clusters_parity(solver, cuda, cube10, invert_mode):
+    _, A, M = _mas_setup(solver, cube10, cuda, partition_rcb(cube10.positions), invert_mode)
+    hess, inv = solver.mas_clusters()
+    ohess, oinv = M.clusters_arrays()
+    scale = np.abs(ohess).max()
+    assert np.abs(hess - ohess).max() <= 1e-12 * scale
+    iscale = np.abs(oinv).max()
+    assert np.abs(inv.astype(np.float64) - oinv).max() <= 1e-4 * iscale
+
+
+def test_mas_apply_parity(solver, cuda, cube10):
+    import torch
+
+    _, A, M = _mas_setup(solver, cube10, cuda, partition_rcb(cube10.positions))
+    r = np.random.default_rng(5).standard_normal(3 * cube10.n_verts)
+    rd = to_dev(r, cuda)
+    zd = torch.empty_like(rd)
+    solver.precond_apply(rd, zd)
+    z = zd.cpu().numpy()
+    ref = M.apply(r)
+    assert np.abs(z - ref).max() <= 1e-4 * np.abs(ref).max()
+
+
+# ---------------------------------------------------------------------------
+# PCG
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("pre", [_abi.B2S_PRECOND_NONE, _abi.B2S_PRECOND_JACOBI])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_pcg_parity_jacobi(solver, cuda, cube10, pre, use_graph):
+    import torch
+
+    b = _assemble(solver, cube10, cuda)
+    solver.precond_assemble(pre)
+    A = O.OracleMatrix(cube10.n_verts, cube10.rows, cube10.cols, cube10.vals)
+    x = torch.zeros_like(b)
+    st = solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=1, use_graph=use_graph)
+    xo, info = O.pcg(A, cube10.b, precond=pre, tol=1e-4, stop_rule=O.ORC_STOP_RELRES)
+    assert st["converged"] == 1 and info["converged"] == 1
+    # same algorithm, FP64 rounding differs only through the SpMV's atomics:
+    # the stop fires within a couple of iterations of the oracle's
+    slack = 2 if pre == _abi.B2S_PRECOND_JACOBI else max(3, info["iterations"] // 30)
+    assert abs(st["iterations_exact"] - info["iterations"]) <= slack
+    assert st["rel_res"] <= 1e-4 * 1.01
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(xs - xo) <= 1e-3 * np.linalg.norm(xo)
+
+
+def test_pcg_reference_stop_rule_and_interval(solver, cuda, cube10):
+    """|r.z| <= tol |r0.z0| checked every 5 iterations, reported as the
+    reference's fused solver reports it."""
+    import torch
+
+    b = _assemble(solver, cube10, cuda)
+    solver.precond_assemble(_abi.B2S_PRECOND_JACOBI)
+    A = O.OracleMatrix(cube10.n_verts, cube10.rows, cube10.cols, cube10.vals)
+    x = torch.zeros_like(b)
+    st = solver.pcg(b, x, tol=1e-3, stop_rule=_abi.B2S_STOP_RZ, check_interval=5)
+    _, info = O.pcg(A, cube10.b, precond=O.ORC_PRECOND_JACOBI, tol=1e-3, stop_rule=O.ORC_STOP_RZ, check_interval=5)
+    assert st["iterations"] == info["iterations"] and st["iterations"] % 5 == 0
+    assert abs(st["rz0"] - info["rz0"]) <= 1e-12 * abs(info["rz0"])
+
+
+@pytest.mark.parametrize("which", ["cube10", "stack_small"])
+def test_pcg_mas_parity(request, solver, cuda, which):
+    import torch
+
+    s = request.getfixturevalue(which)
+    b, A, M = _mas_setup(solver, s, cuda, partition_rcb(s.positions))
+    x = torch.zeros_like(b)
+    st = solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=1)
+    xo, info = O.pcg(A, s.b, precond=O.ORC_PRECOND_MAS, mas=M, tol=1e-4, stop_rule=O.ORC_STOP_RELRES)
+    assert st["converged"] == 1 and info["converged"] == 1
+    assert abs(st["iterations_exact"] - info["iterations"]) <= 2
+    assert st["rel_res"] <= 1e-4 * 1.01
+
+
+@pytest.mark.parametrize("pre", [_abi.B2S_PRECOND_JACOBI, _abi.B2S_PRECOND_MAS])
+def test_solution_parity_tight_tolerance(solver, cuda, cube10, pre):
+    """At a matched tight tolerance the GPU solution agrees with the FP64
+    direct solution within 1e-6 relative."""
+    import scipy.sparse.linalg as spla
+    import torch
+
+    if pre == _abi.B2S_PRECOND_MAS:
+        b, A, M = _mas_setup(solver, cube10, cuda, partition_rcb(cube10.positions))
+    else:
+        b = _assemble(solver, cube10, cuda)
+        solver.precond_assemble(pre)
+        A = O.OracleMatrix(cube10.n_verts, cube10.rows, cube10.cols, cube10.vals)
+    x = torch.zeros_like(b)
+    st = solver.pcg(b, x, tol=1e-11, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5)
+    xt = spla.spsolve(A.to_scipy().tocsc(), cube10.b)
+    assert st["converged"] == 1
+    assert np.linalg.norm(x.cpu().numpy() - xt) <= 1e-6 * np.linalg.norm(xt)
+
+
+def test_pcg_warm_start(solver, cuda, cube10):
+    import torch
+
+    b = _assemble(solver, cube10, cuda)
+    solver.precond_assemble(_abi.B2S_PRECOND_JACOBI)
+    x = torch.zeros_like(b)
+    st0 = solver.pcg(b, x, tol=1e-8, stop_rule=_abi.B2S_STOP_RELRES, check_interval=1)
+    x2 = x.clone()
+    st1 = solver.pcg(b, x2, tol=1e-8, stop_rule=_abi.B2S_STOP_RELRES, check_interval=1, x0_given=True)
+    assert st1["iterations_exact"] <= 1
+    assert st1["rel_res"] <= 1e-8 * 1.01
+
+
+def test_pcg_zero_rhs(solver, cuda, cube5):
+    import torch
+
+    b = _assemble(solver, cube5, cuda)
+    solver.precond_assemble(_abi.B2S_PRECOND_JACOBI)
+    z = torch.zeros_like(b)
+    x = torch.ones_like(b)
+    st = solver.pcg(z, x, tol=1e-4)
+    assert st["converged"] == 1 and st["iterations"] == 0
+    assert float(x.abs().max()) == 0.0
+
+
+def test_calls_out_of_order_are_state_errors(solver, cuda):
+    import torch
+
+    from libuipc_b200.linear_system import B200SolveError
+
+    v = torch.zeros(9, dtype=torch.float64, device=cuda)
+    with pytest.raises(B200SolveError) as ei:
+        solver.pcg(v, v.clone())
+    assert ei.value.code == _abi.B2S_ERR_STATE
+    with pytest.raises(B200SolveError):
+        solver.precond_apply(v, v.clone())
