@@ -31,6 +31,8 @@ WORKLOADS = {
     "stack8x40": dict(cells=40, n_cubes=8, seed=0),
     # the reference's CPU-runnable small case
     "cube10": dict(cells=10, n_cubes=1, seed=0),
+    # profiling case of the same kernels: 4 cubes (matrix 164 MB > L2)
+    "stack4x40": dict(cells=40, n_cubes=4, seed=0),
 }
 METRIC = "Newton linear-solve ms & PCG iters to 1e-4 rel-res: mixed+learned vs plain, 1 B200"
 
@@ -198,6 +200,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="stack8x40")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) pass (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
 
@@ -282,32 +285,34 @@ def main() -> None:
         ms = float(t.item())
 
     # ---- e2e: host (pinned) inputs through the same public API -------------------
-    h_rows = torch.from_numpy(s.rows).pin_memory()
-    h_cols = torch.from_numpy(s.cols).pin_memory()
-    h_vals = torch.from_numpy(s.vals).pin_memory()
-    h_b = torch.from_numpy(s.b).pin_memory()
-    h_x = torch.empty_like(h_b).pin_memory()
-    e2e_steps = max(1, min(args.steps, 3))
-    barrier()
-    ev0.record(stream)
-    for _ in range(e2e_steps):
-        with torch.cuda.stream(stream):
-            rows.copy_(h_rows, non_blocking=True)
-            cols.copy_(h_cols, non_blocking=True)
-            vals.copy_(h_vals, non_blocking=True)
-            b.copy_(h_b, non_blocking=True)
-        solve_step()
-        with torch.cuda.stream(stream):
-            h_x.copy_(x, non_blocking=True)
-    ev1.record(stream)
-    ev1.synchronize()
-    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
-    if pg is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    h2d = (h_rows.numel() * 4 + h_cols.numel() * 4 + h_vals.numel() * 8 + h_b.numel() * 8)
-    d2h = h_x.numel() * 8
+    e2e_ms, h2d, d2h = None, 0, 0
+    if not args.no_e2e:
+        h_rows = torch.from_numpy(s.rows).pin_memory()
+        h_cols = torch.from_numpy(s.cols).pin_memory()
+        h_vals = torch.from_numpy(s.vals).pin_memory()
+        h_b = torch.from_numpy(s.b).pin_memory()
+        h_x = torch.empty_like(h_b).pin_memory()
+        e2e_steps = max(1, min(args.steps, 3))
+        barrier()
+        ev0.record(stream)
+        for _ in range(e2e_steps):
+            with torch.cuda.stream(stream):
+                rows.copy_(h_rows, non_blocking=True)
+                cols.copy_(h_cols, non_blocking=True)
+                vals.copy_(h_vals, non_blocking=True)
+                b.copy_(h_b, non_blocking=True)
+            solve_step()
+            with torch.cuda.stream(stream):
+                h_x.copy_(x, non_blocking=True)
+        ev1.record(stream)
+        ev1.synchronize()
+        e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
+        if pg is not None:
+            t = torch.tensor([e2e_ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        h2d = (h_rows.numel() * 4 + h_cols.numel() * 4 + h_vals.numel() * 8 + h_b.numel() * 8)
+        d2h = h_x.numel() * 8
 
     # ---- roofline of the dominant kernel (SpMV) --------------------------------------
     peak, peak_kind = _peaks()

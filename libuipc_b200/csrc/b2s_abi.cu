@@ -156,7 +156,7 @@ int b2s_assemble(b2s_solver* s, int32_t nb, int64_t T, const int32_t* rows, cons
                        B2S_REQUIRE(T == 0 || (rows && cols && vals), B2S_ERR_ARGUMENT, "null triplet array");
                        B2S_REQUIRE(nb <= INT32_MAX / 3, B2S_ERR_ARGUMENT, "too many block rows");
                        timed_stage(s, &b2s_timers::assemble_ms,
-                                   [&] { b2s::assemble_triplets(s, s->A, nb, T, rows, cols, vals, false, 0); });
+                                   [&] { b2s::assemble_triplets(s, s->A, nb, T, rows, cols, vals, true); });
                        s->precond_kind = -1;  // any preconditioner must be rebuilt
                        B2S_CUDA(cudaStreamSynchronize(s->stream));
                    });
@@ -191,7 +191,7 @@ int b2s_get_upper_bsr(b2s_solver* s, int32_t* rowptr, int32_t* colidx, double* v
                        {
                            // planes -> column-major blocks: one strided copy per component
                            for(int q = 0; q < 9; ++q)
-                               B2S_CUDA(cudaMemcpy2DAsync(vals + q, 9 * sizeof(double), A.vals.data() + (size_t)q * A.nnz,
+                               B2S_CUDA(cudaMemcpy2DAsync(vals + q, 9 * sizeof(double), A.vals.data() + (size_t)q * A.stride,
                                                           sizeof(double), sizeof(double), A.nnz, cudaMemcpyDefault, st));
                        }
                        B2S_CUDA(cudaStreamSynchronize(st));
@@ -207,6 +207,7 @@ int b2s_spmv(b2s_solver* s, const double* x, double* y, double* h_dot)
                        B2S_REQUIRE(x && y, B2S_ERR_ARGUMENT, "null vector");
                        s->dot_out.resize(4);
                        b2s::spmv_f64(s, s->A, x, y, h_dot ? s->dot_out.data() : nullptr);
+                       b2s::check_device_errors(s);
                        if(h_dot)
                            B2S_CUDA(cudaMemcpyAsync(h_dot, s->dot_out.data(), sizeof(double), cudaMemcpyDeviceToHost,
                                                     s->stream));

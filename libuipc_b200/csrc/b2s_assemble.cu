@@ -337,6 +337,30 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_reduce_rows(int32_t nb, const int
     }
 }
 
+// rank of every block in (column, index) order within its SPMV_TILE-block
+// tile, by counting (one CTA per tile)
+__global__ void __launch_bounds__(SPMV_TILE) k_tile_rank(int64_t U, const int32_t* __restrict__ cols,
+                                                          uint16_t* __restrict__ trank)
+{
+    __shared__ int32_t sc[SPMV_TILE];
+    const int64_t base = (int64_t)blockIdx.x * SPMV_TILE;
+    const int     t    = threadIdx.x;
+    const int64_t rem  = U - base;
+    const int     n    = rem < SPMV_TILE ? (int)rem : SPMV_TILE;
+    sc[t]              = t < n ? cols[base + t] : 0x7fffffff;
+    __syncthreads();
+    if(t >= n)
+        return;
+    const int32_t c    = sc[t];
+    int           rank = 0;
+    for(int j = 0; j < n; ++j)
+    {
+        const int32_t cj = sc[j];
+        rank += (cj < c || (cj == c && j < t)) ? 1 : 0;
+    }
+    trank[base + t] = (uint16_t)rank;
+}
+
 int asm_grid(int64_t work, int block)
 {
     int64_t g = (work + block - 1) / block;
@@ -350,7 +374,7 @@ int asm_grid(int64_t work, int block)
 }  // namespace
 
 void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const int32_t* rows, const int32_t* cols,
-                       const double* vals, bool /*vals_planar*/, int64_t /*plane_stride*/)
+                       const double* vals, bool spmv_tiles)
 {
     B2S_REQUIRE(nb >= 0 && T >= 0, B2S_ERR_ARGUMENT, "negative matrix size");
     B2S_REQUIRE(T < (int64_t)INT32_MAX, B2S_ERR_ARGUMENT, "more than 2^31-1 triplets");
@@ -403,16 +427,30 @@ void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const in
                 "triplet column index outside [0, n_block_rows)");
     B2S_REQUIRE(!(herr & DERR_ROW_OVERFLOW), B2S_ERR_ARGUMENT,
                 "triplet arrays changed during assembly (row bucket overflow)");
-    M.nnz = U;
-    M.rows.resize(std::max<int64_t>(U, 1), 1.2);
-    M.cols.resize(std::max<int64_t>(U, 1), 1.2);
-    M.vals.resize((size_t)9 * std::max<int64_t>(U, 1), 1.2);
+    M.nnz    = U;
+    M.stride = ((std::max<int64_t>(U, 1) + 15) / 16) * 16;
+    M.rows.resize(M.stride, 1.2);
+    M.cols.resize(M.stride, 1.2);
+    M.vals.resize((size_t)9 * M.stride, 1.2);
+    // padding past U: row -1 / col 0 (never used: every reader checks k < U)
+    B2S_CUDA(cudaMemsetAsync(M.rows.data() + U, 0xff, sizeof(int32_t) * (M.stride - U), st));
+    B2S_CUDA(cudaMemsetAsync(M.cols.data() + U, 0, sizeof(int32_t) * (M.stride - U), st));
     if(nb > 0)
     {
+        // values are written as planes with stride M.stride
         k_reduce_rows<<<asm_grid((int64_t)nb * 32, ASM_BLOCK), ASM_BLOCK, 0, st>>>(
             nb, w.row_start.data(), w.sorted_col.data(), w.sorted_src.data(), vals, M.rowptr.data(),
-            M.rows.data(), M.cols.data(), M.vals.data(), U, M.diag_index.data());
+            M.rows.data(), M.cols.data(), M.vals.data(), M.stride, M.diag_index.data());
         B2S_CHECK_LAUNCH();
+    }
+    M.has_trank = false;
+    if(spmv_tiles && U > 0)
+    {
+        M.trank.resize(M.stride, 1.2);
+        k_tile_rank<<<(unsigned)((U + SPMV_TILE - 1) / SPMV_TILE), SPMV_TILE, 0, st>>>(U, M.cols.data(),
+                                                                                     M.trank.data());
+        B2S_CHECK_LAUNCH();
+        M.has_trank = true;
     }
     M.valid = true;
 }

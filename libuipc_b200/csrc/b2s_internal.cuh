@@ -63,6 +63,7 @@ enum DeviceError : int
     DERR_TRIPLET_INDEX = 1,  // triplet row/col outside [0, n_block_rows)
     DERR_ROW_OVERFLOW  = 2,  // a row's bucket exceeded its counted size
     DERR_MAS_INDEX     = 4,  // MAS hierarchy index out of range
+    DERR_TMA_TIMEOUT   = 8,  // a bounded wait on a bulk-copy barrier ran out
 };
 
 // ---------------------------------------------------------------------------
@@ -114,10 +115,17 @@ struct Matrix
 {
     int32_t        nb  = 0;  // block rows
     int64_t        nnz = 0;  // unique upper blocks U
+    int64_t        stride = 0;  // plane stride: U rounded up to 16 (16-byte aligned bulk copies)
     DBuf<int32_t>  rowptr;   // [nb+1]
-    DBuf<int32_t>  rows;     // [U] block row of each block (BCOO row index)
-    DBuf<int32_t>  cols;     // [U]
-    DBuf<double>   vals;     // [9][U]: component q (column-major index) at vals[q*U + k]
+    DBuf<int32_t>  rows;     // [stride] block row of each block (BCOO row index), -1 in the padding
+    DBuf<int32_t>  cols;     // [stride]
+    DBuf<double>   vals;     // [9][stride]: component q (column-major index) at vals[q*stride + k]
+    DBuf<float>    vals32;   // FP32 copy of vals (mixed precision), same layout
+    // rank of each block in (column, index) order inside its 512-block SpMV
+    // tile: the SpMV sorts the transposed contributions of a tile by column
+    // in shared memory and merges equal columns before its atomics
+    DBuf<uint16_t> trank;    // [stride]
+    bool           has_trank = false;
     DBuf<int32_t>  diag_index;  // [nb] position of block (i,i), -1 if absent
     bool           valid = false;
 };
@@ -219,6 +227,7 @@ struct b2s_solver
     b2s::DBuf<double>    dinv;  // [nb*9] row-major inverses of diagonal blocks
     b2s::DBuf<double>    dot_out;
     b2s::Reduction       red;
+    b2s::DBuf<int>       dev_err;  // DeviceError bits raised by kernels
     // stage timers (CUDA events on `stream`)
     bool                     timing = false;
     b2s_timers               timers{};
@@ -233,9 +242,12 @@ namespace b2s
 void exclusive_scan(b2s_solver* s, const int32_t* in, int32_t* out, int64_t n, DBuf<int32_t>& tmp);
 
 // assembly of raw triplets into a block-upper matrix (shared by the global
-// matrix and the MAS coarse levels)
+// matrix and the MAS coarse levels); `spmv_tiles` also computes the per-tile
+// column ranks the SpMV uses
 void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const int32_t* rows,
-                       const int32_t* cols, const double* vals, bool vals_planar, int64_t plane_stride);
+                       const int32_t* cols, const double* vals, bool spmv_tiles);
+
+constexpr int SPMV_TILE = 512;  // blocks per SpMV stage / tile
 
 // y = A x (+ optional pAp into partial reduction slot)
 void spmv_f64(b2s_solver* s, const Matrix& A, const double* x, double* y, double* d_dot);
@@ -247,6 +259,7 @@ void launch_dot(b2s_solver* s, const double* a, const double* b, int64_t n, doub
 // preconditioners
 void precond_assemble(b2s_solver* s, int kind, int invert_mode);
 void precond_apply(b2s_solver* s, const double* r, double* z);
+void check_device_errors(b2s_solver* s);
 void mas_init(b2s_solver* s, int32_t offset, int32_t vn, const int32_t* adj_start,
               const int32_t* adj_list, int32_t N, const int32_t* p2r, const int32_t* r2p);
 void mas_assemble(b2s_solver* s, int invert_mode);

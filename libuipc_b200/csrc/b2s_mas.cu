@@ -23,11 +23,14 @@
 // level computed in the same pass (no atomics, bit-reproducible).
 #include "b2s_internal.cuh"
 #include "b2s_reduce.cuh"
+#include "b2s_tma.cuh"
 
 #include <algorithm>
 
 namespace b2s
 {
+int* device_error_flag(b2s_solver* s);
+
 namespace
 {
 inline int bank_align(int n) { return (n + BANK - 1) / BANK * BANK; }
@@ -227,7 +230,7 @@ __global__ void k_h_ctable(int vn, int L, const int32_t* cst, const int32_t* lev
 // ---------------------------------------------------------------------------
 
 // level 0: blocks of A inside one partition bank, stored oriented by slot
-__global__ void k_g_level0(int64_t U, const int32_t* rows, const int32_t* cols, const double* vals, int off, int vn,
+__global__ void k_g_level0(int64_t U, const int32_t* rows, const int32_t* cols, const double* vals, int64_t S, int off, int vn,
                            const int32_t* r2p, double* hess)
 {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -247,8 +250,8 @@ __global__ void k_g_level0(int64_t U, const int32_t* rows, const int32_t* cols, 
 #pragma unroll
         for(int q = 0; q < 3; ++q)
         {
-            // dst(p,q) column-major; source B(p,q) = vals[(q*3+p)*U + k]
-            const double v = swap ? vals[(int64_t)(p * 3 + q) * U + k] : vals[(int64_t)(q * 3 + p) * U + k];
+            // dst(p,q) column-major; source B(p,q) = vals[(q*3+p)*S + k]
+            const double v = swap ? vals[(int64_t)(p * 3 + q) * S + k] : vals[(int64_t)(q * 3 + p) * S + k];
             dst[q * 3 + p] = v;
         }
 }
@@ -256,7 +259,7 @@ __global__ void k_g_level0(int64_t U, const int32_t* rows, const int32_t* cols, 
 // restriction of a block-upper matrix to the next level as raw triplets:
 // (a, b, B) -> (P a, P b) with B, B^T or (a != b) B + B^T when both map to
 // one node. Entries that leave the MAS range are written with row -1.
-__global__ void k_g_restrict(int64_t U, const int32_t* rows, const int32_t* cols, const double* vals, int off,
+__global__ void k_g_restrict(int64_t U, const int32_t* rows, const int32_t* cols, const double* vals, int64_t S, int off,
                              int n_in, const int32_t* map, int32_t* out_rows, int32_t* out_cols, double* out_vals)
 {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -281,7 +284,7 @@ __global__ void k_g_restrict(int64_t U, const int32_t* rows, const int32_t* cols
     double B[9];
 #pragma unroll
     for(int q = 0; q < 9; ++q)
-        B[q] = vals[(int64_t)q * U + k];
+        B[q] = vals[(int64_t)q * S + k];
     double o[9];
     if(ca < cb)
     {
@@ -319,7 +322,7 @@ __global__ void k_g_restrict(int64_t U, const int32_t* rows, const int32_t* cols
 }
 
 // level l >= 1: in-bank blocks of the level-l Galerkin matrix into clusters
-__global__ void k_g_extract(int64_t U, const int32_t* rows, const int32_t* cols, const double* vals,
+__global__ void k_g_extract(int64_t U, const int32_t* rows, const int32_t* cols, const double* vals, int64_t S,
                             int level_begin, double* hess)
 {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -332,7 +335,7 @@ __global__ void k_g_extract(int64_t U, const int32_t* rows, const int32_t* cols,
     double*   dst = hess + ((size_t)(ga / BANK) * SYM + sym_index(ga % BANK, gb % BANK)) * 9;
 #pragma unroll
     for(int q = 0; q < 9; ++q)
-        dst[q] = vals[(int64_t)q * U + k];
+        dst[q] = vals[(int64_t)q * S + k];
 }
 
 // ---------------------------------------------------------------------------
@@ -429,19 +432,14 @@ __global__ void __launch_bounds__(INV_BLOCK) k_invert(int clusters, const double
 }
 
 // ---------------------------------------------------------------------------
-// apply: one warp per bank. Lanes 0-15 own the bank's nodes; the 48x48
-// product is split over the two half-warps (columns 0-7 / 8-15).
+// apply: one warp per bank, persistent over banks. The bank's 4896-byte FP32
+// inverse is brought into shared memory by a bulk asynchronous copy (TMA),
+// double-buffered per warp so the next bank's copy is in flight while this
+// one computes. Lanes 0-15 own the bank's nodes; the 48x48 product is split
+// over the two half-warps (columns 0-7 / 8-15).
 // ---------------------------------------------------------------------------
-constexpr int APPLY_WARPS = 8;
-
-// stage one cluster's 1224-float inverse in shared memory (coalesced float4)
-__device__ __forceinline__ void stage_inverse(const float* __restrict__ src, float* dst, int lane)
-{
-    const float4* s4 = reinterpret_cast<const float4*>(src);
-    float4*       d4 = reinterpret_cast<float4*>(dst);
-    for(int e = lane; e < SYM * 9 / 4; e += 32)
-        d4[e] = __ldg(s4 + e);
-}
+constexpr int APPLY_WARPS = 4;
+constexpr uint32_t INV_BYTES = SYM * 9 * sizeof(float);  // 4896, a multiple of 16
 
 __device__ __forceinline__ void cluster_product(const float* M, const float (*r)[3], int lane, float out[3])
 {
@@ -476,128 +474,131 @@ __device__ __forceinline__ void cluster_product(const float* M, const float (*r)
     out[2] = acc2;
 }
 
-// level-0 banks: gather r, push the level-1 sums, local solve -> Z
-template <typename VT>
-__global__ void __launch_bounds__(APPLY_WARPS * 32) k_apply_fine(int n_banks, const int32_t* __restrict__ p2r,
-                                                                 const uint16_t* __restrict__ comp_mask,
-                                                                 const int32_t* __restrict__ new_local0,
-                                                                 int level1_begin, const VT* __restrict__ r,
-                                                                 int off3, const float* __restrict__ inv,
-                                                                 float* __restrict__ R, float* __restrict__ Z,
-                                                                 const int* converged)
+// One level of the apply. FINE: level 0, the residual is gathered from the
+// FP64 vector r through part_to_real; otherwise R_l is read from the node
+// buffer. With `push`, the restriction sums of the next level (one per
+// connected component of the bank, summed by its lowest lane in lane order)
+// are written to R_{l+1}. Z_l = A_l^{-1} R_l for every node of the bank.
+template <bool FINE, typename VT>
+__global__ void __launch_bounds__(APPLY_WARPS * 32)
+    k_apply_level(int n_banks, int cnt, int level_begin, const int32_t* __restrict__ p2r, const VT* __restrict__ r,
+                  int off3, const uint16_t* __restrict__ comp_mask, const int32_t* __restrict__ new_local,
+                  int next_begin, int push, const float* __restrict__ inv, float* R, float* __restrict__ Z,
+                  const int* converged, int* err)
 {
     if(converged && *converged)
         return;
-    __shared__ __align__(16) float s_inv[APPLY_WARPS][SYM * 9];
-    __shared__ float s_r[APPLY_WARPS][BANK][3];
+    __shared__ __align__(128) float s_inv[APPLY_WARPS][2][SYM * 9];
+    __shared__ float    s_r[APPLY_WARPS][BANK][3];
+    __shared__ uint64_t s_bar[APPLY_WARPS][2];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int bank = blockIdx.x * APPLY_WARPS + w;
-    if(bank >= n_banks)
-        return;
-    stage_inverse(inv + (size_t)bank * SYM * 9, s_inv[w], lane);
-    const int p = bank * BANK + (lane & 15);
-    float     rv[3] = {0.f, 0.f, 0.f};
-    int       v     = -1;
-    if(lane < 16)
+    const int gw = blockIdx.x * APPLY_WARPS + w, W = gridDim.x * APPLY_WARPS;
+    const int mine = gw < n_banks ? (n_banks - 1 - gw) / W + 1 : 0;
+    const int64_t gbank0 = level_begin / BANK;
+    if(lane == 0)
     {
-        v = p2r[p];
-        if(v >= 0)
+        mbar_init(&s_bar[w][0], 1);
+        mbar_init(&s_bar[w][1], 1);
+        mbar_fence_init();
+        for(int j = 0; j < mine && j < 2; ++j)
         {
-            rv[0] = (float)r[off3 + 3 * (int64_t)v];
-            rv[1] = (float)r[off3 + 3 * (int64_t)v + 1];
-            rv[2] = (float)r[off3 + 3 * (int64_t)v + 2];
+            mbar_arrive_expect_tx(&s_bar[w][j], INV_BYTES);
+            bulk_copy_g2s(s_inv[w][j], inv + (size_t)(gbank0 + gw + (int64_t)j * W) * SYM * 9, INV_BYTES,
+                          &s_bar[w][j]);
         }
-        s_r[w][lane][0] = rv[0];
-        s_r[w][lane][1] = rv[1];
-        s_r[w][lane][2] = rv[2];
     }
     __syncwarp();
-    // restriction: the lowest lane of each component sums it in lane order
-    if(lane < 16 && v >= 0)
+    int j = 0;
+    for(; j < mine; ++j)
     {
-        const uint32_t cm = comp_mask[p];
-        if((cm & ((1u << lane) - 1u)) == 0)
+        const int bank = gw + j * W;
+        const int slot = j & 1;
+        // residual of the bank's 16 nodes (overlaps the inverse's copy)
+        const int node = bank * BANK + (lane & 15);
+        bool      live = false;
+        if(lane < 16)
         {
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-            for(uint32_t m = cm; m; m &= m - 1)
+            float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+            if(FINE)
             {
-                const int l = __ffs(m) - 1;
-                s0 += s_r[w][l][0];
-                s1 += s_r[w][l][1];
-                s2 += s_r[w][l][2];
+                const int v = p2r[node];
+                live        = v >= 0;
+                if(live)
+                {
+                    r0 = (float)r[off3 + 3 * (int64_t)v];
+                    r1 = (float)r[off3 + 3 * (int64_t)v + 1];
+                    r2 = (float)r[off3 + 3 * (int64_t)v + 2];
+                }
             }
-            const int64_t g = (int64_t)level1_begin + new_local0[p];
-            R[3 * g]     = s0;
-            R[3 * g + 1] = s1;
-            R[3 * g + 2] = s2;
+            else
+            {
+                live = node < cnt;
+                if(live)
+                {
+                    const int64_t g = (int64_t)level_begin + node;
+                    r0 = R[3 * g];
+                    r1 = R[3 * g + 1];
+                    r2 = R[3 * g + 2];
+                }
+            }
+            s_r[w][lane][0] = r0;
+            s_r[w][lane][1] = r1;
+            s_r[w][lane][2] = r2;
+        }
+        __syncwarp();
+        if(push && live)
+        {
+            const uint32_t cm = comp_mask[node];
+            if((cm & ((1u << lane) - 1u)) == 0)
+            {
+                float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+                for(uint32_t m = cm; m; m &= m - 1)
+                {
+                    const int l = __ffs(m) - 1;
+                    s0 += s_r[w][l][0];
+                    s1 += s_r[w][l][1];
+                    s2 += s_r[w][l][2];
+                }
+                const int64_t g = (int64_t)next_begin + new_local[node];
+                R[3 * g]     = s0;
+                R[3 * g + 1] = s1;
+                R[3 * g + 2] = s2;
+            }
+        }
+        const bool ok = mbar_wait(&s_bar[w][slot], (uint32_t)((j >> 1) & 1), err, DERR_TMA_TIMEOUT);
+        if(!__all_sync(0xffffffffu, ok))
+            break;
+        float out[3];
+        cluster_product(s_inv[w][slot], s_r[w], lane, out);
+        if(lane < 16)
+        {
+            const int64_t g = (int64_t)level_begin + node;
+            Z[3 * g]     = out[0];
+            Z[3 * g + 1] = out[1];
+            Z[3 * g + 2] = out[2];
+        }
+        __syncwarp();
+        if(lane == 0 && j + 2 < mine)
+        {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&s_bar[w][slot], INV_BYTES);
+            bulk_copy_g2s(s_inv[w][slot], inv + (size_t)(gbank0 + bank + 2 * (int64_t)W) * SYM * 9, INV_BYTES,
+                          &s_bar[w][slot]);
         }
     }
-    float out[3];
-    cluster_product(s_inv[w], s_r[w], lane, out);
-    if(lane < 16)
+    if(j < mine && lane == 0)
     {
-        Z[3 * (int64_t)p]     = out[0];
-        Z[3 * (int64_t)p + 1] = out[1];
-        Z[3 * (int64_t)p + 2] = out[2];
+        // a wait ran out: drain this warp's copies still in flight (bounded)
+        for(int q = j; q < mine && q < j + 2; ++q)
+            mbar_wait(&s_bar[w][q & 1], (uint32_t)((q >> 1) & 1), nullptr, 0);
     }
 }
 
-// level-l banks (l >= 1): R_l from the previous pass, push R_{l+1}, solve -> Z_l
-__global__ void __launch_bounds__(APPLY_WARPS * 32) k_apply_coarse(int n_banks, int cnt, int level_begin,
-                                                                   const uint16_t* __restrict__ comp_mask,
-                                                                   const int32_t* __restrict__ new_local,
-                                                                   int next_begin, int push,
-                                                                   const float* __restrict__ inv, float* R,
-                                                                   float* __restrict__ Z, const int* converged)
+int apply_grid(int n_banks)
 {
-    if(converged && *converged)
-        return;
-    __shared__ __align__(16) float s_inv[APPLY_WARPS][SYM * 9];
-    __shared__ float s_r[APPLY_WARPS][BANK][3];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int bank = blockIdx.x * APPLY_WARPS + w;
-    if(bank >= n_banks)
-        return;
-    const int64_t gbank = level_begin / BANK + bank;
-    stage_inverse(inv + (size_t)gbank * SYM * 9, s_inv[w], lane);
-    const int c = bank * BANK + (lane & 15);
-    if(lane < 16)
-    {
-        const bool live = c < cnt;
-        const int64_t g = (int64_t)level_begin + c;
-        s_r[w][lane][0] = live ? R[3 * g] : 0.f;
-        s_r[w][lane][1] = live ? R[3 * g + 1] : 0.f;
-        s_r[w][lane][2] = live ? R[3 * g + 2] : 0.f;
-    }
-    __syncwarp();
-    if(push && lane < 16 && c < cnt)
-    {
-        const uint32_t cm = comp_mask[c];
-        if((cm & ((1u << lane) - 1u)) == 0)
-        {
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-            for(uint32_t m = cm; m; m &= m - 1)
-            {
-                const int l = __ffs(m) - 1;
-                s0 += s_r[w][l][0];
-                s1 += s_r[w][l][1];
-                s2 += s_r[w][l][2];
-            }
-            const int64_t g = (int64_t)next_begin + new_local[c];
-            R[3 * g]     = s0;
-            R[3 * g + 1] = s1;
-            R[3 * g + 2] = s2;
-        }
-    }
-    float out[3];
-    cluster_product(s_inv[w], s_r[w], lane, out);
-    if(lane < 16)
-    {
-        const int64_t g = (int64_t)level_begin + c;
-        Z[3 * g]     = out[0];
-        Z[3 * g + 1] = out[1];
-        Z[3 * g + 2] = out[2];
-    }
+    const int max_warps = NUM_SMS_HINT * 5 * APPLY_WARPS;
+    const int warps     = n_banks < max_warps ? n_banks : max_warps;
+    return (warps + APPLY_WARPS - 1) / APPLY_WARPS;
 }
 }  // namespace
 
@@ -770,7 +771,8 @@ void mas_assemble(b2s_solver* s, int invert_mode)
     B2S_CUDA(cudaMemsetAsync(M.hess.data(), 0, M.hess.bytes(), st));
     if(A.nnz > 0)
     {
-        k_g_level0<<<grid_for(A.nnz, TB), TB, 0, st>>>(A.nnz, A.rows.data(), A.cols.data(), A.vals.data(), M.offset,
+        k_g_level0<<<grid_for(A.nnz, TB), TB, 0, st>>>(A.nnz, A.rows.data(), A.cols.data(), A.vals.data(), A.stride,
+                                                       M.offset,
                                                        M.vn, M.r2p.data(), M.hess.data());
         B2S_CHECK_LAUNCH();
     }
@@ -789,16 +791,16 @@ void mas_assemble(b2s_solver* s, int invert_mode)
         if(T > 0)
         {
             k_g_restrict<<<grid_for(T, TB), TB, 0, st>>>(T, prev->rows.data(), prev->cols.data(), prev->vals.data(),
-                                                         prev_off, prev_n, map, M.trip_rows.data(),
+                                                         prev->stride, prev_off, prev_n, map, M.trip_rows.data(),
                                                          M.trip_cols.data(), M.trip_vals.data());
             B2S_CHECK_LAUNCH();
         }
         assemble_triplets(s, C, M.level_count[level], T, M.trip_rows.data(), M.trip_cols.data(), M.trip_vals.data(),
-                          false, 0);
+                          false);
         if(C.nnz > 0)
         {
             k_g_extract<<<grid_for(C.nnz, TB), TB, 0, st>>>(C.nnz, C.rows.data(), C.cols.data(), C.vals.data(),
-                                                            M.level_begin[level], M.hess.data());
+                                                            C.stride, M.level_begin[level], M.hess.data());
             B2S_CHECK_LAUNCH();
         }
         prev     = &C;
@@ -821,15 +823,19 @@ void mas_assemble(b2s_solver* s, int invert_mode)
 // handled by the caller (collect kernel in the PCG, or precond_apply)
 void mas_apply_levels(b2s_solver* s, const double* r, const int* converged)
 {
-    MasState& M = s->mas;
-    MasState& X = s->mas;
+    MasState&    M  = s->mas;
+    MasState&    X  = s->mas;
     cudaStream_t st = s->stream;
-    const int n_banks0 = M.N / BANK;
-    const int tb       = APPLY_WARPS * 32;
-    k_apply_fine<double><<<grid_for(n_banks0, APPLY_WARPS), tb, 0, st>>>(
-        n_banks0, M.p2r.data(), X.comp_mask[0].data(), X.new_local[0].data(), M.level_begin[1], r, 3 * M.offset,
-        M.inv.data(), M.R.data(), M.Z.data(), converged);
-    B2S_CHECK_LAUNCH();
+    int*         err = device_error_flag(s);
+    const int    n_banks0 = M.N / BANK;
+    const int    tb       = APPLY_WARPS * 32;
+    if(n_banks0 > 0)
+    {
+        k_apply_level<true, double><<<apply_grid(n_banks0), tb, 0, st>>>(
+            n_banks0, M.N, 0, M.p2r.data(), r, 3 * M.offset, X.comp_mask[0].data(), X.new_local[0].data(),
+            M.level_begin[1], M.L > 1 ? 1 : 0, M.inv.data(), M.R.data(), M.Z.data(), converged, err);
+        B2S_CHECK_LAUNCH();
+    }
     for(int level = 1; level < M.L; ++level)
     {
         const int cnt = M.level_count[level];
@@ -837,12 +843,11 @@ void mas_apply_levels(b2s_solver* s, const double* r, const int* converged)
             break;
         const int n_banks = (cnt + BANK - 1) / BANK;
         const int push    = level + 1 < M.L ? 1 : 0;
-        k_apply_coarse<<<grid_for(n_banks, APPLY_WARPS), tb, 0, st>>>(
-            n_banks, cnt, M.level_begin[level], X.comp_mask[level].data(),
-            push ? X.new_local[level].data() : X.new_local[0].data(), push ? M.level_begin[level + 1] : 0, push,
-            M.inv.data(), M.R.data(), M.Z.data(), converged);
+        k_apply_level<false, double><<<apply_grid(n_banks), tb, 0, st>>>(
+            n_banks, cnt, M.level_begin[level], nullptr, nullptr, 0, X.comp_mask[level].data(),
+            X.new_local[level].data(), push ? M.level_begin[level + 1] : 0, push, M.inv.data(), M.R.data(),
+            M.Z.data(), converged, err);
         B2S_CHECK_LAUNCH();
     }
 }
-
 }  // namespace b2s

@@ -20,8 +20,10 @@
 
 namespace b2s
 {
-void spmv_f64_launch(cudaStream_t st, const Matrix& A, const double* x, double* y, Reduction& red, double* d_dot,
+void spmv_f64_launch(b2s_solver* s, const Matrix& A, const double* x, double* y, Reduction& red, double* d_dot,
                      const int* stop);
+int* device_error_flag(b2s_solver* s);
+void check_device_errors(b2s_solver* s);
 int  spmv_grid(int64_t U);
 void ensure_reduction(Reduction& red, int grid, int nv);
 void mas_apply_levels(b2s_solver* s, const double* r, const int* converged);
@@ -252,7 +254,7 @@ void precond_assemble(b2s_solver* s, int kind, int invert_mode)
     s->dinv.resize((size_t)std::max(A.nb, 1) * 9);
     if(A.nb > 0)
     {
-        k_diag_inverse<<<grid_for(A.nb, 256), 256, 0, st>>>(A.nb, A.diag_index.data(), A.vals.data(), A.nnz,
+        k_diag_inverse<<<grid_for(A.nb, 256), 256, 0, st>>>(A.nb, A.diag_index.data(), A.vals.data(), A.stride,
                                                             s->dinv.data());
         B2S_CHECK_LAUNCH();
     }
@@ -300,6 +302,7 @@ void precond_apply(b2s_solver* s, const double* r, double* z)
 {
     B2S_REQUIRE(s->precond_kind >= 0, B2S_ERR_STATE, "precond_apply before b2s_precond_assemble");
     precond_launch(s, s->precond_kind, r, z, nullptr, s->red);
+    check_device_errors(s);
     B2S_CUDA(cudaStreamSynchronize(s->stream));
 }
 
@@ -327,7 +330,7 @@ static void pcg_iteration(b2s_solver* s, int kind, double* x, int slot)
     cudaEvent_t*  ev = s->timing ? &s->iter_events[(size_t)slot * 4] : nullptr;
     if(ev)
         B2S_CUDA(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
-    spmv_f64_launch(st, A, P.p.data(), P.Ap.data(), P.red, &P.sc.data()->pAp, &P.sc.data()->converged);
+    spmv_f64_launch(s, A, P.p.data(), P.Ap.data(), P.red, &P.sc.data()->pAp, &P.sc.data()->converged);
     if(ev)
         B2S_CUDA(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
     k_update_xr<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), x, P.p.data(), P.r.data(), P.Ap.data());
@@ -377,6 +380,8 @@ void pcg_solve(b2s_solver* s, const double* b, double* x, const b2s_pcg_options&
     if(!P.h_sc)
         B2S_CUDA(cudaMallocHost(&P.h_sc, sizeof(PcgScalars)));
     ensure_reduction(P.red, std::max(spmv_grid(A.nnz), reduction_grid()), 2);
+    device_error_flag(s);  // allocated before any graph capture
+    B2S_REQUIRE(A.nnz == 0 || A.has_trank, B2S_ERR_STATE, "matrix lacks the SpMV tile ranks");
     s->dot_out.resize(4);
     const int ci = o.check_interval > 0 ? o.check_interval : 1;
     const int64_t max_iter = o.max_iter > 0 ? o.max_iter : std::max<int64_t>(2 * n, 1);
@@ -568,6 +573,7 @@ void pcg_solve(b2s_solver* s, const double* b, double* x, const b2s_pcg_options&
         }
     }
     st_out.replacements = replacements;
+    check_device_errors(s);
     if(st_out.converged)
         st_out.iterations = ci > 1 ? std::min<int64_t>(((st_out.iterations_exact + ci - 1) / ci) * ci, max_iter)
                                    : st_out.iterations_exact;

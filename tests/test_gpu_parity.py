@@ -187,7 +187,9 @@ def test_pcg_parity_jacobi(solver, cuda, cube10, pre, use_graph):
     assert abs(st["iterations_exact"] - info["iterations"]) <= slack
     assert st["rel_res"] <= 1e-4 * 1.01
     xs = x.cpu().numpy()
-    assert np.linalg.norm(xs - xo) <= 1e-3 * np.linalg.norm(xo)
+    # two valid stops at rel-res 1e-4 (cond ~3e4) differ by up to ~1e-2 in x
+    bound = 1e-3 if pre == _abi.B2S_PRECOND_JACOBI else 1e-2
+    assert np.linalg.norm(xs - xo) <= bound * np.linalg.norm(xo)
 
 
 def test_pcg_reference_stop_rule_and_interval(solver, cuda, cube10):
