@@ -186,6 +186,28 @@ int b2s_set_timing(b2s_solver* s, int enable);
 int b2s_get_timers(const b2s_solver* s, b2s_timers* out);
 int b2s_reset_timers(b2s_solver* s);
 
+/* ---- SpMV for callers that cannot allocate -------------------------------------------
+ * No counterpart in the reference. The same y = A x and x.(A x) as b2s_spmv,
+ * for callers that must not (or cannot) call cudaMalloc: code running inside
+ * a host callback or an allocator hook, a process whose device memory is
+ * owned by another framework's caching allocator, or a loop that may not
+ * touch the allocator after start-up. It takes no solver handle and
+ * allocates nothing: the caller owns the block-upper BCOO (d_rows, d_cols,
+ * d_vals: 9 doubles per block, column-major, row <= col, no duplicates --
+ * the layout b2s_get_upper_bsr returns), d_x, d_y [3 * n_block_rows] and
+ * d_dot (one double, may be NULL). Its scratch is a fixed device array in
+ * the library (about 256 KB per device that loads it, held until exit), so
+ * n_blocks is limited to 8,388,608; larger inputs are rejected with
+ * B2S_ERR_ARGUMENT. Work is queued on `stream` (cudaStream_t, NULL = legacy
+ * stream) and the call returns without waiting. The first call on a device
+ * looks up the scratch array's device address; make that first call before
+ * any stream capture. Every call shares the scratch array, so calls that
+ * overlap on the GPU (concurrent streams) race: serialise them. Errors are
+ * reported through b2s_last_error(NULL). */
+int b2s_spmv_noalloc(int32_t n_block_rows, int64_t n_blocks, const int32_t* d_rows,
+                     const int32_t* d_cols, const double* d_vals, const double* d_x,
+                     double* d_y, double* d_dot, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,7 @@ SIGNATURES = {
     "b2s_set_timing": (C.c_int, [vp, C.c_int]),
     "b2s_get_timers": (C.c_int, [vp, C.POINTER(Timers)]),
     "b2s_reset_timers": (C.c_int, [vp]),
+    "b2s_spmv_noalloc": (C.c_int, [i32, i64, vp, vp, vp, vp, vp, vp, vp]),
 }
 
 

@@ -7,14 +7,20 @@
 #include <cstring>
 #include <numeric>
 
-namespace b2s
-{
-thread_local long long g_kernel_launches = 0;
-}
-
 namespace
 {
 thread_local std::string g_create_error;
+}
+
+namespace b2s
+{
+thread_local long long g_kernel_launches = 0;
+
+void set_handle_free_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace b2s
+
+namespace
+{
 
 template <typename F>
 int guarded(b2s_solver* s, F&& f)

@@ -260,6 +260,10 @@ void launch_dot(b2s_solver* s, const double* a, const double* b, int64_t n, doub
 void precond_assemble(b2s_solver* s, int kind, int invert_mode);
 void precond_apply(b2s_solver* s, const double* r, double* z);
 void check_device_errors(b2s_solver* s);
+
+// message of the last failed call made without a solver handle (read back
+// through b2s_last_error(NULL))
+void set_handle_free_error(const std::string& msg);
 void mas_init(b2s_solver* s, int32_t offset, int32_t vn, const int32_t* adj_start,
               const int32_t* adj_list, int32_t N, const int32_t* p2r, const int32_t* r2p);
 void mas_assemble(b2s_solver* s, int invert_mode);
