@@ -97,11 +97,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def spmv_bytes(U: int, nb: int) -> int:
-    """Algorithmic bytes of one FP64 symmetric SpMV from the block-upper
-    minimal format: blocks (4 B column index + 72 B values), row pointers,
-    x read and y written once."""
-    return U * (4 + 72) + 4 * (nb + 1) + 3 * nb * (8 + 8)
+def spmv_bytes(U: int, nb: int, s: int = 8) -> int:
+    """Algorithmic bytes of one symmetric SpMV from the block-upper minimal
+    format with s-byte values (8 = FP64, 4 = FP32): blocks (4 B column index +
+    9 s value bytes), row pointers, x read and y written once."""
+    return U * (4 + 9 * s) + 4 * (nb + 1) + 3 * nb * (s + s)
 
 
 def build_workload(name: str):
@@ -245,14 +245,13 @@ def main() -> None:
     stream.synchronize()
     solver.mas_init(0, s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
 
-    def solve_step():
+    precisions = {"plain": _abi.B2S_PRECISION_FP64, "mixed": _abi.B2S_PRECISION_MIXED}
+
+    def solve_step(mode):
         solver.assemble(s.n_verts, rows, cols, vals)
         solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_SWEEP_F32)
-        return solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5)
-
-    for _ in range(args.warmup):
-        st = solve_step()
-    nb, U = solver.matrix_info()
+        return solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5,
+                          precision=precisions[mode], replace_every=50)
 
     def barrier():
         torch.cuda.synchronize()
@@ -260,29 +259,40 @@ def main() -> None:
             pg.barrier()
         torch.cuda.synchronize()
 
-    # ---- timed region: device-resident inputs ------------------------------------
-    solver.set_timing(True)
-    solve_step()  # capture the graph with timing nodes outside the timed region
-    solver.reset_timers()
-    clocks = ClockSampler(local_rank)
-    barrier()
-    clocks.start()
+    def max_over_ranks(v):
+        if pg is None:
+            return v
+        t = torch.tensor([v], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    stats = []
-    for _ in range(args.steps):
-        stats.append(solve_step())
-    ev1.record(stream)
-    ev1.synchronize()
-    barrier()
-    clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    tm = solver.timers()
-    if pg is not None:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+
+    def timed(mode):
+        """W untimed warm-up solves, then K solves between CUDA events on the
+        solver's stream (barrier + synchronize on both sides)."""
+        solver.set_timing(False)
+        for _ in range(args.warmup):
+            solve_step(mode)
+        solver.set_timing(True)
+        solve_step(mode)  # captures the graph with its timing nodes outside the timed region
+        solver.reset_timers()
+        clocks = ClockSampler(local_rank)
+        barrier()
+        clocks.start()
+        ev0.record(stream)
+        stats = [solve_step(mode) for _ in range(args.steps)]
+        ev1.record(stream)
+        ev1.synchronize()
+        barrier()
+        clk = clocks.stop()
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+        return ms, stats, solver.timers(), clk
+
+    res = {mode: timed(mode) for mode in ("plain", "mixed")}
+    nb, U = solver.matrix_info()
+    ms, stats, tm, clk = res["mixed"]
 
     # ---- e2e: host (pinned) inputs through the same public API -------------------
     e2e_ms, h2d, d2h = None, 0, 0
@@ -293,6 +303,8 @@ def main() -> None:
         h_b = torch.from_numpy(s.b).pin_memory()
         h_x = torch.empty_like(h_b).pin_memory()
         e2e_steps = max(1, min(args.steps, 3))
+        solver.set_timing(False)
+        solve_step("mixed")
         barrier()
         ev0.record(stream)
         for _ in range(e2e_steps):
@@ -301,31 +313,31 @@ def main() -> None:
                 cols.copy_(h_cols, non_blocking=True)
                 vals.copy_(h_vals, non_blocking=True)
                 b.copy_(h_b, non_blocking=True)
-            solve_step()
+            solve_step("mixed")
             with torch.cuda.stream(stream):
                 h_x.copy_(x, non_blocking=True)
         ev1.record(stream)
         ev1.synchronize()
-        e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
-        if pg is not None:
-            t = torch.tensor([e2e_ms], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / e2e_steps)
         h2d = (h_rows.numel() * 4 + h_cols.numel() * 4 + h_vals.numel() * 8 + h_b.numel() * 8)
         d2h = h_x.numel() * 8
 
-    # ---- roofline of the dominant kernel (SpMV) --------------------------------------
+    # ---- roofline of the dominant kernel (the SpMV) -----------------------------------
     peak, peak_kind = _peaks()
-    spmv_avg_ms = tm["spmv_ms"] / max(tm["spmv_launches"], 1)
-    abytes = spmv_bytes(U, nb)
-    achieved = abytes / (spmv_avg_ms * 1e-3) / 1e9 if spmv_avg_ms > 0 else 0.0
+
+    def roof(mode, t):
+        avg_ms = t["spmv_ms"] / max(t["spmv_launches"], 1)
+        ab = spmv_bytes(U, nb, 8 if mode == "plain" else 4)
+        ach = ab / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+        return avg_ms, ab, ach
+
+    spmv_avg, abytes, achieved = roof("mixed", tm)
     traffic = None
     tr_path = os.path.join(ROOT, "profiles", "spmv_traffic.json")
     if os.path.exists(tr_path):
         try:
             tr = json.load(open(tr_path))
-            if tr.get("workload") == args.workload:
-                traffic = tr.get("bytes_per_launch")
+            traffic = tr.get(args.workload, {}).get("mixed")
         except Exception:
             pass
 
@@ -336,6 +348,13 @@ def main() -> None:
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "error": str(e)}
 
+    def stages(t, steps):
+        return {"assemble": t["assemble_ms"] / steps, "precond_build": t["precond_build_ms"] / steps,
+                "pcg": t["pcg_ms"] / steps, "spmv_avg": t["spmv_ms"] / max(t["spmv_launches"], 1),
+                "precond_apply_avg": t["precond_apply_ms"] / max(t["precond_apply_launches"], 1)}
+
+    pms, pstats, ptm, pclk = res["plain"]
+    p_avg, p_ab, p_ach = roof("plain", ptm)
     last = stats[-1]
     line = {
         "metric": METRIC,
@@ -348,22 +367,25 @@ def main() -> None:
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f32/bf16 (f64 dots, solution, residual replacement)",
         "data": "synthetic",
-        "mode": "plain",
+        "mode": "mixed",
         "config": {"workload": args.workload, "n_dof": 3 * s.n_verts, "n_triplets": s.n_triplets,
-                   "upper_blocks": U, "contacts": s.n_contacts, "precision": "fp64 (FP32 MAS inverses)",
-                   "preconditioner": "mas", "stop": "FP64-verified rel-res 1e-4", "parallelism": "replicas",
+                   "upper_blocks": U, "contacts": s.n_contacts, "preconditioner": "mas",
+                   "stop": "FP64-verified rel-res 1e-4", "warm_start": "zero", "parallelism": "replicas",
                    "l2": "inputs larger than L2 (matrix 0.33 GB, triplets 2.5 GB)"},
         "pcg_iterations": int(last["iterations_exact"]),
         "rel_res": float(last["rel_res"]),
-        "stages_ms": {"assemble": tm["assemble_ms"] / args.steps, "precond_build": tm["precond_build_ms"] / args.steps,
-                      "pcg": tm["pcg_ms"] / args.steps, "spmv_avg": spmv_avg_ms,
-                      "precond_apply_avg": tm["precond_apply_ms"] / max(tm["precond_apply_launches"], 1)},
+        "replacements": int(last["replacements"]),
+        "stages_ms": stages(tm, args.steps),
+        "plain": {"value": pms, "unit": "ms/solve", "dtype": "f64", "pcg_iterations": int(pstats[-1]["iterations_exact"]),
+                  "rel_res": float(pstats[-1]["rel_res"]), "stages_ms": stages(ptm, args.steps),
+                  "spmv_gbs": p_ach, "spmv_frac": p_ach / peak if peak else None, "clocks": pclk},
+        "speedup_vs_plain": pms / ms if ms > 0 else None,
         "gpu_launches": int(tm["kernel_launches"]),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
-                     "kernel": "k_spmv_sym_f64", "algorithmic_bytes": abytes, "peak_source": peak_kind},
+                     "kernel": "k_spmv_tile<float>", "algorithmic_bytes": abytes, "peak_source": peak_kind},
         "e2e": {"value": e2e_ms, "unit": "ms/solve", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "clocks": clk,
         "cpu_baseline": cpu,

@@ -97,6 +97,10 @@ int b2s_mas_get_hierarchy(b2s_solver* s, int32_t* h_level_begin, int32_t* h_leve
 /* Cluster matrices after b2s_precond_assemble: Galerkin matrices (FP64) and
  * inverses (FP32), 136 column-major 3x3 blocks per 16-node cluster. */
 int b2s_mas_get_clusters(b2s_solver* s, double* h_hess, float* h_inv);
+/* Node buffers of the last MAS apply (FP32, 3 per node slot, total_nodes
+ * slots): the restricted residual R of every coarse node and the local
+ * solution Z of every node. */
+int b2s_mas_get_nodes(b2s_solver* s, float* h_R, float* h_Z);
 
 /* Partition utility (the caller-side step of FEMMASPreconditioner::do_init):
  * recursive coordinate bisection into parts of at most max_part vertices,
@@ -125,6 +129,11 @@ int b2s_precond_assemble(b2s_solver* s, int kind, int invert_mode);
 /* z = P r (FP64 vectors). Replaces GlobalPreconditioner::do_apply
  * (global_preconditioner.h:17; mas_preconditioner_engine.cu:2887-2960). */
 int b2s_precond_apply(b2s_solver* s, const double* d_r, double* d_z);
+/* The same z = P r as the mixed-precision PCG applies it: FP32 vectors
+ * [3 * n_block_rows], MAS cluster inverses stored as BF16 of the
+ * diagonal-scaled inverse S M S (S = diag(M)^-1/2 in FP32), FP32 accumulation.
+ * No counterpart in the reference (which applies FP32 inverses only). */
+int b2s_precond_apply_mixed(b2s_solver* s, const float* d_r, float* d_z);
 
 /* ---- PCG ---------------------------------------------------------------------------
  * Replaces IterativeSolver::do_solve as implemented by LinearFusedPCG

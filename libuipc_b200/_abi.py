@@ -91,10 +91,12 @@ SIGNATURES = {
     "b2s_mas_info": (C.c_int, [vp, i32p, i32p]),
     "b2s_mas_get_hierarchy": (C.c_int, [vp, vp, vp, vp]),
     "b2s_mas_get_clusters": (C.c_int, [vp, vp, vp]),
+    "b2s_mas_get_nodes": (C.c_int, [vp, vp, vp]),
     "b2s_partition_rcb": (C.c_int, [i32, vp, i32, vp]),
     "b2s_partition_maps": (C.c_int, [i32, vp, i32, vp, vp, i32p]),
     "b2s_precond_assemble": (C.c_int, [vp, C.c_int, C.c_int]),
     "b2s_precond_apply": (C.c_int, [vp, vp, vp]),
+    "b2s_precond_apply_mixed": (C.c_int, [vp, vp, vp]),
     "b2s_pcg_default_options": (None, [C.POINTER(PcgOptions)]),
     "b2s_pcg": (C.c_int, [vp, vp, vp, C.POINTER(PcgOptions), C.POINTER(PcgStats)]),
     "b2s_set_timing": (C.c_int, [vp, C.c_int]),

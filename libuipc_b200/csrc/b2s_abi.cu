@@ -120,8 +120,7 @@ int b2s_destroy(b2s_solver* s)
         return B2S_OK;
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->stream);
-    if(s->pcg.graph)
-        cudaGraphExecDestroy(s->pcg.graph);
+    b2s::drop_graphs(s);
     if(s->pcg.h_sc)
         cudaFreeHost(s->pcg.h_sc);
     if(s->ev_begin)
@@ -145,11 +144,7 @@ int b2s_set_stream(b2s_solver* s, void* stream)
                    {
                        B2S_CUDA(cudaStreamSynchronize(s->stream));
                        s->stream = stream ? (cudaStream_t)stream : s->own_stream;
-                       if(s->pcg.graph)
-                       {
-                           cudaGraphExecDestroy(s->pcg.graph);
-                           s->pcg.graph = nullptr;
-                       }
+                       b2s::drop_graphs(s);
                    });
 }
 
@@ -278,6 +273,23 @@ int b2s_mas_get_clusters(b2s_solver* s, double* hess, float* inv)
                    });
 }
 
+int b2s_mas_get_nodes(b2s_solver* s, float* R, float* Z)
+{
+    return guarded(s,
+                   [&]
+                   {
+                       const b2s::MasState& M = s->mas;
+                       B2S_REQUIRE(M.initialized, B2S_ERR_STATE, "MAS not initialised");
+                       B2S_CUDA(cudaStreamSynchronize(s->stream));
+                       if(R)
+                           B2S_CUDA(cudaMemcpy(R, M.R.data(), sizeof(float) * 3 * (size_t)M.total,
+                                               cudaMemcpyDeviceToHost));
+                       if(Z)
+                           B2S_CUDA(cudaMemcpy(Z, M.Z.data(), sizeof(float) * 3 * (size_t)M.total,
+                                               cudaMemcpyDeviceToHost));
+                   });
+}
+
 int b2s_precond_assemble(b2s_solver* s, int kind, int invert_mode)
 {
     return guarded(s, [&]
@@ -291,6 +303,16 @@ int b2s_precond_apply(b2s_solver* s, const double* r, double* z)
                    {
                        B2S_REQUIRE(r && z, B2S_ERR_ARGUMENT, "null vector");
                        b2s::precond_apply(s, r, z);
+                   });
+}
+
+int b2s_precond_apply_mixed(b2s_solver* s, const float* r, float* z)
+{
+    return guarded(s,
+                   [&]
+                   {
+                       B2S_REQUIRE(r && z, B2S_ERR_ARGUMENT, "null vector");
+                       b2s::precond_apply_mixed(s, r, z);
                    });
 }
 
@@ -339,12 +361,8 @@ int b2s_set_timing(b2s_solver* s, int enable)
                            B2S_CUDA(cudaEventCreate(&s->ev_end));
                        }
                        s->timing = enable != 0;
-                       if(s->pcg.graph)
-                       {
-                           // the captured graph carries (or lacks) the event nodes
-                           cudaGraphExecDestroy(s->pcg.graph);
-                           s->pcg.graph = nullptr;
-                       }
+                       // the captured graphs carry (or lack) the event nodes
+                       b2s::drop_graphs(s);
                    });
 }
 

@@ -381,6 +381,7 @@ void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const in
     cudaStream_t     st = s->stream;
     AssemblyScratch& w  = s->asmb;
     M.valid             = false;
+    M.generation += 1;
     M.nb                = nb;
     w.err.resize(1);
     B2S_CUDA(cudaMemsetAsync(w.err.data(), 0, sizeof(int), st));

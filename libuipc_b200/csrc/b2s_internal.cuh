@@ -128,6 +128,8 @@ struct Matrix
     bool           has_trank = false;
     DBuf<int32_t>  diag_index;  // [nb] position of block (i,i), -1 if absent
     bool           valid = false;
+    long long      generation = 0;         // bumped by every assembly
+    long long      vals32_generation = -1;  // assembly the FP32 planes were made from
 };
 
 // scratch of the assembly pipeline (reused across calls)
@@ -162,6 +164,8 @@ struct MasState
     // per assembly
     DBuf<double>  hess;            // [clusters * 136 * 9]
     DBuf<float>   inv;             // [clusters * 136 * 9]
+    DBuf<unsigned char> inv16;     // [clusters * 2640]: FP32 scale S (48) + BF16(S inv S)
+    long long     inv16_generation = -1;  // assembly generation inv16 was packed from
     // coarse-level Galerkin matrices (upper BCOO per level, in level-local ids)
     Matrix        coarse[MAX_LEVELS];
     DBuf<int32_t> trip_rows, trip_cols;
@@ -207,6 +211,11 @@ struct PcgState
     cudaGraphExec_t  graph = nullptr;
     size_t           graph_key = 0;
     long long        graph_kernels = 0;  // kernel nodes per graph launch
+    // mixed precision: FP32 recursion vectors and their own graph
+    DBuf<float>      r32, z32, p32, Ap32;
+    cudaGraphExec_t  graph_mixed = nullptr;
+    size_t           graph_mixed_key = 0;
+    long long        graph_mixed_kernels = 0;
 };
 
 }  // namespace b2s
@@ -224,6 +233,7 @@ struct b2s_solver
     b2s::PcgState        pcg;
     int                  precond_kind = -1;
     int                  invert_mode  = 0;
+    long long            precond_generation = 0;  // bumped by every preconditioner build
     b2s::DBuf<double>    dinv;  // [nb*9] row-major inverses of diagonal blocks
     b2s::DBuf<double>    dot_out;
     b2s::Reduction       red;
@@ -259,6 +269,7 @@ void launch_dot(b2s_solver* s, const double* a, const double* b, int64_t n, doub
 // preconditioners
 void precond_assemble(b2s_solver* s, int kind, int invert_mode);
 void precond_apply(b2s_solver* s, const double* r, double* z);
+void precond_apply_mixed(b2s_solver* s, const float* r, float* z);
 void check_device_errors(b2s_solver* s);
 
 // message of the last failed call made without a solver handle (read back
@@ -271,6 +282,7 @@ void mas_apply(b2s_solver* s, const double* r, double* z);
 
 // PCG
 void pcg_solve(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st);
+void drop_graphs(b2s_solver* s);
 
 inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
 }  // namespace b2s

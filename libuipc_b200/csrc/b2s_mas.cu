@@ -25,6 +25,8 @@
 #include "b2s_reduce.cuh"
 #include "b2s_tma.cuh"
 
+#include <cuda_bf16.h>
+
 #include <algorithm>
 
 namespace b2s
@@ -440,6 +442,88 @@ __global__ void __launch_bounds__(INV_BLOCK) k_invert(int clusters, const double
 // ---------------------------------------------------------------------------
 constexpr int APPLY_WARPS = 4;
 constexpr uint32_t INV_BYTES = SYM * 9 * sizeof(float);  // 4896, a multiple of 16
+// mixed precision: per cluster the FP32 diagonal factor D = diag(M)^1/2 (48
+// floats) then the BF16 entries of D^-1 M D^-1 in the same upper-block
+// layout: 192 + 2448 = 2640 B
+constexpr uint32_t INV16_SCALE_BYTES = BANK * 3 * sizeof(float);
+constexpr uint32_t INV16_BYTES       = INV16_SCALE_BYTES + SYM * 9 * 2;
+
+// Z = D (M_s (D r)) for the BF16 diagonal-scaled storage, M_s = D^-1 M D^-1
+// (FP32 accumulation)
+__device__ __forceinline__ void cluster_product_bf16(const unsigned char* slot, const float (*r)[3], int lane,
+                                                     float out[3])
+{
+    const float*          S  = reinterpret_cast<const float*>(slot);  // D
+    const __nv_bfloat16*  Mh = reinterpret_cast<const __nv_bfloat16*>(slot + INV16_SCALE_BYTES);
+    const int rn = lane & 15, c0 = (lane >> 4) * 8;
+    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
+#pragma unroll
+    for(int cc = 0; cc < 8; ++cc)
+    {
+        const int   cn = c0 + cc;
+        const float x0 = r[cn][0] * S[cn * 3], x1 = r[cn][1] * S[cn * 3 + 1], x2 = r[cn][2] * S[cn * 3 + 2];
+        float       B[9];
+        const bool  up = cn >= rn;
+        const __nv_bfloat16* src = Mh + (up ? sym_index(rn, cn) : sym_index(cn, rn)) * 9;
+#pragma unroll
+        for(int q = 0; q < 9; ++q)
+            B[q] = __bfloat162float(src[q]);
+        if(up)
+        {
+            acc0 = __fmaf_rn(B[0], x0, acc0); acc0 = __fmaf_rn(B[3], x1, acc0); acc0 = __fmaf_rn(B[6], x2, acc0);
+            acc1 = __fmaf_rn(B[1], x0, acc1); acc1 = __fmaf_rn(B[4], x1, acc1); acc1 = __fmaf_rn(B[7], x2, acc1);
+            acc2 = __fmaf_rn(B[2], x0, acc2); acc2 = __fmaf_rn(B[5], x1, acc2); acc2 = __fmaf_rn(B[8], x2, acc2);
+        }
+        else
+        {
+            acc0 = __fmaf_rn(B[0], x0, acc0); acc0 = __fmaf_rn(B[1], x1, acc0); acc0 = __fmaf_rn(B[2], x2, acc0);
+            acc1 = __fmaf_rn(B[3], x0, acc1); acc1 = __fmaf_rn(B[4], x1, acc1); acc1 = __fmaf_rn(B[5], x2, acc1);
+            acc2 = __fmaf_rn(B[6], x0, acc2); acc2 = __fmaf_rn(B[7], x1, acc2); acc2 = __fmaf_rn(B[8], x2, acc2);
+        }
+    }
+    acc0 += __shfl_down_sync(0xffffffffu, acc0, 16);
+    acc1 += __shfl_down_sync(0xffffffffu, acc1, 16);
+    acc2 += __shfl_down_sync(0xffffffffu, acc2, 16);
+    out[0] = acc0 * S[rn * 3];
+    out[1] = acc1 * S[rn * 3 + 1];
+    out[2] = acc2 * S[rn * 3 + 2];
+}
+
+// pack the FP32 inverse M of every cluster as D (FP32) + BF16(D^-1 M D^-1),
+// D = diag(M)^1/2: the stored matrix has a unit diagonal, so BF16 rounds every
+// entry relative to O(1), and M = D (D^-1 M D^-1) D is recovered in the apply
+__global__ void k_pack_inverse_bf16(int clusters, const float* __restrict__ inv, unsigned char* __restrict__ out)
+{
+    const int c = blockIdx.x;
+    if(c >= clusters)
+        return;
+    __shared__ float S[BANK * 3];  // 1 / D
+    const float* M = inv + (size_t)c * SYM * 9;
+    unsigned char* o = out + (size_t)c * INV16_BYTES;
+    if(threadIdx.x < BANK * 3)
+    {
+        const int   nd = threadIdx.x / 3, a = threadIdx.x % 3;
+        const float d  = M[sym_index(nd, nd) * 9 + a * 3 + a];
+        const float Dv = d > 0.f ? sqrtf(d) : 1.0f;
+        S[threadIdx.x] = 1.0f / Dv;
+        reinterpret_cast<float*>(o)[threadIdx.x] = Dv;
+    }
+    __syncthreads();
+    __nv_bfloat16* Mh = reinterpret_cast<__nv_bfloat16*>(o + INV16_SCALE_BYTES);
+    for(int e = threadIdx.x; e < SYM * 9; e += blockDim.x)
+    {
+        // block si = e / 9 is (rn, cn) with rn <= cn; entry (p, q) column-major
+        const int si = e / 9, q = (e % 9) / 3, p = e % 3;
+        int       rn = 0, rem = si;
+        while(rem >= BANK - rn)
+        {
+            rem -= BANK - rn;
+            ++rn;
+        }
+        const int cn = rn + rem;
+        Mh[e]        = __float2bfloat16_rn(M[e] * S[rn * 3 + p] * S[cn * 3 + q]);
+    }
+}
 
 __device__ __forceinline__ void cluster_product(const float* M, const float (*r)[3], int lane, float out[3])
 {
@@ -479,16 +563,19 @@ __device__ __forceinline__ void cluster_product(const float* M, const float (*r)
 // buffer. With `push`, the restriction sums of the next level (one per
 // connected component of the bank, summed by its lowest lane in lane order)
 // are written to R_{l+1}. Z_l = A_l^{-1} R_l for every node of the bank.
-template <bool FINE, typename VT>
+// BF: the inverse is stored as S + BF16(S M S) (INV16_BYTES per cluster),
+// otherwise FP32 (INV_BYTES per cluster). VT: type of the fine residual.
+template <bool FINE, typename VT, bool BF>
 __global__ void __launch_bounds__(APPLY_WARPS * 32)
     k_apply_level(int n_banks, int cnt, int level_begin, const int32_t* __restrict__ p2r, const VT* __restrict__ r,
                   int off3, const uint16_t* __restrict__ comp_mask, const int32_t* __restrict__ new_local,
-                  int next_begin, int push, const float* __restrict__ inv, float* R, float* __restrict__ Z,
+                  int next_begin, int push, const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
                   const int* converged, int* err)
 {
     if(converged && *converged)
         return;
-    __shared__ __align__(128) float s_inv[APPLY_WARPS][2][SYM * 9];
+    constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
+    __shared__ __align__(128) unsigned char s_inv[APPLY_WARPS][2][INV_BYTES];
     __shared__ float    s_r[APPLY_WARPS][BANK][3];
     __shared__ uint64_t s_bar[APPLY_WARPS][2];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -502,9 +589,8 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
         mbar_fence_init();
         for(int j = 0; j < mine && j < 2; ++j)
         {
-            mbar_arrive_expect_tx(&s_bar[w][j], INV_BYTES);
-            bulk_copy_g2s(s_inv[w][j], inv + (size_t)(gbank0 + gw + (int64_t)j * W) * SYM * 9, INV_BYTES,
-                          &s_bar[w][j]);
+            mbar_arrive_expect_tx(&s_bar[w][j], CB);
+            bulk_copy_g2s(s_inv[w][j], inv + (size_t)(gbank0 + gw + (int64_t)j * W) * CB, CB, &s_bar[w][j]);
         }
     }
     __syncwarp();
@@ -569,7 +655,10 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
         if(!__all_sync(0xffffffffu, ok))
             break;
         float out[3];
-        cluster_product(s_inv[w][slot], s_r[w], lane, out);
+        if(BF)
+            cluster_product_bf16(s_inv[w][slot], s_r[w], lane, out);
+        else
+            cluster_product(reinterpret_cast<const float*>(s_inv[w][slot]), s_r[w], lane, out);
         if(lane < 16)
         {
             const int64_t g = (int64_t)level_begin + node;
@@ -581,9 +670,8 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
         if(lane == 0 && j + 2 < mine)
         {
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&s_bar[w][slot], INV_BYTES);
-            bulk_copy_g2s(s_inv[w][slot], inv + (size_t)(gbank0 + bank + 2 * (int64_t)W) * SYM * 9, INV_BYTES,
-                          &s_bar[w][slot]);
+            mbar_arrive_expect_tx(&s_bar[w][slot], CB);
+            bulk_copy_g2s(s_inv[w][slot], inv + (size_t)(gbank0 + bank + 2 * (int64_t)W) * CB, CB, &s_bar[w][slot]);
         }
     }
     if(j < mine && lane == 0)
@@ -820,20 +908,23 @@ void mas_assemble(b2s_solver* s, int invert_mode)
 }
 
 // z[off..off+vn) gets the MAS part of z = P r; Jacobi/identity elsewhere is
-// handled by the caller (collect kernel in the PCG, or precond_apply)
-void mas_apply_levels(b2s_solver* s, const double* r, const int* converged)
+// handled by the caller (collect kernel in the PCG, or precond_apply).
+// bf16: use the packed S + BF16(S M S) inverses (mas_pack_bf16 first).
+template <typename VT>
+static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, bool bf16)
 {
-    MasState&    M  = s->mas;
-    MasState&    X  = s->mas;
-    cudaStream_t st = s->stream;
+    MasState&    M   = s->mas;
+    cudaStream_t st  = s->stream;
     int*         err = device_error_flag(s);
     const int    n_banks0 = M.N / BANK;
     const int    tb       = APPLY_WARPS * 32;
+    const unsigned char* inv = bf16 ? M.inv16.data() : reinterpret_cast<const unsigned char*>(M.inv.data());
     if(n_banks0 > 0)
     {
-        k_apply_level<true, double><<<apply_grid(n_banks0), tb, 0, st>>>(
-            n_banks0, M.N, 0, M.p2r.data(), r, 3 * M.offset, X.comp_mask[0].data(), X.new_local[0].data(),
-            M.level_begin[1], M.L > 1 ? 1 : 0, M.inv.data(), M.R.data(), M.Z.data(), converged, err);
+        auto k = bf16 ? k_apply_level<true, VT, true> : k_apply_level<true, VT, false>;
+        k<<<apply_grid(n_banks0), tb, 0, st>>>(n_banks0, M.N, 0, M.p2r.data(), r, 3 * M.offset,
+                                               M.comp_mask[0].data(), M.new_local[0].data(), M.level_begin[1],
+                                               M.L > 1 ? 1 : 0, inv, M.R.data(), M.Z.data(), converged, err);
         B2S_CHECK_LAUNCH();
     }
     for(int level = 1; level < M.L; ++level)
@@ -843,10 +934,33 @@ void mas_apply_levels(b2s_solver* s, const double* r, const int* converged)
             break;
         const int n_banks = (cnt + BANK - 1) / BANK;
         const int push    = level + 1 < M.L ? 1 : 0;
-        k_apply_level<false, double><<<apply_grid(n_banks), tb, 0, st>>>(
-            n_banks, cnt, M.level_begin[level], nullptr, nullptr, 0, X.comp_mask[level].data(),
-            X.new_local[level].data(), push ? M.level_begin[level + 1] : 0, push, M.inv.data(), M.R.data(),
-            M.Z.data(), converged, err);
+        auto k = bf16 ? k_apply_level<false, VT, true> : k_apply_level<false, VT, false>;
+        k<<<apply_grid(n_banks), tb, 0, st>>>(n_banks, cnt, M.level_begin[level], nullptr, nullptr, 0,
+                                              M.comp_mask[level].data(), M.new_local[level].data(),
+                                              push ? M.level_begin[level + 1] : 0, push, inv, M.R.data(),
+                                              M.Z.data(), converged, err);
+        B2S_CHECK_LAUNCH();
+    }
+}
+
+void mas_apply_levels(b2s_solver* s, const double* r, const int* converged)
+{
+    apply_levels_t<double>(s, r, converged, false);
+}
+
+void mas_apply_levels_f32(b2s_solver* s, const float* r, const int* converged, bool bf16)
+{
+    apply_levels_t<float>(s, r, converged, bf16);
+}
+
+// BF16 diagonal-scaled copy of the current FP32 inverses
+void mas_pack_bf16(b2s_solver* s)
+{
+    MasState& M = s->mas;
+    M.inv16.resize((size_t)M.clusters * INV16_BYTES);
+    if(M.clusters > 0)
+    {
+        k_pack_inverse_bf16<<<M.clusters, 128, 0, s->stream>>>(M.clusters, M.inv.data(), M.inv16.data());
         B2S_CHECK_LAUNCH();
     }
 }

@@ -16,7 +16,9 @@
 #include "b2s_reduce.cuh"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 
 namespace b2s
 {
@@ -27,6 +29,11 @@ void check_device_errors(b2s_solver* s);
 int  spmv_grid(int64_t U);
 void ensure_reduction(Reduction& red, int grid, int nv);
 void mas_apply_levels(b2s_solver* s, const double* r, const int* converged);
+void mas_apply_levels_f32(b2s_solver* s, const float* r, const int* converged, bool bf16);
+void mas_pack_bf16(b2s_solver* s);
+void spmv_f32_launch(b2s_solver* s, const Matrix& A, const float* x, float* y, Reduction& red, double* d_dot,
+                     const int* stop);
+void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st_out);
 
 namespace
 {
@@ -95,7 +102,8 @@ struct MasView
 
 // z_i for block row i: MAS (partitioned vertices of its range), else 3x3
 // block Jacobi (kind 1 / 2), else identity (kind 0)
-__device__ __forceinline__ void precond_row(int kind, const MasView& mv, const double* dinv, const double* r, int i,
+template <typename VT>
+__device__ __forceinline__ void precond_row(int kind, const MasView& mv, const double* dinv, const VT* r, int i,
                                             double z[3])
 {
     const double r0 = r[3 * (int64_t)i], r1 = r[3 * (int64_t)i + 1], r2 = r[3 * (int64_t)i + 2];
@@ -135,11 +143,12 @@ __device__ __forceinline__ void precond_row(int kind, const MasView& mv, const d
     z[2] = D[6] * r0 + D[7] * r1 + D[8] * r2;
 }
 
-// z = P r for every block row; with `sc`, also r.z and r.r and the scalar
-// update of the iteration (last block)
+// z = P r for every block row; with `sc`, also r.z and r.r (FP64 sums) and
+// the scalar update of the iteration (last block). VT: vector storage type.
+template <typename VT>
 __global__ void __launch_bounds__(RED_BLOCK) k_precond_finish(int32_t nb, int kind, MasView mv,
                                                               const double* __restrict__ dinv,
-                                                              const double* __restrict__ r, double* __restrict__ z,
+                                                              const VT* __restrict__ r, VT* __restrict__ z,
                                                               PcgScalars* sc, double* partials,
                                                               unsigned int* counter)
 {
@@ -149,14 +158,15 @@ __global__ void __launch_bounds__(RED_BLOCK) k_precond_finish(int32_t nb, int ki
     for(int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < nb; i += gridDim.x * RED_BLOCK)
     {
         double zi[3];
-        precond_row(kind, mv, dinv, r, i, zi);
-        z[3 * (int64_t)i]     = zi[0];
-        z[3 * (int64_t)i + 1] = zi[1];
-        z[3 * (int64_t)i + 2] = zi[2];
+        precond_row<VT>(kind, mv, dinv, r, i, zi);
+        const VT z0 = (VT)zi[0], z1 = (VT)zi[1], z2 = (VT)zi[2];
+        z[3 * (int64_t)i]     = z0;
+        z[3 * (int64_t)i + 1] = z1;
+        z[3 * (int64_t)i + 2] = z2;
         if(sc)
         {
             const double r0 = r[3 * (int64_t)i], r1 = r[3 * (int64_t)i + 1], r2 = r[3 * (int64_t)i + 2];
-            rz += r0 * zi[0] + r1 * zi[1] + r2 * zi[2];
+            rz += r0 * (double)z0 + r1 * (double)z1 + r2 * (double)z2;
             rr += r0 * r0 + r1 * r1 + r2 * r2;
         }
     }
@@ -213,6 +223,69 @@ __global__ void k_update_p(int64_t n, const PcgScalars* sc, const double* __rest
         p[i] = z[i] + beta * p[i];
 }
 
+// ---- mixed precision (FP32 vectors, FP64 solution and scalars) ----------------
+__global__ void k_update_xr_mixed(int64_t n, PcgScalars* sc, double* __restrict__ x, const float* __restrict__ p,
+                                  float* __restrict__ r, float* __restrict__ Ap)
+{
+    if(frozen(sc))
+        return;
+    const double alpha = sc->rz / sc->pAp;
+    if(blockIdx.x == 0 && threadIdx.x == 0)
+        sc->alpha = alpha;
+    const float af = (float)alpha;
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
+    {
+        const float api = Ap[i];
+        x[i] += alpha * (double)p[i];
+        r[i] = __fmaf_rn(-af, api, r[i]);
+        Ap[i] = 0.0f;
+    }
+}
+
+__global__ void k_update_p_mixed(int64_t n, const PcgScalars* sc, const float* __restrict__ z, float* __restrict__ p)
+{
+    if(frozen(sc))
+        return;
+    const float beta = (float)sc->beta;
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
+        p[i] = __fmaf_rn(beta, p[i], z[i]);
+}
+
+// r32 = b - Ax computed in FP64, stored FP32
+__global__ void k_residual_f32(int64_t n, const double* __restrict__ b, const double* __restrict__ Ax,
+                               float* __restrict__ r)
+{
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
+        r[i] = (float)(b[i] - Ax[i]);
+}
+
+// FP32 vectors, FP64 sums: out[0] = a.b, out[1] = a.a
+__global__ void __launch_bounds__(RED_BLOCK) k_dot2_f32(int64_t n, const float* __restrict__ a,
+                                                        const float* __restrict__ b, double* partials,
+                                                        unsigned int* counter, double* out)
+{
+    double ab = 0.0, aa = 0.0;
+    for(int64_t i = (int64_t)blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_BLOCK)
+    {
+        const double ai = a[i];
+        ab += ai * (double)b[i];
+        aa += ai * ai;
+    }
+    double v[2] = {ab, aa}, tot[2];
+    if(grid_sum<2>(v, partials, counter, tot))
+    {
+        out[0] = tot[0];
+        out[1] = tot[1];
+    }
+}
+
+// FP32 copy of the value planes (mixed-precision SpMV)
+__global__ void k_planes_f32(int64_t count, const double* __restrict__ src, float* __restrict__ dst)
+{
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < count; i += (int64_t)gridDim.x * VEC_BLOCK)
+        dst[i] = (float)src[i];
+}
+
 __global__ void k_residual(int64_t n, const double* __restrict__ b, const double* __restrict__ Ax,
                            double* __restrict__ r)
 {
@@ -264,6 +337,7 @@ void precond_assemble(b2s_solver* s, int kind, int invert_mode)
         mas_assemble(s, invert_mode);
     }
     s->precond_kind = kind;
+    s->precond_generation += 1;
     s->invert_mode  = invert_mode;
     B2S_CUDA(cudaStreamSynchronize(st));
 }
@@ -293,7 +367,7 @@ static void precond_launch(b2s_solver* s, int kind, const double* r, double* z, 
         mas_apply_levels(s, r, sc ? &sc->converged : nullptr);
     const int grid = reduction_grid();
     ensure_reduction(red, grid, 2);
-    k_precond_finish<<<grid, RED_BLOCK, 0, st>>>(nb, kind, mas_view(s), s->dinv.data(), r, z, sc,
+    k_precond_finish<double><<<grid, RED_BLOCK, 0, st>>>(nb, kind, mas_view(s), s->dinv.data(), r, z, sc,
                                                  red.partials.data(), red.counter.data());
     B2S_CHECK_LAUNCH();
 }
@@ -358,7 +432,13 @@ void pcg_solve(b2s_solver* s, const double* b, double* x, const b2s_pcg_options&
 {
     B2S_REQUIRE(s->A.valid, B2S_ERR_STATE, "b2s_pcg before b2s_assemble");
     B2S_REQUIRE(s->precond_kind >= 0, B2S_ERR_STATE, "b2s_pcg before b2s_precond_assemble");
-    B2S_REQUIRE(o.precision == B2S_PRECISION_FP64, B2S_ERR_ARGUMENT, "this entry point runs the FP64 path");
+    B2S_REQUIRE(o.precision == B2S_PRECISION_FP64 || o.precision == B2S_PRECISION_MIXED, B2S_ERR_ARGUMENT,
+                "unknown precision");
+    if(o.precision == B2S_PRECISION_MIXED)
+    {
+        pcg_solve_mixed(s, b, x, o, st_out);
+        return;
+    }
     B2S_REQUIRE(o.tol > 0.0 && std::isfinite(o.tol), B2S_ERR_ARGUMENT, "tolerance must be positive");
     B2S_REQUIRE(o.stop_rule == B2S_STOP_RZ || o.stop_rule == B2S_STOP_RELRES, B2S_ERR_ARGUMENT, "unknown stop rule");
     cudaStream_t  st = s->stream;
@@ -571,6 +651,325 @@ void pcg_solve(b2s_solver* s, const double* b, double* x, const b2s_pcg_options&
             h.rz = rz;
             done = false;
         }
+    }
+    st_out.replacements = replacements;
+    check_device_errors(s);
+    if(st_out.converged)
+        st_out.iterations = ci > 1 ? std::min<int64_t>(((st_out.iterations_exact + ci - 1) / ci) * ci, max_iter)
+                                   : st_out.iterations_exact;
+    else
+        st_out.iterations = max_iter;
+}
+
+// ---------------------------------------------------------------------------
+// mixed precision PCG
+// ---------------------------------------------------------------------------
+void drop_graphs(b2s_solver* s)
+{
+    if(s->pcg.graph)
+        cudaGraphExecDestroy(s->pcg.graph);
+    if(s->pcg.graph_mixed)
+        cudaGraphExecDestroy(s->pcg.graph_mixed);
+    s->pcg.graph       = nullptr;
+    s->pcg.graph_mixed = nullptr;
+}
+
+// storage of the MAS inverses in the mixed path: BF16 diagonal-scaled
+// (default) or FP32, from B2S_MIXED_MAS_INVERSE=bf16|fp32, read once
+static bool mixed_inverse_bf16()
+{
+    static const bool v = []
+    {
+        const char* e = std::getenv("B2S_MIXED_MAS_INVERSE");
+        return !(e && std::string(e) == "fp32");
+    }();
+    return v;
+}
+
+// z = P r on FP32 vectors (MAS with BF16 inverses), optionally fused with the
+// iteration's dots and scalar update
+static void precond_launch_f32(b2s_solver* s, int kind, const float* r, float* z, PcgScalars* sc, Reduction& red)
+{
+    const int32_t nb = s->A.nb;
+    if(nb == 0)
+        return;
+    if(kind == B2S_PRECOND_MAS)
+        mas_apply_levels_f32(s, r, sc ? &sc->converged : nullptr, mixed_inverse_bf16());
+    const int grid = reduction_grid();
+    ensure_reduction(red, grid, 2);
+    k_precond_finish<float><<<grid, RED_BLOCK, 0, s->stream>>>(nb, kind, mas_view(s), s->dinv.data(), r, z, sc,
+                                                               red.partials.data(), red.counter.data());
+    B2S_CHECK_LAUNCH();
+}
+
+static void ensure_bf16_inverses(b2s_solver* s)
+{
+    if(s->precond_kind == B2S_PRECOND_MAS && s->mas.inv16_generation != s->precond_generation)
+    {
+        mas_pack_bf16(s);
+        s->mas.inv16_generation = s->precond_generation;
+    }
+}
+
+void precond_apply_mixed(b2s_solver* s, const float* r, float* z)
+{
+    B2S_REQUIRE(s->precond_kind >= 0, B2S_ERR_STATE, "precond_apply before b2s_precond_assemble");
+    ensure_bf16_inverses(s);
+    ensure_reduction(s->red, reduction_grid(), 2);
+    precond_launch_f32(s, s->precond_kind, r, z, nullptr, s->red);
+    check_device_errors(s);
+}
+
+static void pcg_iteration_mixed(b2s_solver* s, int kind, double* x, int slot)
+{
+    PcgState&     P  = s->pcg;
+    const Matrix& A  = s->A;
+    cudaStream_t  st = s->stream;
+    const int64_t n  = 3 * (int64_t)A.nb;
+    cudaEvent_t*  ev = s->timing ? &s->iter_events[(size_t)slot * 4] : nullptr;
+    if(ev)
+        B2S_CUDA(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
+    spmv_f32_launch(s, A, P.p32.data(), P.Ap32.data(), P.red, &P.sc.data()->pAp, &P.sc.data()->converged);
+    if(ev)
+        B2S_CUDA(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
+    k_update_xr_mixed<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), x, P.p32.data(), P.r32.data(),
+                                                         P.Ap32.data());
+    B2S_CHECK_LAUNCH();
+    if(ev)
+        B2S_CUDA(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
+    precond_launch_f32(s, kind, P.r32.data(), P.z32.data(), P.sc.data(), P.red);
+    if(ev)
+        B2S_CUDA(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
+    k_update_p_mixed<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), P.z32.data(), P.p32.data());
+    B2S_CHECK_LAUNCH();
+}
+
+// Mixed precision: the matrix in FP32 (planes converted once per assembly),
+// r, z, p, Ap in FP32, the solution x and every scalar (alpha, beta, r.z,
+// p.Ap, r.r) in FP64, MAS inverses as BF16 of the diagonal-scaled inverse
+// with FP32 accumulation. Every `replace_every` iterations the recursive
+// residual is replaced by b - A x computed in FP64 with the FP64 matrix
+// (p, z and r.z are kept: a reliable update); the stop is always confirmed
+// by the FP64 residual, and a stop the FP64 residual does not confirm
+// continues from the true residual (with p = z).
+void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st_out)
+{
+    cudaStream_t st = s->stream;
+    Matrix&      A  = s->A;
+    PcgState&    P  = s->pcg;
+    const int64_t n = 3 * (int64_t)A.nb;
+    std::memset(&st_out, 0, sizeof(st_out));
+    if(n == 0)
+    {
+        st_out.converged = 1;
+        return;
+    }
+    P.r32.resize(n, 1.1);
+    P.z32.resize(n, 1.1);
+    P.p32.resize(n, 1.1);
+    P.Ap32.resize(n, 1.1);
+    P.tmp.resize(n, 1.1);
+    P.sc.resize(1);
+    if(!P.h_sc)
+        B2S_CUDA(cudaMallocHost(&P.h_sc, sizeof(PcgScalars)));
+    ensure_reduction(P.red, std::max(spmv_grid(A.nnz), reduction_grid()), 2);
+    ensure_reduction(s->red, reduction_grid(), 2);
+    device_error_flag(s);
+    s->dot_out.resize(4);
+    B2S_REQUIRE(A.nnz == 0 || A.has_trank, B2S_ERR_STATE, "matrix lacks the SpMV tile ranks");
+    const int     ci       = o.check_interval > 0 ? o.check_interval : 1;
+    const int64_t max_iter = o.max_iter > 0 ? o.max_iter : std::max<int64_t>(2 * n, 1);
+    int           kind     = s->precond_kind;
+
+    // FP32 matrix planes, BF16 MAS inverses (once per assembly / build)
+    if(A.vals32_generation != A.generation)
+    {
+        A.vals32.resize((size_t)9 * A.stride, 1.2);
+        k_planes_f32<<<vec_grid(9 * A.stride), VEC_BLOCK, 0, st>>>(9 * A.stride, A.vals.data(), A.vals32.data());
+        B2S_CHECK_LAUNCH();
+        A.vals32_generation = A.generation;
+    }
+    ensure_bf16_inverses(s);
+
+    // r = b - A x0 (FP64), stored FP32
+    if(o.x0_given)
+        spmv_f64(s, A, x, P.tmp.data(), nullptr);
+    else
+    {
+        B2S_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+        B2S_CUDA(cudaMemsetAsync(P.tmp.data(), 0, sizeof(double) * n, st));
+    }
+    k_residual_f32<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, b, P.tmp.data(), P.r32.data());
+    B2S_CHECK_LAUNCH();
+
+    auto restart_from_r = [&](int k) -> double
+    {
+        // z = P r, p = z; returns r.z (FP64 sum); also leaves r.r in dot_out[1]
+        precond_launch_f32(s, k, P.r32.data(), P.z32.data(), nullptr, s->red);
+        k_dot2_f32<<<reduction_grid(), RED_BLOCK, 0, st>>>(n, P.r32.data(), P.z32.data(), s->red.partials.data(),
+                                                            s->red.counter.data(), s->dot_out.data());
+        B2S_CHECK_LAUNCH();
+        B2S_CUDA(cudaMemcpyAsync(P.p32.data(), P.z32.data(), sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        double h2[2];
+        B2S_CUDA(cudaMemcpyAsync(h2, s->dot_out.data(), sizeof(h2), cudaMemcpyDeviceToHost, st));
+        B2S_CUDA(cudaStreamSynchronize(st));
+        return h2[0];
+    };
+    launch_dot(s, b, b, n, s->dot_out.data() + 2);
+    double bb = 0.0;
+    B2S_CUDA(cudaMemcpyAsync(&bb, s->dot_out.data() + 2, sizeof(double), cudaMemcpyDeviceToHost, st));
+    double rz0 = restart_from_r(kind);
+    B2S_REQUIRE(std::isfinite(bb), B2S_ERR_NUMERIC, "non-finite right-hand side");
+    bool bypass = false;
+    if(kind != B2S_PRECOND_NONE && (rz0 < 0.0 || !std::isfinite(rz0)))
+    {
+        bypass = true;  // PSD guard: plain CG
+        kind   = B2S_PRECOND_NONE;
+        rz0    = restart_from_r(kind);
+    }
+    st_out.rz0      = rz0;
+    st_out.bypassed = bypass ? 1 : 0;
+    const double bnorm = std::sqrt(bb);
+    auto true_residual = [&]() -> double
+    {
+        spmv_f64(s, A, x, P.tmp.data(), nullptr);
+        k_res_norms<<<reduction_grid(), RED_BLOCK, 0, st>>>(n, b, P.tmp.data(), s->red.partials.data(),
+                                                            s->red.counter.data(), s->dot_out.data());
+        B2S_CHECK_LAUNCH();
+        double h2[2];
+        B2S_CUDA(cudaMemcpyAsync(h2, s->dot_out.data(), sizeof(h2), cudaMemcpyDeviceToHost, st));
+        B2S_CUDA(cudaStreamSynchronize(st));
+        return h2[1] > 0 ? std::sqrt(h2[0] / h2[1]) : 0.0;
+    };
+    auto replace_residual = [&]()
+    {
+        spmv_f64(s, A, x, P.tmp.data(), nullptr);
+        k_residual_f32<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, b, P.tmp.data(), P.r32.data());
+        B2S_CHECK_LAUNCH();
+    };
+    if(rz0 == 0.0 || bb == 0.0)
+    {
+        st_out.converged = 1;
+        st_out.rel_res   = true_residual();
+        return;
+    }
+
+    PcgScalars h{};
+    h.rz        = rz0;
+    h.rz_tol    = o.tol * std::fabs(rz0);
+    h.rr_tol    = (o.tol * bnorm) * (o.tol * bnorm);
+    h.stop_rule = o.stop_rule;
+    h.max_iter  = max_iter;
+    int64_t iter_total = 0, replacements = 0, last_replace = 0;
+    bool    done = false;
+    while(!done)
+    {
+        h.converged = 0;
+        h.iter      = iter_total;
+        h.iter_conv = 0;
+        B2S_CUDA(cudaMemcpyAsync(P.sc.data(), &h, sizeof(h), cudaMemcpyHostToDevice, st));
+        B2S_CUDA(cudaMemsetAsync(P.Ap32.data(), 0, sizeof(float) * n, st));
+        bool use_graph = o.use_graph && st != nullptr;
+        if(s->timing)
+            ensure_iter_events(s, ci);
+        if(use_graph)
+        {
+            const void*   ptrs[10] = {x,          A.vals32.data(), A.rows.data(),     P.r32.data(),
+                                      s->mas.inv16.data(), s->dinv.data(), P.red.partials.data(), s->mas.Z.data(),
+                                      A.cols.data(), P.p32.data()};
+            const int64_t ints[6]  = {A.nnz, A.nb, kind, ci, s->mas.initialized ? s->mas.total : -1,
+                                      s->mas.L + (s->timing ? 1000 : 0)};
+            size_t hk = 1469598103934665603ull;
+            for(const void* q : ptrs)
+                hk = (hk ^ (size_t)q) * 1099511628211ull;
+            for(int64_t q : ints)
+                hk = (hk ^ (size_t)q) * 1099511628211ull;
+            if(!P.graph_mixed || P.graph_mixed_key != hk)
+            {
+                if(P.graph_mixed)
+                {
+                    cudaGraphExecDestroy(P.graph_mixed);
+                    P.graph_mixed = nullptr;
+                }
+                cudaGraph_t     g      = nullptr;
+                const long long before = g_kernel_launches;
+                B2S_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                for(int it = 0; it < ci; ++it)
+                    pcg_iteration_mixed(s, kind, x, it);
+                B2S_CUDA(cudaStreamEndCapture(st, &g));
+                P.graph_mixed_kernels = g_kernel_launches - before;
+                g_kernel_launches     = before;
+                cudaError_t e         = cudaGraphInstantiate(&P.graph_mixed, g, 0);
+                cudaGraphDestroy(g);
+                if(e != cudaSuccess)
+                {
+                    P.graph_mixed = nullptr;
+                    use_graph     = false;
+                    cudaGetLastError();
+                }
+                else
+                    P.graph_mixed_key = hk;
+            }
+        }
+        long long iter_before = h.iter;
+        while(true)
+        {
+            if(use_graph)
+            {
+                B2S_CUDA(cudaGraphLaunch(P.graph_mixed, st));
+                g_kernel_launches += P.graph_mixed_kernels;
+            }
+            else
+                for(int it = 0; it < ci; ++it)
+                    pcg_iteration_mixed(s, kind, x, it);
+            B2S_CUDA(cudaMemcpyAsync(P.h_sc, P.sc.data(), sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+            B2S_CUDA(cudaStreamSynchronize(st));
+            if(s->timing)
+            {
+                const long long live = std::min<long long>(P.h_sc->iter - iter_before, ci);
+                for(long long it = 0; it < live; ++it)
+                {
+                    float a = 0.f, c = 0.f;
+                    B2S_CUDA(cudaEventElapsedTime(&a, s->iter_events[it * 4 + 0], s->iter_events[it * 4 + 1]));
+                    B2S_CUDA(cudaEventElapsedTime(&c, s->iter_events[it * 4 + 2], s->iter_events[it * 4 + 3]));
+                    s->timers.spmv_ms += a;
+                    s->timers.spmv_launches += 1;
+                    s->timers.precond_apply_ms += c;
+                    s->timers.precond_apply_launches += 1;
+                }
+            }
+            iter_before = P.h_sc->iter;
+            if(P.h_sc->converged != 0)
+                break;
+            if(o.replace_every > 0 && P.h_sc->iter - last_replace >= o.replace_every)
+            {
+                // reliable update: FP64 residual of the FP64 iterate, p and r.z kept
+                replace_residual();
+                ++replacements;
+                last_replace = P.h_sc->iter;
+            }
+        }
+        const PcgScalars r = *P.h_sc;
+        iter_total         = r.iter;
+        if(r.converged == 3)
+            throw Error(B2S_ERR_NUMERIC, "mixed PCG breakdown: r.z non-finite at iteration " + std::to_string(r.iter));
+        st_out.iterations_exact = r.converged == 1 ? r.iter_conv : r.iter;
+        st_out.converged        = r.converged == 1 ? 1 : 0;
+        st_out.rel_res          = true_residual();
+        done                    = true;
+        const bool verified = o.stop_rule != B2S_STOP_RELRES || st_out.rel_res <= o.tol;
+        if(r.converged == 1 && !verified && replacements < 64 && iter_total < max_iter - 1)
+        {
+            // the FP32 recursion claimed a stop the FP64 residual does not
+            // confirm: continue from the true residual
+            replace_residual();
+            ++replacements;
+            last_replace = iter_total;
+            h.rz         = restart_from_r(kind);
+            done         = false;
+        }
+        else if(r.converged == 1 && !verified)
+            st_out.converged = 0;
     }
     st_out.replacements = replacements;
     check_device_errors(s);

@@ -125,12 +125,24 @@ class Solver:
         self._check(self.lib.b2s_mas_get_clusters(self.h, hess.ctypes.data, inv.ctypes.data))
         return hess, inv
 
+    def mas_nodes(self):
+        """(R, Z) node buffers of the last apply, float32 [total_nodes, 3]."""
+        L, tot = self.mas_info()
+        R = np.zeros((tot, 3), np.float32)
+        Z = np.zeros((tot, 3), np.float32)
+        self._check(self.lib.b2s_mas_get_nodes(self.h, R.ctypes.data, Z.ctypes.data))
+        return R, Z
+
     # ---- preconditioner ----------------------------------------------------------
     def precond_assemble(self, kind: int, invert_mode: int = _abi.B2S_INVERT_SWEEP_F32):
         self._check(self.lib.b2s_precond_assemble(self.h, int(kind), int(invert_mode)))
 
     def precond_apply(self, r, z):
         self._check(self.lib.b2s_precond_apply(self.h, _ptr(r), _ptr(z)))
+
+    def precond_apply_mixed(self, r32, z32):
+        """Mixed-precision apply (FP32 vectors, BF16 diagonal-scaled MAS inverses)."""
+        self._check(self.lib.b2s_precond_apply_mixed(self.h, _ptr(r32), _ptr(z32)))
 
     # ---- PCG -------------------------------------------------------------------------
     def pcg(self, b, x, tol=1e-3, stop_rule=_abi.B2S_STOP_RZ, check_interval=5, max_iter=0,

@@ -708,6 +708,57 @@ int orc_mas_assemble(orc_mas* s, const orc_matrix* A, int32_t off, int invert_mo
     return 0;
 }
 
+}  // extern "C"
+
+namespace
+{
+// FP32 -> BF16 -> FP32, round to nearest even (finite inputs)
+inline float bf16_round(float v)
+{
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    u &= 0xFFFF0000u;
+    float o;
+    std::memcpy(&o, &u, 4);
+    return o;
+}
+}  // namespace
+
+extern "C" {
+
+void orc_mas_quantize(orc_mas* s, int mode)
+{
+    if(mode == 0)
+        return;
+    for(int c = 0; c < s->clusters; ++c)
+    {
+        float* M = &s->inv[(size_t)c * SYM * 9];
+        float  sc[BANK * 3];
+        for(int nd = 0; nd < BANK; ++nd)
+        {
+            const float* D = &M[sym_index(nd, nd) * 9];
+            for(int a = 0; a < 3; ++a)
+            {
+                const float d  = D[a * 3 + a];
+                sc[nd * 3 + a] = (mode == 2 && d > 0.f) ? 1.0f / std::sqrt(d) : 1.0f;
+            }
+        }
+        for(int rn = 0; rn < BANK; ++rn)
+            for(int cn = rn; cn < BANK; ++cn)
+            {
+                float* B = &M[sym_index(rn, cn) * 9];
+                for(int q = 0; q < 3; ++q)      // column
+                    for(int p = 0; p < 3; ++p)  // row
+                    {
+                        const float si = sc[rn * 3 + p], sj = sc[cn * 3 + q];
+                        const float scaled = bf16_round(B[q * 3 + p] * si * sj);
+                        B[q * 3 + p]       = scaled / (si * sj);
+                    }
+            }
+    }
+}
+
 void orc_mas_clusters(const orc_mas* s, double* hess, float* inv)
 {
     if(hess)

@@ -57,6 +57,11 @@ int  orc_mas_assemble(orc_mas* s, const orc_matrix* A, int32_t dof_offset_blocks
 void orc_mas_clusters(const orc_mas* s, double* cluster_hess, float* cluster_inv);
 // z = M^{-1} r on the MAS vertex range (r, z point at that range); FP32 inside.
 void orc_mas_apply(const orc_mas* s, const double* r, double* z);
+// Storage precision of the cluster inverses (applied to the current inverses
+// in place): 0 = FP32 (as assembled), 1 = BF16 (round to nearest even),
+// 2 = BF16 of the symmetrically diagonal-scaled inverse S M S with
+// S = diag(M)^-1/2, the scale kept in FP32 (z = S (S M S)_bf16 S r).
+void orc_mas_quantize(orc_mas* s, int mode);
 
 // ---- PCG (LinearPCG::pcg, linear_pcg.cu:558-644; LinearFusedPCG::fused_pcg,
 // linear_fused_pcg.cu:1782-2005)

@@ -69,6 +69,7 @@ def lib() -> C.CDLL:
     L.orc_mas_assemble.argtypes = [vp, vp, i32, C.c_int]
     L.orc_mas_clusters.argtypes = [vp, vp, vp]
     L.orc_mas_apply.argtypes = [vp, vp, vp]
+    L.orc_mas_quantize.argtypes = [vp, C.c_int]
     L.orc_pcg.restype = C.c_int
     L.orc_pcg.argtypes = [vp, C.c_int, vp, i32, vp, vp, d, C.c_int, C.c_int, i64, C.c_int, C.POINTER(OrcPcgResult)]
     L.orc_cg_truth.restype = C.c_int
@@ -170,6 +171,10 @@ class OracleMAS:
         inv = np.zeros((self.clusters, 136, 9), np.float32)
         lib().orc_mas_clusters(self.h, _p(hess), _p(inv))
         return hess, inv
+
+    def quantize(self, mode: int):
+        """0 = FP32 inverses, 1 = BF16, 2 = BF16 of the diagonal-scaled inverse."""
+        lib().orc_mas_quantize(self.h, int(mode))
 
     def apply(self, r: np.ndarray) -> np.ndarray:
         r = np.ascontiguousarray(r, dtype=np.float64)

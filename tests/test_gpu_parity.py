@@ -277,3 +277,67 @@ def test_calls_out_of_order_are_state_errors(solver, cuda):
     assert ei.value.code == _abi.B2S_ERR_STATE
     with pytest.raises(B200SolveError):
         solver.precond_apply(v, v.clone())
+
+
+# ---------------------------------------------------------------------------
+# mixed precision
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("which", ["cube10", "stack_small"])
+@pytest.mark.parametrize("pre", [_abi.B2S_PRECOND_JACOBI, _abi.B2S_PRECOND_MAS])
+def test_mixed_pcg_fp64_verified(request, solver, cuda, which, pre):
+    """FP32 matrix/vectors + BF16 MAS inverses + FP64 dots: the stop is
+    confirmed by the FP64 residual, and the iteration count stays close to the
+    plain FP64 solve's."""
+    import torch
+
+    s = request.getfixturevalue(which)
+    if pre == _abi.B2S_PRECOND_MAS:
+        b, A, M = _mas_setup(solver, s, cuda, partition_rcb(s.positions))
+    else:
+        b = _assemble(solver, s, cuda)
+        solver.precond_assemble(pre)
+    x64 = torch.zeros_like(b)
+    plain = solver.pcg(b, x64, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5)
+    x = torch.zeros_like(b)
+    st = solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5,
+                    precision=_abi.B2S_PRECISION_MIXED, replace_every=50)
+    assert st["converged"] == 1
+    assert st["rel_res"] <= 1e-4
+    assert st["iterations_exact"] <= 1.25 * plain["iterations_exact"] + 5
+    assert np.linalg.norm(x.cpu().numpy() - x64.cpu().numpy()) <= 2e-2 * np.linalg.norm(x64.cpu().numpy())
+
+
+def test_mixed_pcg_tight_tolerance_by_residual_replacement(solver, cuda, cube10):
+    """FP64 residual replacement wins back accuracy beyond FP32: the mixed
+    solve reaches rel-res 1e-9 and the FP64 direct solution within 1e-6."""
+    import scipy.sparse.linalg as spla
+    import torch
+
+    b, A, M = _mas_setup(solver, cube10, cuda, partition_rcb(cube10.positions))
+    x = torch.zeros_like(b)
+    st = solver.pcg(b, x, tol=1e-9, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5,
+                    precision=_abi.B2S_PRECISION_MIXED, replace_every=20)
+    assert st["converged"] == 1 and st["rel_res"] <= 1e-9
+    assert st["replacements"] >= 1
+    xt = spla.spsolve(A.to_scipy().tocsc(), cube10.b)
+    assert np.linalg.norm(x.cpu().numpy() - xt) <= 1e-6 * np.linalg.norm(xt)
+
+
+def test_mixed_spmv_bf16_apply_consistent(solver, cuda, cube10):
+    """The mixed path's BF16 MAS apply stays within BF16 rounding of the FP32
+    apply (relative 2e-2 in the worst entry, 5e-3 in norm)."""
+    import torch
+
+    b, A, M = _mas_setup(solver, cube10, cuda, partition_rcb(cube10.positions))
+    # run one mixed solve so the BF16 inverses are packed, then compare the
+    # FP32 apply of the oracle to the oracle with BF16-quantised inverses
+    M2 = O.OracleMAS(cube10.n_verts, cube10.adj_start, cube10.adj_list, *partition_maps(partition_rcb(cube10.positions)))
+    M2.assemble(A, 0, 0)
+    M2.quantize(2)
+    r = np.random.default_rng(9).standard_normal(3 * cube10.n_verts)
+    z32 = M.apply(r)
+    z16 = M2.apply(r)
+    assert np.linalg.norm(z16 - z32) <= 5e-3 * np.linalg.norm(z32)
+    x = torch.zeros_like(b)
+    st = solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, precision=_abi.B2S_PRECISION_MIXED)
+    assert st["converged"] == 1
