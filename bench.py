@@ -201,6 +201,8 @@ def main() -> None:
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="stack8x40")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) pass (profiling runs)")
+    ap.add_argument("--modes", default="plain,mixed",
+                    help="solver modes to time (profiling runs may time one); the JSON needs both")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
 
@@ -290,7 +292,17 @@ def main() -> None:
         ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
         return ms, stats, solver.timers(), clk
 
-    res = {mode: timed(mode) for mode in ("plain", "mixed")}
+    modes = [m for m in args.modes.split(",") if m in precisions]
+    res = {mode: timed(mode) for mode in modes}
+    if "mixed" not in res or "plain" not in res:
+        # profiling run of a single mode: report it and stop
+        only = modes[0]
+        ms1, st1, tm1, _ = res[only]
+        if rank == 0:
+            print(json.dumps({"profiling_mode": only, "ms_per_solve": ms1, "iterations": st1[-1]["iterations_exact"],
+                              "timers": tm1}), flush=True)
+        solver.close()
+        return
     nb, U = solver.matrix_info()
     ms, stats, tm, clk = res["mixed"]
 
