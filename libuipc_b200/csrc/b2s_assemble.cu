@@ -338,27 +338,38 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_reduce_rows(int32_t nb, const int
 }
 
 // rank of every block in (column, index) order within its SPMV_TILE-block
-// tile, by counting (one CTA per tile)
-__global__ void __launch_bounds__(SPMV_TILE) k_tile_rank(int64_t U, const int32_t* __restrict__ cols,
-                                                          uint16_t* __restrict__ trank)
+// tile: bitonic sort of the unique keys (column << 16 | index) in shared memory
+constexpr int RANK_THREADS = 512;
+__global__ void __launch_bounds__(RANK_THREADS) k_tile_rank(int64_t U, const int32_t* __restrict__ cols,
+                                                            uint16_t* __restrict__ trank)
 {
-    __shared__ int32_t sc[SPMV_TILE];
+    static_assert(SPMV_TILE <= 65536 && (SPMV_TILE & (SPMV_TILE - 1)) == 0, "tile: power of two <= 2^16");
+    __shared__ uint64_t key[SPMV_TILE];
     const int64_t base = (int64_t)blockIdx.x * SPMV_TILE;
-    const int     t    = threadIdx.x;
     const int64_t rem  = U - base;
     const int     n    = rem < SPMV_TILE ? (int)rem : SPMV_TILE;
-    sc[t]              = t < n ? cols[base + t] : 0x7fffffff;
+    for(int i = threadIdx.x; i < SPMV_TILE; i += RANK_THREADS)
+        key[i] = i < n ? ((uint64_t)(uint32_t)cols[base + i] << 16) | (uint64_t)i : ~0ull;
     __syncthreads();
-    if(t >= n)
-        return;
-    const int32_t c    = sc[t];
-    int           rank = 0;
-    for(int j = 0; j < n; ++j)
-    {
-        const int32_t cj = sc[j];
-        rank += (cj < c || (cj == c && j < t)) ? 1 : 0;
-    }
-    trank[base + t] = (uint16_t)rank;
+    for(int size = 2; size <= SPMV_TILE; size <<= 1)
+        for(int stride = size >> 1; stride > 0; stride >>= 1)
+        {
+            for(int i = threadIdx.x; i < SPMV_TILE / 2; i += RANK_THREADS)
+            {
+                const int      lo = 2 * i - (i & (stride - 1));
+                const int      hi = lo + stride;
+                const bool     up = (lo & size) == 0;
+                const uint64_t a = key[lo], b = key[hi];
+                if((a > b) == up)
+                {
+                    key[lo] = b;
+                    key[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    for(int i = threadIdx.x; i < n; i += RANK_THREADS)
+        trank[base + (int64_t)(key[i] & 0xFFFFu)] = (uint16_t)i;
 }
 
 int asm_grid(int64_t work, int block)
@@ -448,7 +459,7 @@ void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const in
     if(spmv_tiles && U > 0)
     {
         M.trank.resize(M.stride, 1.2);
-        k_tile_rank<<<(unsigned)((U + SPMV_TILE - 1) / SPMV_TILE), SPMV_TILE, 0, st>>>(U, M.cols.data(),
+        k_tile_rank<<<(unsigned)((U + SPMV_TILE - 1) / SPMV_TILE), RANK_THREADS, 0, st>>>(U, M.cols.data(),
                                                                                      M.trank.data());
         B2S_CHECK_LAUNCH();
         M.has_trank = true;

@@ -164,7 +164,7 @@ struct MasState
     // per assembly
     DBuf<double>  hess;            // [clusters * 136 * 9]
     DBuf<float>   inv;             // [clusters * 136 * 9]
-    DBuf<unsigned char> inv16;     // [clusters * 2640]: FP32 scale S (48) + BF16(S inv S)
+    DBuf<unsigned char> inv16;     // [clusters * 3264]: FP32 factor D (48) + six BF16 16x16 tiles of D^-1 inv D^-1
     long long     inv16_generation = -1;  // assembly generation inv16 was packed from
     // coarse-level Galerkin matrices (upper BCOO per level, in level-local ids)
     Matrix        coarse[MAX_LEVELS];
@@ -257,7 +257,7 @@ void exclusive_scan(b2s_solver* s, const int32_t* in, int32_t* out, int64_t n, D
 void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const int32_t* rows,
                        const int32_t* cols, const double* vals, bool spmv_tiles);
 
-constexpr int SPMV_TILE = 512;  // blocks per SpMV stage / tile
+constexpr int SPMV_TILE = 1024;  // blocks per SpMV tile (the span of the transposed-half ranks)
 
 // y = A x (+ optional pAp into partial reduction slot)
 void spmv_f64(b2s_solver* s, const Matrix& A, const double* x, double* y, double* d_dot);

@@ -434,71 +434,138 @@ __global__ void __launch_bounds__(INV_BLOCK) k_invert(int clusters, const double
 }
 
 // ---------------------------------------------------------------------------
-// apply: one warp per bank, persistent over banks. The bank's 4896-byte FP32
-// inverse is brought into shared memory by a bulk asynchronous copy (TMA),
-// double-buffered per warp so the next bank's copy is in flight while this
-// one computes. Lanes 0-15 own the bank's nodes; the 48x48 product is split
-// over the two half-warps (columns 0-7 / 8-15).
+// apply: one warp per bank, persistent over banks. The bank's inverse is
+// brought into shared memory by bulk asynchronous copies (TMA), NST deep per
+// warp, so later banks' copies are in flight while this one computes. The
+// residual of the next bank (and, at level 0, the part_to_real index of the
+// bank after it) is loaded into registers one bank ahead, so the dependent
+// part_to_real -> r gather never stalls the product.
+//
+// FP32 inverses (4,896 B: the 136 upper 3x3 blocks, column-major) are applied
+// on the CUDA cores: lanes 0-15 own the bank's nodes and the 48x48 product is
+// split over the two half-warps (columns 0-7 / 8-15).
+//
+// BF16 inverses (mixed precision) are applied on the tensor cores. Per cluster:
+// the FP32 factor D = diag(M)^1/2 (48 floats, 192 B), then the six upper 16x16
+// tiles (I <= J) of the 48x48 matrix D^-1 M D^-1 in BF16 (6 x 512 B), 3,264 B
+// in all. Tile rows are 32 B; the two 16-B halves of row R are swapped when
+// bit 2 of R is set, so each 8-row ldmatrix phase touches all 32 banks once.
+// z = D (M_s (D r)) by mma.m16n8k16 (BF16 operands, FP32 accumulation): A is
+// tile (I, J), for J < I the stored tile (J, I) loaded transposed; B column 0
+// is BF16(D r) and column 1 its BF16 rounding remainder, so the FP32 residual
+// enters with ~16 significant bits and the stored inverse is the only 8-bit
+// rounding. (A 48x48 matrix times one vector is an HBM-bound GEMV; the tensor
+// cores are used to cut the instruction count per byte, not for FLOPs.)
 // ---------------------------------------------------------------------------
 constexpr int APPLY_WARPS = 4;
 constexpr uint32_t INV_BYTES = SYM * 9 * sizeof(float);  // 4896, a multiple of 16
-// mixed precision: per cluster the FP32 diagonal factor D = diag(M)^1/2 (48
-// floats) then the BF16 entries of D^-1 M D^-1 in the same upper-block
-// layout: 192 + 2448 = 2640 B
-constexpr uint32_t INV16_SCALE_BYTES = BANK * 3 * sizeof(float);
-constexpr uint32_t INV16_BYTES       = INV16_SCALE_BYTES + SYM * 9 * 2;
+constexpr uint32_t INV16_SCALE_BYTES = BANK * 3 * sizeof(float);                    // 192
+constexpr uint32_t INV16_TILE_BYTES  = 16 * 16 * 2;                                 // 512
+constexpr uint32_t INV16_BYTES       = INV16_SCALE_BYTES + 6 * INV16_TILE_BYTES;  // 3264
+constexpr int APPLY_STAGES_F32  = 2;
+constexpr int APPLY_STAGES_BF16 = 2;
 
-// Z = D (M_s (D r)) for the BF16 diagonal-scaled storage, M_s = D^-1 M D^-1
-// (FP32 accumulation)
-__device__ __forceinline__ void cluster_product_bf16(const unsigned char* slot, const float (*r)[3], int lane,
-                                                     float out[3])
+// index of the upper tile (I, J), I <= J: (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+__host__ __device__ __forceinline__ int tile_id(int I, int J) { return I * 3 - I * (I + 1) / 2 + J; }
+// byte offset of 16-B half `half` of row `row` inside a tile
+__host__ __device__ __forceinline__ uint32_t tile_off(int row, int half)
 {
-    const float*          S  = reinterpret_cast<const float*>(slot);  // D
-    const __nv_bfloat16*  Mh = reinterpret_cast<const __nv_bfloat16*>(slot + INV16_SCALE_BYTES);
-    const int rn = lane & 15, c0 = (lane >> 4) * 8;
-    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
-#pragma unroll
-    for(int cc = 0; cc < 8; ++cc)
-    {
-        const int   cn = c0 + cc;
-        const float x0 = r[cn][0] * S[cn * 3], x1 = r[cn][1] * S[cn * 3 + 1], x2 = r[cn][2] * S[cn * 3 + 2];
-        float       B[9];
-        const bool  up = cn >= rn;
-        const __nv_bfloat16* src = Mh + (up ? sym_index(rn, cn) : sym_index(cn, rn)) * 9;
-#pragma unroll
-        for(int q = 0; q < 9; ++q)
-            B[q] = __bfloat162float(src[q]);
-        if(up)
-        {
-            acc0 = __fmaf_rn(B[0], x0, acc0); acc0 = __fmaf_rn(B[3], x1, acc0); acc0 = __fmaf_rn(B[6], x2, acc0);
-            acc1 = __fmaf_rn(B[1], x0, acc1); acc1 = __fmaf_rn(B[4], x1, acc1); acc1 = __fmaf_rn(B[7], x2, acc1);
-            acc2 = __fmaf_rn(B[2], x0, acc2); acc2 = __fmaf_rn(B[5], x1, acc2); acc2 = __fmaf_rn(B[8], x2, acc2);
-        }
-        else
-        {
-            acc0 = __fmaf_rn(B[0], x0, acc0); acc0 = __fmaf_rn(B[1], x1, acc0); acc0 = __fmaf_rn(B[2], x2, acc0);
-            acc1 = __fmaf_rn(B[3], x0, acc1); acc1 = __fmaf_rn(B[4], x1, acc1); acc1 = __fmaf_rn(B[5], x2, acc1);
-            acc2 = __fmaf_rn(B[6], x0, acc2); acc2 = __fmaf_rn(B[7], x1, acc2); acc2 = __fmaf_rn(B[8], x2, acc2);
-        }
-    }
-    acc0 += __shfl_down_sync(0xffffffffu, acc0, 16);
-    acc1 += __shfl_down_sync(0xffffffffu, acc1, 16);
-    acc2 += __shfl_down_sync(0xffffffffu, acc2, 16);
-    out[0] = acc0 * S[rn * 3];
-    out[1] = acc1 * S[rn * 3 + 1];
-    out[2] = acc2 * S[rn * 3 + 2];
+    return (uint32_t)row * 32u + ((uint32_t)(half ^ ((row >> 2) & 1)) << 4);
 }
 
-// pack the FP32 inverse M of every cluster as D (FP32) + BF16(D^-1 M D^-1),
-// D = diag(M)^1/2: the stored matrix has a unit diagonal, so BF16 rounds every
-// entry relative to O(1), and M = D (D^-1 M D^-1) D is recovered in the apply
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t& a3)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
+                 : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t addr, uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t& a3)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
+                 : "r"(addr));
+}
+// c += A (16x16, row) * B (16x8, col), BF16 in, FP32 accumulate
+__device__ __forceinline__ void mma_bf16_16816(float& c0, float& c1, float& c2, float& c3, uint32_t a0, uint32_t a1,
+                                               uint32_t a2, uint32_t a3, uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(c0), "+f"(c1), "+f"(c2), "+f"(c3)
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo, __nv_bfloat16 hi)
+{
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// Zb[0..48) = D M_s D r for one cluster; r48: the bank's residual (node-major)
+__device__ __forceinline__ void cluster_product_mma(const unsigned char* slot, const float* r48, int lane,
+                                                    float* __restrict__ Zb)
+{
+    const float*   D     = reinterpret_cast<const float*>(slot);
+    const uint32_t tiles = smem_addr(slot + INV16_SCALE_BYTES);
+    const int      g = lane >> 2, t = lane & 3;
+    uint32_t       b[3][2];
+#pragma unroll
+    for(int J = 0; J < 3; ++J)
+    {
+#pragma unroll
+        for(int h = 0; h < 2; ++h)
+        {
+            const int           k  = J * 16 + 2 * t + 8 * h;
+            const float         x0 = r48[k] * D[k], x1 = r48[k + 1] * D[k + 1];
+            const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+            uint32_t            v  = 0;
+            if(g == 0)
+                v = pack_bf16x2(h0, h1);
+            else if(g == 1)
+                v = pack_bf16x2(__float2bfloat16_rn(x0 - __bfloat162float(h0)),
+                                __float2bfloat16_rn(x1 - __bfloat162float(h1)));
+            b[J][h] = v;
+        }
+    }
+    // row address this lane gives ldmatrix: matrix q = lane / 8 of the four
+    // 8x8 quarters, row lane % 8 of it
+    const int      q = lane >> 3, rr = lane & 7;
+    const uint32_t offN = tile_off(rr + ((q & 1) << 3), q >> 1);
+    const uint32_t offT = tile_off(rr + ((q >> 1) << 3), q & 1);
+#pragma unroll
+    for(int I = 0; I < 3; ++I)
+    {
+        float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+#pragma unroll
+        for(int J = 0; J < 3; ++J)
+        {
+            uint32_t a0, a1, a2, a3;
+            if(J >= I)
+                ldsm_x4(tiles + tile_id(I, J) * INV16_TILE_BYTES + offN, a0, a1, a2, a3);
+            else
+                ldsm_x4_trans(tiles + tile_id(J, I) * INV16_TILE_BYTES + offT, a0, a1, a2, a3);
+            mma_bf16_16816(c0, c1, c2, c3, a0, a1, a2, a3, b[J][0], b[J][1]);
+        }
+        if(t == 0)
+        {
+            const int k0 = I * 16 + g, k1 = k0 + 8;
+            Zb[k0] = (c0 + c1) * D[k0];
+            Zb[k1] = (c2 + c3) * D[k1];
+        }
+    }
+}
+
+// pack the FP32 inverse M of every cluster as D (FP32) + the BF16 tiles of
+// D^-1 M D^-1, D = diag(M)^1/2: the stored matrix has a unit diagonal, so BF16
+// rounds every entry relative to O(1), and M = D (D^-1 M D^-1) D is recovered
+// in the apply. Entry (a, b) comes from the stored upper 3x3 block of nodes
+// (min, max) and is scaled as stored row times stored column.
 __global__ void k_pack_inverse_bf16(int clusters, const float* __restrict__ inv, unsigned char* __restrict__ out)
 {
     const int c = blockIdx.x;
     if(c >= clusters)
         return;
     __shared__ float S[BANK * 3];  // 1 / D
-    const float* M = inv + (size_t)c * SYM * 9;
+    const float*   M = inv + (size_t)c * SYM * 9;
     unsigned char* o = out + (size_t)c * INV16_BYTES;
     if(threadIdx.x < BANK * 3)
     {
@@ -509,19 +576,20 @@ __global__ void k_pack_inverse_bf16(int clusters, const float* __restrict__ inv,
         reinterpret_cast<float*>(o)[threadIdx.x] = Dv;
     }
     __syncthreads();
-    __nv_bfloat16* Mh = reinterpret_cast<__nv_bfloat16*>(o + INV16_SCALE_BYTES);
-    for(int e = threadIdx.x; e < SYM * 9; e += blockDim.x)
+    for(int e = threadIdx.x; e < 6 * 256; e += blockDim.x)
     {
-        // block si = e / 9 is (rn, cn) with rn <= cn; entry (p, q) column-major
-        const int si = e / 9, q = (e % 9) / 3, p = e % 3;
-        int       rn = 0, rem = si;
-        while(rem >= BANK - rn)
-        {
-            rem -= BANK - rn;
-            ++rn;
-        }
-        const int cn = rn + rem;
-        Mh[e]        = __float2bfloat16_rn(M[e] * S[rn * 3 + p] * S[cn * 3 + q]);
+        const int t = e >> 8, row = (e >> 4) & 15, col = e & 15;
+        const int I = t < 3 ? 0 : (t < 5 ? 1 : 2);
+        const int J = t - (I * 3 - I * (I + 1) / 2);
+        const int a = I * 16 + row, b = J * 16 + col;
+        const int na = a / 3, pa = a % 3, nb = b / 3, pb = b % 3;
+        float     v;
+        if(na <= nb)
+            v = M[sym_index(na, nb) * 9 + pb * 3 + pa] * S[a] * S[b];
+        else
+            v = M[sym_index(nb, na) * 9 + pa * 3 + pb] * S[b] * S[a];
+        *reinterpret_cast<__nv_bfloat16*>(o + INV16_SCALE_BYTES + t * INV16_TILE_BYTES + tile_off(row, col >> 3) +
+                                          (col & 7) * 2) = __float2bfloat16_rn(v);
     }
 }
 
@@ -558,14 +626,186 @@ __device__ __forceinline__ void cluster_product(const float* M, const float (*r)
     out[2] = acc2;
 }
 
-// One level of the apply. FINE: level 0, the residual is gathered from the
-// FP64 vector r through part_to_real; otherwise R_l is read from the node
-// buffer. With `push`, the restriction sums of the next level (one per
-// connected component of the bank, summed by its lowest lane in lane order)
-// are written to R_{l+1}. Z_l = A_l^{-1} R_l for every node of the bank.
-// BF: the inverse is stored as S + BF16(S M S) (INV16_BYTES per cluster),
-// otherwise FP32 (INV_BYTES per cluster). VT: type of the fine residual.
-template <bool FINE, typename VT, bool BF>
+// The banks of one level handled by one warp (warp gw of W): FINE: level 0,
+// the residual is gathered from r through part_to_real; otherwise R_l is read
+// from the node buffer. With `push`, the restriction sums of the next level
+// (one per connected component of the bank, summed by its lowest lane in lane
+// order) are written to R_{l+1}. Z_l = A_l^{-1} R_l for every node of the
+// bank. BF: BF16 tiles on the tensor cores (INV16_BYTES per cluster),
+// otherwise FP32 (INV_BYTES). VT: type of the fine residual. NST: copies in
+// flight per warp. `u` counts the banks this warp has run through its slots
+// (slot and phase of the next copy), so one warp can go through several
+// levels. Returns false when a copy wait ran out (the error flag is set and
+// the warp's copies in flight are drained).
+
+// the copies of a level's first NST banks of warp gw (lane 0 issues)
+template <bool BF, int NST>
+__device__ __forceinline__ void issue_first_copies(int gw, int W, int lane, int u, int n_banks, int level_begin,
+                                                   const unsigned char* __restrict__ inv, unsigned char* s_inv,
+                                                   uint64_t* s_bar)
+{
+    constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
+    const int     mine   = gw < n_banks ? (n_banks - 1 - gw) / W + 1 : 0;
+    const int64_t gbank0 = level_begin / BANK;
+    if(lane == 0)
+    {
+        fence_proxy_async_smem();
+        for(int j = 0; j < mine && j < NST; ++j)
+        {
+            const int slot = (u + j) % NST;
+            mbar_arrive_expect_tx(&s_bar[slot], CB);
+            bulk_copy_g2s(s_inv + slot * CB, inv + (size_t)(gbank0 + gw + (int64_t)j * W) * CB, CB, &s_bar[slot]);
+        }
+    }
+    __syncwarp();
+}
+
+template <bool FINE, typename VT, bool BF, int NST>
+__device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int n_banks, int cnt, int level_begin,
+                                            const int32_t* __restrict__ p2r, const VT* __restrict__ r, int off3,
+                                            const uint16_t* __restrict__ comp_mask,
+                                            const int32_t* __restrict__ new_local, int next_begin, int push,
+                                            const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
+                                            int* err, unsigned char* s_inv, float (*s_r)[3], uint64_t* s_bar)
+{
+    constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
+    const int     sub    = lane & 15;
+    const int     mine   = gw < n_banks ? (n_banks - 1 - gw) / W + 1 : 0;
+    const int64_t gbank0 = level_begin / BANK;
+    issue_first_copies<BF, NST>(gw, W, lane, u, n_banks, level_begin, inv, s_inv, s_bar);
+    // registers of the next bank (lanes 0-15): residual, liveness, component
+    // mask and next-level index; at level 0 also part_to_real two banks ahead
+    float    n0 = 0.f, n1 = 0.f, n2 = 0.f;
+    bool     nlive = false;
+    uint32_t ncm   = 0;
+    int      nnl   = 0;
+    int      v_ahead = -1;
+    auto load_index = [&](int jj) -> int {
+        return (FINE && lane < 16 && jj < mine) ? p2r[(gw + jj * W) * BANK + sub] : -1;
+    };
+    auto load_bank = [&](int jj, int v) {
+        n0 = n1 = n2 = 0.f;
+        nlive = false;
+        ncm   = 0;
+        nnl   = 0;
+        if(lane >= 16 || jj >= mine)
+            return;
+        const int node = (gw + jj * W) * BANK + sub;
+        if(FINE)
+        {
+            nlive = v >= 0;
+            if(nlive)
+            {
+                n0 = (float)r[off3 + 3 * (int64_t)v];
+                n1 = (float)r[off3 + 3 * (int64_t)v + 1];
+                n2 = (float)r[off3 + 3 * (int64_t)v + 2];
+            }
+        }
+        else
+        {
+            nlive = node < cnt;
+            if(nlive)
+            {
+                const int64_t g = (int64_t)level_begin + node;
+                n0 = R[3 * g];
+                n1 = R[3 * g + 1];
+                n2 = R[3 * g + 2];
+            }
+        }
+        if(push && nlive)
+        {
+            ncm = comp_mask[node];
+            nnl = new_local[node];
+        }
+    };
+    if(FINE)
+    {
+        const int v0 = load_index(0);
+        v_ahead      = load_index(1);
+        load_bank(0, v0);
+    }
+    else
+        load_bank(0, -1);
+    int j = 0;
+    for(; j < mine; ++j)
+    {
+        const int      bank = gw + j * W;
+        const int      slot = (u + j) % NST;
+        const bool     live = nlive;
+        const uint32_t cm   = ncm;
+        const int      nl   = nnl;
+        if(lane < 16)
+        {
+            s_r[sub][0] = n0;
+            s_r[sub][1] = n1;
+            s_r[sub][2] = n2;
+        }
+        // the next bank's loads are issued now and land while this one computes
+        if(FINE)
+        {
+            const int v1 = v_ahead;
+            v_ahead      = load_index(j + 2);
+            load_bank(j + 1, v1);
+        }
+        else
+            load_bank(j + 1, -1);
+        __syncwarp();
+        if(push && live && (cm & ((1u << lane) - 1u)) == 0)
+        {
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+            for(uint32_t m = cm; m; m &= m - 1)
+            {
+                const int l = __ffs(m) - 1;
+                s0 += s_r[l][0];
+                s1 += s_r[l][1];
+                s2 += s_r[l][2];
+            }
+            const int64_t g = (int64_t)next_begin + nl;
+            R[3 * g]     = s0;
+            R[3 * g + 1] = s1;
+            R[3 * g + 2] = s2;
+        }
+        const bool ok = mbar_wait(&s_bar[slot], (uint32_t)(((u + j) / NST) & 1), err, DERR_TMA_TIMEOUT);
+        if(!__all_sync(0xffffffffu, ok))
+            break;
+        float* Zb = Z + 3 * ((int64_t)level_begin + (int64_t)bank * BANK);
+        if(BF)
+            cluster_product_mma(s_inv + slot * CB, &s_r[0][0], lane, Zb);
+        else
+        {
+            float out[3];
+            cluster_product(reinterpret_cast<const float*>(s_inv + slot * CB), s_r, lane, out);
+            if(lane < 16)
+            {
+                Zb[3 * sub]     = out[0];
+                Zb[3 * sub + 1] = out[1];
+                Zb[3 * sub + 2] = out[2];
+            }
+        }
+        __syncwarp();
+        if(lane == 0 && j + NST < mine)
+        {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&s_bar[slot], CB);
+            bulk_copy_g2s(s_inv + slot * CB, inv + (size_t)(gbank0 + bank + (int64_t)NST * W) * CB, CB,
+                          &s_bar[slot]);
+        }
+    }
+    if(j < mine)
+    {
+        // a wait ran out: drain this warp's copies still in flight (bounded)
+        if(lane == 0)
+            for(int q = j; q < mine && q < j + NST; ++q)
+                mbar_wait(&s_bar[(u + q) % NST], (uint32_t)(((u + q) / NST) & 1), nullptr, 0);
+        __syncwarp();
+        return false;
+    }
+    u += mine;
+    return true;
+}
+
+// one level over a persistent grid of APPLY_WARPS-warp CTAs
+template <bool FINE, typename VT, bool BF, int NST>
 __global__ void __launch_bounds__(APPLY_WARPS * 32)
     k_apply_level(int n_banks, int cnt, int level_begin, const int32_t* __restrict__ p2r, const VT* __restrict__ r,
                   int off3, const uint16_t* __restrict__ comp_mask, const int32_t* __restrict__ new_local,
@@ -575,119 +815,35 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
     if(converged && *converged)
         return;
     constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
-    __shared__ __align__(128) unsigned char s_inv[APPLY_WARPS][2][INV_BYTES];
+    __shared__ __align__(128) unsigned char s_inv[APPLY_WARPS][NST][CB];
     __shared__ float    s_r[APPLY_WARPS][BANK][3];
-    __shared__ uint64_t s_bar[APPLY_WARPS][2];
+    __shared__ uint64_t s_bar[APPLY_WARPS][NST];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int gw = blockIdx.x * APPLY_WARPS + w, W = gridDim.x * APPLY_WARPS;
-    const int mine = gw < n_banks ? (n_banks - 1 - gw) / W + 1 : 0;
-    const int64_t gbank0 = level_begin / BANK;
     if(lane == 0)
     {
-        mbar_init(&s_bar[w][0], 1);
-        mbar_init(&s_bar[w][1], 1);
+        for(int q = 0; q < NST; ++q)
+            mbar_init(&s_bar[w][q], 1);
         mbar_fence_init();
-        for(int j = 0; j < mine && j < 2; ++j)
-        {
-            mbar_arrive_expect_tx(&s_bar[w][j], CB);
-            bulk_copy_g2s(s_inv[w][j], inv + (size_t)(gbank0 + gw + (int64_t)j * W) * CB, CB, &s_bar[w][j]);
-        }
     }
     __syncwarp();
-    int j = 0;
-    for(; j < mine; ++j)
-    {
-        const int bank = gw + j * W;
-        const int slot = j & 1;
-        // residual of the bank's 16 nodes (overlaps the inverse's copy)
-        const int node = bank * BANK + (lane & 15);
-        bool      live = false;
-        if(lane < 16)
-        {
-            float r0 = 0.f, r1 = 0.f, r2 = 0.f;
-            if(FINE)
-            {
-                const int v = p2r[node];
-                live        = v >= 0;
-                if(live)
-                {
-                    r0 = (float)r[off3 + 3 * (int64_t)v];
-                    r1 = (float)r[off3 + 3 * (int64_t)v + 1];
-                    r2 = (float)r[off3 + 3 * (int64_t)v + 2];
-                }
-            }
-            else
-            {
-                live = node < cnt;
-                if(live)
-                {
-                    const int64_t g = (int64_t)level_begin + node;
-                    r0 = R[3 * g];
-                    r1 = R[3 * g + 1];
-                    r2 = R[3 * g + 2];
-                }
-            }
-            s_r[w][lane][0] = r0;
-            s_r[w][lane][1] = r1;
-            s_r[w][lane][2] = r2;
-        }
-        __syncwarp();
-        if(push && live)
-        {
-            const uint32_t cm = comp_mask[node];
-            if((cm & ((1u << lane) - 1u)) == 0)
-            {
-                float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-                for(uint32_t m = cm; m; m &= m - 1)
-                {
-                    const int l = __ffs(m) - 1;
-                    s0 += s_r[w][l][0];
-                    s1 += s_r[w][l][1];
-                    s2 += s_r[w][l][2];
-                }
-                const int64_t g = (int64_t)next_begin + new_local[node];
-                R[3 * g]     = s0;
-                R[3 * g + 1] = s1;
-                R[3 * g + 2] = s2;
-            }
-        }
-        const bool ok = mbar_wait(&s_bar[w][slot], (uint32_t)((j >> 1) & 1), err, DERR_TMA_TIMEOUT);
-        if(!__all_sync(0xffffffffu, ok))
-            break;
-        float out[3];
-        if(BF)
-            cluster_product_bf16(s_inv[w][slot], s_r[w], lane, out);
-        else
-            cluster_product(reinterpret_cast<const float*>(s_inv[w][slot]), s_r[w], lane, out);
-        if(lane < 16)
-        {
-            const int64_t g = (int64_t)level_begin + node;
-            Z[3 * g]     = out[0];
-            Z[3 * g + 1] = out[1];
-            Z[3 * g + 2] = out[2];
-        }
-        __syncwarp();
-        if(lane == 0 && j + 2 < mine)
-        {
-            fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&s_bar[w][slot], CB);
-            bulk_copy_g2s(s_inv[w][slot], inv + (size_t)(gbank0 + bank + 2 * (int64_t)W) * CB, CB, &s_bar[w][slot]);
-        }
-    }
-    if(j < mine && lane == 0)
-    {
-        // a wait ran out: drain this warp's copies still in flight (bounded)
-        for(int q = j; q < mine && q < j + 2; ++q)
-            mbar_wait(&s_bar[w][q & 1], (uint32_t)((q >> 1) & 1), nullptr, 0);
-    }
+    int u = 0;
+    apply_banks<FINE, VT, BF, NST>(blockIdx.x * APPLY_WARPS + w, gridDim.x * APPLY_WARPS, lane, u, n_banks, cnt,
+                                   level_begin, p2r, r, off3, comp_mask, new_local, next_begin, push, inv, R, Z, err,
+                                   &s_inv[w][0][0], s_r[w], s_bar[w]);
 }
 
-int apply_grid(int n_banks)
+// persistent grid: as many CTAs as fit on the SMs at once, capped by the banks
+template <typename K>
+int apply_grid(K kernel, int n_banks)
 {
-    const int max_warps = NUM_SMS_HINT * 5 * APPLY_WARPS;
+    int occ = 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, APPLY_WARPS * 32, 0) != cudaSuccess || occ < 1)
+        occ = 1;
+    const int max_warps = NUM_SMS_HINT * occ * APPLY_WARPS;
     const int warps     = n_banks < max_warps ? n_banks : max_warps;
     return (warps + APPLY_WARPS - 1) / APPLY_WARPS;
 }
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -909,7 +1065,7 @@ void mas_assemble(b2s_solver* s, int invert_mode)
 
 // z[off..off+vn) gets the MAS part of z = P r; Jacobi/identity elsewhere is
 // handled by the caller (collect kernel in the PCG, or precond_apply).
-// bf16: use the packed S + BF16(S M S) inverses (mas_pack_bf16 first).
+// bf16: use the packed D + BF16 tiles of D^-1 M D^-1 (mas_pack_bf16 first).
 template <typename VT>
 static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, bool bf16)
 {
@@ -921,12 +1077,16 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
     const unsigned char* inv = bf16 ? M.inv16.data() : reinterpret_cast<const unsigned char*>(M.inv.data());
     if(n_banks0 > 0)
     {
-        auto k = bf16 ? k_apply_level<true, VT, true> : k_apply_level<true, VT, false>;
-        k<<<apply_grid(n_banks0), tb, 0, st>>>(n_banks0, M.N, 0, M.p2r.data(), r, 3 * M.offset,
-                                               M.comp_mask[0].data(), M.new_local[0].data(), M.level_begin[1],
-                                               M.L > 1 ? 1 : 0, inv, M.R.data(), M.Z.data(), converged, err);
+        auto k = bf16 ? k_apply_level<true, VT, true, APPLY_STAGES_BF16>
+                      : k_apply_level<true, VT, false, APPLY_STAGES_F32>;
+        k<<<apply_grid(k, n_banks0), tb, 0, st>>>(n_banks0, M.N, 0, M.p2r.data(), r, 3 * M.offset,
+                                                  M.comp_mask[0].data(), M.new_local[0].data(), M.level_begin[1],
+                                                  M.L > 1 ? 1 : 0, inv, M.R.data(), M.Z.data(), converged, err);
         B2S_CHECK_LAUNCH();
     }
+    // coarse levels: one persistent launch each (on the graph's stream the
+    // launches follow each other within microseconds; one thread-block cluster
+    // running all small levels with cluster barriers between them was slower)
     for(int level = 1; level < M.L; ++level)
     {
         const int cnt = M.level_count[level];
@@ -934,11 +1094,12 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
             break;
         const int n_banks = (cnt + BANK - 1) / BANK;
         const int push    = level + 1 < M.L ? 1 : 0;
-        auto k = bf16 ? k_apply_level<false, VT, true> : k_apply_level<false, VT, false>;
-        k<<<apply_grid(n_banks), tb, 0, st>>>(n_banks, cnt, M.level_begin[level], nullptr, nullptr, 0,
-                                              M.comp_mask[level].data(), M.new_local[level].data(),
-                                              push ? M.level_begin[level + 1] : 0, push, inv, M.R.data(),
-                                              M.Z.data(), converged, err);
+        auto k = bf16 ? k_apply_level<false, VT, true, APPLY_STAGES_BF16>
+                      : k_apply_level<false, VT, false, APPLY_STAGES_F32>;
+        k<<<apply_grid(k, n_banks), tb, 0, st>>>(n_banks, cnt, M.level_begin[level], nullptr, nullptr, 0,
+                                                 M.comp_mask[level].data(), M.new_local[level].data(),
+                                                 push ? M.level_begin[level + 1] : 0, push, inv, M.R.data(),
+                                                 M.Z.data(), converged, err);
         B2S_CHECK_LAUNCH();
     }
 }

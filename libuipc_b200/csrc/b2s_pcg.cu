@@ -96,7 +96,8 @@ struct MasView
     int            active;  // MAS present
     int            off, vn, L;
     const int32_t* r2p;
-    const int32_t* ctable;  // [vn * (L-1)]
+    const int32_t* ctable;  // [vn * (L-1)] node of each vertex at levels 1..L-1
+    int            T;       // coarse levels to collect (L-1)
     const float*   Z;
 };
 
@@ -116,13 +117,19 @@ __device__ __forceinline__ void precond_row(int kind, const MasView& mv, const d
             if(p >= 0)
             {
                 float c0 = mv.Z[3 * (int64_t)p], c1 = mv.Z[3 * (int64_t)p + 1], c2 = mv.Z[3 * (int64_t)p + 2];
-                for(int l = 1; l < mv.L; ++l)
-                {
-                    const int64_t node = mv.ctable[(int64_t)v * (mv.L - 1) + (l - 1)];
-                    c0 += mv.Z[3 * node];
-                    c1 += mv.Z[3 * node + 1];
-                    c2 += mv.Z[3 * node + 2];
-                }
+                // all coarse node ids first, then the gathers (independent loads)
+                int32_t nodes[MAX_LEVELS - 1];
+#pragma unroll
+                for(int l = 0; l < MAX_LEVELS - 1; ++l)
+                    nodes[l] = l < mv.T ? mv.ctable[(int64_t)v * (mv.L - 1) + l] : 0;
+#pragma unroll
+                for(int l = 0; l < MAX_LEVELS - 1; ++l)
+                    if(l < mv.T)
+                    {
+                        c0 += mv.Z[3 * (int64_t)nodes[l]];
+                        c1 += mv.Z[3 * (int64_t)nodes[l] + 1];
+                        c2 += mv.Z[3 * (int64_t)nodes[l] + 2];
+                    }
                 z[0] = (double)c0;
                 z[1] = (double)c1;
                 z[2] = (double)c2;
@@ -352,6 +359,7 @@ static MasView mas_view(b2s_solver* s)
     mv.L      = M.L;
     mv.r2p    = M.r2p.data();
     mv.ctable = M.ctable.data();
+    mv.T      = M.L <= 1 ? 0 : M.L - 1;
     mv.Z      = M.Z.data();
     return mv;
 }

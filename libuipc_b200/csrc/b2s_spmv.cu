@@ -6,15 +6,17 @@
 // adds B x_j to y_i and, off the diagonal, B^T x_i to y_j; the dot is
 // sum (2 - delta_ij) x_i^T B x_j.
 //
-// Design: one persistent CTA per SM streams a contiguous range of the block
-// stream through a 4-stage shared-memory ring filled by bulk asynchronous
-// copies (cp.async.bulk, TMA) -- row ids, column ids and the 9 value planes
-// of 512 blocks per stage -- so the DRAM stream runs ahead of the threads
-// independently of their register-bound loads. Each thread takes one block
-// of a stage: it gathers x_j and x_i (L2-resident), forms B x_j and B^T x_i,
-// the warp merges runs of equal rows with an in-register segmented scan and
-// writes one atomic per run, and the transposed contributions scatter with
-// atomics that resolve in L2.
+// Design: persistent CTAs walk SPMV_TILE-block tiles of the row-sorted block
+// stream. Each thread owns SPMV_BPT consecutive blocks and reads their row and
+// column ids, tile ranks and the 9 value planes with 16-byte vector loads
+// (the planes are padded to a multiple of 16 blocks). The row halves B x_j of
+// a thread's blocks are merged in registers (runs of equal rows) and each run
+// goes to y with one fire-and-forget reduction per component (red.global,
+// resolved in L2). The transposed halves B^T x_i are placed in shared memory
+// at the block's precomputed rank in (column, index) order; after a barrier
+// each thread merges its SPMV_BPT consecutive slots, so runs of equal columns
+// also leave as one reduction each. With FP32 values the next tile's stream is
+// loaded into registers while the current tile is reduced.
 #include "b2s_internal.cuh"
 #include "b2s_reduce.cuh"
 
@@ -25,7 +27,8 @@ namespace b2s
 {
 namespace
 {
-constexpr int SPMV_THREADS = SPMV_TILE;  // = blocks per tile
+constexpr int SPMV_BPT     = 4;                     // blocks per thread
+constexpr int SPMV_THREADS = SPMV_TILE / SPMV_BPT;  // threads per CTA
 
 // fire-and-forget reductions in L2 (no value returned to the SM)
 __device__ __forceinline__ void atomic_add_t(double* p, double v)
@@ -37,106 +40,197 @@ __device__ __forceinline__ void atomic_add_t(float* p, float v)
     asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }
 
-// warp-level segmented inclusive scan of (a0,a1,a2) over equal keys; returns
-// true in the last lane of each run
-template <typename XT>
-__device__ __forceinline__ bool seg_scan3(int32_t key, XT& a0, XT& a1, XT& a2, int lane)
+// four consecutive elements from a 16-byte (8-byte for uint16) aligned address
+__device__ __forceinline__ void ld4(const float* p, float v[4])
 {
-#pragma unroll
-    for(int o = 1; o < 32; o <<= 1)
-    {
-        const XT      t0 = __shfl_up_sync(0xffffffffu, a0, o);
-        const XT      t1 = __shfl_up_sync(0xffffffffu, a1, o);
-        const XT      t2 = __shfl_up_sync(0xffffffffu, a2, o);
-        const int32_t tk = __shfl_up_sync(0xffffffffu, key, o);
-        if(lane >= o && tk == key)
-        {
-            a0 += t0;
-            a1 += t1;
-            a2 += t2;
-        }
-    }
-    const int32_t knext = __shfl_down_sync(0xffffffffu, key, 1);
-    return lane == 31 || knext != key;
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double v[4])
+{
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void ld4(const int32_t* p, int32_t v[4])
+{
+    const int4 q = __ldg(reinterpret_cast<const int4*>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const uint16_t* p, int v[4])
+{
+    const uint2 q = __ldg(reinterpret_cast<const uint2*>(p));
+    v[0] = (int)(q.x & 0xFFFFu); v[1] = (int)(q.x >> 16); v[2] = (int)(q.y & 0xFFFFu); v[3] = (int)(q.y >> 16);
 }
 
-// Tile variant: a 512-thread CTA takes one 512-block tile at a time with
-// plain coalesced loads. The row part is merged in-warp (runs of equal rows);
-// the transposed contributions are placed in shared memory at the block's
-// precomputed rank in (column, index) order, so runs of equal columns become
-// contiguous and are merged by a second segmented scan before the reductions
-// go to L2 -- about half the reduction traffic of a direct scatter.
+template <typename XT>
+__device__ __forceinline__ void red3(XT* y, int32_t node, XT a0, XT a1, XT a2)
+{
+    atomic_add_t(y + 3 * (int64_t)node, a0);
+    atomic_add_t(y + 3 * (int64_t)node + 1, a1);
+    atomic_add_t(y + 3 * (int64_t)node + 2, a2);
+}
+
+// the streamed data of one thread's SPMV_BPT blocks
+template <typename VT>
+struct TileLoad
+{
+    int32_t r[4], c[4];
+    int     rk[4];
+    VT      b[9][4];
+};
+
+// S: plane stride (a multiple of 16, rows past the stored blocks are -1)
+template <typename VT>
+__device__ __forceinline__ void load_tile(TileLoad<VT>& t, int64_t e0, int64_t S, bool live,
+                                          const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
+                                          const uint16_t* __restrict__ trank, const VT* __restrict__ vals)
+{
+    if(!live)
+    {
+#pragma unroll
+        for(int k = 0; k < 4; ++k)
+            t.r[k] = -1;
+        return;
+    }
+    ld4(rows + e0, t.r);
+    ld4(cols + e0, t.c);
+    ld4(trank + e0, t.rk);
+#pragma unroll
+    for(int q = 0; q < 9; ++q)
+        ld4(vals + (int64_t)q * S + e0, t.b[q]);
+}
+
+// row halves of a thread's blocks to y (runs of equal rows merged), the
+// transposed halves into shared memory at the blocks' ranks, and the dot
 template <typename VT, typename XT, bool WITH_DOT>
-__global__ void __launch_bounds__(SPMV_THREADS, 3)
+__device__ __forceinline__ void tile_rows(const TileLoad<VT>& t, const XT* __restrict__ x, XT* y,
+                                          XT (*s_t)[SPMV_TILE], int32_t* s_col, double& dot)
+{
+    int32_t cur = -1;
+    XT      a0 = 0, a1 = 0, a2 = 0;
+    XT      xi0 = 0, xi1 = 0, xi2 = 0;
+#pragma unroll
+    for(int k = 0; k < 4; ++k)
+    {
+        if(t.r[k] < 0)
+            break;  // padding: only at the end of the stream
+        const int32_t ck  = t.c[k];
+        const XT      xj0 = __ldg(x + 3 * (int64_t)ck), xj1 = __ldg(x + 3 * (int64_t)ck + 1),
+                 xj2 = __ldg(x + 3 * (int64_t)ck + 2);
+        if(t.r[k] != cur)
+        {
+            if(cur >= 0)
+                red3(y, cur, a0, a1, a2);
+            cur = t.r[k];
+            a0 = a1 = a2 = 0;
+            xi0 = __ldg(x + 3 * (int64_t)cur);
+            xi1 = __ldg(x + 3 * (int64_t)cur + 1);
+            xi2 = __ldg(x + 3 * (int64_t)cur + 2);
+        }
+        // column-major: B(p,q) = b[q*3 + p]
+        const XT y0 = (XT)t.b[0][k] * xj0 + (XT)t.b[3][k] * xj1 + (XT)t.b[6][k] * xj2;
+        const XT y1 = (XT)t.b[1][k] * xj0 + (XT)t.b[4][k] * xj1 + (XT)t.b[7][k] * xj2;
+        const XT y2 = (XT)t.b[2][k] * xj0 + (XT)t.b[5][k] * xj1 + (XT)t.b[8][k] * xj2;
+        a0 += y0;
+        a1 += y1;
+        a2 += y2;
+        const bool off = cur != ck;
+        if(WITH_DOT)
+        {
+            const double d = (double)xi0 * (double)y0 + (double)xi1 * (double)y1 + (double)xi2 * (double)y2;
+            dot += off ? 2.0 * d : d;
+        }
+        const int rk = t.rk[k];
+        s_t[0][rk]   = off ? (XT)t.b[0][k] * xi0 + (XT)t.b[1][k] * xi1 + (XT)t.b[2][k] * xi2 : XT(0);
+        s_t[1][rk]   = off ? (XT)t.b[3][k] * xi0 + (XT)t.b[4][k] * xi1 + (XT)t.b[5][k] * xi2 : XT(0);
+        s_t[2][rk]   = off ? (XT)t.b[6][k] * xi0 + (XT)t.b[7][k] * xi1 + (XT)t.b[8][k] * xi2 : XT(0);
+        s_col[rk]    = ck;
+    }
+    if(cur >= 0)
+        red3(y, cur, a0, a1, a2);
+}
+
+// transposed halves in (column, index) order: this thread's slots, runs of
+// equal columns merged; n = blocks in the tile
+template <typename XT>
+__device__ __forceinline__ void tile_cols(int tid, int n, const XT (*s_t)[SPMV_TILE], const int32_t* s_col, XT* y)
+{
+    const int s0  = SPMV_BPT * tid;
+    int32_t   cur = -1;
+    XT        t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+    for(int k = 0; k < SPMV_BPT; ++k)
+    {
+        const int sl = s0 + k;
+        if(sl >= n)
+            break;
+        const int32_t cc = s_col[sl];
+        if(cc != cur)
+        {
+            if(cur >= 0)
+                red3(y, cur, t0, t1, t2);
+            cur = cc;
+            t0 = t1 = t2 = 0;
+        }
+        t0 += s_t[0][sl];
+        t1 += s_t[1][sl];
+        t2 += s_t[2][sl];
+    }
+    if(cur >= 0)
+        red3(y, cur, t0, t1, t2);
+}
+
+// U: stored blocks; S: plane stride. FP32 values: the next tile's stream is
+// loaded into registers before this tile's gathers and reductions (software
+// pipelining) and the shared buffers alternate, one barrier per tile. FP64
+// values: the registers of two tiles do not fit, one tile at a time.
+template <typename VT, typename XT, bool WITH_DOT>
+__global__ void __launch_bounds__(SPMV_THREADS)
     k_spmv_tile(int64_t U, int64_t S, const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
                 const uint16_t* __restrict__ trank, const VT* __restrict__ vals, const XT* __restrict__ x, XT* y,
                 double* partials, unsigned int* counter, double* dot_out, const int* stop)
 {
     if(stop && *stop)
         return;
-    __shared__ XT      s_t[3][SPMV_THREADS];
-    __shared__ int32_t s_col[SPMV_THREADS];
+    constexpr bool PF = sizeof(VT) == 4;
+    constexpr int  NB = PF ? 2 : 1;
+    __shared__ __align__(16) XT      s_t[NB][3][SPMV_TILE];
+    __shared__ __align__(16) int32_t s_col[NB][SPMV_TILE];
     const int     tid     = threadIdx.x;
-    const int     lane    = tid & 31;
-    const int64_t n_tiles = (U + SPMV_THREADS - 1) / SPMV_THREADS;
+    const int64_t n_tiles = (U + SPMV_TILE - 1) / SPMV_TILE;
+    const int64_t G       = gridDim.x;
     double        dot     = 0.0;
-    for(int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
+    TileLoad<VT>  cur;
+    int64_t       tile = blockIdx.x;
+    if(PF)
     {
-        const int64_t base = tile * SPMV_THREADS;
-        const int64_t rem  = U - base;
-        const int     n    = rem < SPMV_THREADS ? (int)rem : SPMV_THREADS;
-        const int64_t k    = base + tid;
-        int32_t       r    = -1;
-        XT            a0 = 0, a1 = 0, a2 = 0;
-        if(tid < n)
+        const int64_t e0 = tile * SPMV_TILE + SPMV_BPT * tid;
+        load_tile(cur, e0, S, tile < n_tiles && e0 < S, rows, cols, trank, vals);
+    }
+    for(int it = 0; tile < n_tiles; ++it, tile += G)
+    {
+        const int     buf = NB == 2 ? (it & 1) : 0;
+        const int64_t rem = U - tile * SPMV_TILE;
+        const int     n   = rem < SPMV_TILE ? (int)rem : SPMV_TILE;
+        if(PF)
         {
-            r               = __ldg(rows + k);
-            const int32_t c = __ldg(cols + k);
-            const int     rk = __ldg(trank + k);
-            XT b[9];
-#pragma unroll
-            for(int q = 0; q < 9; ++q)
-                b[q] = (XT)__ldg(vals + (int64_t)q * S + k);
-            const XT xj0 = __ldg(x + 3 * (int64_t)c), xj1 = __ldg(x + 3 * (int64_t)c + 1),
-                     xj2 = __ldg(x + 3 * (int64_t)c + 2);
-            const XT xi0 = __ldg(x + 3 * (int64_t)r), xi1 = __ldg(x + 3 * (int64_t)r + 1),
-                     xi2 = __ldg(x + 3 * (int64_t)r + 2);
-            // column-major: B(p,q) = b[q*3 + p]
-            a0 = b[0] * xj0 + b[3] * xj1 + b[6] * xj2;
-            a1 = b[1] * xj0 + b[4] * xj1 + b[7] * xj2;
-            a2 = b[2] * xj0 + b[5] * xj1 + b[8] * xj2;
-            const double d = (double)xi0 * (double)a0 + (double)xi1 * (double)a1 + (double)xi2 * (double)a2;
-            const bool   off = r != c;
-            s_t[0][rk] = off ? b[0] * xi0 + b[1] * xi1 + b[2] * xi2 : XT(0);
-            s_t[1][rk] = off ? b[3] * xi0 + b[4] * xi1 + b[5] * xi2 : XT(0);
-            s_t[2][rk] = off ? b[6] * xi0 + b[7] * xi1 + b[8] * xi2 : XT(0);
-            s_col[rk]  = c;
-            if(WITH_DOT)
-                dot += off ? 2.0 * d : d;
+            TileLoad<VT>  nxt;
+            const int64_t tn = tile + G, en = tn * SPMV_TILE + SPMV_BPT * tid;
+            load_tile(nxt, en, S, tn < n_tiles && en < S, rows, cols, trank, vals);
+            tile_rows<VT, XT, WITH_DOT>(cur, x, y, s_t[buf], s_col[buf], dot);
+            cur = nxt;
         }
-        if(seg_scan3<XT>(r, a0, a1, a2, lane) && r >= 0)
+        else
         {
-            atomic_add_t(y + 3 * (int64_t)r, a0);
-            atomic_add_t(y + 3 * (int64_t)r + 1, a1);
-            atomic_add_t(y + 3 * (int64_t)r + 2, a2);
+            const int64_t e0 = tile * SPMV_TILE + SPMV_BPT * tid;
+            load_tile(cur, e0, S, e0 < S, rows, cols, trank, vals);
+            tile_rows<VT, XT, WITH_DOT>(cur, x, y, s_t[buf], s_col[buf], dot);
         }
         __syncthreads();
-        int32_t tc = -1;
-        XT      t0 = 0, t1 = 0, t2 = 0;
-        if(tid < n)
-        {
-            tc = s_col[tid];
-            t0 = s_t[0][tid];
-            t1 = s_t[1][tid];
-            t2 = s_t[2][tid];
-        }
-        if(seg_scan3<XT>(tc, t0, t1, t2, lane) && tc >= 0)
-        {
-            atomic_add_t(y + 3 * (int64_t)tc, t0);
-            atomic_add_t(y + 3 * (int64_t)tc + 1, t1);
-            atomic_add_t(y + 3 * (int64_t)tc + 2, t2);
-        }
-        __syncthreads();
+        tile_cols<XT>(tid, n, s_t[buf], s_col[buf], y);
+        if(NB == 1)
+            __syncthreads();
     }
     if(WITH_DOT)
     {
@@ -146,114 +240,36 @@ __global__ void __launch_bounds__(SPMV_THREADS, 3)
     }
 }
 
-// Many-warp variant: one thread per block, grid-stride, no staging; the
-// warp merges runs of equal rows, the transposed half scatters directly.
-constexpr int WARP_KERNEL_BLOCK = 256;
-
-template <typename VT, typename XT, bool WITH_DOT>
-__global__ void __launch_bounds__(WARP_KERNEL_BLOCK)
-    k_spmv_warp(int64_t U, int64_t S, const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
-                const VT* __restrict__ vals, const XT* __restrict__ x, XT* y, double* partials,
-                unsigned int* counter, double* dot_out, const int* stop)
+// persistent grid: the CTAs that fit on the SMs at once, capped by the tiles
+// (and by spmv_grid, which sizes the reduction partials)
+template <typename K>
+int tile_grid(K kernel, int64_t U)
 {
-    if(stop && *stop)
-        return;
-    const int     lane   = threadIdx.x & 31;
-    double        dot    = 0.0;
-    const int64_t stride = (int64_t)gridDim.x * WARP_KERNEL_BLOCK;
-    for(int64_t base = (int64_t)blockIdx.x * WARP_KERNEL_BLOCK; base < U; base += stride)
-    {
-        const int64_t k = base + threadIdx.x;
-        int32_t       r = -1;
-        XT            a0 = 0, a1 = 0, a2 = 0;
-        if(k < U)
-        {
-            r               = __ldg(rows + k);
-            const int32_t c = __ldg(cols + k);
-            XT b[9];
-#pragma unroll
-            for(int q = 0; q < 9; ++q)
-                b[q] = (XT)__ldg(vals + (int64_t)q * S + k);
-            const XT xj0 = __ldg(x + 3 * (int64_t)c), xj1 = __ldg(x + 3 * (int64_t)c + 1),
-                     xj2 = __ldg(x + 3 * (int64_t)c + 2);
-            const XT xi0 = __ldg(x + 3 * (int64_t)r), xi1 = __ldg(x + 3 * (int64_t)r + 1),
-                     xi2 = __ldg(x + 3 * (int64_t)r + 2);
-            a0 = b[0] * xj0 + b[3] * xj1 + b[6] * xj2;
-            a1 = b[1] * xj0 + b[4] * xj1 + b[7] * xj2;
-            a2 = b[2] * xj0 + b[5] * xj1 + b[8] * xj2;
-            const double d = (double)xi0 * (double)a0 + (double)xi1 * (double)a1 + (double)xi2 * (double)a2;
-            if(r != c)
-            {
-                atomic_add_t(y + 3 * (int64_t)c, b[0] * xi0 + b[1] * xi1 + b[2] * xi2);
-                atomic_add_t(y + 3 * (int64_t)c + 1, b[3] * xi0 + b[4] * xi1 + b[5] * xi2);
-                atomic_add_t(y + 3 * (int64_t)c + 2, b[6] * xi0 + b[7] * xi1 + b[8] * xi2);
-                if(WITH_DOT)
-                    dot += 2.0 * d;
-            }
-            else if(WITH_DOT)
-                dot += d;
-        }
-        if(seg_scan3<XT>(r, a0, a1, a2, lane) && r >= 0)
-        {
-            atomic_add_t(y + 3 * (int64_t)r, a0);
-            atomic_add_t(y + 3 * (int64_t)r + 1, a1);
-            atomic_add_t(y + 3 * (int64_t)r + 2, a2);
-        }
-    }
-    if(WITH_DOT)
-    {
-        double v[1] = {dot}, tot[1];
-        if(grid_sum<1>(v, partials, counter, tot))
-            *dot_out = tot[0];
-    }
-}
-
-// kernel selection: "tile" (default) or "warp", from B2S_SPMV_KERNEL, read once
-int spmv_variant()
-{
-    static const int v = []
-    {
-        const char* e = std::getenv("B2S_SPMV_KERNEL");
-        return (e && std::string(e) == "warp") ? 0 : 1;
-    }();
-    return v;
-}
-
-int tile_grid(int64_t U)
-{
-    const int64_t t = (U + SPMV_THREADS - 1) / SPMV_THREADS;
-    return (int)std::max<int64_t>(1, std::min<int64_t>(t, (int64_t)NUM_SMS_HINT * 3));
-}
-
-int warp_grid(int64_t U)
-{
-    const int64_t g = (U + WARP_KERNEL_BLOCK - 1) / WARP_KERNEL_BLOCK;
-    return (int)std::max<int64_t>(1, std::min<int64_t>(g, (int64_t)NUM_SMS_HINT * 8));
+    int occ = 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, SPMV_THREADS, 0) != cudaSuccess || occ < 1)
+        occ = 1;
+    const int64_t t = (U + SPMV_TILE - 1) / SPMV_TILE;
+    const int64_t g = std::min<int64_t>(t, (int64_t)NUM_SMS_HINT * std::min(occ, 8));
+    return (int)std::max<int64_t>(1, g);
 }
 
 template <typename VT, typename XT, bool DOT>
 void launch_stream(cudaStream_t st, int64_t U, int64_t S, const int32_t* rows, const int32_t* cols,
                    const uint16_t* trank, const VT* vals, const XT* x, XT* y, Reduction* red, double* d_dot,
-                   const int* stop, int* err)
+                   const int* stop)
 {
-    if(spmv_variant() == 0)
-    {
-        k_spmv_warp<VT, XT, DOT><<<warp_grid(U), WARP_KERNEL_BLOCK, 0, st>>>(
-            U, S, rows, cols, vals, x, y, red ? red->partials.data() : nullptr, red ? red->counter.data() : nullptr,
-            d_dot, stop);
-        B2S_CHECK_LAUNCH();
-        return;
-    }
-    k_spmv_tile<VT, XT, DOT><<<tile_grid(U), SPMV_THREADS, 0, st>>>(
-        U, S, rows, cols, trank, vals, x, y, red ? red->partials.data() : nullptr,
-        red ? red->counter.data() : nullptr, d_dot, stop);
+    auto k = k_spmv_tile<VT, XT, DOT>;
+    k<<<tile_grid(k, U), SPMV_THREADS, 0, st>>>(U, S, rows, cols, trank, vals, x, y,
+                                                red ? red->partials.data() : nullptr,
+                                                red ? red->counter.data() : nullptr, d_dot, stop);
     B2S_CHECK_LAUNCH();
 }
 }  // namespace
 
 int spmv_grid(int64_t U)
 {
-    return std::max(tile_grid(U), warp_grid(U));
+    const int64_t t = (U + SPMV_TILE - 1) / SPMV_TILE;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(t, (int64_t)NUM_SMS_HINT * 8));
 }
 
 void ensure_reduction(Reduction& red, int grid, int nv)
@@ -305,15 +321,14 @@ void spmv_f64(b2s_solver* s, const Matrix& A, const double* x, double* y, double
             B2S_CUDA(cudaMemsetAsync(d_dot, 0, sizeof(double), st));
         return;
     }
-    int* err = device_error_flag(s);
     B2S_REQUIRE(A.has_trank, B2S_ERR_STATE, "matrix lacks the SpMV tile ranks");
     ensure_reduction(s->red, spmv_grid(A.nnz), 1);
     if(d_dot)
         launch_stream<double, double, true>(st, A.nnz, A.stride, A.rows.data(), A.cols.data(), A.trank.data(), A.vals.data(), x, y,
-                                            &s->red, d_dot, nullptr, err);
+                                            &s->red, d_dot, nullptr);
     else
         launch_stream<double, double, false>(st, A.nnz, A.stride, A.rows.data(), A.cols.data(), A.trank.data(), A.vals.data(), x,
-                                             y, nullptr, nullptr, nullptr, err);
+                                             y, nullptr, nullptr, nullptr);
 }
 
 // launch shared with the PCG graph (y must be zero beforehand)
@@ -323,7 +338,7 @@ void spmv_f64_launch(b2s_solver* s, const Matrix& A, const double* x, double* y,
     if(A.nnz == 0)
         return;
     launch_stream<double, double, true>(s->stream, A.nnz, A.stride, A.rows.data(), A.cols.data(), A.trank.data(), A.vals.data(), x,
-                                        y, &red, d_dot, stop, device_error_flag(s));
+                                        y, &red, d_dot, stop);
 }
 
 // FP32 values and vectors (mixed precision), FP64 dot
@@ -333,7 +348,7 @@ void spmv_f32_launch(b2s_solver* s, const Matrix& A, const float* x, float* y, R
     if(A.nnz == 0)
         return;
     launch_stream<float, float, true>(s->stream, A.nnz, A.stride, A.rows.data(), A.cols.data(), A.trank.data(), A.vals32.data(), x,
-                                      y, &red, d_dot, stop, device_error_flag(s));
+                                      y, &red, d_dot, stop);
 }
 
 // ---------------------------------------------------------------------------
@@ -354,7 +369,7 @@ __global__ void __launch_bounds__(RED_BLOCK) k_dot(const double* __restrict__ a,
 }
 }  // namespace
 
-int reduction_grid() { return NUM_SMS_HINT * 4; }
+int reduction_grid() { return NUM_SMS_HINT * 8; }
 
 void launch_dot(b2s_solver* s, const double* a, const double* b, int64_t n, double* d_out)
 {

@@ -323,6 +323,29 @@ def test_mixed_pcg_tight_tolerance_by_residual_replacement(solver, cuda, cube10)
     assert np.linalg.norm(x.cpu().numpy() - xt) <= 1e-6 * np.linalg.norm(xt)
 
 
+@pytest.mark.parametrize("which", ["cube10", "stack_small"])
+def test_mixed_mas_apply_matches_oracle_bf16(request, solver, cuda, which):
+    """Tensor-core apply of the BF16 diagonal-scaled inverses against the
+    oracle's apply with the same BF16 entries: they differ only by the FP32
+    accumulation order and the ~16-bit (hi + lo BF16) residual operand, so
+    relative 1e-4 in norm and 1e-3 of max|z| per entry."""
+    import torch
+
+    s = request.getfixturevalue(which)
+    b, A, M = _mas_setup(solver, s, cuda, partition_rcb(s.positions))
+    M.quantize(2)
+    rng = np.random.default_rng(21)
+    for trial in range(3):
+        r = rng.standard_normal(3 * s.n_verts) * (10.0 ** (3 * trial))
+        zr = M.apply(r)
+        r32 = torch.tensor(r, dtype=torch.float32, device=cuda)
+        z32 = torch.zeros_like(r32)
+        solver.precond_apply_mixed(r32, z32)
+        z = z32.double().cpu().numpy()
+        assert np.linalg.norm(z - zr) <= 1e-4 * np.linalg.norm(zr)
+        assert np.max(np.abs(z - zr)) <= 1e-3 * np.max(np.abs(zr))
+
+
 def test_mixed_spmv_bf16_apply_consistent(solver, cuda, cube10):
     """The mixed path's BF16 MAS apply stays within BF16 rounding of the FP32
     apply (relative 2e-2 in the worst entry, 5e-3 in norm)."""
