@@ -195,6 +195,66 @@ int b2s_set_timing(b2s_solver* s, int enable);
 int b2s_get_timers(const b2s_solver* s, b2s_timers* out);
 int b2s_reset_timers(b2s_solver* s);
 
+/* ---- learned PCG warm start ------------------------------------------------------------
+ * No counterpart in the reference (its PCG starts from x0 = 0,
+ * linear_fused_pcg.cu:1782-2005). A small MLP on MAS level-1 aggregates
+ * predicts the initial guess of the next Newton solve from the gradient b and
+ * the solutions of earlier solves of the same run (history h1 = the latest,
+ * h2, h3 older; at most B2S_WS_HISTORY device vectors of 3 n doubles).
+ * Per aggregate, the network reads 22 features (mean of b, and of each field
+ * f = {h1, h1 - h2, h1 - 2 h2 + h3, z = P b}: its mean and log RMS, plus the
+ * mean products of consecutive fields) and outputs 4 coefficients c; the
+ * predicted field is d_v = sum_i c_i f_i(v) on every vertex of the aggregate.
+ * The start x0 is the A-optimal (Galerkin) combination of the candidate
+ * vectors of `mode`, checked by its FP64 residual: when ||b - A x0|| is not
+ * below ||b||, x0 = 0 (the plain start). Training uses Newton systems of the
+ * same run (b2s_ws_add_sample with the solved x), a quadratic per-aggregate
+ * loss sum_v |d_v - x_v|^2 / sum_v |x_v|^2 (fields scaled by RMS(z)), Adam,
+ * FP32 weights; inference reads BF16 copies of the weights. Requires an
+ * assembled matrix and the MAS preconditioner (b2s_precond_assemble). */
+#define B2S_WS_HISTORY 3
+#define B2S_WS_FEATURES 22
+#define B2S_WS_OUTPUTS 4
+#define B2S_WS_MODE_ZERO 0    /* x0 = 0 */
+#define B2S_WS_MODE_PREV 1    /* Galerkin on {h1}: the scaled previous solution */
+#define B2S_WS_MODE_HISTORY 2 /* Galerkin on {h1, h2, h3}, no network */
+#define B2S_WS_MODE_LEARNED 3 /* Galerkin on {network field, h1, h2, h3} */
+
+typedef struct b2s_ws_info
+{
+    int    mode;          /* mode used (ZERO when the residual check rejected the start) */
+    int    n_candidates;  /* vectors in the Galerkin combination */
+    double coeff[4];      /* their coefficients */
+    double rel_res0;      /* ||b - A x0|| / ||b|| of the returned x0 (FP64) */
+    double rel_res_tried; /* the same for the candidate before the check */
+    double predict_ms;    /* device time of the prediction (features, MLP, Galerkin) */
+} b2s_ws_info;
+
+/* allocate the network (hidden width `hidden`, 3 layers) with seeded random weights */
+int b2s_ws_init(b2s_solver* s, int32_t hidden, uint64_t seed);
+/* append one training sample: this system's aggregates with the solved x (device) */
+int b2s_ws_add_sample(b2s_solver* s, const double* d_b, int32_t n_hist, const double* const* d_hist,
+                      const double* d_x);
+int b2s_ws_num_samples(const b2s_solver* s, int32_t* n_samples, int64_t* n_rows);
+/* feature mean / std over the stored samples (inputs are standardised with them) */
+int b2s_ws_fit_normalization(b2s_solver* s);
+/* `epochs` passes over the stored samples (one Adam step per sample, order from `seed`) */
+int b2s_ws_train(b2s_solver* s, int32_t epochs, double lr, uint64_t seed, double* h_mean_loss);
+/* loss and gradient (n_params floats, host) of stored sample `index`, no update */
+int b2s_ws_loss_grad(b2s_solver* s, int32_t index, double* h_loss, float* h_grad);
+/* parameters: W0[F x H] b0[H] W1[H x H] b1[H] W2[H x O] b2[O] (row-major, x W + b), then
+ * feature mean[F] and std[F]; h_params NULL = size query into *n */
+int b2s_ws_get_params(const b2s_solver* s, float* h_params, int64_t* n);
+int b2s_ws_set_params(b2s_solver* s, const float* h_params, int64_t n);
+/* a stored sample for checking: raw features [rows x F], H [rows x 10] (upper
+ * triangle of the 4x4 field Gram), q [rows x 4], c0 [rows], loss normaliser;
+ * NULL pointers = size query of *rows */
+int b2s_ws_get_sample(const b2s_solver* s, int32_t index, int32_t* rows, float* h_feat, float* h_H,
+                      float* h_q, float* h_c0, double* h_norm);
+/* the warm start x0 (device, 3 n doubles) for the current system */
+int b2s_ws_predict(b2s_solver* s, int32_t mode, const double* d_b, int32_t n_hist,
+                   const double* const* d_hist, double* d_x0, b2s_ws_info* info);
+
 /* ---- SpMV for callers that cannot allocate -------------------------------------------
  * No counterpart in the reference. The same y = A x and x.(A x) as b2s_spmv,
  * for callers that must not (or cannot) call cudaMalloc: code running inside

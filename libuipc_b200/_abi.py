@@ -24,6 +24,31 @@ B2S_PRECISION_FP64 = 0
 B2S_PRECISION_MIXED = 1
 
 
+B2S_WS_MODE_ZERO = 0
+B2S_WS_MODE_PREV = 1
+B2S_WS_MODE_HISTORY = 2
+B2S_WS_MODE_LEARNED = 3
+B2S_WS_HISTORY = 3
+B2S_WS_FEATURES = 22
+B2S_WS_OUTPUTS = 4
+
+
+class WsInfo(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int32),
+        ("n_candidates", C.c_int32),
+        ("coeff", C.c_double * 4),
+        ("rel_res0", C.c_double),
+        ("rel_res_tried", C.c_double),
+        ("predict_ms", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["coeff"] = list(self.coeff)[: self.n_candidates]
+        return d
+
+
 class PcgOptions(C.Structure):
     _fields_ = [
         ("tol", C.c_double),
@@ -102,6 +127,16 @@ SIGNATURES = {
     "b2s_set_timing": (C.c_int, [vp, C.c_int]),
     "b2s_get_timers": (C.c_int, [vp, C.POINTER(Timers)]),
     "b2s_reset_timers": (C.c_int, [vp]),
+    "b2s_ws_init": (C.c_int, [vp, i32, C.c_uint64]),
+    "b2s_ws_add_sample": (C.c_int, [vp, vp, i32, vp, vp]),
+    "b2s_ws_num_samples": (C.c_int, [vp, i32p, i64p]),
+    "b2s_ws_fit_normalization": (C.c_int, [vp]),
+    "b2s_ws_train": (C.c_int, [vp, i32, C.c_double, C.c_uint64, dp]),
+    "b2s_ws_loss_grad": (C.c_int, [vp, i32, dp, fp]),
+    "b2s_ws_get_params": (C.c_int, [vp, fp, i64p]),
+    "b2s_ws_set_params": (C.c_int, [vp, fp, i64]),
+    "b2s_ws_get_sample": (C.c_int, [vp, i32, i32p, fp, fp, fp, fp, dp]),
+    "b2s_ws_predict": (C.c_int, [vp, i32, vp, i32, vp, vp, C.POINTER(WsInfo)]),
     "b2s_spmv_noalloc": (C.c_int, [i32, i64, vp, vp, vp, vp, vp, vp, vp]),
 }
 

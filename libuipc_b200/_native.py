@@ -47,6 +47,8 @@ def load_scene_lib() -> C.CDLL:
         lib.b2g_default_config.restype = None
         lib.b2g_generate.argtypes = [C.c_void_p, C.POINTER(vp)]
         lib.b2g_generate.restype = C.c_int
+        lib.b2g_generate_state.argtypes = [C.c_void_p, c_dbl_p, c_dbl_p, C.POINTER(vp)]
+        lib.b2g_generate_state.restype = C.c_int
         lib.b2g_free.argtypes = [vp]
         lib.b2g_free.restype = None
         lib.b2g_last_error.argtypes = []

@@ -36,7 +36,15 @@ NVFLAGS = ARCH + [
     "-Xcompiler",
     "-Wall",
 ]
-SOLVE_SOURCES = ["b2s_assemble.cu", "b2s_spmv.cu", "b2s_mas.cu", "b2s_pcg.cu", "b2s_abi.cu", "b2s_noalloc.cu"]
+SOLVE_SOURCES = [
+    "b2s_assemble.cu",
+    "b2s_spmv.cu",
+    "b2s_mas.cu",
+    "b2s_pcg.cu",
+    "b2s_learned.cu",
+    "b2s_abi.cu",
+    "b2s_noalloc.cu",
+]
 
 
 def _run(cmd: list[str]) -> None:

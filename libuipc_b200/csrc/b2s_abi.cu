@@ -129,6 +129,7 @@ int b2s_destroy(b2s_solver* s)
         cudaEventDestroy(s->ev_end);
     for(cudaEvent_t e : s->iter_events)
         cudaEventDestroy(e);
+    b2s::ws_free(s->ws);
     if(s->own_stream)
         cudaStreamDestroy(s->own_stream);
     delete s;
@@ -483,6 +484,86 @@ int b2s_partition_maps(int32_t n, const int32_t* part_ids, int32_t max_part, int
         r2p[v]             = slot;
     }
     return B2S_OK;
+}
+
+// ---- learned warm start -------------------------------------------------------------
+int b2s_ws_init(b2s_solver* s, int32_t hidden, uint64_t seed)
+{
+    return guarded(s, [&] { b2s::ws_init(s, hidden, seed); });
+}
+
+int b2s_ws_add_sample(b2s_solver* s, const double* d_b, int32_t n_hist, const double* const* d_hist,
+                      const double* d_x)
+{
+    return guarded(s, [&] { b2s::ws_add_sample(s, d_b, n_hist, d_hist, d_x); });
+}
+
+int b2s_ws_num_samples(const b2s_solver* s, int32_t* n_samples, int64_t* n_rows)
+{
+    b2s_solver* m = const_cast<b2s_solver*>(s);
+    return guarded(m, [&] { b2s::ws_num_samples(m, n_samples, n_rows); });
+}
+
+int b2s_ws_fit_normalization(b2s_solver* s)
+{
+    return guarded(s, [&] { b2s::ws_fit_normalization(s); });
+}
+
+int b2s_ws_train(b2s_solver* s, int32_t epochs, double lr, uint64_t seed, double* h_mean_loss)
+{
+    return guarded(s,
+                   [&]
+                   {
+                       const double l = b2s::ws_train(s, epochs, lr, seed);
+                       if(h_mean_loss)
+                           *h_mean_loss = l;
+                   });
+}
+
+int b2s_ws_loss_grad(b2s_solver* s, int32_t index, double* h_loss, float* h_grad)
+{
+    return guarded(s,
+                   [&]
+                   {
+                       const double l = b2s::ws_loss_grad(s, index, h_grad);
+                       if(h_loss)
+                           *h_loss = l;
+                   });
+}
+
+int b2s_ws_get_params(const b2s_solver* s, float* h_params, int64_t* n)
+{
+    b2s_solver* m = const_cast<b2s_solver*>(s);
+    return guarded(m,
+                   [&]
+                   {
+                       B2S_REQUIRE(n, B2S_ERR_ARGUMENT, "null size");
+                       *n = b2s::ws_get_params(m, h_params);
+                   });
+}
+
+int b2s_ws_set_params(b2s_solver* s, const float* h_params, int64_t n)
+{
+    return guarded(s, [&] { b2s::ws_set_params(s, h_params, n); });
+}
+
+int b2s_ws_get_sample(const b2s_solver* s, int32_t index, int32_t* rows, float* h_feat, float* h_H, float* h_q,
+                      float* h_c0, double* h_norm)
+{
+    b2s_solver* m = const_cast<b2s_solver*>(s);
+    return guarded(m,
+                   [&]
+                   {
+                       const int r = b2s::ws_get_sample(m, index, h_feat, h_H, h_q, h_c0, h_norm);
+                       if(rows)
+                           *rows = r;
+                   });
+}
+
+int b2s_ws_predict(b2s_solver* s, int32_t mode, const double* d_b, int32_t n_hist, const double* const* d_hist,
+                   double* d_x0, b2s_ws_info* info)
+{
+    return guarded(s, [&] { b2s::ws_predict(s, mode, d_b, n_hist, d_hist, d_x0, info); });
 }
 
 }  // extern "C"

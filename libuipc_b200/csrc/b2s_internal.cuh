@@ -121,9 +121,9 @@ struct Matrix
     DBuf<int32_t>  cols;     // [stride]
     DBuf<double>   vals;     // [9][stride]: component q (column-major index) at vals[q*stride + k]
     DBuf<float>    vals32;   // FP32 copy of vals (mixed precision), same layout
-    // rank of each block in (column, index) order inside its 512-block SpMV
-    // tile: the SpMV sorts the transposed contributions of a tile by column
-    // in shared memory and merges equal columns before its atomics
+    // rank of each block in (column, index) order inside its SPMV_TILE-block
+    // tile: the SpMV places the transposed contributions of a tile by column
+    // in shared memory and merges equal columns before its reductions
     DBuf<uint16_t> trank;    // [stride]
     bool           has_trank = false;
     DBuf<int32_t>  diag_index;  // [nb] position of block (i,i), -1 if absent
@@ -218,6 +218,9 @@ struct PcgState
     long long        graph_mixed_kernels = 0;
 };
 
+struct LearnedState;  // learned warm start (b2s_learned.cu)
+void ws_free(LearnedState* w);
+
 }  // namespace b2s
 
 // the opaque ABI handle
@@ -243,6 +246,7 @@ struct b2s_solver
     b2s_timers               timers{};
     cudaEvent_t              ev_begin = nullptr, ev_end = nullptr;
     std::vector<cudaEvent_t> iter_events;  // 4 per iteration of a graph block
+    b2s::LearnedState*       ws = nullptr;  // learned warm start, created on first use
 };
 
 namespace b2s
@@ -283,6 +287,19 @@ void mas_apply(b2s_solver* s, const double* r, double* z);
 // PCG
 void pcg_solve(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st);
 void drop_graphs(b2s_solver* s);
+
+// learned warm start
+void    ws_init(b2s_solver* s, int hidden, uint64_t seed);
+void    ws_add_sample(b2s_solver* s, const double* b, int n_hist, const double* const* hist, const double* x);
+void    ws_num_samples(b2s_solver* s, int32_t* n, int64_t* rows);
+void    ws_fit_normalization(b2s_solver* s);
+double  ws_train(b2s_solver* s, int epochs, double lr, uint64_t seed);
+double  ws_loss_grad(b2s_solver* s, int index, float* h_grad);
+int64_t ws_get_params(b2s_solver* s, float* h);
+void    ws_set_params(b2s_solver* s, const float* h, int64_t n);
+int     ws_get_sample(b2s_solver* s, int index, float* feat, float* Hs, float* q, float* c0, double* norm);
+void    ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const double* const* hist, double* x0,
+                   b2s_ws_info* info);
 
 inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
 }  // namespace b2s

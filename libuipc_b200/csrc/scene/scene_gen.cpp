@@ -234,7 +234,13 @@ void b2g_default_config(b2g_config* c)
 
 const char* b2g_last_error(void) { return g_err.c_str(); }
 
-int b2g_generate(const b2g_config* cfg, b2g_system** out)
+}  // extern "C"
+
+namespace
+{
+// x_in / xt_in (optional, [n_verts*3]): current positions and kinetic target
+// x_tilde; null = the scene's default first Newton step from rest
+int generate_impl(const b2g_config* cfg, const double* x_in, const double* xt_in, b2g_system** out)
 {
     try
     {
@@ -332,7 +338,17 @@ int b2g_generate(const b2g_config* cfg, b2g_system** out)
         // ---- current positions ----
         sys->x = sys->x_rest;
         std::vector<uint8_t> fixed(nv, 0);
-        if(C.scene == 2)
+        if(x_in)
+        {
+            std::memcpy(sys->x.data(), x_in, sizeof(double) * nv * 3);
+            if(C.scene == 2)
+                for(int64_t g = 0; g < nv; ++g)
+                {
+                    const int64_t i = (g % verts_per) % vx;
+                    fixed[g]        = (i == 0 || i == nx) ? 1 : 0;
+                }
+        }
+        else if(C.scene == 2)
         {
             // bar along x, ends rotated by +-twist about the x axis through the
             // cross-section centre; the twist is linear along the bar and both
@@ -405,7 +421,7 @@ int b2g_generate(const b2g_config* cfg, b2g_system** out)
             double miny = 1e300;
             for(int64_t k = 0; k < vz; ++k)
                 for(int64_t i = 0; i < vx; ++i)
-                    miny = std::min(miny, sys->x[vid(0, i, 0, k) * 3 + 1]);
+                    miny = std::min(miny, sys->x_rest[vid(0, i, 0, k) * 3 + 1]);
             ground_y = miny - C.ground_offset;
             for(int64_t k = 0; k < vz; ++k)
                 for(int64_t i = 0; i < vx; ++i)
@@ -580,13 +596,16 @@ int b2g_generate(const b2g_config* cfg, b2g_system** out)
                 }
         };
 
-        // kinetic: x_tilde = x_prev + dt v + dt^2 g with x_prev = rest, v = 0
+        // kinetic: x_tilde = x_prev + dt v + dt^2 g (default: x_prev = rest, v = 0)
 #pragma omp parallel for schedule(static)
         for(int64_t g = 0; g < nv; ++g)
         {
             double H[9] = {mass[g], 0, 0, 0, mass[g], 0, 0, 0, mass[g]};
             write_block(g, (int32_t)g, (int32_t)g, H);
             double xt[3] = {sys->x_rest[g * 3], sys->x_rest[g * 3 + 1] - dt2 * C.gravity, sys->x_rest[g * 3 + 2]};
+            if(xt_in)
+                for(int a = 0; a < 3; ++a)
+                    xt[a] = xt_in[g * 3 + a];
             for(int a = 0; a < 3; ++a)
                 sys->grad[g * 3 + a] += mass[g] * (sys->x[g * 3 + a] - xt[a]);
         }
@@ -775,6 +794,21 @@ int b2g_generate(const b2g_config* cfg, b2g_system** out)
         g_err = e.what();
         return 1;
     }
+}
+}  // namespace
+
+extern "C" {
+
+int b2g_generate(const b2g_config* cfg, b2g_system** out) { return generate_impl(cfg, nullptr, nullptr, out); }
+
+int b2g_generate_state(const b2g_config* cfg, const double* x, const double* x_tilde, b2g_system** out)
+{
+    if(!x || !x_tilde)
+    {
+        g_err = "b2g_generate_state: null state";
+        return 1;
+    }
+    return generate_impl(cfg, x, x_tilde, out);
 }
 
 void b2g_free(b2g_system* s) { delete s; }

@@ -53,6 +53,11 @@ void b2g_default_config(b2g_config* cfg);
 // Generate one Newton system. Returns 0 on success, non-zero on error
 // (message through b2g_last_error()).
 int b2g_generate(const b2g_config* cfg, b2g_system** out);
+// The Newton system of the same mesh at a given state: x = current positions,
+// x_tilde = x_prev + dt v + dt^2 g (both [n_verts*3]). The ground plane stays
+// where the rest shape puts it; in the twisted bar the end layers are fixed
+// (the caller places them). Used to step a scene through time.
+int b2g_generate_state(const b2g_config* cfg, const double* x, const double* x_tilde, b2g_system** out);
 void b2g_free(b2g_system* sys);
 const char* b2g_last_error(void);
 

@@ -178,6 +178,79 @@ class Solver:
     def set_stream(self, stream_handle: int | None):
         self._check(self.lib.b2s_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None))
 
+    # ---- learned warm start (no counterpart in the reference) ---------------
+    @staticmethod
+    def _hist(history):
+        history = [h for h in (history or []) if h is not None][: _abi.B2S_WS_HISTORY]
+        arr = (C.c_void_p * max(len(history), 1))(*[h.data_ptr() for h in history])
+        return len(history), arr
+
+    def ws_init(self, hidden: int = 128, seed: int = 0):
+        self._check(self.lib.b2s_ws_init(self.h, int(hidden), int(seed)))
+
+    def ws_add_sample(self, b, x, history=()):
+        """Store this system's aggregates with its solved x (device tensors);
+        history: the latest earlier solutions, newest first."""
+        n, arr = self._hist(history)
+        self._check(self.lib.b2s_ws_add_sample(self.h, _ptr(b), n, C.cast(arr, C.c_void_p), _ptr(x)))
+
+    def ws_num_samples(self):
+        n = C.c_int32()
+        rows = C.c_int64()
+        self._check(self.lib.b2s_ws_num_samples(self.h, C.byref(n), C.byref(rows)))
+        return int(n.value), int(rows.value)
+
+    def ws_fit_normalization(self):
+        self._check(self.lib.b2s_ws_fit_normalization(self.h))
+
+    def ws_train(self, epochs: int, lr: float = 1e-3, seed: int = 0) -> float:
+        loss = C.c_double()
+        self._check(self.lib.b2s_ws_train(self.h, int(epochs), float(lr), int(seed), C.byref(loss)))
+        return float(loss.value)
+
+    def ws_params(self) -> np.ndarray:
+        n = C.c_int64()
+        self._check(self.lib.b2s_ws_get_params(self.h, None, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        self._check(self.lib.b2s_ws_get_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), C.byref(n)))
+        return out
+
+    def ws_set_params(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self.lib.b2s_ws_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), int(p.size)))
+
+    def ws_loss_grad(self, index: int):
+        n_all = self.ws_params().size - 2 * _abi.B2S_WS_FEATURES
+        g = np.zeros(n_all, np.float32)
+        loss = C.c_double()
+        self._check(self.lib.b2s_ws_loss_grad(self.h, int(index), C.byref(loss),
+                                              g.ctypes.data_as(C.POINTER(C.c_float))))
+        return float(loss.value), g
+
+    def ws_sample(self, index: int) -> dict:
+        rows = C.c_int32()
+        fp = C.POINTER(C.c_float)
+        self._check(self.lib.b2s_ws_get_sample(self.h, int(index), C.byref(rows), None, None, None, None, None))
+        r = rows.value
+        F, O = _abi.B2S_WS_FEATURES, _abi.B2S_WS_OUTPUTS
+        feat = np.zeros((r, F), np.float32)
+        H = np.zeros((r, O * (O + 1) // 2), np.float32)
+        q = np.zeros((r, O), np.float32)
+        c0 = np.zeros(r, np.float32)
+        norm = C.c_double()
+        self._check(self.lib.b2s_ws_get_sample(self.h, int(index), C.byref(rows), feat.ctypes.data_as(fp),
+                                               H.ctypes.data_as(fp), q.ctypes.data_as(fp), c0.ctypes.data_as(fp),
+                                               C.byref(norm)))
+        return {"feat": feat, "H": H, "q": q, "c0": c0, "norm": float(norm.value)}
+
+    def ws_predict(self, b, x0, history=(), mode=_abi.B2S_WS_MODE_LEARNED) -> dict:
+        """Warm start x0 (device tensor, written) for the current system."""
+        n, arr = self._hist(history)
+        info = _abi.WsInfo()
+        self._check(self.lib.b2s_ws_predict(self.h, int(mode), _ptr(b), n, C.cast(arr, C.c_void_p), _ptr(x0),
+                                            C.byref(info)))
+        return info.as_dict()
+
 
 def partition_rcb(positions: np.ndarray, max_part: int = 16) -> np.ndarray:
     lib = load_solve_lib()

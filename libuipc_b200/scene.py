@@ -72,21 +72,47 @@ def default_config() -> B2GConfig:
     return cfg
 
 
-def generate(**overrides) -> NewtonSystem:
-    """Generate a Newton system; keyword arguments override the defaults
-    (10x10x10 Kuhn-split cube, E=1e5, nu=0.45, rho=1e3, dt=0.01, dhat=1e-3)."""
-    lib = load_scene_lib()
+def _config(overrides: dict) -> B2GConfig:
     cfg = default_config()
     for k, v in overrides.items():
         if not hasattr(cfg, k):
             raise KeyError(f"unknown generator option {k!r}")
         setattr(cfg, k, v)
+    return cfg
+
+
+def generate(**overrides) -> NewtonSystem:
+    """Generate a Newton system; keyword arguments override the defaults
+    (10x10x10 Kuhn-split cube, E=1e5, nu=0.45, rho=1e3, dt=0.01, dhat=1e-3)."""
+    return _generate(_config(overrides), None, None)
+
+
+def generate_state(x: np.ndarray, x_tilde: np.ndarray, **overrides) -> NewtonSystem:
+    """The Newton system of the configured mesh at positions ``x`` with the
+    kinetic target ``x_tilde = x_prev + dt v + dt^2 g`` (both ``[n_verts, 3]``).
+    The ground stays where the rest shape puts it; the twisted bar's end
+    layers are fixed at the positions ``x`` gives them."""
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    xt = np.ascontiguousarray(x_tilde, dtype=np.float64).reshape(-1)
+    if x.shape != xt.shape:
+        raise ValueError("x and x_tilde differ in size")
+    return _generate(_config(overrides), x, xt)
+
+
+def _generate(cfg: B2GConfig, x, xt) -> NewtonSystem:
+    lib = load_scene_lib()
     handle = C.c_void_p()
-    rc = lib.b2g_generate(C.byref(cfg), C.byref(handle))
+    if x is None:
+        rc = lib.b2g_generate(C.byref(cfg), C.byref(handle))
+    else:
+        dp = C.POINTER(C.c_double)
+        rc = lib.b2g_generate_state(C.byref(cfg), x.ctypes.data_as(dp), xt.ctypes.data_as(dp), C.byref(handle))
     if rc != 0:
         raise RuntimeError("scene generator failed: " + lib.b2g_last_error().decode())
     try:
         nv = lib.b2g_num_verts(handle)
+        if x is not None and x.size != 3 * nv:
+            raise ValueError(f"state has {x.size // 3} vertices, the mesh {nv}")
         nt = lib.b2g_num_tets(handle)
         T = lib.b2g_num_triplets(handle)
         nadj = lib.b2g_num_adjacency(handle)
