@@ -1,11 +1,17 @@
 """Benchmark: Newton-step linear solve on one B200.
 
 One step = one Newton linear solve of the workload: triplet assembly, MAS
-preconditioner build, PCG to a relative residual of 1e-4 verified in FP64.
-The workload is 8 jittered Kuhn-split tet cubes of 40^3 cells stacked with
-1 mm gaps (551,368 vertices, 1.65 M DoF, 31.8 M raw triplets, ~4.3 M unique
-upper blocks incl. point-triangle / edge-edge contact blocks), synthetic
-(seeded) data generated on the host.
+preconditioner build, warm start, PCG to a relative residual of 1e-4 verified
+in FP64. The workload is 8 jittered Kuhn-split tet cubes of 40^3 cells
+stacked with 1 mm gaps (551,368 vertices, 1.65 M DoF, 31.8 M raw triplets,
+~4.3 M unique upper blocks incl. point-triangle / edge-edge contact blocks),
+synthetic (seeded) data generated on the host. The stack is stepped under
+gravity (backward Euler, one Newton iteration per step) for --history-steps
+steps; those solves give the solution history and the training systems of
+the learned warm start, and the measured system is the next step's. Timed
+modes: plain (FP64, zero start), mixed (FP32/BF16, zero start),
+mixed+history (Galerkin start on the 3 latest solutions, no network) and
+mixed+learned (the headline: network field + history, Galerkin start).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
 
@@ -201,8 +207,12 @@ def main() -> None:
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="stack8x40")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) pass (profiling runs)")
-    ap.add_argument("--modes", default="plain,mixed",
-                    help="solver modes to time (profiling runs may time one); the JSON needs both")
+    ap.add_argument("--modes", default="plain,mixed,mixed+history,mixed+learned",
+                    help="solver modes to time (profiling runs may time a subset); the JSON line needs "
+                         "plain and mixed+learned")
+    ap.add_argument("--history-steps", type=int, default=6,
+                    help="time steps run (and learned from) before the measured system")
+    ap.add_argument("--train-epochs", type=int, default=30)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
 
@@ -231,13 +241,30 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         pg = dist
 
-    s, gen_s = build_workload(args.workload)
-    pid = partition_rcb(s.positions)
-    p2r, r2p = partition_maps(pid)
+    # ---- the run: step the scene, keep the solutions, train the warm start ----------
+    from libuipc_b200.learned import MODES, SequenceRunner
+    from libuipc_b200.sequence import SceneSequence
 
+    w = WORKLOADS[args.workload]
+    t_gen = time.time()
+    seq = SceneSequence(scene=1, cells_x=w["cells"], cells_y=w["cells"], cells_z=w["cells"], n_cubes=w["n_cubes"],
+                        seed=w["seed"])
     stream = torch.cuda.Stream(device=dev)
     solver = Solver(local_rank)
     solver.set_stream(stream.cuda_stream)
+    runner = SequenceRunner(solver, seq, dev)
+    solver.ws_init(128, seed=0)
+    with torch.cuda.stream(stream):
+        runner.run(args.history_steps, newton_iters=1, collect=True)
+    t_train = time.time()
+    solver.ws_fit_normalization()
+    train_loss = solver.ws_train(args.train_epochs, lr=1e-3, seed=0)
+    train_s = time.time() - t_train
+    # the measured system: the next step's Newton system, with the run's history
+    seq.begin_step()
+    s = seq.system()
+    gen_s = time.time() - t_gen - train_s
+    hist = runner.hist(0)
     with torch.cuda.stream(stream):
         rows = torch.from_numpy(s.rows).to(dev)
         cols = torch.from_numpy(s.cols).to(dev)
@@ -245,15 +272,23 @@ def main() -> None:
         b = torch.from_numpy(s.b).to(dev)
         x = torch.zeros_like(b)
     stream.synchronize()
-    solver.mas_init(0, s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
 
-    precisions = {"plain": _abi.B2S_PRECISION_FP64, "mixed": _abi.B2S_PRECISION_MIXED}
+    starts = {"plain": (_abi.B2S_PRECISION_FP64, "zero"), "mixed": (_abi.B2S_PRECISION_MIXED, "zero"),
+              "mixed+history": (_abi.B2S_PRECISION_MIXED, "history"),
+              "mixed+learned": (_abi.B2S_PRECISION_MIXED, "learned")}
+    ws_ms = {"v": 0.0}
 
     def solve_step(mode):
+        precision, start = starts[mode]
         solver.assemble(s.n_verts, rows, cols, vals)
         solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_SWEEP_F32)
-        return solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5,
-                          precision=precisions[mode], replace_every=50)
+        given = start != "zero"
+        if given:
+            info = solver.ws_predict(b, x, hist, MODES[start])
+            ws_ms["v"] += info["predict_ms"]
+            ws_ms["info"] = info
+        return solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, precision=precision,
+                          replace_every=50, x0_given=given)
 
     def barrier():
         torch.cuda.synchronize()
@@ -280,6 +315,7 @@ def main() -> None:
         solver.set_timing(True)
         solve_step(mode)  # captures the graph with its timing nodes outside the timed region
         solver.reset_timers()
+        ws_ms["v"] = 0.0
         clocks = ClockSampler(local_rank)
         barrier()
         clocks.start()
@@ -290,21 +326,22 @@ def main() -> None:
         barrier()
         clk = clocks.stop()
         ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
-        return ms, stats, solver.timers(), clk
+        t = solver.timers()
+        t["warm_start_ms"] = ws_ms["v"]
+        return ms, stats, t, clk, ws_ms.get("info")
 
-    modes = [m for m in args.modes.split(",") if m in precisions]
+    modes = [m for m in args.modes.split(",") if m in starts]
     res = {mode: timed(mode) for mode in modes}
-    if "mixed" not in res or "plain" not in res:
-        # profiling run of a single mode: report it and stop
-        only = modes[0]
-        ms1, st1, tm1, _ = res[only]
+    if "mixed+learned" not in res or "plain" not in res:
+        # profiling run: report the timed modes and stop
         if rank == 0:
-            print(json.dumps({"profiling_mode": only, "ms_per_solve": ms1, "iterations": st1[-1]["iterations_exact"],
-                              "timers": tm1}), flush=True)
+            print(json.dumps({m: {"ms_per_solve": r[0], "iterations": r[1][-1]["iterations_exact"], "timers": r[2]}
+                              for m, r in res.items()}), flush=True)
         solver.close()
         return
     nb, U = solver.matrix_info()
-    ms, stats, tm, clk = res["mixed"]
+    head = "mixed+learned"
+    ms, stats, tm, clk, ws_info = res[head]
 
     # ---- e2e: host (pinned) inputs through the same public API -------------------
     e2e_ms, h2d, d2h = None, 0, 0
@@ -316,7 +353,7 @@ def main() -> None:
         h_x = torch.empty_like(h_b).pin_memory()
         e2e_steps = max(1, min(args.steps, 3))
         solver.set_timing(False)
-        solve_step("mixed")
+        solve_step(head)
         barrier()
         ev0.record(stream)
         for _ in range(e2e_steps):
@@ -325,7 +362,7 @@ def main() -> None:
                 cols.copy_(h_cols, non_blocking=True)
                 vals.copy_(h_vals, non_blocking=True)
                 b.copy_(h_b, non_blocking=True)
-            solve_step("mixed")
+            solve_step(head)
             with torch.cuda.stream(stream):
                 h_x.copy_(x, non_blocking=True)
         ev1.record(stream)
@@ -362,11 +399,19 @@ def main() -> None:
 
     def stages(t, steps):
         return {"assemble": t["assemble_ms"] / steps, "precond_build": t["precond_build_ms"] / steps,
-                "pcg": t["pcg_ms"] / steps, "spmv_avg": t["spmv_ms"] / max(t["spmv_launches"], 1),
+                "warm_start": t.get("warm_start_ms", 0.0) / steps, "pcg": t["pcg_ms"] / steps,
+                "spmv_avg": t["spmv_ms"] / max(t["spmv_launches"], 1),
                 "precond_apply_avg": t["precond_apply_ms"] / max(t["precond_apply_launches"], 1)}
 
-    pms, pstats, ptm, pclk = res["plain"]
-    p_avg, p_ab, p_ach = roof("plain", ptm)
+    def sub(mode):
+        m_ms, m_st, m_tm, m_clk, _ = res[mode]
+        _, _, ach = roof("plain" if mode == "plain" else "mixed", m_tm)
+        return {"value": m_ms, "unit": "ms/solve", "dtype": "f64" if mode == "plain" else "f32/bf16",
+                "pcg_iterations": int(m_st[-1]["iterations_exact"]), "rel_res": float(m_st[-1]["rel_res"]),
+                "stages_ms": stages(m_tm, args.steps), "spmv_gbs": ach, "spmv_frac": ach / peak if peak else None,
+                "clocks": m_clk}
+
+    pms = res["plain"][0]
     last = stats[-1]
     line = {
         "metric": METRIC,
@@ -381,19 +426,23 @@ def main() -> None:
         "vs_baseline": None,
         "dtype": "f32/bf16 (f64 dots, solution, residual replacement)",
         "data": "synthetic",
-        "mode": "mixed",
-        "config": {"workload": args.workload, "n_dof": 3 * s.n_verts, "n_triplets": s.n_triplets,
-                   "upper_blocks": U, "contacts": s.n_contacts, "preconditioner": "mas",
-                   "stop": "FP64-verified rel-res 1e-4", "warm_start": "zero", "parallelism": "replicas",
-                   "l2": "inputs larger than L2 (matrix 0.33 GB, triplets 2.5 GB)"},
+        "mode": head,
+        "config": {"workload": args.workload, "system": f"Newton system of step {seq.step} of the falling stack "
+                   f"(1 Newton iteration per step; history and training from steps 1-{seq.step - 1})",
+                   "n_dof": 3 * s.n_verts, "n_triplets": s.n_triplets, "upper_blocks": U, "contacts": s.n_contacts,
+                   "preconditioner": "mas", "stop": "FP64-verified rel-res 1e-4",
+                   "warm_start": "learned (MLP on MAS level-1 aggregates + Galerkin with the 3 latest solutions)",
+                   "train": {"samples": solver.ws_num_samples()[0], "epochs": args.train_epochs,
+                             "final_loss": train_loss, "seconds": train_s},
+                   "parallelism": "replicas", "l2": "inputs larger than L2 (matrix 0.33 GB, triplets 2.5 GB)"},
         "pcg_iterations": int(last["iterations_exact"]),
         "rel_res": float(last["rel_res"]),
         "replacements": int(last["replacements"]),
+        "warm_start": ws_info,
         "stages_ms": stages(tm, args.steps),
-        "plain": {"value": pms, "unit": "ms/solve", "dtype": "f64", "pcg_iterations": int(pstats[-1]["iterations_exact"]),
-                  "rel_res": float(pstats[-1]["rel_res"]), "stages_ms": stages(ptm, args.steps),
-                  "spmv_gbs": p_ach, "spmv_frac": p_ach / peak if peak else None, "clocks": pclk},
+        "plain": sub("plain"),
         "speedup_vs_plain": pms / ms if ms > 0 else None,
+        "ablation": {m: sub(m) for m in res if m not in ("plain", head)},
         "gpu_launches": int(tm["kernel_launches"]),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
@@ -409,7 +458,6 @@ def main() -> None:
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
-
 
 if __name__ == "__main__":
     main()

@@ -206,8 +206,8 @@ int b2s_reset_timers(b2s_solver* s);
  * mean products of consecutive fields) and outputs 4 coefficients c; the
  * predicted field is d_v = sum_i c_i f_i(v) on every vertex of the aggregate.
  * The start x0 is the A-optimal (Galerkin) combination of the candidate
- * vectors of `mode`, checked by its FP64 residual: when ||b - A x0|| is not
- * below ||b||, x0 = 0 (the plain start). Training uses Newton systems of the
+ * vectors of `mode`, checked in FP64 by the PCG's own residual measure:
+ * when r^T P r (r = b - A x0) is not below b^T P b, x0 = 0 (the plain start). Training uses Newton systems of the
  * same run (b2s_ws_add_sample with the solved x), a quadratic per-aggregate
  * loss sum_v |d_v - x_v|^2 / sum_v |x_v|^2 (fields scaled by RMS(z)), Adam,
  * FP32 weights; inference reads BF16 copies of the weights. Requires an
@@ -227,7 +227,9 @@ typedef struct b2s_ws_info
     double coeff[4];      /* their coefficients */
     double rel_res0;      /* ||b - A x0|| / ||b|| of the returned x0 (FP64) */
     double rel_res_tried; /* the same for the candidate before the check */
-    double predict_ms;    /* device time of the prediction (features, MLP, Galerkin) */
+    double rz_ratio;      /* (r^T P r) / (b^T P b) of the candidate, r = b - A x0, P the preconditioner:
+                             the check; the start is kept when it is below 1 */
+    double predict_ms;    /* device time of the prediction (features, MLP, Galerkin, check) */
 } b2s_ws_info;
 
 /* allocate the network (hidden width `hidden`, 3 layers) with seeded random weights */

@@ -40,6 +40,7 @@ class WsInfo(C.Structure):
         ("coeff", C.c_double * 4),
         ("rel_res0", C.c_double),
         ("rel_res_tried", C.c_double),
+        ("rz_ratio", C.c_double),
         ("predict_ms", C.c_double),
     ]
 

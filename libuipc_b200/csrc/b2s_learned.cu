@@ -17,7 +17,8 @@
 //  5. field d_v = sum_i c_{a(v), i} f_i(v); the start x0 is the A-optimal
 //     combination of the candidate vectors of the mode (Galerkin: solve
 //     G alpha = g with G_kl = c_k . A c_l, g_k = c_k . b in FP64, pseudo-
-//     inverse on the host), checked by ||b - A x0|| < ||b|| in FP64.
+//     inverse on the host), checked in FP64 by r^T P r < b^T P b (r = b - A x0),
+//     the residual measure of the PCG itself; otherwise x0 = 0.
 // Training minimises sum_a (c_a^T H_a c_a - 2 c_a^T q_a + c0_a) / sum_a c0_a,
 // i.e. the squared error of the predicted field against the solved x, with
 // one Adam step per stored system; the GEMMs of the forward and backward
@@ -1105,7 +1106,16 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
             out.n_candidates  = k;
             for(int i = 0; i < k; ++i)
                 out.coeff[i] = alpha[i];
-            if(std::isfinite(rr) && rr < bb)
+            // the judge is the PCG's own residual measure, r^T P r (the
+            // quantity the reference's stop rule |r.z| <= tol |r0.z0| tracks):
+            // accept the start when it is below b^T P b of the zero start
+            double* zr = W.Ac.data();
+            double* zb = W.Ac.data() + (size_t)n;
+            precond_apply(s, y, zr);
+            precond_apply(s, b, zb);
+            const double rz = host_dot(s, y, zr, n), bz = host_dot(s, b, zb, n);
+            out.rz_ratio    = bz > 0 ? rz / bz : INFINITY;
+            if(std::isfinite(rr) && std::isfinite(rz) && bz > 0 && rz < bz)
             {
                 have         = true;
                 out.mode     = mode;
