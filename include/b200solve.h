@@ -121,6 +121,17 @@ int b2s_partition_maps(int32_t n, const int32_t* h_part_ids, int32_t max_part,
 #define B2S_INVERT_SWEEP_F32 0 /* FP32 symmetric sweep (mas_preconditioner_engine.cu:1077-1175) */
 #define B2S_INVERT_GJ_F64 1    /* FP64 Gauss-Jordan, stored FP32 */
 
+/* Affine bodies: block rows [block_offset, block_offset + 4 n_bodies) hold
+ * n_bodies affine bodies of 12 DoF (4 block rows each). Every preconditioner
+ * kind but NONE then applies, on that range, the inverse of each body's full
+ * 12x12 diagonal Hessian block (FP64, built by b2s_precond_assemble): the
+ * reference's ABDDiagPreconditioner, which has no configuration gate and acts
+ * after any global preconditioner on the affine-body sub-range
+ * (src/backends/cuda/affine_body/abd_diag_preconditioner.cu:15-125,185-191,
+ *  src/backends/cuda/linear_system/global_linear_system.cu:555-576). The MAS
+ * range (b2s_mas_init) must not overlap it. n_bodies = 0 removes the range. */
+int b2s_abd_init(b2s_solver* s, int32_t block_offset, int32_t n_bodies);
+
 /* Build the preconditioner from the current assembled matrix. Replaces
  * GlobalPreconditioner::do_assemble / LocalPreconditioner::do_assemble
  * (src/backends/cuda/linear_system/global_preconditioner.h:16,

@@ -53,7 +53,8 @@ def load_scene_lib() -> C.CDLL:
         lib.b2g_free.restype = None
         lib.b2g_last_error.argtypes = []
         lib.b2g_last_error.restype = C.c_char_p
-        for fn in ("b2g_num_verts", "b2g_num_tets", "b2g_num_triplets", "b2g_num_contacts", "b2g_num_adjacency"):
+        for fn in ("b2g_num_verts", "b2g_num_tets", "b2g_num_triplets", "b2g_num_contacts", "b2g_num_adjacency",
+                   "b2g_num_bodies"):
             getattr(lib, fn).argtypes = [vp]
             getattr(lib, fn).restype = C.c_int64
         for fn in ("b2g_positions", "b2g_rest_positions", "b2g_triplet_vals", "b2g_gradient"):

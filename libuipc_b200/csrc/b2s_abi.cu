@@ -291,6 +291,28 @@ int b2s_mas_get_nodes(b2s_solver* s, float* R, float* Z)
                    });
 }
 
+int b2s_abd_init(b2s_solver* s, int32_t block_offset, int32_t n_bodies)
+{
+    return guarded(s,
+                   [&]
+                   {
+                       B2S_REQUIRE(block_offset >= 0 && n_bodies >= 0, B2S_ERR_ARGUMENT, "negative affine-body range");
+                       B2S_REQUIRE((int64_t)block_offset + 4 * (int64_t)n_bodies <= INT32_MAX / 3, B2S_ERR_ARGUMENT,
+                                   "affine-body range too large");
+                       if(s->mas.initialized && n_bodies > 0)
+                       {
+                           const int64_t a0 = block_offset, a1 = a0 + 4 * (int64_t)n_bodies;
+                           const int64_t m0 = s->mas.offset, m1 = m0 + s->mas.vn;
+                           B2S_REQUIRE(a1 <= m0 || m1 <= a0, B2S_ERR_ARGUMENT,
+                                       "affine-body range overlaps the MAS range");
+                       }
+                       s->abd_offset   = block_offset;
+                       s->abd_n        = n_bodies;
+                       s->precond_kind = -1;  // rebuild before the next apply
+                       b2s::drop_graphs(s);
+                   });
+}
+
 int b2s_precond_assemble(b2s_solver* s, int kind, int invert_mode)
 {
     return guarded(s, [&]

@@ -238,6 +238,8 @@ struct b2s_solver
     int                  invert_mode  = 0;
     long long            precond_generation = 0;  // bumped by every preconditioner build
     b2s::DBuf<double>    dinv;  // [nb*9] row-major inverses of diagonal blocks
+    int32_t              abd_offset = 0, abd_n = 0;  // affine bodies: block rows abd_offset + [0, 4 abd_n)
+    b2s::DBuf<double>    abd_inv;  // [abd_n * 144] row-major 12x12 inverses
     b2s::DBuf<double>    dot_out;
     b2s::Reduction       red;
     b2s::DBuf<int>       dev_err;  // DeviceError bits raised by kernels

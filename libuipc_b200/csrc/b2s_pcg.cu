@@ -91,10 +91,95 @@ __global__ void k_diag_inverse(int32_t nb, const int32_t* diag_index, const doub
     o[8] = (m[0] * m[4] - m[1] * m[3]) * id;
 }
 
+// 12x12 block-Jacobi inverses of the affine bodies (ABDDiagPreconditioner,
+// src/backends/cuda/affine_body/abd_diag_preconditioner.cu:15-125: the inverse
+// of each body's full 12x12 diagonal Hessian block): body b owns block rows
+// off + 4b .. off + 4b + 3; its 10 stored upper 3x3 blocks are gathered from
+// the BSR (binary search of the sorted columns), mirrored, and inverted in FP64
+// by Gauss-Jordan with partial pivoting (identity when singular). One thread
+// per body; out: 144 doubles per body, row-major.
+__global__ void k_abd_inverse(int n_bodies, int off, const int32_t* __restrict__ rowptr,
+                              const int32_t* __restrict__ cols, const double* __restrict__ vals, int64_t S,
+                              double* __restrict__ out)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if(b >= n_bodies)
+        return;
+    double H[12][24];
+    for(int i = 0; i < 12; ++i)
+        for(int j = 0; j < 24; ++j)
+            H[i][j] = (j == 12 + i) ? 1.0 : 0.0;
+    for(int bi = 0; bi < 4; ++bi)
+    {
+        const int row = off + 4 * b + bi;
+        int       lo = rowptr[row], hi = rowptr[row + 1];
+        for(int bj = bi; bj < 4; ++bj)
+        {
+            const int col = off + 4 * b + bj;
+            int       l = lo, h = hi;
+            while(l < h)
+            {
+                const int m = (l + h) >> 1;
+                if(cols[m] < col)
+                    l = m + 1;
+                else
+                    h = m;
+            }
+            if(l >= hi || cols[l] != col)
+                continue;
+            for(int p = 0; p < 3; ++p)
+                for(int q = 0; q < 3; ++q)
+                {
+                    const double v = vals[(int64_t)(q * 3 + p) * S + l];
+                    H[3 * bi + p][3 * bj + q] = v;
+                    if(bi != bj)
+                        H[3 * bj + q][3 * bi + p] = v;
+                }
+        }
+    }
+    bool ok = true;
+    for(int c = 0; c < 12 && ok; ++c)
+    {
+        int piv = c;
+        for(int r = c + 1; r < 12; ++r)
+            if(fabs(H[r][c]) > fabs(H[piv][c]))
+                piv = r;
+        if(!(fabs(H[piv][c]) > 0.0) || !isfinite(H[piv][c]))
+        {
+            ok = false;
+            break;
+        }
+        if(piv != c)
+            for(int j = 0; j < 24; ++j)
+            {
+                const double t = H[c][j];
+                H[c][j]        = H[piv][j];
+                H[piv][j]      = t;
+            }
+        const double inv = 1.0 / H[c][c];
+        for(int j = 0; j < 24; ++j)
+            H[c][j] *= inv;
+        for(int r = 0; r < 12; ++r)
+            if(r != c)
+            {
+                const double f = H[r][c];
+                if(f != 0.0)
+                    for(int j = 0; j < 24; ++j)
+                        H[r][j] -= f * H[c][j];
+            }
+    }
+    double* o = out + (size_t)b * 144;
+    for(int i = 0; i < 12; ++i)
+        for(int j = 0; j < 12; ++j)
+            o[i * 12 + j] = ok ? H[i][12 + j] : (i == j ? 1.0 : 0.0);
+}
+
 struct MasView
 {
     int            active;  // MAS present
     int            off, vn, L;
+    int            abd_off, abd_n;  // affine-body range: block rows abd_off .. abd_off + 4 abd_n
+    const double*  abd_inv;         // [abd_n * 144]
     const int32_t* r2p;
     const int32_t* ctable;  // [vn * (L-1)] node of each vertex at levels 1..L-1
     int            T;       // coarse levels to collect (L-1)
@@ -142,6 +227,25 @@ __device__ __forceinline__ void precond_row(int kind, const MasView& mv, const d
         z[0] = r0;
         z[1] = r1;
         z[2] = r2;
+        return;
+    }
+    if(mv.abd_n > 0 && i >= mv.abd_off && i < mv.abd_off + 4 * mv.abd_n)
+    {
+        // row l of body b: z = (H_b^-1)[3l .. 3l+2][0 .. 11] r_b
+        const int     b = (i - mv.abd_off) >> 2, l = (i - mv.abd_off) & 3;
+        const double* Hi = mv.abd_inv + (size_t)b * 144 + 36 * l;
+        const int64_t r0i = 3 * ((int64_t)mv.abd_off + 4 * b);
+        double        a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for(int j = 0; j < 12; ++j)
+        {
+            const double rj = r[r0i + j];
+            a0 += Hi[j] * rj;
+            a1 += Hi[12 + j] * rj;
+            a2 += Hi[24 + j] * rj;
+        }
+        z[0] = a0;
+        z[1] = a1;
+        z[2] = a2;
         return;
     }
     const double* D = dinv + (size_t)i * 9;
@@ -343,6 +447,16 @@ void precond_assemble(b2s_solver* s, int kind, int invert_mode)
         B2S_REQUIRE(s->mas.initialized, B2S_ERR_STATE, "MAS preconditioner requested before b2s_mas_init");
         mas_assemble(s, invert_mode);
     }
+    if(s->abd_n > 0)
+    {
+        B2S_REQUIRE(s->abd_offset + 4 * (int64_t)s->abd_n <= A.nb, B2S_ERR_ARGUMENT,
+                    "affine-body range exceeds the matrix");
+        s->abd_inv.resize((size_t)s->abd_n * 144);
+        k_abd_inverse<<<grid_for(s->abd_n, 128), 128, 0, st>>>(s->abd_n, s->abd_offset, A.rowptr.data(),
+                                                               A.cols.data(), A.vals.data(), A.stride,
+                                                               s->abd_inv.data());
+        B2S_CHECK_LAUNCH();
+    }
     s->precond_kind = kind;
     s->precond_generation += 1;
     s->invert_mode  = invert_mode;
@@ -354,6 +468,9 @@ static MasView mas_view(b2s_solver* s)
     MasView mv{};
     const MasState& M = s->mas;
     mv.active = (s->precond_kind == B2S_PRECOND_MAS && M.initialized) ? 1 : 0;
+    mv.abd_n   = s->abd_n;
+    mv.abd_off = s->abd_offset;
+    mv.abd_inv = s->abd_inv.data();
     mv.off    = M.offset;
     mv.vn     = M.vn;
     mv.L      = M.L;

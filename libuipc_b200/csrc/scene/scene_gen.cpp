@@ -203,6 +203,7 @@ struct b2g_system
     std::vector<double>  grad;
     std::vector<int32_t> adj_start, adj_list;
     int64_t              n_contacts = 0;
+    int64_t              n_bodies   = 0;
 };
 
 extern "C" {
@@ -230,6 +231,9 @@ void b2g_default_config(b2g_config* c)
     c->ground_offset = 0.1e-3;
     c->twist_deg     = 2.0;
     c->n_threads     = 0;
+    c->body_kappa    = 1e8;
+    c->bend_k        = 1e-2;
+    c->cloth_size    = 2.0;
 }
 
 const char* b2g_last_error(void) { return g_err.c_str(); }
@@ -238,6 +242,242 @@ const char* b2g_last_error(void) { return g_err.c_str(); }
 
 namespace
 {
+// Scene 3: a square cloth (N x N vertices, two triangles per cell) resting
+// on an nbs x nbs grid of affine bodies (cubes rotated about +y by seeded
+// angles), first Newton step from rest. Bodies first in the DoF order.
+//  * affine body b: q = (p, A[:,0], A[:,1], A[:,2]), x = p + A xbar; the
+//    kinetic Hessian is the body mass matrix (m I; m s^2/12 I per column, the
+//    cube's second moments), the orthogonality potential kappa V |A A^T - I|^2
+//    at A = R has Hessian 8 kappa V |sym(R^T dA)|^2; 16 triplets per body
+//    (4 x 4 grid of 3x3 blocks), the lower ones written as zero blocks, as the
+//    reference's affine-body subsystem writes them;
+//  * cloth: lumped mass (1 mm sheet), membrane edge springs of stiffness E
+//    (stand-in for the Baraff-Witkin stretch), bending springs between
+//    vertices two apart along both grid axes (stiffness bend_k / h^2);
+//  * contact: cloth vertex above a body's top face at distance d < dhat,
+//    barrier b(d^2) along +y, coupling the vertex with the body's 12 DoF
+//    (rank-1 Hessian over 5 block rows: 15 triplets, 4 vertex-body blocks);
+//  * potentials scaled by dt^2, gravity -y.
+void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
+{
+    const int N = C.cells_x, nbs = C.n_cubes;
+    if(N < 2 || nbs < 1)
+        throw std::runtime_error("scene 3 needs cells_x >= 2 and n_cubes >= 1");
+    const int64_t nbod = (int64_t)nbs * nbs, ncv = (int64_t)N * N, rows = 4 * nbod + ncv;
+    if(rows > (int64_t)INT32_MAX / 3)
+        throw std::runtime_error("system too large for 32-bit DoF indices");
+    const double Lc = C.cloth_size > 0 ? C.cloth_size : 2.0, hc = Lc / (N - 1);
+    const double pitch = Lc / nbs, s = 0.6 * pitch, dt2 = C.dt * C.dt, Dh = C.dhat * C.dhat;
+    const double rho_b = C.rho, m_b = rho_b * s * s * s, I_b = m_b * s * s / 12.0, V = s * s * s;
+    const double m_v = C.rho * 1e-3 * hc * hc;
+    const double y_cloth = 0.5 * C.dhat;  // tops at y = 0
+    sys->n_bodies = nbod;
+    sys->x.assign(rows * 3, 0.0);
+    std::vector<double> theta(nbod);
+    for(int64_t b = 0; b < nbod; ++b)
+    {
+        const int64_t i = b % nbs, k = b / nbs;
+        sys->x[(4 * b) * 3 + 0] = (i + 0.5) * pitch - 0.5 * Lc;
+        sys->x[(4 * b) * 3 + 1] = -0.5 * s;
+        sys->x[(4 * b) * 3 + 2] = (k + 0.5) * pitch - 0.5 * Lc;
+        theta[b] = urand(C.seed, 4, b) * (M_PI / 4);
+        // rows 4b+1..4b+3 carry the body centre too (positions are per block row)
+        for(int r = 1; r < 4; ++r)
+            for(int a = 0; a < 3; ++a)
+                sys->x[(4 * b + r) * 3 + a] = sys->x[(4 * b) * 3 + a];
+    }
+    for(int64_t v = 0; v < ncv; ++v)
+    {
+        const int64_t i = v % N, k = v / N, g = 4 * nbod + v;
+        sys->x[g * 3 + 0] = i * hc - 0.5 * Lc;
+        sys->x[g * 3 + 1] = y_cloth;
+        sys->x[g * 3 + 2] = k * hc - 0.5 * Lc;
+    }
+    sys->x_rest = sys->x;
+    sys->grad.assign(rows * 3, 0.0);
+    Builder B;
+    B.reserve((size_t)nbod * 16 + ncv * 8);
+    auto put = [&](int32_t r, int32_t c, const double* Hrc /*row-major 3x3 of block (r,c)*/)
+    {
+        const bool tp = r > c;
+        B.rows.push_back(tp ? c : r);
+        B.cols.push_back(tp ? r : c);
+        for(int q = 0; q < 3; ++q)
+            for(int p = 0; p < 3; ++p)
+                B.vals.push_back(tp ? Hrc[q * 3 + p] : Hrc[p * 3 + q]);  // column-major
+    };
+    // ---- affine bodies ----
+    for(int64_t b = 0; b < nbod; ++b)
+    {
+        double H[12][12] = {};
+        for(int a = 0; a < 3; ++a)
+        {
+            H[a][a] = m_b;
+            for(int k = 0; k < 3; ++k)
+                H[3 + 3 * k + a][3 + 3 * k + a] = I_b;
+        }
+        const double cs = std::cos(theta[b]), sn = std::sin(theta[b]);
+        const double R[3][3] = {{cs, 0, sn}, {0, 1, 0}, {-sn, 0, cs}};
+        // q index 3 + 3 k + r <-> A[r][k]; S_m = sym(R^T E_m)
+        double S[9][3][3];
+        for(int m = 0; m < 9; ++m)
+        {
+            const int k = m / 3, r = m % 3;  // E_m has a 1 at (r, k)
+            double RtE[3][3];
+            for(int i = 0; i < 3; ++i)
+                for(int j = 0; j < 3; ++j)
+                    RtE[i][j] = (j == k) ? R[r][i] : 0.0;
+            for(int i = 0; i < 3; ++i)
+                for(int j = 0; j < 3; ++j)
+                    S[m][i][j] = 0.5 * (RtE[i][j] + RtE[j][i]);
+        }
+        const double ko = dt2 * 8.0 * C.body_kappa * V;
+        for(int m = 0; m < 9; ++m)
+            for(int n = 0; n < 9; ++n)
+            {
+                double d = 0.0;
+                for(int i = 0; i < 3; ++i)
+                    for(int j = 0; j < 3; ++j)
+                        d += S[m][i][j] * S[n][i][j];
+                H[3 + m][3 + n] += ko * d;
+            }
+        // kinetic gradient: m (x - x_tilde) with x_tilde = x - dt^2 g on p
+        sys->grad[(4 * b) * 3 + 1] += m_b * dt2 * C.gravity;
+        for(int bi = 0; bi < 4; ++bi)
+            for(int bj = 0; bj < 4; ++bj)
+            {
+                const int32_t r = (int32_t)(4 * b + bi), c = (int32_t)(4 * b + bj);
+                B.rows.push_back(r);
+                B.cols.push_back(c);
+                for(int q = 0; q < 3; ++q)
+                    for(int p = 0; p < 3; ++p)
+                        B.vals.push_back(bi > bj ? 0.0 : H[3 * bi + p][3 * bj + q]);
+            }
+    }
+    // ---- cloth ----
+    const int32_t c0 = (int32_t)(4 * nbod);
+    for(int64_t v = 0; v < ncv; ++v)
+    {
+        const double Hm[9] = {m_v, 0, 0, 0, m_v, 0, 0, 0, m_v};
+        put(c0 + (int32_t)v, c0 + (int32_t)v, Hm);
+        sys->grad[(c0 + v) * 3 + 1] += m_v * dt2 * C.gravity;
+    }
+    auto spring = [&](int64_t va, int64_t vb, double k)
+    {
+        const int32_t ga = c0 + (int32_t)va, gb = c0 + (int32_t)vb;
+        double d[3], l = 0.0;
+        for(int a = 0; a < 3; ++a)
+        {
+            d[a] = sys->x[gb * 3 + a] - sys->x[ga * 3 + a];
+            l += d[a] * d[a];
+        }
+        l = std::sqrt(l);
+        double H[9], Hn[9];
+        for(int p = 0; p < 3; ++p)
+            for(int q = 0; q < 3; ++q)
+            {
+                H[p * 3 + q]  = dt2 * k * d[p] * d[q] / (l * l);
+                Hn[p * 3 + q] = -H[p * 3 + q];
+            }
+        put(ga, ga, H);
+        put(gb, gb, H);
+        put(ga, gb, Hn);
+    };
+    auto vid = [&](int64_t i, int64_t k) { return i + (int64_t)N * k; };
+    std::vector<std::vector<int32_t>> nb(rows);
+    auto link = [&](int64_t va, int64_t vb)
+    {
+        nb[c0 + va].push_back(c0 + (int32_t)vb);
+        nb[c0 + vb].push_back(c0 + (int32_t)va);
+    };
+    for(int64_t k = 0; k < N; ++k)
+        for(int64_t i = 0; i < N; ++i)
+        {
+            if(i + 1 < N)
+            {
+                spring(vid(i, k), vid(i + 1, k), C.E);
+                link(vid(i, k), vid(i + 1, k));
+            }
+            if(k + 1 < N)
+            {
+                spring(vid(i, k), vid(i, k + 1), C.E);
+                link(vid(i, k), vid(i, k + 1));
+            }
+            if(i + 1 < N && k + 1 < N)
+            {
+                spring(vid(i, k), vid(i + 1, k + 1), C.E);
+                link(vid(i, k), vid(i + 1, k + 1));
+            }
+            if(i + 2 < N)
+                spring(vid(i, k), vid(i + 2, k), C.bend_k / (hc * hc));
+            if(k + 2 < N)
+                spring(vid(i, k), vid(i, k + 2), C.bend_k / (hc * hc));
+        }
+    // ---- cloth-body contacts ----
+    int64_t n_contacts = 0;
+    for(int64_t v = 0; v < ncv; ++v)
+    {
+        const int32_t g  = c0 + (int32_t)v;
+        const double  xv = sys->x[g * 3], yv = sys->x[g * 3 + 1], zv = sys->x[g * 3 + 2];
+        const int64_t bi = (int64_t)std::floor((xv + 0.5 * Lc) / pitch), bk = (int64_t)std::floor((zv + 0.5 * Lc) / pitch);
+        if(bi < 0 || bi >= nbs || bk < 0 || bk >= nbs)
+            continue;
+        const int64_t b  = bi + nbs * bk;
+        const double  px = sys->x[(4 * b) * 3], py = sys->x[(4 * b) * 3 + 1], pz = sys->x[(4 * b) * 3 + 2];
+        const double  cs = std::cos(theta[b]), sn = std::sin(theta[b]);
+        // body-frame position of the vertex (R^T (x - p), R about +y)
+        const double ux = cs * (xv - px) - sn * (zv - pz), uz = sn * (xv - px) + cs * (zv - pz);
+        if(std::fabs(ux) > 0.5 * s || std::fabs(uz) > 0.5 * s)
+            continue;
+        const double d = yv - (py + 0.5 * s);
+        if(d <= 0.0 || d >= C.dhat)
+            continue;
+        ++n_contacts;
+        // a = dd/d(x_v, q_b): +e_y on the vertex; -e_y, -xbar_k e_y on the body
+        const double xbar[3] = {ux, 0.5 * s, uz};
+        double       avec[5][3] = {};
+        int32_t      rws[5]     = {g, (int32_t)(4 * b), (int32_t)(4 * b + 1), (int32_t)(4 * b + 2),
+                                   (int32_t)(4 * b + 3)};
+        avec[0][1] = 1.0;
+        avec[1][1] = -1.0;
+        for(int k = 0; k < 3; ++k)
+            avec[2 + k][1] = -xbar[k];
+        double D = d * d, b1, b2;
+        barrier_d(D, Dh, b1, b2);
+        double kc = dt2 * C.kappa * (b2 * 4.0 * D + 2.0 * b1);
+        if(kc < 0.0)
+            kc = 0.0;
+        for(int q = 0; q < 5; ++q)
+            for(int r = q; r < 5; ++r)
+            {
+                double Hb[9];
+                for(int p = 0; p < 3; ++p)
+                    for(int c = 0; c < 3; ++c)
+                        Hb[p * 3 + c] = kc * avec[q][p] * avec[r][c];
+                put(rws[q], rws[r], Hb);
+            }
+        for(int q = 0; q < 5; ++q)
+            for(int a = 0; a < 3; ++a)
+                sys->grad[rws[q] * 3 + a] += dt2 * C.kappa * b1 * 2.0 * d * avec[q][a];
+    }
+    sys->n_contacts = n_contacts;
+    sys->rows       = std::move(B.rows);
+    sys->cols       = std::move(B.cols);
+    sys->vals       = std::move(B.vals);
+    // neighbour graph: cloth triangle edges (bodies have none)
+    sys->adj_start.assign(rows + 1, 0);
+    for(int64_t r = 0; r < rows; ++r)
+    {
+        auto& L = nb[r];
+        std::sort(L.begin(), L.end());
+        L.erase(std::unique(L.begin(), L.end()), L.end());
+        sys->adj_start[r + 1] = sys->adj_start[r] + (int32_t)L.size();
+    }
+    sys->adj_list.resize(sys->adj_start[rows]);
+    for(int64_t r = 0; r < rows; ++r)
+        std::copy(nb[r].begin(), nb[r].end(), sys->adj_list.begin() + sys->adj_start[r]);
+}
+
 // x_in / xt_in (optional, [n_verts*3]): current positions and kinetic target
 // x_tilde; null = the scene's default first Newton step from rest
 int generate_impl(const b2g_config* cfg, const double* x_in, const double* xt_in, b2g_system** out)
@@ -247,6 +487,15 @@ int generate_impl(const b2g_config* cfg, const double* x_in, const double* xt_in
         if(!cfg || !out)
             throw std::runtime_error("null argument");
         const b2g_config C = *cfg;
+        if(C.scene == 3)
+        {
+            if(x_in || xt_in)
+                throw std::runtime_error("scene 3 has no state input");
+            auto sys = std::make_unique<b2g_system>();
+            generate_cloth_abd(C, sys.get());
+            *out = sys.release();
+            return 0;
+        }
         if(C.cells_x < 1 || C.cells_y < 1 || C.cells_z < 1 || C.n_cubes < 1 || C.h <= 0 || C.dt <= 0)
             throw std::runtime_error("invalid configuration sizes");
         if(C.scene != 1 && C.scene != 2)
@@ -817,6 +1066,7 @@ int64_t b2g_num_verts(const b2g_system* s) { return (int64_t)s->x.size() / 3; }
 int64_t b2g_num_tets(const b2g_system* s) { return (int64_t)s->tets.size() / 4; }
 int64_t b2g_num_triplets(const b2g_system* s) { return (int64_t)s->rows.size(); }
 int64_t b2g_num_contacts(const b2g_system* s) { return s->n_contacts; }
+int64_t b2g_num_bodies(const b2g_system* s) { return s->n_bodies; }
 const double* b2g_positions(const b2g_system* s) { return s->x.data(); }
 const double* b2g_rest_positions(const b2g_system* s) { return s->x_rest.data(); }
 const int32_t* b2g_tets(const b2g_system* s) { return s->tets.data(); }

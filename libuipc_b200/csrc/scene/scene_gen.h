@@ -43,6 +43,11 @@ typedef struct b2g_config
     double ground_offset;  // ground plane sits this far below the lowest vertex [m]
     double twist_deg;      // scene 2: end rotation (+-) about the bar axis [deg]
     int    n_threads;      // OpenMP threads (0 = default)
+    // scene 3 (cloth draped over affine bodies): cells_x = cloth vertices per
+    // side, n_cubes = bodies per side, E = cloth stretch stiffness [N/m]
+    double body_kappa;     // affine-body orthogonality stiffness [Pa]
+    double bend_k;         // cloth bending stiffness [N m]
+    double cloth_size;     // cloth side length [m]
 } b2g_config;
 
 typedef struct b2g_system b2g_system;
@@ -65,7 +70,11 @@ const char* b2g_last_error(void);
 int64_t b2g_num_verts(const b2g_system* s);
 int64_t b2g_num_tets(const b2g_system* s);
 int64_t b2g_num_triplets(const b2g_system* s);
-int64_t b2g_num_contacts(const b2g_system* s);  // PT + EE + ground pairs
+int64_t b2g_num_contacts(const b2g_system* s);  // PT + EE + ground pairs (scene 3: cloth-body pairs)
+// scene 3: affine bodies come first in the DoF order, 4 block rows (12 DoF:
+// translation, then the 3 columns of the affine matrix) per body; the cloth
+// vertices follow from block row 4 * n_bodies on
+int64_t b2g_num_bodies(const b2g_system* s);
 
 // Data (owned by the system; valid until b2g_free)
 const double* b2g_positions(const b2g_system* s);    // [n_verts*3]

@@ -134,6 +134,11 @@ class Solver:
         return R, Z
 
     # ---- preconditioner ----------------------------------------------------------
+    def abd_init(self, block_offset: int, n_bodies: int):
+        """Affine bodies on block rows [block_offset, block_offset + 4 n_bodies):
+        12x12 block-Jacobi there (ABDDiagPreconditioner)."""
+        self._check(self.lib.b2s_abd_init(self.h, int(block_offset), int(n_bodies)))
+
     def precond_assemble(self, kind: int, invert_mode: int = _abi.B2S_INVERT_SWEEP_F32):
         self._check(self.lib.b2s_precond_assemble(self.h, int(kind), int(invert_mode)))
 

@@ -37,6 +37,9 @@ class B2GConfig(C.Structure):
         ("ground_offset", C.c_double),
         ("twist_deg", C.c_double),
         ("n_threads", C.c_int),
+        ("body_kappa", C.c_double),
+        ("bend_k", C.c_double),
+        ("cloth_size", C.c_double),
     ]
 
 
@@ -55,6 +58,7 @@ class NewtonSystem:
     adj_list: np.ndarray  # int32 [nnz]
     n_contacts: int = 0
     config: dict = field(default_factory=dict)
+    n_bodies: int = 0  # affine bodies (4 block rows each, first in the DoF order)
 
     @property
     def n_triplets(self) -> int:
@@ -134,6 +138,7 @@ def _generate(cfg: B2GConfig, x, xt) -> NewtonSystem:
             adj_list=arr(lib.b2g_adjacency_list(handle), nadj, np.int32),
             n_contacts=int(lib.b2g_num_contacts(handle)),
             config={k: getattr(cfg, k) for k, _ in B2GConfig._fields_},
+            n_bodies=int(lib.b2g_num_bodies(handle)),
         )
     finally:
         lib.b2g_free(handle)
@@ -157,3 +162,13 @@ def twisted_bar(nx: int = 200, ny: int = 20, nz: int = 20, twist_deg: float = 2.
     kw.setdefault("E", 1e6)
     kw.setdefault("nu", 0.49)
     return generate(scene=2, cells_x=nx, cells_y=ny, cells_z=nz, n_cubes=1, twist_deg=twist_deg, seed=seed, **kw)
+
+
+def cloth_on_bodies(n: int = 256, bodies_per_side: int = 8, seed: int = 0, **kw) -> NewtonSystem:
+    """n x n-vertex cloth (1 mm sheet, stretch stiffness E, bending bend_k)
+    resting on bodies_per_side^2 affine bodies (cubes rotated about +y from
+    the seed, orthogonality stiffness body_kappa): 3x3 cloth blocks, 12x12
+    body blocks (as 16 3x3 triplets) and 12x3 cloth-body contact couplings.
+    The bodies' 4 * n_bodies block rows come first."""
+    kw.setdefault("E", 1e3)
+    return generate(scene=3, cells_x=n, cells_y=1, cells_z=1, n_cubes=bodies_per_side, seed=seed, **kw)

@@ -194,6 +194,19 @@ def pcg(A: OracleMatrix, b, precond=ORC_PRECOND_JACOBI, mas: OracleMAS | None = 
     return x, {k: getattr(res, k) for k, _ in OrcPcgResult._fields_}
 
 
+def abd_block_jacobi(A_scipy, block_offset: int, n_bodies: int, r: np.ndarray) -> np.ndarray:
+    """ABDDiagPreconditioner (src/backends/cuda/affine_body/abd_diag_preconditioner.cu:15-125):
+    on block rows [block_offset, block_offset + 4 n_bodies), z_b = H_b^-1 r_b with H_b the
+    full 12x12 diagonal block of body b (the symmetric matrix A = U + U^T - diag U), FP64;
+    returns z on that range only (length 12 n_bodies)."""
+    z = np.zeros(12 * n_bodies)
+    for b in range(n_bodies):
+        lo = 3 * (block_offset + 4 * b)
+        H = A_scipy[lo:lo + 12, lo:lo + 12].toarray()
+        z[12 * b:12 * b + 12] = np.linalg.solve(H, r[lo:lo + 12])
+    return z
+
+
 def cg_truth(A: OracleMatrix, b, tol=1e-13, max_iter=0, threads=1):
     b = np.ascontiguousarray(b, dtype=np.float64)
     x = np.zeros_like(b)
