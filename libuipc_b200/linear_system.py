@@ -293,6 +293,52 @@ class SolvingInfo:
     x: object  # DenseVectorView<Float> (device tensor)
     b: object  # CDenseVectorView<Float>
     iter_count: int = 0
+    # B200 extension: which solution history a warm start reads (e.g. the
+    # Newton iteration index within a time step)
+    history_slot: int = 0
+
+
+# linear_system/* keys of libuipc's scene configuration
+# (src/core/core/scene_default_config.cpp:146-175) with their defaults, and the
+# B200 extensions (precision, warm start)
+SCENE_CONFIG_DEFAULTS = {
+    "linear_system/tol_rate": 1e-3,
+    "linear_system/solver": "fused_pcg",
+    "linear_system/fem_preconditioner": "diag",
+    "linear_system/use_cuda_graph": 1,
+    "linear_system/check_interval": 5,
+    "linear_system/b200/precision": "fp64",
+    "linear_system/b200/warm_start": "zero",
+}
+
+
+def linear_system_config(config: dict | None = None) -> dict:
+    """The linear_system/* settings with defaults filled in, checked against
+    the reference's schema (tol_rate in (0, 1), solver in {fused_pcg,
+    linear_pcg}, fem_preconditioner in {diag, mas}, use_cuda_graph in
+    {0, 1, 2}, check_interval >= 1); ValueError otherwise."""
+    c = dict(SCENE_CONFIG_DEFAULTS)
+    for k, v in (config or {}).items():
+        if k.startswith("linear_system/"):
+            if k not in SCENE_CONFIG_DEFAULTS:
+                raise ValueError(f"unknown linear-system option {k!r}")
+            c[k] = v
+    tol = float(c["linear_system/tol_rate"])
+    if not 0.0 < tol < 1.0:
+        raise ValueError("linear_system/tol_rate must lie in (0, 1)")
+    if c["linear_system/solver"] not in ("fused_pcg", "linear_pcg"):
+        raise ValueError("linear_system/solver must be fused_pcg or linear_pcg")
+    if c["linear_system/fem_preconditioner"] not in ("diag", "mas"):
+        raise ValueError("linear_system/fem_preconditioner must be diag or mas")
+    if int(c["linear_system/use_cuda_graph"]) not in (0, 1, 2):
+        raise ValueError("linear_system/use_cuda_graph must be 0, 1 or 2")
+    if int(c["linear_system/check_interval"]) < 1:
+        raise ValueError("linear_system/check_interval must be >= 1")
+    if c["linear_system/b200/precision"] not in ("fp64", "mixed"):
+        raise ValueError("linear_system/b200/precision must be fp64 or mixed")
+    if c["linear_system/b200/warm_start"] not in ("zero", "prev", "history", "learned"):
+        raise ValueError("linear_system/b200/warm_start must be zero, prev, history or learned")
+    return c
 
 
 class GlobalPreconditioner:
@@ -314,17 +360,22 @@ class IterativeSolver:
 
 class B200MAS(GlobalPreconditioner):
     """MAS over the FEM vertex range, 3x3 block Jacobi elsewhere (the role of
-    FEMMASPreconditioner + FEMDiagPreconditioner on this path)."""
+    FEMMASPreconditioner + FEMDiagPreconditioner on this path); with ``abd``
+    = (block_offset, n_bodies), the affine bodies' 12x12 block Jacobi
+    (ABDDiagPreconditioner) on their range."""
 
     def __init__(self, block_offset, vert_num, adj_start, adj_list, part_to_real, real_to_part,
-                 invert_mode=_abi.B2S_INVERT_SWEEP_F32):
+                 invert_mode=_abi.B2S_INVERT_SWEEP_F32, abd=None):
         self.args = (block_offset, vert_num, adj_start, adj_list, part_to_real, real_to_part)
         self.invert_mode = invert_mode
+        self.abd = abd
         self._initialised_for = None
 
     def do_assemble(self, system):
         if self._initialised_for is not system.solver:
             system.solver.mas_init(*self.args)
+            if self.abd:
+                system.solver.abd_init(*self.abd)
             self._initialised_for = system.solver
         system.solver.precond_assemble(_abi.B2S_PRECOND_MAS, self.invert_mode)
 
@@ -333,7 +384,17 @@ class B200MAS(GlobalPreconditioner):
 
 
 class B200Jacobi(GlobalPreconditioner):
+    """3x3 block Jacobi (FEMDiagPreconditioner); with ``abd``, the affine
+    bodies' 12x12 block Jacobi on their range."""
+
+    def __init__(self, abd=None):
+        self.abd = abd
+        self._initialised_for = None
+
     def do_assemble(self, system):
+        if self.abd and self._initialised_for is not system.solver:
+            system.solver.abd_init(*self.abd)
+            self._initialised_for = system.solver
         system.solver.precond_assemble(_abi.B2S_PRECOND_JACOBI)
 
     def do_apply(self, system, r, z):
@@ -341,17 +402,50 @@ class B200Jacobi(GlobalPreconditioner):
 
 
 class B200PCG(IterativeSolver):
-    """LinearFusedPCG's role (linear_fused_pcg.cu:851-943) on the B200 path."""
+    """LinearFusedPCG's role (linear_fused_pcg.cu:851-943) on the B200 path.
+    B200 extensions: ``precision`` (FP64 or mixed) and ``warm_start`` (zero,
+    prev, history or learned): the solver keeps the last solutions of each
+    history slot on the device and starts the PCG from the b2s_ws_predict
+    start; the FP64-checked start falls back to zero by itself."""
+
+    WARM = {"zero": _abi.B2S_WS_MODE_ZERO, "prev": _abi.B2S_WS_MODE_PREV, "history": _abi.B2S_WS_MODE_HISTORY,
+            "learned": _abi.B2S_WS_MODE_LEARNED}
 
     def __init__(self, tol_rate=1e-3, stop_rule=_abi.B2S_STOP_RZ, check_interval=5,
-                 precision=_abi.B2S_PRECISION_FP64, use_graph=True):
+                 precision=_abi.B2S_PRECISION_FP64, use_graph=True, warm_start: str = "zero"):
+        if warm_start not in self.WARM:
+            raise ValueError(f"unknown warm start {warm_start!r}")
         self.kw = dict(tol=tol_rate, stop_rule=stop_rule, check_interval=check_interval, precision=precision,
                        use_graph=use_graph)
+        self.warm_start = warm_start
+        self.history: dict[int, list] = {}
         self.last_stats: dict | None = None
+        self.last_warm_start: dict | None = None
+
+    @classmethod
+    def from_config(cls, config: dict | None = None) -> "B200PCG":
+        """From libuipc's linear_system/* scene settings: tol_rate with the
+        reference's |r.z| stop rule, check_interval (1 for linear_pcg, which
+        checks every iteration on the host), use_cuda_graph != 0 = graph
+        replay; plus the b200/precision and b200/warm_start extensions."""
+        c = linear_system_config(config)
+        ci = 1 if c["linear_system/solver"] == "linear_pcg" else int(c["linear_system/check_interval"])
+        prec = _abi.B2S_PRECISION_MIXED if c["linear_system/b200/precision"] == "mixed" else _abi.B2S_PRECISION_FP64
+        return cls(tol_rate=float(c["linear_system/tol_rate"]), stop_rule=_abi.B2S_STOP_RZ, check_interval=ci,
+                   precision=prec, use_graph=int(c["linear_system/use_cuda_graph"]) != 0,
+                   warm_start=c["linear_system/b200/warm_start"])
 
     def do_solve(self, system, info: SolvingInfo):
-        self.last_stats = system.solver.pcg(info.b, info.x, **self.kw)
+        hist = self.history.setdefault(info.history_slot, [])
+        given = False
+        if self.warm_start != "zero" and hist:
+            self.last_warm_start = system.solver.ws_predict(info.b, info.x, hist, self.WARM[self.warm_start])
+            given = True
+        self.last_stats = system.solver.pcg(info.b, info.x, x0_given=given, **self.kw)
         info.iter_count = int(self.last_stats["iterations"])
+        if self.warm_start != "zero":
+            hist.insert(0, info.x.clone())
+            del hist[_abi.B2S_WS_HISTORY:]
 
 
 class GlobalLinearSystem:
@@ -369,11 +463,11 @@ class GlobalLinearSystem:
         self.solver.assemble(n_block_rows, rows, cols, vals)
         self.preconditioner.do_assemble(self)
 
-    def solve(self, n_block_rows, rows, cols, vals, b):
+    def solve(self, n_block_rows, rows, cols, vals, b, history_slot: int = 0):
         torch = _torch()
         self.build_linear_system(n_block_rows, rows, cols, vals)
         x = torch.zeros_like(b)
-        info = SolvingInfo(x=x, b=b)
+        info = SolvingInfo(x=x, b=b, history_slot=history_slot)
         self.iterative_solver.do_solve(self, info)
         self.last_solve_iterations = info.iter_count
         return -x  # distribute_solution: dx = -x

@@ -90,3 +90,28 @@ def test_abd_pcg_solves(solver, cuda, cloth_abd, precision):
     st2 = solver.pcg(b, x2, tol=1e-9, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, precision=precision,
                      replace_every=20)
     assert st2["iterations_exact"] >= st["iterations_exact"]
+
+
+def test_global_linear_system_mirror_with_bodies(solver, cuda, cloth_abd):
+    """The libuipc-shaped host mirror: GlobalLinearSystem with the MAS + 12x12
+    block-Jacobi preconditioner and the PCG configured from scene settings
+    returns dx = -x with A x = b."""
+    import scipy.sparse.linalg as spla
+
+    from libuipc_b200.linear_system import B200MAS, B200PCG, GlobalLinearSystem, partition_maps, partition_rcb
+
+    s = cloth_abd
+    off = 4 * s.n_bodies
+    a0 = s.adj_start[off]
+    adj_start = (s.adj_start[off:] - a0).astype(np.int32)
+    adj_list = (s.adj_list[a0:] - off).astype(np.int32)
+    p2r, r2p = partition_maps(partition_rcb(s.positions[off:]))
+    pre = B200MAS(off, s.n_verts - off, adj_start, adj_list, p2r, r2p, abd=(0, s.n_bodies))
+    # the reference's stop rule |r.z| <= tol |r0.z0| is quadratic in the residual
+    pcg = B200PCG.from_config({"linear_system/tol_rate": 1e-14, "linear_system/fem_preconditioner": "mas"})
+    gls = GlobalLinearSystem(solver, pcg, pre)
+    dx = gls.solve(s.n_verts, to_dev(s.rows, cuda), to_dev(s.cols, cuda), to_dev(s.vals, cuda), to_dev(s.b, cuda))
+    A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals).to_scipy().tocsc()
+    xt = spla.spsolve(A, s.b)
+    assert gls.last_solve_iterations > 0
+    assert np.linalg.norm(-dx.cpu().numpy() - xt) <= 1e-5 * np.linalg.norm(xt)

@@ -116,6 +116,32 @@ def test_inference_matches_oracle(solver, cuda, bar_system):
         assert info["rz_ratio"] >= 1.0
 
 
+def test_mirror_pcg_with_history_start(solver, cuda):
+    """B200PCG(warm_start='history') through GlobalLinearSystem over a run:
+    once three earlier solutions exist the solves need far fewer iterations
+    than the first one, and each still meets its stop rule."""
+    from libuipc_b200.linear_system import B200MAS, B200PCG, GlobalLinearSystem, partition_maps, partition_rcb
+    from libuipc_b200.sequence import SceneSequence
+
+    seq = SceneSequence(scene=2, cells_x=30, cells_y=5, cells_z=5, E=1e6, nu=0.49, twist_per_step=2.0)
+    p2r, r2p = partition_maps(partition_rcb(seq.rest))
+    pre = B200MAS(0, seq.n_verts, seq.adj_start, seq.adj_list, p2r, r2p)
+    pcg = B200PCG(tol_rate=1e-4, stop_rule=_abi.B2S_STOP_RELRES, warm_start="history")
+    gls = GlobalLinearSystem(solver, pcg, pre)
+    its = []
+
+    def solve(sysm, step, k):
+        dx = gls.solve(sysm.n_verts, to_dev(sysm.rows, cuda), to_dev(sysm.cols, cuda), to_dev(sysm.vals, cuda),
+                       to_dev(sysm.b, cuda), history_slot=k)
+        assert pcg.last_stats["rel_res"] <= 1e-4
+        its.append(gls.last_solve_iterations)
+        return -dx.cpu().numpy()
+
+    for _ in seq.run(8, 1, solve):
+        pass
+    assert max(its[4:]) < 0.5 * its[0]
+
+
 def test_learned_start_beats_plain_starts(solver, cuda):
     """Train on the first systems of a twisted-bar run, then solve the later
     ones (FP64-verified rel-res 1e-4) from each start: the trained network's
