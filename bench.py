@@ -257,8 +257,12 @@ def main() -> None:
     with torch.cuda.stream(stream):
         runner.run(args.history_steps, newton_iters=1, collect=True)
     t_train = time.time()
-    solver.ws_fit_normalization()
-    train_loss = solver.ws_train(args.train_epochs, lr=1e-3, seed=0)
+    train_loss = None
+    if args.history_steps > 0:
+        solver.ws_fit_normalization()
+        train_loss = solver.ws_train(args.train_epochs, lr=1e-3, seed=0)
+    elif any(m in args.modes for m in ("history", "learned")):
+        raise SystemExit("--history-steps 0 leaves no history: time plain / mixed only")
     train_s = time.time() - t_train
     # the measured system: the next step's Newton system, with the run's history
     seq.begin_step()

@@ -278,17 +278,15 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32
     }
 }
 
-// One warp per row: each run of equal columns is summed by one lane, in source
-// order, and written to its slot of the block-upper BSR (values in planes).
-__global__ void __launch_bounds__(ASM_BLOCK) k_reduce_rows(int32_t nb, const int32_t* __restrict__ row_start,
-                                                           const int32_t* __restrict__ sorted_col,
-                                                           const int32_t* __restrict__ sorted_src,
-                                                           const double* __restrict__ src_vals,
-                                                           const int32_t* __restrict__ rowptr,
-                                                           int32_t* __restrict__ out_rows,
-                                                           int32_t* __restrict__ out_cols,
-                                                           double* __restrict__ out_vals, int64_t U,
-                                                           int32_t* __restrict__ diag_index)
+// One warp per row: every run of equal columns becomes one slot of the
+// block-upper BSR: its row, column and the position of its first source in
+// the sorted order (run_start; run_start[U] = T written by the caller).
+__global__ void __launch_bounds__(ASM_BLOCK) k_mark_runs(int32_t nb, const int32_t* __restrict__ row_start,
+                                                         const int32_t* __restrict__ sorted_col,
+                                                         const int32_t* __restrict__ rowptr,
+                                                         int32_t* __restrict__ out_rows, int32_t* __restrict__ out_cols,
+                                                         int32_t* __restrict__ run_start,
+                                                         int32_t* __restrict__ diag_index)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int warps_total = gridDim.x * (ASM_BLOCK / 32);
@@ -311,29 +309,65 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_reduce_rows(int32_t nb, const int
             const int      slot = heads_before + __popc(hm & ((1u << lane) - 1u));
             if(head)
             {
-                double acc[9];
-                int32_t s0 = sorted_src[beg + k];
-#pragma unroll
-                for(int q = 0; q < 9; ++q)
-                    acc[q] = src_vals[(int64_t)s0 * 9 + q];
-                for(int e = k + 1; e < L && sorted_col[beg + e] == c; ++e)
-                {
-                    const int32_t se = sorted_src[beg + e];
-#pragma unroll
-                    for(int q = 0; q < 9; ++q)
-                        acc[q] += src_vals[(int64_t)se * 9 + q];
-                }
                 const int64_t o = (int64_t)obeg + slot;
-                out_rows[o] = r;
-                out_cols[o] = c;
-#pragma unroll
-                for(int q = 0; q < 9; ++q)
-                    out_vals[(int64_t)q * U + o] = acc[q];
+                out_rows[o]  = r;
+                out_cols[o]  = c;
+                run_start[o] = beg + k;
             }
             heads_before += __popc(hm);
         }
         if(lane == 0)
             diag_index[r] = (L > 0 && sorted_col[beg] == r) ? obeg : -1;
+    }
+}
+
+// One thread per unique block: the sum of its run's source blocks in source
+// order (the sorted order), written to the value planes. Sources are fetched
+// four at a time so each thread keeps 36 independent loads in flight; the
+// additions stay in order, so the sums are those of the sequential loop.
+__global__ void __launch_bounds__(ASM_BLOCK) k_sum_runs(int64_t U, const int32_t* __restrict__ run_start,
+                                                        const int32_t* __restrict__ sorted_src,
+                                                        const double* __restrict__ src_vals,
+                                                        double* __restrict__ out_vals, int64_t S)
+{
+    for(int64_t o = (int64_t)blockIdx.x * ASM_BLOCK + threadIdx.x; o < U; o += (int64_t)gridDim.x * ASM_BLOCK)
+    {
+        const int32_t b = run_start[o], e = run_start[o + 1];
+        double        acc[9];
+        {
+            const int64_t s = sorted_src[b];
+#pragma unroll
+            for(int q = 0; q < 9; ++q)
+                acc[q] = src_vals[s * 9 + q];
+        }
+        int32_t k = b + 1;
+        for(; k + 4 <= e; k += 4)
+        {
+            double v[4][9];
+#pragma unroll
+            for(int t = 0; t < 4; ++t)
+            {
+                const int64_t s = sorted_src[k + t];
+#pragma unroll
+                for(int q = 0; q < 9; ++q)
+                    v[t][q] = src_vals[s * 9 + q];
+            }
+#pragma unroll
+            for(int t = 0; t < 4; ++t)
+#pragma unroll
+                for(int q = 0; q < 9; ++q)
+                    acc[q] += v[t][q];
+        }
+        for(; k < e; ++k)
+        {
+            const int64_t s = sorted_src[k];
+#pragma unroll
+            for(int q = 0; q < 9; ++q)
+                acc[q] += src_vals[s * 9 + q];
+        }
+#pragma unroll
+        for(int q = 0; q < 9; ++q)
+            out_vals[(int64_t)q * S + o] = acc[q];
     }
 }
 
@@ -449,11 +483,20 @@ void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const in
     B2S_CUDA(cudaMemsetAsync(M.cols.data() + U, 0, sizeof(int32_t) * (M.stride - U), st));
     if(nb > 0)
     {
-        // values are written as planes with stride M.stride
-        k_reduce_rows<<<asm_grid((int64_t)nb * 32, ASM_BLOCK), ASM_BLOCK, 0, st>>>(
-            nb, w.row_start.data(), w.sorted_col.data(), w.sorted_src.data(), vals, M.rowptr.data(),
-            M.rows.data(), M.cols.data(), M.vals.data(), M.stride, M.diag_index.data());
+        // slots of the runs, then their sums (values as planes with stride M.stride)
+        w.run_start.resize((size_t)U + 1, 1.2);
+        k_mark_runs<<<asm_grid((int64_t)nb * 32, ASM_BLOCK), ASM_BLOCK, 0, st>>>(
+            nb, w.row_start.data(), w.sorted_col.data(), M.rowptr.data(), M.rows.data(), M.cols.data(),
+            w.run_start.data(), M.diag_index.data());
         B2S_CHECK_LAUNCH();
+        B2S_CUDA(cudaMemcpyAsync(w.run_start.data() + U, w.row_start.data() + nb, sizeof(int32_t),
+                                 cudaMemcpyDeviceToDevice, st));
+        if(U > 0)
+        {
+            k_sum_runs<<<asm_grid(U, ASM_BLOCK), ASM_BLOCK, 0, st>>>(U, w.run_start.data(), w.sorted_src.data(), vals,
+                                                                     M.vals.data(), M.stride);
+            B2S_CHECK_LAUNCH();
+        }
     }
     M.has_trank = false;
     if(spmv_tiles && U > 0)

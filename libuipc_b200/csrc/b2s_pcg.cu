@@ -33,6 +33,7 @@ void mas_apply_levels_f32(b2s_solver* s, const float* r, const int* converged, b
 void mas_pack_bf16(b2s_solver* s);
 void spmv_f32_launch(b2s_solver* s, const Matrix& A, const float* x, float* y, Reduction& red, double* d_dot,
                      const int* stop);
+void spmv_prepare_f32(b2s_solver* s);
 void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st_out);
 
 namespace
@@ -359,6 +360,70 @@ __global__ void k_update_p_mixed(int64_t n, const PcgScalars* sc, const float* _
         return;
     const float beta = (float)sc->beta;
     for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
+        p[i] = __fmaf_rn(beta, p[i], z[i]);
+}
+
+// the same two updates, four entries per thread and step with 16-byte
+// accesses (all vectors 16-byte aligned; the last n % 4 entries scalar)
+__global__ void k_update_xr_mixed4(int64_t n, PcgScalars* sc, double* __restrict__ x, const float* __restrict__ p,
+                                   float* __restrict__ r, float* __restrict__ Ap)
+{
+    if(frozen(sc))
+        return;
+    const double alpha = sc->rz / sc->pAp;
+    if(blockIdx.x == 0 && threadIdx.x == 0)
+        sc->alpha = alpha;
+    const float   af     = (float)alpha;
+    const int64_t n4     = n >> 2;
+    const int64_t stride = (int64_t)gridDim.x * VEC_BLOCK;
+    const int64_t t0     = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x;
+    for(int64_t i = t0; i < n4; i += stride)
+    {
+        const float4 ap = reinterpret_cast<const float4*>(Ap)[i];
+        const float4 pp = reinterpret_cast<const float4*>(p)[i];
+        float4       rr = reinterpret_cast<float4*>(r)[i];
+        double2      x0 = reinterpret_cast<double2*>(x)[2 * i], x1 = reinterpret_cast<double2*>(x)[2 * i + 1];
+        x0.x += alpha * (double)pp.x;
+        x0.y += alpha * (double)pp.y;
+        x1.x += alpha * (double)pp.z;
+        x1.y += alpha * (double)pp.w;
+        rr.x = __fmaf_rn(-af, ap.x, rr.x);
+        rr.y = __fmaf_rn(-af, ap.y, rr.y);
+        rr.z = __fmaf_rn(-af, ap.z, rr.z);
+        rr.w = __fmaf_rn(-af, ap.w, rr.w);
+        reinterpret_cast<double2*>(x)[2 * i]     = x0;
+        reinterpret_cast<double2*>(x)[2 * i + 1] = x1;
+        reinterpret_cast<float4*>(r)[i]          = rr;
+        reinterpret_cast<float4*>(Ap)[i]         = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for(int64_t i = 4 * n4 + t0; i < n; i += stride)
+    {
+        const float api = Ap[i];
+        x[i] += alpha * (double)p[i];
+        r[i] = __fmaf_rn(-af, api, r[i]);
+        Ap[i] = 0.0f;
+    }
+}
+
+__global__ void k_update_p_mixed4(int64_t n, const PcgScalars* sc, const float* __restrict__ z, float* __restrict__ p)
+{
+    if(frozen(sc))
+        return;
+    const float   beta   = (float)sc->beta;
+    const int64_t n4     = n >> 2;
+    const int64_t stride = (int64_t)gridDim.x * VEC_BLOCK;
+    const int64_t t0     = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x;
+    for(int64_t i = t0; i < n4; i += stride)
+    {
+        const float4 zz = reinterpret_cast<const float4*>(z)[i];
+        float4       pp = reinterpret_cast<float4*>(p)[i];
+        pp.x = __fmaf_rn(beta, pp.x, zz.x);
+        pp.y = __fmaf_rn(beta, pp.y, zz.y);
+        pp.z = __fmaf_rn(beta, pp.z, zz.z);
+        pp.w = __fmaf_rn(beta, pp.w, zz.w);
+        reinterpret_cast<float4*>(p)[i] = pp;
+    }
+    for(int64_t i = 4 * n4 + t0; i < n; i += stride)
         p[i] = __fmaf_rn(beta, p[i], z[i]);
 }
 
@@ -857,15 +922,19 @@ static void pcg_iteration_mixed(b2s_solver* s, int kind, double* x, int slot)
     spmv_f32_launch(s, A, P.p32.data(), P.Ap32.data(), P.red, &P.sc.data()->pAp, &P.sc.data()->converged);
     if(ev)
         B2S_CUDA(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
-    k_update_xr_mixed<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), x, P.p32.data(), P.r32.data(),
-                                                         P.Ap32.data());
+    if(((uintptr_t)x & 15u) == 0)
+        k_update_xr_mixed4<<<vec_grid((n + 3) / 4), VEC_BLOCK, 0, st>>>(n, P.sc.data(), x, P.p32.data(),
+                                                                       P.r32.data(), P.Ap32.data());
+    else
+        k_update_xr_mixed<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), x, P.p32.data(), P.r32.data(),
+                                                             P.Ap32.data());
     B2S_CHECK_LAUNCH();
     if(ev)
         B2S_CUDA(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
     precond_launch_f32(s, kind, P.r32.data(), P.z32.data(), P.sc.data(), P.red);
     if(ev)
         B2S_CUDA(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
-    k_update_p_mixed<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), P.z32.data(), P.p32.data());
+    k_update_p_mixed4<<<vec_grid((n + 3) / 4), VEC_BLOCK, 0, st>>>(n, P.sc.data(), P.z32.data(), P.p32.data());
     B2S_CHECK_LAUNCH();
 }
 
@@ -900,6 +969,7 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
     ensure_reduction(P.red, std::max(spmv_grid(A.nnz), reduction_grid()), 2);
     ensure_reduction(s->red, reduction_grid(), 2);
     device_error_flag(s);
+    spmv_prepare_f32(s);  // kernel attributes set before any graph capture
     s->dot_out.resize(4);
     B2S_REQUIRE(A.nnz == 0 || A.has_trank, B2S_ERR_STATE, "matrix lacks the SpMV tile ranks");
     const int     ci       = o.check_interval > 0 ? o.check_interval : 1;

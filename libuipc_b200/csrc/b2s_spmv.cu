@@ -15,10 +15,15 @@
 // resolved in L2). The transposed halves B^T x_i are placed in shared memory
 // at the block's precomputed rank in (column, index) order; after a barrier
 // each thread merges its SPMV_BPT consecutive slots, so runs of equal columns
-// also leave as one reduction each. With FP32 values the next tile's stream is
-// loaded into registers while the current tile is reduced.
+// also leave as one reduction each. With FP32 values (mixed precision) the
+// tile's stream is staged in shared memory by bulk asynchronous copies (TMA).
+// Fraction of the HBM roofline reached (B200, 4.28 M blocks): FP64 ~0.60,
+// FP32 ~0.48; the limit is the per-tile chain of L2 gathers of x, shared-
+// memory placement and barriers, not the DRAM stream (doubling the bytes in
+// flight with two TMA stages did not change the time).
 #include "b2s_internal.cuh"
 #include "b2s_reduce.cuh"
+#include "b2s_tma.cuh"
 
 #include <cstdlib>
 #include <string>
@@ -181,10 +186,8 @@ __device__ __forceinline__ void tile_cols(int tid, int n, const XT (*s_t)[SPMV_T
         red3(y, cur, t0, t1, t2);
 }
 
-// U: stored blocks; S: plane stride. FP32 values: the next tile's stream is
-// loaded into registers before this tile's gathers and reductions (software
-// pipelining) and the shared buffers alternate, one barrier per tile. FP64
-// values: the registers of two tiles do not fit, one tile at a time.
+// U: stored blocks; S: plane stride. FP64 values, loaded straight into
+// registers (16-byte loads), one tile at a time.
 template <typename VT, typename XT, bool WITH_DOT>
 __global__ void __launch_bounds__(SPMV_THREADS)
     k_spmv_tile(int64_t U, int64_t S, const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
@@ -193,44 +196,148 @@ __global__ void __launch_bounds__(SPMV_THREADS)
 {
     if(stop && *stop)
         return;
-    constexpr bool PF = sizeof(VT) == 4;
-    constexpr int  NB = PF ? 2 : 1;
-    __shared__ __align__(16) XT      s_t[NB][3][SPMV_TILE];
-    __shared__ __align__(16) int32_t s_col[NB][SPMV_TILE];
+    __shared__ __align__(16) XT      s_t[3][SPMV_TILE];
+    __shared__ __align__(16) int32_t s_col[SPMV_TILE];
+    const int     tid     = threadIdx.x;
+    const int64_t n_tiles = (U + SPMV_TILE - 1) / SPMV_TILE;
+    double        dot     = 0.0;
+    for(int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
+    {
+        const int64_t rem = U - tile * SPMV_TILE;
+        const int     n   = rem < SPMV_TILE ? (int)rem : SPMV_TILE;
+        const int64_t e0  = tile * SPMV_TILE + SPMV_BPT * tid;
+        TileLoad<VT>  cur;
+        load_tile(cur, e0, S, e0 < S, rows, cols, trank, vals);
+        tile_rows<VT, XT, WITH_DOT>(cur, x, y, s_t, s_col, dot);
+        __syncthreads();
+        tile_cols<XT>(tid, n, s_t, s_col, y);
+        __syncthreads();
+    }
+    if(WITH_DOT)
+    {
+        double v[1] = {dot}, tot[1];
+        if(grid_sum<1>(v, partials, counter, tot))
+            *dot_out = tot[0];
+    }
+}
+
+// FP32 values, TMA-staged: the tile's block stream (row and column ids, tile
+// ranks, the 9 value planes: 46 B per block) is brought into shared memory by
+// bulk asynchronous copies issued by one thread as soon as the previous tile
+// is read out of the stage, so the copy overlaps that tile's reductions and
+// the other CTAs' work, with no registers held for it (one 47 KB stage per
+// CTA: three CTAs per SM; two stages were slower).
+// The reductions are those of k_spmv_tile (same order, same results).
+constexpr int      TMA_STAGES  = 1;
+constexpr uint32_t STAGE_BYTES = SPMV_TILE * (4 + 4 + 2 + 9 * 4);  // 47,104
+
+size_t spmv_tma_smem()
+{
+    return (size_t)TMA_STAGES * STAGE_BYTES + sizeof(float) * 3 * SPMV_TILE + sizeof(int32_t) * SPMV_TILE +
+           sizeof(uint64_t) * TMA_STAGES;
+}
+
+template <bool WITH_DOT>
+__global__ void __launch_bounds__(SPMV_THREADS)
+    k_spmv_tma(int64_t U, int64_t S, const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
+               const uint16_t* __restrict__ trank, const float* __restrict__ vals, const float* __restrict__ x,
+               float* y, double* partials, unsigned int* counter, double* dot_out, const int* stop, int* err)
+{
+    if(stop && *stop)
+        return;
+    extern __shared__ __align__(128) unsigned char sm[];
+    float*        s_t   = reinterpret_cast<float*>(sm + (size_t)TMA_STAGES * STAGE_BYTES);
+    int32_t*      s_col = reinterpret_cast<int32_t*>(s_t + 3 * SPMV_TILE);
+    uint64_t*     bar   = reinterpret_cast<uint64_t*>(s_col + SPMV_TILE);
     const int     tid     = threadIdx.x;
     const int64_t n_tiles = (U + SPMV_TILE - 1) / SPMV_TILE;
     const int64_t G       = gridDim.x;
-    double        dot     = 0.0;
-    TileLoad<VT>  cur;
-    int64_t       tile = blockIdx.x;
-    if(PF)
+    // stage layout: rows[TILE] | cols[TILE] | trank[TILE] | vals[9][TILE]
+    auto st_rows  = [&](int s) { return reinterpret_cast<int32_t*>(sm + (size_t)s * STAGE_BYTES); };
+    auto st_cols  = [&](int s) { return st_rows(s) + SPMV_TILE; };
+    auto st_trank = [&](int s) { return reinterpret_cast<uint16_t*>(st_cols(s) + SPMV_TILE); };
+    auto st_vals  = [&](int s) { return reinterpret_cast<float*>(st_trank(s) + SPMV_TILE); };
+    // blocks of a tile present in the planes: the stride S is a multiple of 16,
+    // so every copy is a multiple of 16 bytes
+    auto tile_count = [&](int64_t tile) -> int {
+        const int64_t left = S - tile * SPMV_TILE;
+        return left < SPMV_TILE ? (int)left : SPMV_TILE;
+    };
+    int issued = 0;  // thread 0: copies issued so far
+    auto issue = [&](int64_t tile) {
+        const int      s   = issued % TMA_STAGES;
+        const int64_t  b   = tile * SPMV_TILE;
+        const uint32_t cnt = (uint32_t)tile_count(tile);
+        mbar_arrive_expect_tx(&bar[s], cnt * (4 + 4 + 2 + 9 * 4));
+        bulk_copy_g2s(st_rows(s), rows + b, cnt * 4, &bar[s]);
+        bulk_copy_g2s(st_cols(s), cols + b, cnt * 4, &bar[s]);
+        bulk_copy_g2s(st_trank(s), trank + b, cnt * 2, &bar[s]);
+        for(int q = 0; q < 9; ++q)
+            bulk_copy_g2s(st_vals(s) + q * SPMV_TILE, vals + (int64_t)q * S + b, cnt * 4, &bar[s]);
+        ++issued;
+    };
+    if(tid == 0)
     {
-        const int64_t e0 = tile * SPMV_TILE + SPMV_BPT * tid;
-        load_tile(cur, e0, S, tile < n_tiles && e0 < S, rows, cols, trank, vals);
+        for(int s = 0; s < TMA_STAGES; ++s)
+            mbar_init(&bar[s], 1);
+        mbar_fence_init();
+        for(int64_t t = blockIdx.x, k = 0; t < n_tiles && k < TMA_STAGES; t += G, ++k)
+            issue(t);
     }
-    for(int it = 0; tile < n_tiles; ++it, tile += G)
+    __syncthreads();
+    double dot = 0.0;
+    int    it  = 0;
+    bool   ok  = true;
+    for(int64_t tile = blockIdx.x; tile < n_tiles; tile += G, ++it)
     {
-        const int     buf = NB == 2 ? (it & 1) : 0;
+        const int  s    = it % TMA_STAGES;
+        const bool good = mbar_wait(&bar[s], (uint32_t)((it / TMA_STAGES) & 1), err, DERR_TMA_TIMEOUT);
+        if(__syncthreads_or(!good))
+        {
+            ok = false;
+            break;
+        }
         const int64_t rem = U - tile * SPMV_TILE;
         const int     n   = rem < SPMV_TILE ? (int)rem : SPMV_TILE;
-        if(PF)
+        const int     e   = SPMV_BPT * tid;
+        TileLoad<float> t;
+        if(e < tile_count(tile))
         {
-            TileLoad<VT>  nxt;
-            const int64_t tn = tile + G, en = tn * SPMV_TILE + SPMV_BPT * tid;
-            load_tile(nxt, en, S, tn < n_tiles && en < S, rows, cols, trank, vals);
-            tile_rows<VT, XT, WITH_DOT>(cur, x, y, s_t[buf], s_col[buf], dot);
-            cur = nxt;
+            const int4  r4 = *reinterpret_cast<const int4*>(st_rows(s) + e);
+            const int4  c4 = *reinterpret_cast<const int4*>(st_cols(s) + e);
+            const uint2 k2 = *reinterpret_cast<const uint2*>(st_trank(s) + e);
+            t.r[0] = r4.x; t.r[1] = r4.y; t.r[2] = r4.z; t.r[3] = r4.w;
+            t.c[0] = c4.x; t.c[1] = c4.y; t.c[2] = c4.z; t.c[3] = c4.w;
+            t.rk[0] = (int)(k2.x & 0xFFFFu); t.rk[1] = (int)(k2.x >> 16);
+            t.rk[2] = (int)(k2.y & 0xFFFFu); t.rk[3] = (int)(k2.y >> 16);
+#pragma unroll
+            for(int q = 0; q < 9; ++q)
+            {
+                const float4 v = *reinterpret_cast<const float4*>(st_vals(s) + q * SPMV_TILE + e);
+                t.b[q][0] = v.x; t.b[q][1] = v.y; t.b[q][2] = v.z; t.b[q][3] = v.w;
+            }
         }
         else
         {
-            const int64_t e0 = tile * SPMV_TILE + SPMV_BPT * tid;
-            load_tile(cur, e0, S, e0 < S, rows, cols, trank, vals);
-            tile_rows<VT, XT, WITH_DOT>(cur, x, y, s_t[buf], s_col[buf], dot);
+#pragma unroll
+            for(int k = 0; k < 4; ++k)
+                t.r[k] = -1;
         }
-        __syncthreads();
-        tile_cols<XT>(tid, n, s_t[buf], s_col[buf], y);
-        if(NB == 1)
-            __syncthreads();
+        tile_rows<float, float, WITH_DOT>(t, x, y, reinterpret_cast<float(*)[SPMV_TILE]>(s_t), s_col, dot);
+        __syncthreads();  // the stage is read and the transposed halves are placed
+        if(tid == 0 && tile + (int64_t)TMA_STAGES * G < n_tiles)
+        {
+            fence_proxy_async_smem();
+            issue(tile + (int64_t)TMA_STAGES * G);
+        }
+        tile_cols<float>(tid, n, reinterpret_cast<const float(*)[SPMV_TILE]>(s_t), s_col, y);
+        __syncthreads();  // s_t is free for the next tile
+    }
+    if(!ok && tid == 0)
+    {
+        // a wait ran out: drain the copies still in flight (bounded)
+        for(int k = it; k < issued; ++k)
+            mbar_wait(&bar[k % TMA_STAGES], (uint32_t)((k / TMA_STAGES) & 1), nullptr, 0);
     }
     if(WITH_DOT)
     {
@@ -342,13 +449,35 @@ void spmv_f64_launch(b2s_solver* s, const Matrix& A, const double* x, double* y,
 }
 
 // FP32 values and vectors (mixed precision), FP64 dot
+// the TMA SpMV's shared-memory opt-in (once per device; outside graph capture)
+void spmv_prepare_f32(b2s_solver* s)
+{
+    static thread_local int prepared_device = -1;
+    if(prepared_device == s->device)
+        return;
+    B2S_CUDA(cudaFuncSetAttribute(k_spmv_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)spmv_tma_smem()));
+    prepared_device = s->device;
+}
+
 void spmv_f32_launch(b2s_solver* s, const Matrix& A, const float* x, float* y, Reduction& red, double* d_dot,
                      const int* stop)
 {
     if(A.nnz == 0)
         return;
-    launch_stream<float, float, true>(s->stream, A.nnz, A.stride, A.rows.data(), A.cols.data(), A.trank.data(), A.vals32.data(), x,
-                                      y, &red, d_dot, stop);
+    int* err = device_error_flag(s);
+    auto k   = k_spmv_tma<true>;
+    const size_t smem = spmv_tma_smem();
+    spmv_prepare_f32(s);
+    int occ = 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, SPMV_THREADS, smem) != cudaSuccess || occ < 1)
+        occ = 1;
+    const int64_t tiles = (A.nnz + SPMV_TILE - 1) / SPMV_TILE;
+    const int     grid  = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)NUM_SMS_HINT * std::min(occ, 8)));
+    k<<<grid, SPMV_THREADS, smem, s->stream>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(), A.trank.data(),
+                                                A.vals32.data(), x, y, red.partials.data(), red.counter.data(), d_dot,
+                                                stop, err);
+    B2S_CHECK_LAUNCH();
 }
 
 // ---------------------------------------------------------------------------
