@@ -226,7 +226,61 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32
     {
         const int32_t beg = row_start[r], L = row_start[r + 1] - beg;
         int           uniq = 0;
-        if(L <= ROW_CAP)
+        if(L <= 64)
+        {
+            // bitonic sort of the (column << 32 | source) keys in registers,
+            // two per lane (positions lane and lane + 32), padding = max key
+            uint64_t key[2];
+#pragma unroll
+            for(int j = 0; j < 2; ++j)
+            {
+                const int p = j * 32 + lane;
+                key[j]      = p < L ? ((uint64_t)(uint32_t)bucket_col[beg + p] << 32) |
+                                     (uint64_t)(uint32_t)bucket_src[beg + p]
+                                    : ~0ull;
+            }
+#pragma unroll
+            for(int k = 2; k <= 64; k <<= 1)
+#pragma unroll
+                for(int s = k >> 1; s > 0; s >>= 1)
+                {
+                    if(s == 32)
+                    {
+                        // k = 64: ascending; the partner is this lane's other key
+                        const uint64_t lo = key[0] < key[1] ? key[0] : key[1];
+                        const uint64_t hi = key[0] < key[1] ? key[1] : key[0];
+                        key[0]            = lo;
+                        key[1]            = hi;
+                    }
+                    else
+                    {
+#pragma unroll
+                        for(int j = 0; j < 2; ++j)
+                        {
+                            const int      p     = j * 32 + lane;
+                            const uint64_t other = __shfl_xor_sync(0xffffffffu, key[j], s);
+                            const bool     up    = (p & k) == 0;
+                            const bool     keep_min = ((p & s) == 0) == up;
+                            key[j] = keep_min ? (key[j] < other ? key[j] : other) : (key[j] < other ? other : key[j]);
+                        }
+                    }
+                }
+            const uint64_t last0 = __shfl_sync(0xffffffffu, key[0], 31);
+#pragma unroll
+            for(int j = 0; j < 2; ++j)
+            {
+                const int      p    = j * 32 + lane;
+                const uint64_t up1  = __shfl_up_sync(0xffffffffu, key[j], 1);
+                const uint64_t prev = lane > 0 ? up1 : (j == 1 ? last0 : ~0ull);
+                if(p < L)
+                {
+                    sorted_col[beg + p] = (int32_t)(key[j] >> 32);
+                    sorted_src[beg + p] = (int32_t)(key[j] & 0xFFFFFFFFull);
+                    uniq += (p == 0 || (prev >> 32) != (key[j] >> 32)) ? 1 : 0;
+                }
+            }
+        }
+        else if(L <= ROW_CAP)
         {
             for(int k = lane; k < L; k += 32)
             {

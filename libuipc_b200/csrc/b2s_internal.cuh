@@ -276,6 +276,7 @@ void launch_dot(b2s_solver* s, const double* a, const double* b, int64_t n, doub
 // preconditioners
 void precond_assemble(b2s_solver* s, int kind, int invert_mode);
 void precond_apply(b2s_solver* s, const double* r, double* z);
+void precond_launch(b2s_solver* s, const double* r, double* z);  // queued, no sync
 void precond_apply_mixed(b2s_solver* s, const float* r, float* z);
 void check_device_errors(b2s_solver* s);
 

@@ -570,11 +570,23 @@ __global__ void k_ws_lincomb(int64_t n, int nc, const double* __restrict__ c0, c
     }
 }
 
-// r = b - y (r may be y)
-__global__ void k_ws_residual(int64_t n, const double* __restrict__ b, const double* y, double* r)
+// r = b - sum_k alpha_k y_k (k < nc)
+__global__ void k_ws_residual_comb(int64_t n, int nc, const double* __restrict__ b, const double* __restrict__ y0,
+                                   const double* __restrict__ y1, const double* __restrict__ y2,
+                                   const double* __restrict__ y3, double a0, double a1, double a2, double a3,
+                                   double* __restrict__ r)
 {
     for(int64_t i = (int64_t)blockIdx.x * WS_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * WS_BLOCK)
-        r[i] = b[i] - y[i];
+    {
+        double v = b[i] - a0 * y0[i];
+        if(nc > 1)
+            v -= a1 * y1[i];
+        if(nc > 2)
+            v -= a2 * y2[i];
+        if(nc > 3)
+            v -= a3 * y3[i];
+        r[i] = v;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -603,16 +615,6 @@ MasGeom mas_geom(b2s_solver* s)
     return MasGeom{M.vn, M.offset, M.L, M.level_begin[1], M.level_count[1], M.ctable.data()};
 }
 
-double host_dot(b2s_solver* s, const double* a, const double* b, int64_t n)
-{
-    LearnedState& W = *s->ws;
-    W.dots.resize(1);
-    launch_dot(s, a, b, n, W.dots.data());
-    double h = 0.0;
-    B2S_CUDA(cudaMemcpyAsync(&h, W.dots.data(), sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-    B2S_CUDA(cudaStreamSynchronize(s->stream));
-    return h;
-}
 
 // fields, scales and the per-aggregate accumulators of the current system;
 // x (nullable) adds the training statistics. Returns the aggregate count.
@@ -626,13 +628,18 @@ int system_aggregates(b2s_solver* s, const double* b, int n_hist, const double* 
     for(int i = 0; i < n_hist; ++i)
         B2S_REQUIRE(hist && hist[i], B2S_ERR_ARGUMENT, "null history vector");
     W.fields.resize((size_t)WS_FIELDS * n);
-    W.Ac.resize((size_t)4 * n);
-    precond_apply(s, b, W.Ac.data());  // z = P b
+    W.Ac.resize((size_t)5 * n);
+    W.dots.resize(32);
+    precond_launch(s, b, W.Ac.data());  // z = P b
     k_ws_fields<<<ws_grid(n), WS_BLOCK, 0, st>>>(n, n_hist > 0 ? hist[0] : nullptr, n_hist > 1 ? hist[1] : nullptr,
                                                   n_hist > 2 ? hist[2] : nullptr, W.Ac.data(), W.fields.data());
     B2S_CHECK_LAUNCH();
-    const double zz = host_dot(s, W.Ac.data(), W.Ac.data(), n);
-    const double bb = host_dot(s, b, b, n);
+    launch_dot(s, W.Ac.data(), W.Ac.data(), n, W.dots.data() + 28);
+    launch_dot(s, b, b, n, W.dots.data() + 29);
+    double h2[2];
+    B2S_CUDA(cudaMemcpyAsync(h2, W.dots.data() + 28, sizeof(h2), cudaMemcpyDeviceToHost, st));
+    B2S_CUDA(cudaStreamSynchronize(st));
+    const double zz = h2[0], bb = h2[1];
     const double sz = zz > 0 ? std::sqrt(zz / (double)n) : 1.0;
     const double sb = bb > 0 ? std::sqrt(bb / (double)n) : 1.0;
     W.acc.resize((size_t)g.n_agg * WS_ACC);
@@ -1096,24 +1103,36 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
                                                          k > 2 ? cand[2] : cand[0], k > 3 ? cand[3] : cand[0],
                                                          alpha[0], alpha[1], alpha[2], alpha[3], x0);
             B2S_CHECK_LAUNCH();
-            // FP64 residual of the candidate start
+            // FP64 residual of the candidate start, r = b - sum alpha_k (A c_k)
+            // from the products the Gram already needed
             double* y = W.Ac.data() + (size_t)4 * n;
-            spmv_f64(s, s->A, x0, y, nullptr);
-            k_ws_residual<<<ws_grid(n), WS_BLOCK, 0, st>>>(n, b, y, y);
+            k_ws_residual_comb<<<ws_grid(n), WS_BLOCK, 0, st>>>(
+                n, k, b, W.Ac.data(), k > 1 ? W.Ac.data() + n : W.Ac.data(),
+                k > 2 ? W.Ac.data() + 2 * n : W.Ac.data(), k > 3 ? W.Ac.data() + 3 * n : W.Ac.data(), alpha[0],
+                alpha[1], alpha[2], alpha[3], y);
             B2S_CHECK_LAUNCH();
-            const double rr  = host_dot(s, y, y, n);
-            out.rel_res_tried = std::sqrt(rr / bb);
-            out.n_candidates  = k;
+            out.n_candidates = k;
             for(int i = 0; i < k; ++i)
                 out.coeff[i] = alpha[i];
             // the judge is the PCG's own residual measure, r^T P r (the
             // quantity the reference's stop rule |r.z| <= tol |r0.z0| tracks):
             // accept the start when it is below b^T P b of the zero start
-            double* zr = W.Ac.data();
-            double* zb = W.Ac.data() + (size_t)n;
-            precond_apply(s, y, zr);
-            precond_apply(s, b, zb);
-            const double rz = host_dot(s, y, zr, n), bz = host_dot(s, b, zb, n);
+            double*       zr = W.Ac.data();
+            const double* zb = W.fields.data() + 3 * (size_t)n;  // P b of the features
+            precond_launch(s, y, zr);
+            if(mode != B2S_WS_MODE_LEARNED)
+            {
+                precond_launch(s, b, W.Ac.data() + (size_t)n);
+                zb = W.Ac.data() + (size_t)n;
+            }
+            launch_dot(s, y, y, n, W.dots.data() + 24);
+            launch_dot(s, y, zr, n, W.dots.data() + 25);
+            launch_dot(s, b, zb, n, W.dots.data() + 26);
+            double h3[3];
+            B2S_CUDA(cudaMemcpyAsync(h3, W.dots.data() + 24, sizeof(h3), cudaMemcpyDeviceToHost, st));
+            B2S_CUDA(cudaStreamSynchronize(st));
+            const double rr = h3[0], rz = h3[1], bz = h3[2];
+            out.rel_res_tried = std::sqrt(rr / bb);
             out.rz_ratio    = bz > 0 ? rz / bz : INFINITY;
             if(std::isfinite(rr) && std::isfinite(rz) && bz > 0 && rz < bz)
             {

@@ -570,6 +570,13 @@ void precond_apply(b2s_solver* s, const double* r, double* z)
     B2S_CUDA(cudaStreamSynchronize(s->stream));
 }
 
+// z = P r queued on the solver's stream (no synchronisation, no error check)
+void precond_launch(b2s_solver* s, const double* r, double* z)
+{
+    B2S_REQUIRE(s->precond_kind >= 0, B2S_ERR_STATE, "precond_apply before b2s_precond_assemble");
+    precond_launch(s, s->precond_kind, r, z, nullptr, s->red);
+}
+
 // ---------------------------------------------------------------------------
 // PCG
 // ---------------------------------------------------------------------------

@@ -498,6 +498,9 @@ __global__ void __launch_bounds__(RED_BLOCK) k_dot(const double* __restrict__ a,
 }
 }  // namespace
 
+// blocks of the grid-stride reductions and of the preconditioner collect (8
+// per SM; 16 measured slower: the last block's in-order sum of the partials
+// grows with the grid)
 int reduction_grid() { return NUM_SMS_HINT * 8; }
 
 void launch_dot(b2s_solver* s, const double* a, const double* b, int64_t n, double* d_out)
