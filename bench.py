@@ -157,6 +157,68 @@ def cpu_baseline(s, budget_s: float = 20.0) -> dict:
             "rel_res": float(info["rel_res_true"]), "assembly_ms": t_asm * 1e3}
 
 
+def bar_run(dev, steps: int, warmup: int, history_steps: int = 6, epochs: int = 30) -> dict:
+    """A second run beside the headline: the twisted bar of 400 x 30 x 30 cells
+    (385,361 vertices, 1.16 M DoF; E = 1e6, nu = 0.49, ends turned 2 deg per
+    step), stepped and learned from like the headline run; the next step's
+    system is solved from each start, ms per solve by CUDA events."""
+    import torch
+
+    from libuipc_b200 import _abi
+    from libuipc_b200.learned import MODES, SequenceRunner
+    from libuipc_b200.linear_system import Solver
+    from libuipc_b200.sequence import SceneSequence
+
+    seq = SceneSequence(scene=2, cells_x=400, cells_y=30, cells_z=30, E=1e6, nu=0.49, twist_per_step=2.0)
+    stream = torch.cuda.Stream(device=dev)
+    solver = Solver(dev.index or 0)
+    solver.set_stream(stream.cuda_stream)
+    runner = SequenceRunner(solver, seq, dev)
+    solver.ws_init(128, seed=0)
+    with torch.cuda.stream(stream):
+        runner.run(history_steps, newton_iters=1, collect=True)
+    solver.ws_fit_normalization()
+    solver.ws_train(epochs, lr=1e-3, seed=0)
+    seq.begin_step()
+    s = seq.system()
+    hist = runner.hist(0)
+    with torch.cuda.stream(stream):
+        rows = torch.from_numpy(s.rows).to(dev)
+        cols = torch.from_numpy(s.cols).to(dev)
+        vals = torch.from_numpy(s.vals).to(dev)
+        b = torch.from_numpy(s.b).to(dev)
+        x = torch.zeros_like(b)
+    stream.synchronize()
+    starts = {"plain": (_abi.B2S_PRECISION_FP64, "zero"), "mixed": (_abi.B2S_PRECISION_MIXED, "zero"),
+              "mixed+history": (_abi.B2S_PRECISION_MIXED, "history"),
+              "mixed+learned": (_abi.B2S_PRECISION_MIXED, "learned")}
+    out = {"workload": "twisted bar 400x30x30 (385,361 vertices, 1.16 M DoF), Newton system of step "
+                       f"{seq.step} (history and training from steps 1-{seq.step - 1})"}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for mode, (prec, start) in starts.items():
+        def solve():
+            solver.assemble(s.n_verts, rows, cols, vals)
+            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_SWEEP_F32)
+            given = start != "zero"
+            if given:
+                solver.ws_predict(b, x, hist, MODES[start])
+            return solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, precision=prec,
+                              replace_every=50, x0_given=given)
+
+        for _ in range(warmup):
+            solve()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        st = [solve() for _ in range(steps)]
+        ev1.record(stream)
+        ev1.synchronize()
+        out[mode] = {"ms_per_solve": ev0.elapsed_time(ev1) / steps, "pcg_iterations": int(st[-1]["iterations_exact"]),
+                     "rel_res": float(st[-1]["rel_res"])}
+    out["speedup_vs_plain"] = out["plain"]["ms_per_solve"] / out["mixed+learned"]["ms_per_solve"]
+    solver.close()
+    return out
+
+
 def run_reference(args, rank: int) -> None:
     """The reference's algorithm on the host cores (the oracle port of
     libuipc's FP64 MAS-PCG; the CUDA reference cannot be built here)."""
@@ -213,6 +275,8 @@ def main() -> None:
     ap.add_argument("--history-steps", type=int, default=6,
                     help="time steps run (and learned from) before the measured system")
     ap.add_argument("--train-epochs", type=int, default=30)
+    ap.add_argument("--no-bar", action="store_true",
+                    help="skip the second run reported beside the headline: a 1.16 M-DoF twisted bar")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
 
@@ -347,6 +411,13 @@ def main() -> None:
     head = "mixed+learned"
     ms, stats, tm, clk, ws_info = res[head]
 
+    bar = None
+    if rank == 0 and not args.no_bar:
+        try:
+            bar = bar_run(dev, steps=3, warmup=3)
+        except Exception as e:  # reported, not fatal
+            bar = {"error": str(e)}
+
     # ---- e2e: host (pinned) inputs through the same public API -------------------
     e2e_ms, h2d, d2h = None, 0, 0
     if not args.no_e2e:
@@ -455,6 +526,7 @@ def main() -> None:
         "clocks": clk,
         "cpu_baseline": cpu,
         "generate_s": gen_s,
+        "bar_1M": bar,
     }
     solver.close()
     if rank == 0:
