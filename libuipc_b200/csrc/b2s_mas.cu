@@ -632,10 +632,11 @@ __device__ __forceinline__ void cluster_product(const float* M, const float (*r)
 // (one per connected component of the bank, summed by its lowest lane in lane
 // order) are written to R_{l+1}. Z_l = A_l^{-1} R_l for every node of the
 // bank. BF: BF16 tiles on the tensor cores (INV16_BYTES per cluster),
-// otherwise FP32 (INV_BYTES). VT: type of the fine residual. NST: copies in
-// flight per warp. `u` counts the banks this warp has run through its slots
-// (slot and phase of the next copy), so one warp can go through several
-// levels. Returns false when a copy wait ran out (the error flag is set and
+// otherwise FP32 (INV_BYTES). VT: type of the fine residual (FP32: 4 values
+// per node, padded; FP64: 3), roff its element offset of the range's first
+// vertex. NST: copies in flight per warp. `u` counts the banks this warp
+// has run through its slots (slot and phase of the next copy), so one warp
+// can go through several levels. Returns false when a copy wait ran out (the error flag is set and
 // the warp's copies in flight are drained).
 
 // the copies of a level's first NST banks of warp gw (lane 0 issues)
@@ -662,7 +663,7 @@ __device__ __forceinline__ void issue_first_copies(int gw, int W, int lane, int 
 
 template <bool FINE, typename VT, bool BF, int NST>
 __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int n_banks, int cnt, int level_begin,
-                                            const int32_t* __restrict__ p2r, const VT* __restrict__ r, int off3,
+                                            const int32_t* __restrict__ p2r, const VT* __restrict__ r, int roff,
                                             const uint16_t* __restrict__ comp_mask,
                                             const int32_t* __restrict__ new_local, int next_begin, int push,
                                             const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
@@ -696,9 +697,20 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
             nlive = v >= 0;
             if(nlive)
             {
-                n0 = (float)r[off3 + 3 * (int64_t)v];
-                n1 = (float)r[off3 + 3 * (int64_t)v + 1];
-                n2 = (float)r[off3 + 3 * (int64_t)v + 2];
+                if constexpr(sizeof(VT) == 4)
+                {
+                    // padded FP32 residual of the mixed PCG: one 16-byte load
+                    const float4 q = *reinterpret_cast<const float4*>(r + roff + 4 * (int64_t)v);
+                    n0 = q.x;
+                    n1 = q.y;
+                    n2 = q.z;
+                }
+                else
+                {
+                    n0 = (float)r[roff + 3 * (int64_t)v];
+                    n1 = (float)r[roff + 3 * (int64_t)v + 1];
+                    n2 = (float)r[roff + 3 * (int64_t)v + 2];
+                }
             }
         }
         else
@@ -808,7 +820,7 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
 template <bool FINE, typename VT, bool BF, int NST>
 __global__ void __launch_bounds__(APPLY_WARPS * 32)
     k_apply_level(int n_banks, int cnt, int level_begin, const int32_t* __restrict__ p2r, const VT* __restrict__ r,
-                  int off3, const uint16_t* __restrict__ comp_mask, const int32_t* __restrict__ new_local,
+                  int roff, const uint16_t* __restrict__ comp_mask, const int32_t* __restrict__ new_local,
                   int next_begin, int push, const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
                   const int* converged, int* err)
 {
@@ -828,7 +840,7 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
     __syncwarp();
     int u = 0;
     apply_banks<FINE, VT, BF, NST>(blockIdx.x * APPLY_WARPS + w, gridDim.x * APPLY_WARPS, lane, u, n_banks, cnt,
-                                   level_begin, p2r, r, off3, comp_mask, new_local, next_begin, push, inv, R, Z, err,
+                                   level_begin, p2r, r, roff, comp_mask, new_local, next_begin, push, inv, R, Z, err,
                                    &s_inv[w][0][0], s_r[w], s_bar[w]);
 }
 
@@ -1079,7 +1091,9 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
     {
         auto k = bf16 ? k_apply_level<true, VT, true, APPLY_STAGES_BF16>
                       : k_apply_level<true, VT, false, APPLY_STAGES_F32>;
-        k<<<apply_grid(k, n_banks0), tb, 0, st>>>(n_banks0, M.N, 0, M.p2r.data(), r, 3 * M.offset,
+        // element offset of the range's first vertex in r (FP32: 4 per node)
+        const int off = (sizeof(VT) == 4 ? 4 : 3) * M.offset;
+        k<<<apply_grid(k, n_banks0), tb, 0, st>>>(n_banks0, M.N, 0, M.p2r.data(), r, off,
                                                   M.comp_mask[0].data(), M.new_local[0].data(), M.level_begin[1],
                                                   M.L > 1 ? 1 : 0, inv, M.R.data(), M.Z.data(), converged, err);
         B2S_CHECK_LAUNCH();

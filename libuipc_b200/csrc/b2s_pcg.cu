@@ -187,13 +187,34 @@ struct MasView
     const float*   Z;
 };
 
-// z_i for block row i: MAS (partitioned vertices of its range), else 3x3
-// block Jacobi (kind 1 / 2), else identity (kind 0)
-template <typename VT>
-__device__ __forceinline__ void precond_row(int kind, const MasView& mv, const double* dinv, const VT* r, int i,
-                                            double z[3])
+// node i's three entries of r: NS = 3 values per node (FP64 vectors), or 4
+// (the padded FP32 vectors of the mixed PCG: one 16-byte load)
+template <typename VT, int NS>
+__device__ __forceinline__ void load_r(const VT* r, int64_t i, double& a, double& b, double& c)
 {
-    const double r0 = r[3 * (int64_t)i], r1 = r[3 * (int64_t)i + 1], r2 = r[3 * (int64_t)i + 2];
+    if constexpr(NS == 4)
+    {
+        const float4 q = *reinterpret_cast<const float4*>(r + 4 * i);
+        a = q.x;
+        b = q.y;
+        c = q.z;
+    }
+    else
+    {
+        a = r[3 * i];
+        b = r[3 * i + 1];
+        c = r[3 * i + 2];
+    }
+}
+
+// z_i for block row i: MAS (partitioned vertices of its range), else 3x3
+// block Jacobi (kind 1 / 2), else identity (kind 0); r_i is returned in rr
+template <typename VT, int NS>
+__device__ __forceinline__ void precond_row(int kind, const MasView& mv, const double* dinv, const VT* r, int i,
+                                            double z[3], double rr[3])
+{
+    load_r<VT, NS>(r, i, rr[0], rr[1], rr[2]);
+    const double r0 = rr[0], r1 = rr[1], r2 = rr[2];
     if(kind == B2S_PRECOND_MAS && mv.active)
     {
         const int v = i - mv.off;
@@ -235,11 +256,11 @@ __device__ __forceinline__ void precond_row(int kind, const MasView& mv, const d
         // row l of body b: z = (H_b^-1)[3l .. 3l+2][0 .. 11] r_b
         const int     b = (i - mv.abd_off) >> 2, l = (i - mv.abd_off) & 3;
         const double* Hi = mv.abd_inv + (size_t)b * 144 + 36 * l;
-        const int64_t r0i = 3 * ((int64_t)mv.abd_off + 4 * b);
+        const int64_t n0 = (int64_t)mv.abd_off + 4 * b;  // the body's first node
         double        a0 = 0.0, a1 = 0.0, a2 = 0.0;
         for(int j = 0; j < 12; ++j)
         {
-            const double rj = r[r0i + j];
+            const double rj = r[NS * (n0 + j / 3) + j % 3];
             a0 += Hi[j] * rj;
             a1 += Hi[12 + j] * rj;
             a2 += Hi[24 + j] * rj;
@@ -260,7 +281,7 @@ __device__ __forceinline__ void precond_row(int kind, const MasView& mv, const d
 // 32 registers, so the whole reduction grid (8 CTAs per SM) is resident at
 // once (with 40 the last quarter of the grid ran as a second wave: the MAS
 // apply with this finish measured 77.4 -> 73.8 us on 551 k vertices).
-template <typename VT>
+template <typename VT, int NS>
 __global__ void __launch_bounds__(RED_BLOCK, 8) k_precond_finish(int32_t nb, int kind, MasView mv,
                                                               const double* __restrict__ dinv,
                                                               const VT* __restrict__ r, VT* __restrict__ z,
@@ -272,17 +293,21 @@ __global__ void __launch_bounds__(RED_BLOCK, 8) k_precond_finish(int32_t nb, int
     double rz = 0.0, rr = 0.0;
     for(int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < nb; i += gridDim.x * RED_BLOCK)
     {
-        double zi[3];
-        precond_row<VT>(kind, mv, dinv, r, i, zi);
+        double zi[3], ri[3];
+        precond_row<VT, NS>(kind, mv, dinv, r, i, zi, ri);
         const VT z0 = (VT)zi[0], z1 = (VT)zi[1], z2 = (VT)zi[2];
-        z[3 * (int64_t)i]     = z0;
-        z[3 * (int64_t)i + 1] = z1;
-        z[3 * (int64_t)i + 2] = z2;
+        if constexpr(NS == 4)
+            *reinterpret_cast<float4*>(z + 4 * (int64_t)i) = make_float4(z0, z1, z2, 0.0f);
+        else
+        {
+            z[3 * (int64_t)i]     = z0;
+            z[3 * (int64_t)i + 1] = z1;
+            z[3 * (int64_t)i + 2] = z2;
+        }
         if(sc)
         {
-            const double r0 = r[3 * (int64_t)i], r1 = r[3 * (int64_t)i + 1], r2 = r[3 * (int64_t)i + 2];
-            rz += r0 * (double)z0 + r1 * (double)z1 + r2 * (double)z2;
-            rr += r0 * r0 + r1 * r1 + r2 * r2;
+            rz += ri[0] * (double)z0 + ri[1] * (double)z1 + ri[2] * (double)z2;
+            rr += ri[0] * ri[0] + ri[1] * ri[1] + ri[2] * ri[2];
         }
     }
     if(!sc)
@@ -339,36 +364,11 @@ __global__ void k_update_p(int64_t n, const PcgScalars* sc, const double* __rest
 }
 
 // ---- mixed precision (FP32 vectors, FP64 solution and scalars) ----------------
-__global__ void k_update_xr_mixed(int64_t n, PcgScalars* sc, double* __restrict__ x, const float* __restrict__ p,
-                                  float* __restrict__ r, float* __restrict__ Ap)
-{
-    if(frozen(sc))
-        return;
-    const double alpha = sc->rz / sc->pAp;
-    if(blockIdx.x == 0 && threadIdx.x == 0)
-        sc->alpha = alpha;
-    const float af = (float)alpha;
-    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
-    {
-        const float api = Ap[i];
-        x[i] += alpha * (double)p[i];
-        r[i] = __fmaf_rn(-af, api, r[i]);
-        Ap[i] = 0.0f;
-    }
-}
-
-__global__ void k_update_p_mixed(int64_t n, const PcgScalars* sc, const float* __restrict__ z, float* __restrict__ p)
-{
-    if(frozen(sc))
-        return;
-    const float beta = (float)sc->beta;
-    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
-        p[i] = __fmaf_rn(beta, p[i], z[i]);
-}
-
-// the same two updates, four entries per thread and step with 16-byte
-// accesses (all vectors 16-byte aligned; the last n % 4 entries scalar)
-__global__ void k_update_xr_mixed4(int64_t n, PcgScalars* sc, double* __restrict__ x, const float* __restrict__ p,
+// The FP32 vectors (r, z, p, Ap) hold 4 floats per node, the 4th zero
+// (16-byte gathers and vector reductions in the SpMV and the MAS apply); the
+// FP64 solution x holds 3. x += alpha p, r -= alpha Ap, Ap = 0, one node per
+// thread and step.
+__global__ void k_update_xr_mixed4(int32_t nb, PcgScalars* sc, double* __restrict__ x, const float* __restrict__ p,
                                    float* __restrict__ r, float* __restrict__ Ap)
 {
     if(frozen(sc))
@@ -376,38 +376,24 @@ __global__ void k_update_xr_mixed4(int64_t n, PcgScalars* sc, double* __restrict
     const double alpha = sc->rz / sc->pAp;
     if(blockIdx.x == 0 && threadIdx.x == 0)
         sc->alpha = alpha;
-    const float   af     = (float)alpha;
-    const int64_t n4     = n >> 2;
-    const int64_t stride = (int64_t)gridDim.x * VEC_BLOCK;
-    const int64_t t0     = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x;
-    for(int64_t i = t0; i < n4; i += stride)
+    const float af = (float)alpha;
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < nb; i += (int64_t)gridDim.x * VEC_BLOCK)
     {
         const float4 ap = reinterpret_cast<const float4*>(Ap)[i];
         const float4 pp = reinterpret_cast<const float4*>(p)[i];
         float4       rr = reinterpret_cast<float4*>(r)[i];
-        double2      x0 = reinterpret_cast<double2*>(x)[2 * i], x1 = reinterpret_cast<double2*>(x)[2 * i + 1];
-        x0.x += alpha * (double)pp.x;
-        x0.y += alpha * (double)pp.y;
-        x1.x += alpha * (double)pp.z;
-        x1.y += alpha * (double)pp.w;
+        x[3 * i] += alpha * (double)pp.x;
+        x[3 * i + 1] += alpha * (double)pp.y;
+        x[3 * i + 2] += alpha * (double)pp.z;
         rr.x = __fmaf_rn(-af, ap.x, rr.x);
         rr.y = __fmaf_rn(-af, ap.y, rr.y);
         rr.z = __fmaf_rn(-af, ap.z, rr.z);
-        rr.w = __fmaf_rn(-af, ap.w, rr.w);
-        reinterpret_cast<double2*>(x)[2 * i]     = x0;
-        reinterpret_cast<double2*>(x)[2 * i + 1] = x1;
-        reinterpret_cast<float4*>(r)[i]          = rr;
-        reinterpret_cast<float4*>(Ap)[i]         = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    for(int64_t i = 4 * n4 + t0; i < n; i += stride)
-    {
-        const float api = Ap[i];
-        x[i] += alpha * (double)p[i];
-        r[i] = __fmaf_rn(-af, api, r[i]);
-        Ap[i] = 0.0f;
+        reinterpret_cast<float4*>(r)[i]  = rr;
+        reinterpret_cast<float4*>(Ap)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
 }
 
+// p = z + beta p over the padded vectors (n = 4 nb; pads stay zero)
 __global__ void k_update_p_mixed4(int64_t n, const PcgScalars* sc, const float* __restrict__ z, float* __restrict__ p)
 {
     if(frozen(sc))
@@ -430,12 +416,30 @@ __global__ void k_update_p_mixed4(int64_t n, const PcgScalars* sc, const float* 
         p[i] = __fmaf_rn(beta, p[i], z[i]);
 }
 
-// r32 = b - Ax computed in FP64, stored FP32
-__global__ void k_residual_f32(int64_t n, const double* __restrict__ b, const double* __restrict__ Ax,
+// r32 = b - Ax computed in FP64, stored FP32 (padded: 4 floats per node)
+__global__ void k_residual_f32(int32_t nb, const double* __restrict__ b, const double* __restrict__ Ax,
                                float* __restrict__ r)
 {
-    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * VEC_BLOCK)
-        r[i] = (float)(b[i] - Ax[i]);
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < nb; i += (int64_t)gridDim.x * VEC_BLOCK)
+        reinterpret_cast<float4*>(r)[i] = make_float4((float)(b[3 * i] - Ax[3 * i]), (float)(b[3 * i + 1] - Ax[3 * i + 1]),
+                                                      (float)(b[3 * i + 2] - Ax[3 * i + 2]), 0.0f);
+}
+
+// between the 3-per-node FP32 vectors of the ABI and the padded ones
+__global__ void k_pad4(int32_t nb, const float* __restrict__ a, float* __restrict__ b)
+{
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < nb; i += (int64_t)gridDim.x * VEC_BLOCK)
+        reinterpret_cast<float4*>(b)[i] = make_float4(a[3 * i], a[3 * i + 1], a[3 * i + 2], 0.0f);
+}
+__global__ void k_unpad4(int32_t nb, const float* __restrict__ a, float* __restrict__ b)
+{
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < nb; i += (int64_t)gridDim.x * VEC_BLOCK)
+    {
+        const float4 q = reinterpret_cast<const float4*>(a)[i];
+        b[3 * i]       = q.x;
+        b[3 * i + 1]   = q.y;
+        b[3 * i + 2]   = q.z;
+    }
 }
 
 // FP32 vectors, FP64 sums: out[0] = a.b, out[1] = a.a
@@ -560,7 +564,7 @@ static void precond_launch(b2s_solver* s, int kind, const double* r, double* z, 
         mas_apply_levels(s, r, sc ? &sc->converged : nullptr);
     const int grid = reduction_grid();
     ensure_reduction(red, grid, 2);
-    k_precond_finish<double><<<grid, RED_BLOCK, 0, st>>>(nb, kind, mas_view(s), s->dinv.data(), r, z, sc,
+    k_precond_finish<double, 3><<<grid, RED_BLOCK, 0, st>>>(nb, kind, mas_view(s), s->dinv.data(), r, z, sc,
                                                  red.partials.data(), red.counter.data());
     B2S_CHECK_LAUNCH();
 }
@@ -897,7 +901,7 @@ static void precond_launch_f32(b2s_solver* s, int kind, const float* r, float* z
         mas_apply_levels_f32(s, r, sc ? &sc->converged : nullptr, mixed_inverse_bf16());
     const int grid = reduction_grid();
     ensure_reduction(red, grid, 2);
-    k_precond_finish<float><<<grid, RED_BLOCK, 0, s->stream>>>(nb, kind, mas_view(s), s->dinv.data(), r, z, sc,
+    k_precond_finish<float, 4><<<grid, RED_BLOCK, 0, s->stream>>>(nb, kind, mas_view(s), s->dinv.data(), r, z, sc,
                                                                red.partials.data(), red.counter.data());
     B2S_CHECK_LAUNCH();
 }
@@ -911,12 +915,21 @@ static void ensure_bf16_inverses(b2s_solver* s)
     }
 }
 
+// r, z: 3 floats per node (the ABI's layout), padded around the apply
 void precond_apply_mixed(b2s_solver* s, const float* r, float* z)
 {
     B2S_REQUIRE(s->precond_kind >= 0, B2S_ERR_STATE, "precond_apply before b2s_precond_assemble");
     ensure_bf16_inverses(s);
     ensure_reduction(s->red, reduction_grid(), 2);
-    precond_launch_f32(s, s->precond_kind, r, z, nullptr, s->red);
+    const int32_t nb = s->A.nb;
+    PcgState&     P  = s->pcg;
+    P.r32.resize(4 * (size_t)nb, 1.1);
+    P.z32.resize(4 * (size_t)nb, 1.1);
+    k_pad4<<<vec_grid(nb), VEC_BLOCK, 0, s->stream>>>(nb, r, P.r32.data());
+    B2S_CHECK_LAUNCH();
+    precond_launch_f32(s, s->precond_kind, P.r32.data(), P.z32.data(), nullptr, s->red);
+    k_unpad4<<<vec_grid(nb), VEC_BLOCK, 0, s->stream>>>(nb, P.z32.data(), z);
+    B2S_CHECK_LAUNCH();
     check_device_errors(s);
 }
 
@@ -925,26 +938,23 @@ static void pcg_iteration_mixed(b2s_solver* s, int kind, double* x, int slot)
     PcgState&     P  = s->pcg;
     const Matrix& A  = s->A;
     cudaStream_t  st = s->stream;
-    const int64_t n  = 3 * (int64_t)A.nb;
+    const int32_t nb = A.nb;
     cudaEvent_t*  ev = s->timing ? &s->iter_events[(size_t)slot * 4] : nullptr;
     if(ev)
         B2S_CUDA(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
     spmv_f32_launch(s, A, P.p32.data(), P.Ap32.data(), P.red, &P.sc.data()->pAp, &P.sc.data()->converged);
     if(ev)
         B2S_CUDA(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
-    if(((uintptr_t)x & 15u) == 0)
-        k_update_xr_mixed4<<<vec_grid((n + 3) / 4), VEC_BLOCK, 0, st>>>(n, P.sc.data(), x, P.p32.data(),
-                                                                       P.r32.data(), P.Ap32.data());
-    else
-        k_update_xr_mixed<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), x, P.p32.data(), P.r32.data(),
-                                                             P.Ap32.data());
+    k_update_xr_mixed4<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(nb, P.sc.data(), x, P.p32.data(), P.r32.data(),
+                                                           P.Ap32.data());
     B2S_CHECK_LAUNCH();
     if(ev)
         B2S_CUDA(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
     precond_launch_f32(s, kind, P.r32.data(), P.z32.data(), P.sc.data(), P.red);
     if(ev)
         B2S_CUDA(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
-    k_update_p_mixed4<<<vec_grid((n + 3) / 4), VEC_BLOCK, 0, st>>>(n, P.sc.data(), P.z32.data(), P.p32.data());
+    k_update_p_mixed4<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(4 * (int64_t)nb, P.sc.data(), P.z32.data(),
+                                                         P.p32.data());
     B2S_CHECK_LAUNCH();
 }
 
@@ -968,10 +978,12 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
         st_out.converged = 1;
         return;
     }
-    P.r32.resize(n, 1.1);
-    P.z32.resize(n, 1.1);
-    P.p32.resize(n, 1.1);
-    P.Ap32.resize(n, 1.1);
+    const int32_t nb = A.nb;
+    const int64_t n4 = 4 * (int64_t)nb;  // padded FP32 vectors
+    P.r32.resize(n4, 1.1);
+    P.z32.resize(n4, 1.1);
+    P.p32.resize(n4, 1.1);
+    P.Ap32.resize(n4, 1.1);
     P.tmp.resize(n, 1.1);
     P.sc.resize(1);
     if(!P.h_sc)
@@ -1004,17 +1016,17 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
         B2S_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
         B2S_CUDA(cudaMemsetAsync(P.tmp.data(), 0, sizeof(double) * n, st));
     }
-    k_residual_f32<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, b, P.tmp.data(), P.r32.data());
+    k_residual_f32<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(nb, b, P.tmp.data(), P.r32.data());
     B2S_CHECK_LAUNCH();
 
     auto restart_from_r = [&](int k) -> double
     {
         // z = P r, p = z; returns r.z (FP64 sum); also leaves r.r in dot_out[1]
         precond_launch_f32(s, k, P.r32.data(), P.z32.data(), nullptr, s->red);
-        k_dot2_f32<<<reduction_grid(), RED_BLOCK, 0, st>>>(n, P.r32.data(), P.z32.data(), s->red.partials.data(),
+        k_dot2_f32<<<reduction_grid(), RED_BLOCK, 0, st>>>(n4, P.r32.data(), P.z32.data(), s->red.partials.data(),
                                                             s->red.counter.data(), s->dot_out.data());
         B2S_CHECK_LAUNCH();
-        B2S_CUDA(cudaMemcpyAsync(P.p32.data(), P.z32.data(), sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        B2S_CUDA(cudaMemcpyAsync(P.p32.data(), P.z32.data(), sizeof(float) * n4, cudaMemcpyDeviceToDevice, st));
         double h2[2];
         B2S_CUDA(cudaMemcpyAsync(h2, s->dot_out.data(), sizeof(h2), cudaMemcpyDeviceToHost, st));
         B2S_CUDA(cudaStreamSynchronize(st));
@@ -1049,7 +1061,7 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
     auto replace_residual = [&]()
     {
         spmv_f64(s, A, x, P.tmp.data(), nullptr);
-        k_residual_f32<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, b, P.tmp.data(), P.r32.data());
+        k_residual_f32<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(nb, b, P.tmp.data(), P.r32.data());
         B2S_CHECK_LAUNCH();
     };
     if(rz0 == 0.0 || bb == 0.0)
@@ -1073,7 +1085,7 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
         h.iter      = iter_total;
         h.iter_conv = 0;
         B2S_CUDA(cudaMemcpyAsync(P.sc.data(), &h, sizeof(h), cudaMemcpyHostToDevice, st));
-        B2S_CUDA(cudaMemsetAsync(P.Ap32.data(), 0, sizeof(float) * n, st));
+        B2S_CUDA(cudaMemsetAsync(P.Ap32.data(), 0, sizeof(float) * n4, st));
         bool use_graph = o.use_graph && st != nullptr;
         if(s->timing)
             ensure_iter_events(s, ci);

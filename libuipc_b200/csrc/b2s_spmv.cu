@@ -68,12 +68,40 @@ __device__ __forceinline__ void ld4(const uint16_t* p, int v[4])
     v[0] = (int)(q.x & 0xFFFFu); v[1] = (int)(q.x >> 16); v[2] = (int)(q.y & 0xFFFFu); v[3] = (int)(q.y >> 16);
 }
 
-template <typename XT>
-__device__ __forceinline__ void red3(XT* y, int32_t node, XT a0, XT a1, XT a2)
+// A node's three components. P4: the padded FP32 vectors of the mixed PCG
+// (4 floats per node, the 4th zero): one 16-byte load, one vector reduction;
+// otherwise 3 values per node (FP64 vectors).
+template <typename XT, bool P4>
+__device__ __forceinline__ void load_node(const XT* __restrict__ x, int32_t node, XT& a, XT& b, XT& c)
 {
-    atomic_add_t(y + 3 * (int64_t)node, a0);
-    atomic_add_t(y + 3 * (int64_t)node + 1, a1);
-    atomic_add_t(y + 3 * (int64_t)node + 2, a2);
+    if constexpr(P4)
+    {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(x) + node);
+        a = q.x;
+        b = q.y;
+        c = q.z;
+    }
+    else
+    {
+        a = __ldg(x + 3 * (int64_t)node);
+        b = __ldg(x + 3 * (int64_t)node + 1);
+        c = __ldg(x + 3 * (int64_t)node + 2);
+    }
+}
+
+template <typename XT, bool P4>
+__device__ __forceinline__ void red_node(XT* y, int32_t node, XT a0, XT a1, XT a2)
+{
+    if constexpr(P4)
+        asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(y + 4 * (int64_t)node), "f"(a0), "f"(a1),
+                     "f"(a2), "f"(0.0f)
+                     : "memory");
+    else
+    {
+        atomic_add_t(y + 3 * (int64_t)node, a0);
+        atomic_add_t(y + 3 * (int64_t)node + 1, a1);
+        atomic_add_t(y + 3 * (int64_t)node + 2, a2);
+    }
 }
 
 // the streamed data of one thread's SPMV_BPT blocks
@@ -108,7 +136,7 @@ __device__ __forceinline__ void load_tile(TileLoad<VT>& t, int64_t e0, int64_t S
 
 // row halves of a thread's blocks to y (runs of equal rows merged), the
 // transposed halves into shared memory at the blocks' ranks, and the dot
-template <typename VT, typename XT, bool WITH_DOT>
+template <typename VT, typename XT, bool WITH_DOT, bool P4>
 __device__ __forceinline__ void tile_rows(const TileLoad<VT>& t, const XT* __restrict__ x, XT* y,
                                           XT (*s_t)[SPMV_TILE], int32_t* s_col, double& dot)
 {
@@ -120,18 +148,16 @@ __device__ __forceinline__ void tile_rows(const TileLoad<VT>& t, const XT* __res
     {
         if(t.r[k] < 0)
             break;  // padding: only at the end of the stream
-        const int32_t ck  = t.c[k];
-        const XT      xj0 = __ldg(x + 3 * (int64_t)ck), xj1 = __ldg(x + 3 * (int64_t)ck + 1),
-                 xj2 = __ldg(x + 3 * (int64_t)ck + 2);
+        const int32_t ck = t.c[k];
+        XT            xj0, xj1, xj2;
+        load_node<XT, P4>(x, ck, xj0, xj1, xj2);
         if(t.r[k] != cur)
         {
             if(cur >= 0)
-                red3(y, cur, a0, a1, a2);
+                red_node<XT, P4>(y, cur, a0, a1, a2);
             cur = t.r[k];
             a0 = a1 = a2 = 0;
-            xi0 = __ldg(x + 3 * (int64_t)cur);
-            xi1 = __ldg(x + 3 * (int64_t)cur + 1);
-            xi2 = __ldg(x + 3 * (int64_t)cur + 2);
+            load_node<XT, P4>(x, cur, xi0, xi1, xi2);
         }
         // column-major: B(p,q) = b[q*3 + p]
         const XT y0 = (XT)t.b[0][k] * xj0 + (XT)t.b[3][k] * xj1 + (XT)t.b[6][k] * xj2;
@@ -153,12 +179,12 @@ __device__ __forceinline__ void tile_rows(const TileLoad<VT>& t, const XT* __res
         s_col[rk]    = ck;
     }
     if(cur >= 0)
-        red3(y, cur, a0, a1, a2);
+        red_node<XT, P4>(y, cur, a0, a1, a2);
 }
 
 // transposed halves in (column, index) order: this thread's slots, runs of
 // equal columns merged; n = blocks in the tile
-template <typename XT>
+template <typename XT, bool P4>
 __device__ __forceinline__ void tile_cols(int tid, int n, const XT (*s_t)[SPMV_TILE], const int32_t* s_col, XT* y)
 {
     const int s0  = SPMV_BPT * tid;
@@ -174,7 +200,7 @@ __device__ __forceinline__ void tile_cols(int tid, int n, const XT (*s_t)[SPMV_T
         if(cc != cur)
         {
             if(cur >= 0)
-                red3(y, cur, t0, t1, t2);
+                red_node<XT, P4>(y, cur, t0, t1, t2);
             cur = cc;
             t0 = t1 = t2 = 0;
         }
@@ -183,7 +209,7 @@ __device__ __forceinline__ void tile_cols(int tid, int n, const XT (*s_t)[SPMV_T
         t2 += s_t[2][sl];
     }
     if(cur >= 0)
-        red3(y, cur, t0, t1, t2);
+        red_node<XT, P4>(y, cur, t0, t1, t2);
 }
 
 // U: stored blocks; S: plane stride. FP64 values, loaded straight into
@@ -208,9 +234,9 @@ __global__ void __launch_bounds__(SPMV_THREADS)
         const int64_t e0  = tile * SPMV_TILE + SPMV_BPT * tid;
         TileLoad<VT>  cur;
         load_tile(cur, e0, S, e0 < S, rows, cols, trank, vals);
-        tile_rows<VT, XT, WITH_DOT>(cur, x, y, s_t, s_col, dot);
+        tile_rows<VT, XT, WITH_DOT, false>(cur, x, y, s_t, s_col, dot);
         __syncthreads();
-        tile_cols<XT>(tid, n, s_t, s_col, y);
+        tile_cols<XT, false>(tid, n, s_t, s_col, y);
         __syncthreads();
     }
     if(WITH_DOT)
@@ -227,7 +253,10 @@ __global__ void __launch_bounds__(SPMV_THREADS)
 // is read out of the stage, so the copy overlaps that tile's reductions and
 // the other CTAs' work, with no registers held for it (one 47 KB stage per
 // CTA: three CTAs per SM; two stages were slower).
-// The reductions are those of k_spmv_tile (same order, same results).
+// x and y are the padded FP32 vectors of the mixed PCG (4 floats per node,
+// 16-byte aligned, the 4th zero): a gather is one 16-byte load and a run's
+// reduction one red.global.add.v4.f32. The runs and their order are those of
+// k_spmv_tile.
 constexpr int      TMA_STAGES  = 1;
 constexpr uint32_t STAGE_BYTES = SPMV_TILE * (4 + 4 + 2 + 9 * 4);  // 47,104
 
@@ -323,14 +352,14 @@ __global__ void __launch_bounds__(SPMV_THREADS)
             for(int k = 0; k < 4; ++k)
                 t.r[k] = -1;
         }
-        tile_rows<float, float, WITH_DOT>(t, x, y, reinterpret_cast<float(*)[SPMV_TILE]>(s_t), s_col, dot);
+        tile_rows<float, float, WITH_DOT, true>(t, x, y, reinterpret_cast<float(*)[SPMV_TILE]>(s_t), s_col, dot);
         __syncthreads();  // the stage is read and the transposed halves are placed
         if(tid == 0 && tile + (int64_t)TMA_STAGES * G < n_tiles)
         {
             fence_proxy_async_smem();
             issue(tile + (int64_t)TMA_STAGES * G);
         }
-        tile_cols<float>(tid, n, reinterpret_cast<const float(*)[SPMV_TILE]>(s_t), s_col, y);
+        tile_cols<float, true>(tid, n, reinterpret_cast<const float(*)[SPMV_TILE]>(s_t), s_col, y);
         __syncthreads();  // s_t is free for the next tile
     }
     if(!ok && tid == 0)
@@ -448,7 +477,7 @@ void spmv_f64_launch(b2s_solver* s, const Matrix& A, const double* x, double* y,
                                         y, &red, d_dot, stop);
 }
 
-// FP32 values and vectors (mixed precision), FP64 dot
+// FP32 values and padded FP32 vectors (mixed precision), FP64 dot
 // the TMA SpMV's shared-memory opt-in (once per device; outside graph capture)
 void spmv_prepare_f32(b2s_solver* s)
 {
