@@ -166,41 +166,75 @@ namespace
 constexpr int ASM_BLOCK = 256;
 constexpr int ROW_CAP   = 256;  // (col, src) pairs per row held in shared memory
 
+// The triplets of a warp mostly come from one or two elements, so few
+// distinct rows: the lanes holding the same row (__match_any_sync) add their
+// count with one atomic by the lowest of them. The loops step warp by warp so
+// all lanes take part in every match.
 __global__ void k_count_rows(const int32_t* __restrict__ rows, const int32_t* __restrict__ cols, int64_t T,
                              int32_t nb, int32_t* __restrict__ row_count, int* err)
 {
-    for(int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x)
+    const int     lane   = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for(int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < T; base += stride)
     {
-        const int32_t r = rows[t], c = cols[t];
-        if(r < 0 || r > c)
-            continue;
-        if(c >= nb)
+        const int64_t t = base + lane;
+        int32_t       r = -1, c = 0;
+        if(t < T)
+        {
+            r = rows[t];
+            c = cols[t];
+        }
+        bool ok = t < T && r >= 0 && r <= c;
+        if(ok && c >= nb)
         {
             atomicOr(err, DERR_TRIPLET_INDEX);
-            continue;
+            ok = false;
         }
-        atomicAdd(&row_count[r], 1);
+        const unsigned peers = __match_any_sync(0xffffffffu, ok ? r : -1 - lane);
+        if(ok && lane == __ffs(peers) - 1)
+            atomicAdd(&row_count[r], __popc(peers));
     }
 }
 
+// (column, source) of every kept triplet into its row's bucket; the lanes of
+// a row take consecutive places from one atomic of the lowest of them
 __global__ void k_scatter_rows(const int32_t* __restrict__ rows, const int32_t* __restrict__ cols, int64_t T,
                                int32_t nb, const int32_t* __restrict__ row_start, int32_t* __restrict__ row_fill,
-                               int32_t* __restrict__ bucket_col, int32_t* __restrict__ bucket_src, int* err)
+                               int2* __restrict__ bucket, int* err)
 {
-    for(int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x)
+    const int     lane   = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for(int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < T; base += stride)
     {
-        const int32_t r = rows[t], c = cols[t];
-        if(r < 0 || r > c || c >= nb)
+        const int64_t t = base + lane;
+        int32_t       r = -1, c = 0;
+        if(t < T)
+        {
+            r = rows[t];
+            c = cols[t];
+        }
+        const bool ok  = t < T && r >= 0 && r <= c && c < nb;
+        int32_t    beg = 0, len = 0;
+        if(ok)
+        {
+            beg = row_start[r];
+            len = row_start[r + 1] - beg;
+        }
+        const unsigned peers  = __match_any_sync(0xffffffffu, ok ? r : -1 - lane);
+        const int      leader = __ffs(peers) - 1;
+        int32_t        pos    = 0;
+        if(ok && lane == leader)
+            pos = atomicAdd(&row_fill[r], __popc(peers));
+        pos = __shfl_sync(0xffffffffu, pos, leader);
+        if(!ok)
             continue;
-        const int32_t beg = row_start[r], len = row_start[r + 1] - beg;
-        const int32_t k = atomicAdd(&row_fill[r], 1);
+        const int32_t k = pos + __popc(peers & ((1u << lane) - 1u));
         if(k >= len)
         {
             atomicOr(err, DERR_ROW_OVERFLOW);
             continue;
         }
-        bucket_col[beg + k] = c;
-        bucket_src[beg + k] = (int32_t)t;
+        bucket[beg + k] = make_int2(c, (int32_t)t);
     }
 }
 
@@ -212,8 +246,7 @@ __device__ __forceinline__ bool key_less(int32_t ca, int32_t sa, int32_t cb, int
 // One warp per row: rank every (col, src) pair of the row by counting the
 // pairs that order before it, write the sorted row and its unique-column count.
 __global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32_t* __restrict__ row_start,
-                                                         const int32_t* __restrict__ bucket_col,
-                                                         const int32_t* __restrict__ bucket_src,
+                                                         const int2* __restrict__ bucket,
                                                          int32_t* __restrict__ sorted_col,
                                                          int32_t* __restrict__ sorted_src,
                                                          int32_t* __restrict__ uniq_count)
@@ -226,7 +259,34 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32
     {
         const int32_t beg = row_start[r], L = row_start[r + 1] - beg;
         int           uniq = 0;
-        if(L <= 64)
+        if(L <= 32)
+        {
+            // one key per lane (column << 32 | source), bitonic sort across
+            // the warp, padding = max key
+            uint64_t key = ~0ull;
+            if(lane < L)
+            {
+                const int2 q = bucket[beg + lane];
+                key          = ((uint64_t)(uint32_t)q.x << 32) | (uint64_t)(uint32_t)q.y;
+            }
+#pragma unroll
+            for(int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+                for(int s = k >> 1; s > 0; s >>= 1)
+                {
+                    const uint64_t other    = __shfl_xor_sync(0xffffffffu, key, s);
+                    const bool     keep_min = ((lane & s) == 0) == ((lane & k) == 0);
+                    key = keep_min ? (key < other ? key : other) : (key < other ? other : key);
+                }
+            const uint64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+            if(lane < L)
+            {
+                sorted_col[beg + lane] = (int32_t)(key >> 32);
+                sorted_src[beg + lane] = (int32_t)(key & 0xFFFFFFFFull);
+                uniq = (lane == 0 || (prev >> 32) != (key >> 32)) ? 1 : 0;
+            }
+        }
+        else if(L <= 64)
         {
             // bitonic sort of the (column << 32 | source) keys in registers,
             // two per lane (positions lane and lane + 32), padding = max key
@@ -235,9 +295,13 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32
             for(int j = 0; j < 2; ++j)
             {
                 const int p = j * 32 + lane;
-                key[j]      = p < L ? ((uint64_t)(uint32_t)bucket_col[beg + p] << 32) |
-                                     (uint64_t)(uint32_t)bucket_src[beg + p]
-                                    : ~0ull;
+                if(p < L)
+                {
+                    const int2 q = bucket[beg + p];
+                    key[j]       = ((uint64_t)(uint32_t)q.x << 32) | (uint64_t)(uint32_t)q.y;
+                }
+                else
+                    key[j] = ~0ull;
             }
 #pragma unroll
             for(int k = 2; k <= 64; k <<= 1)
@@ -284,8 +348,9 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32
         {
             for(int k = lane; k < L; k += 32)
             {
-                s_col[w][k] = bucket_col[beg + k];
-                s_src[w][k] = bucket_src[beg + k];
+                const int2 q = bucket[beg + k];
+                s_col[w][k]  = q.x;
+                s_src[w][k]  = q.y;
             }
             __syncwarp();
             for(int k = lane; k < L; k += 32)
@@ -310,11 +375,13 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32
             // long row: same ranking straight from global memory
             for(int k = lane; k < L; k += 32)
             {
-                const int32_t c = bucket_col[beg + k], sr = bucket_src[beg + k];
+                const int2    me = bucket[beg + k];
+                const int32_t c = me.x, sr = me.y;
                 int rank = 0, head = 1;
                 for(int q = 0; q < L; ++q)
                 {
-                    const int32_t cq = bucket_col[beg + q], sq = bucket_src[beg + q];
+                    const int2    o  = bucket[beg + q];
+                    const int32_t cq = o.x, sq = o.y;
                     rank += key_less(cq, sq, c, sr) ? 1 : 0;
                     if(cq == c && sq < sr)
                         head = 0;
@@ -377,8 +444,9 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_mark_runs(int32_t nb, const int32
 
 // One thread per unique block: the sum of its run's source blocks in source
 // order (the sorted order), written to the value planes. Sources are fetched
-// four at a time so each thread keeps 36 independent loads in flight; the
-// additions stay in order, so the sums are those of the sequential loop.
+// four at a time, the first included (most runs hold 4 or fewer: one round of
+// 36 independent loads); the additions stay in order starting from the first
+// source, so the sums are those of the sequential loop.
 __global__ void __launch_bounds__(ASM_BLOCK) k_sum_runs(int64_t U, const int32_t* __restrict__ run_start,
                                                         const int32_t* __restrict__ sorted_src,
                                                         const double* __restrict__ src_vals,
@@ -387,37 +455,25 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_sum_runs(int64_t U, const int32_t
     for(int64_t o = (int64_t)blockIdx.x * ASM_BLOCK + threadIdx.x; o < U; o += (int64_t)gridDim.x * ASM_BLOCK)
     {
         const int32_t b = run_start[o], e = run_start[o + 1];
-        double        acc[9];
+        double        acc[9] = {};
+        for(int32_t k = b; k < e; k += 4)
         {
-            const int64_t s = sorted_src[b];
+            int64_t src[4];
 #pragma unroll
-            for(int q = 0; q < 9; ++q)
-                acc[q] = src_vals[s * 9 + q];
-        }
-        int32_t k = b + 1;
-        for(; k + 4 <= e; k += 4)
-        {
+            for(int t = 0; t < 4; ++t)
+                src[t] = k + t < e ? (int64_t)sorted_src[k + t] : -1;
             double v[4][9];
 #pragma unroll
             for(int t = 0; t < 4; ++t)
-            {
-                const int64_t s = sorted_src[k + t];
 #pragma unroll
                 for(int q = 0; q < 9; ++q)
-                    v[t][q] = src_vals[s * 9 + q];
-            }
+                    v[t][q] = src[t] >= 0 ? src_vals[src[t] * 9 + q] : 0.0;
 #pragma unroll
             for(int t = 0; t < 4; ++t)
+                if(src[t] >= 0)
 #pragma unroll
-                for(int q = 0; q < 9; ++q)
-                    acc[q] += v[t][q];
-        }
-        for(; k < e; ++k)
-        {
-            const int64_t s = sorted_src[k];
-#pragma unroll
-            for(int q = 0; q < 9; ++q)
-                acc[q] += src_vals[s * 9 + q];
+                    for(int q = 0; q < 9; ++q)
+                        acc[q] = k + t == b ? v[t][q] : acc[q] + v[t][q];
         }
 #pragma unroll
         for(int q = 0; q < 9; ++q)
@@ -494,8 +550,7 @@ void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const in
     B2S_CUDA(cudaMemsetAsync(w.row_fill.data(), 0, sizeof(int32_t) * ((size_t)nb + 1), st));
     if(T > 0)
     {
-        w.bucket_col.resize(T, 1.25);
-        w.bucket_src.resize(T, 1.25);
+        w.bucket.resize(T, 1.25);
         w.sorted_col.resize(T, 1.25);
         w.sorted_src.resize(T, 1.25);
         k_count_rows<<<asm_grid(T, ASM_BLOCK), ASM_BLOCK, 0, st>>>(rows, cols, T, nb, w.row_count.data(),
@@ -506,14 +561,14 @@ void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const in
     if(T > 0)
     {
         k_scatter_rows<<<asm_grid(T, ASM_BLOCK), ASM_BLOCK, 0, st>>>(rows, cols, T, nb, w.row_start.data(),
-                                                                     w.row_fill.data(), w.bucket_col.data(),
-                                                                     w.bucket_src.data(), w.err.data());
+                                                                     w.row_fill.data(), w.bucket.data(),
+                                                                     w.err.data());
         B2S_CHECK_LAUNCH();
     }
     if(nb > 0)
     {
         k_sort_rows<<<asm_grid((int64_t)nb * 32, ASM_BLOCK), ASM_BLOCK, 0, st>>>(
-            nb, w.row_start.data(), w.bucket_col.data(), w.bucket_src.data(), w.sorted_col.data(),
+            nb, w.row_start.data(), w.bucket.data(), w.sorted_col.data(),
             w.sorted_src.data(), w.uniq_count.data());
         B2S_CHECK_LAUNCH();
     }

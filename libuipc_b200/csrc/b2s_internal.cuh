@@ -136,7 +136,8 @@ struct Matrix
 struct AssemblyScratch
 {
     DBuf<int32_t> row_count, row_start, row_fill, uniq_count;
-    DBuf<int32_t> bucket_col, bucket_src, sorted_col, sorted_src;
+    DBuf<int2>    bucket;  // (column, source) of the kept triplets, bucketed by row
+    DBuf<int32_t> sorted_col, sorted_src;
     DBuf<int32_t> run_start;  // [U+1] sorted position of each unique block's first source
     DBuf<int32_t> scan_tmp;
     DBuf<int>     err;
