@@ -273,6 +273,17 @@ void spmv_f64(b2s_solver* s, const Matrix& A, const double* x, double* y, double
 // reductions
 int  reduction_grid();
 void launch_dot(b2s_solver* s, const double* a, const double* b, int64_t n, double* d_out);
+// several dot products in one pass: d_out[k] = a[k] . b[k], k < m (FP64,
+// deterministic)
+constexpr int MAX_DOTS = 6;
+struct DotPairs
+{
+    const double* a[MAX_DOTS];
+    const double* b[MAX_DOTS];
+};
+void launch_dots(b2s_solver* s, int64_t n, const DotPairs& d, int m, double* d_out);
+// partial-sum storage of the grid reductions for `grid` blocks x `nv` values
+void ensure_reduction(Reduction& red, int grid, int nv);
 
 // preconditioners
 void precond_assemble(b2s_solver* s, int kind, int invert_mode);

@@ -570,6 +570,64 @@ __global__ void k_ws_lincomb(int64_t n, int nc, const double* __restrict__ c0, c
     }
 }
 
+// The Galerkin matrix of the candidate starts, G_ij = c_i . A c_j (i <= j,
+// row-major upper triangle), in one pass over the stored upper blocks with no
+// product vectors: with u_k = B c_k(col), a block B at (row, col) adds
+// c_i(row) . u_j and, off the diagonal (the transposed block), u_i . c_j(row).
+// FP64, fixed grid and order: deterministic.
+struct Cands
+{
+    const double* c[4];
+};
+
+template <int K>
+__global__ void __launch_bounds__(RED_BLOCK) k_ws_gram(int64_t U, int64_t S, const int32_t* __restrict__ rows,
+                                                       const int32_t* __restrict__ cols,
+                                                       const double* __restrict__ vals, Cands cs, double* partials,
+                                                       unsigned int* counter, double* out)
+{
+    constexpr int NP = K * (K + 1) / 2;
+    double        g[NP] = {};
+    for(int64_t o = (int64_t)blockIdx.x * RED_BLOCK + threadIdx.x; o < U; o += (int64_t)gridDim.x * RED_BLOCK)
+    {
+        const int64_t r = rows[o], c = cols[o];
+        double        B[9];
+#pragma unroll
+        for(int q = 0; q < 9; ++q)
+            B[q] = vals[(int64_t)q * S + o];
+        double xr[K][3], u[K][3];
+#pragma unroll
+        for(int k = 0; k < K; ++k)
+        {
+            const double* ck = cs.c[k];
+            xr[k][0]          = ck[3 * r];
+            xr[k][1]          = ck[3 * r + 1];
+            xr[k][2]          = ck[3 * r + 2];
+            const double y0 = ck[3 * c], y1 = ck[3 * c + 1], y2 = ck[3 * c + 2];
+            // column-major: B(p, q) = B[q * 3 + p]
+            u[k][0] = B[0] * y0 + B[3] * y1 + B[6] * y2;
+            u[k][1] = B[1] * y0 + B[4] * y1 + B[7] * y2;
+            u[k][2] = B[2] * y0 + B[5] * y1 + B[8] * y2;
+        }
+        const bool off = r != c;
+        int        p   = 0;
+#pragma unroll
+        for(int i = 0; i < K; ++i)
+#pragma unroll
+            for(int j = i; j < K; ++j, ++p)
+            {
+                double d = xr[i][0] * u[j][0] + xr[i][1] * u[j][1] + xr[i][2] * u[j][2];
+                if(off)
+                    d += u[i][0] * xr[j][0] + u[i][1] * xr[j][1] + u[i][2] * xr[j][2];
+                g[p] += d;
+            }
+    }
+    double tot[NP];
+    if(grid_sum<NP>(g, partials, counter, tot))
+        for(int q = 0; q < NP; ++q)
+            out[q] = tot[q];
+}
+
 // r = b - sum_k alpha_k y_k (k < nc)
 __global__ void k_ws_residual_comb(int64_t n, int nc, const double* __restrict__ b, const double* __restrict__ y0,
                                    const double* __restrict__ y1, const double* __restrict__ y2,
@@ -634,8 +692,10 @@ int system_aggregates(b2s_solver* s, const double* b, int n_hist, const double* 
     k_ws_fields<<<ws_grid(n), WS_BLOCK, 0, st>>>(n, n_hist > 0 ? hist[0] : nullptr, n_hist > 1 ? hist[1] : nullptr,
                                                   n_hist > 2 ? hist[2] : nullptr, W.Ac.data(), W.fields.data());
     B2S_CHECK_LAUNCH();
-    launch_dot(s, W.Ac.data(), W.Ac.data(), n, W.dots.data() + 28);
-    launch_dot(s, b, b, n, W.dots.data() + 29);
+    DotPairs dp{};
+    dp.a[0] = dp.b[0] = W.Ac.data();
+    dp.a[1] = dp.b[1] = b;
+    launch_dots(s, n, dp, 2, W.dots.data() + 28);
     double h2[2];
     B2S_CUDA(cudaMemcpyAsync(h2, W.dots.data() + 28, sizeof(h2), cudaMemcpyDeviceToHost, st));
     B2S_CUDA(cudaStreamSynchronize(st));
@@ -1070,30 +1130,53 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
     bool      have = false;
     if(k > 0)
     {
-        // Galerkin: G alpha = g, G_kl = c_k . A c_l, g_k = c_k . b (FP64)
-        W.Ac.resize((size_t)4 * n + n);
+        // Galerkin: G alpha = g, G_kl = c_k . A c_l (one pass over the
+        // matrix), g_k = c_k . b and b . b (one pass over the vectors), FP64
+        W.Ac.resize((size_t)4 * n);
         W.dots.resize(32);
-        for(int i = 0; i < k; ++i)
-            spmv_f64(s, s->A, cand[i], W.Ac.data() + (size_t)i * n, nullptr);
+        const Matrix& A    = s->A;
+        const int     grid = reduction_grid();
+        ensure_reduction(s->red, grid, 10);
+        Cands cs{};
+        for(int i = 0; i < 4; ++i)
+            cs.c[i] = cand[i < k ? i : 0];
+        double* gram = W.dots.data();
+        switch(k)
+        {
+        case 1: k_ws_gram<1><<<grid, RED_BLOCK, 0, st>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(),
+                                                          A.vals.data(), cs, s->red.partials.data(),
+                                                          s->red.counter.data(), gram); break;
+        case 2: k_ws_gram<2><<<grid, RED_BLOCK, 0, st>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(),
+                                                          A.vals.data(), cs, s->red.partials.data(),
+                                                          s->red.counter.data(), gram); break;
+        case 3: k_ws_gram<3><<<grid, RED_BLOCK, 0, st>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(),
+                                                          A.vals.data(), cs, s->red.partials.data(),
+                                                          s->red.counter.data(), gram); break;
+        default: k_ws_gram<4><<<grid, RED_BLOCK, 0, st>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(),
+                                                           A.vals.data(), cs, s->red.partials.data(),
+                                                           s->red.counter.data(), gram); break;
+        }
+        B2S_CHECK_LAUNCH();
+        DotPairs dp{};
         for(int i = 0; i < k; ++i)
         {
-            for(int j = i; j < k; ++j)
-                launch_dot(s, cand[i], W.Ac.data() + (size_t)j * n, n, W.dots.data() + i * k + j);
-            launch_dot(s, cand[i], b, n, W.dots.data() + 16 + i);
+            dp.a[i] = cand[i];
+            dp.b[i] = b;
         }
-        launch_dot(s, b, b, n, W.dots.data() + 20);
+        dp.a[k] = dp.b[k] = b;
+        launch_dots(s, n, dp, k + 1, W.dots.data() + 16);
         double hd[32];
         B2S_CUDA(cudaMemcpyAsync(hd, W.dots.data(), sizeof(double) * 32, cudaMemcpyDeviceToHost, st));
         B2S_CUDA(cudaStreamSynchronize(st));
         double G[16], gv[4], alpha[4] = {0, 0, 0, 0};
-        for(int i = 0; i < k; ++i)
+        for(int i = 0, q = 0; i < k; ++i)
         {
-            for(int j = i; j < k; ++j)
-                G[i * k + j] = G[j * k + i] = hd[i * k + j];
+            for(int j = i; j < k; ++j, ++q)
+                G[i * k + j] = G[j * k + i] = hd[q];
             gv[i] = hd[16 + i];
         }
         small_pinv_solve(k, G, gv, alpha);
-        const double bb = hd[20];
+        const double bb = hd[16 + k];
         bool finite = std::isfinite(bb);
         for(int i = 0; i < k; ++i)
             finite = finite && std::isfinite(alpha[i]);
@@ -1103,13 +1186,11 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
                                                          k > 2 ? cand[2] : cand[0], k > 3 ? cand[3] : cand[0],
                                                          alpha[0], alpha[1], alpha[2], alpha[3], x0);
             B2S_CHECK_LAUNCH();
-            // FP64 residual of the candidate start, r = b - sum alpha_k (A c_k)
-            // from the products the Gram already needed
-            double* y = W.Ac.data() + (size_t)4 * n;
-            k_ws_residual_comb<<<ws_grid(n), WS_BLOCK, 0, st>>>(
-                n, k, b, W.Ac.data(), k > 1 ? W.Ac.data() + n : W.Ac.data(),
-                k > 2 ? W.Ac.data() + 2 * n : W.Ac.data(), k > 3 ? W.Ac.data() + 3 * n : W.Ac.data(), alpha[0],
-                alpha[1], alpha[2], alpha[3], y);
+            // FP64 residual of the candidate start, r = b - A x0
+            double* Ax = W.Ac.data();
+            double* y  = W.Ac.data() + (size_t)n;
+            spmv_f64(s, A, x0, Ax, nullptr);
+            k_ws_residual_comb<<<ws_grid(n), WS_BLOCK, 0, st>>>(n, 1, b, Ax, Ax, Ax, Ax, 1.0, 0.0, 0.0, 0.0, y);
             B2S_CHECK_LAUNCH();
             out.n_candidates = k;
             for(int i = 0; i < k; ++i)
@@ -1117,17 +1198,22 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
             // the judge is the PCG's own residual measure, r^T P r (the
             // quantity the reference's stop rule |r.z| <= tol |r0.z0| tracks):
             // accept the start when it is below b^T P b of the zero start
-            double*       zr = W.Ac.data();
+            double*       zr = W.Ac.data() + 2 * (size_t)n;
             const double* zb = W.fields.data() + 3 * (size_t)n;  // P b of the features
             precond_launch(s, y, zr);
             if(mode != B2S_WS_MODE_LEARNED)
             {
-                precond_launch(s, b, W.Ac.data() + (size_t)n);
-                zb = W.Ac.data() + (size_t)n;
+                precond_launch(s, b, W.Ac.data() + 3 * (size_t)n);
+                zb = W.Ac.data() + 3 * (size_t)n;
             }
-            launch_dot(s, y, y, n, W.dots.data() + 24);
-            launch_dot(s, y, zr, n, W.dots.data() + 25);
-            launch_dot(s, b, zb, n, W.dots.data() + 26);
+            DotPairs dc{};
+            dc.a[0] = y;
+            dc.b[0] = y;
+            dc.a[1] = y;
+            dc.b[1] = zr;
+            dc.a[2] = b;
+            dc.b[2] = zb;
+            launch_dots(s, n, dc, 3, W.dots.data() + 24);
             double h3[3];
             B2S_CUDA(cudaMemcpyAsync(h3, W.dots.data() + 24, sizeof(h3), cudaMemcpyDeviceToHost, st));
             B2S_CUDA(cudaStreamSynchronize(st));

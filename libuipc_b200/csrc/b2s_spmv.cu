@@ -525,7 +525,33 @@ __global__ void __launch_bounds__(RED_BLOCK) k_dot(const double* __restrict__ a,
     if(grid_sum<1>(v, partials, counter, tot))
         *out = tot[0];
 }
+
+// m <= MAX_DOTS dot products of n-vectors in one pass (repeated vectors are
+// read once from DRAM, the rest from cache); out[k] = a_k . b_k
+__global__ void __launch_bounds__(RED_BLOCK) k_multi_dot(int64_t n, int m, DotPairs d, double* partials,
+                                                         unsigned int* counter, double* out)
+{
+    double acc[MAX_DOTS] = {};
+    for(int64_t i = (int64_t)blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_BLOCK)
+#pragma unroll
+        for(int k = 0; k < MAX_DOTS; ++k)
+            if(k < m)
+                acc[k] += d.a[k][i] * d.b[k][i];
+    double tot[MAX_DOTS];
+    if(grid_sum<MAX_DOTS>(acc, partials, counter, tot))
+        for(int k = 0; k < m; ++k)
+            out[k] = tot[k];
+}
 }  // namespace
+
+void launch_dots(b2s_solver* s, int64_t n, const DotPairs& d, int m, double* d_out)
+{
+    B2S_REQUIRE(m >= 1 && m <= MAX_DOTS, B2S_ERR_ARGUMENT, "launch_dots: 1 to MAX_DOTS products");
+    const int grid = reduction_grid();
+    ensure_reduction(s->red, grid, MAX_DOTS);
+    k_multi_dot<<<grid, RED_BLOCK, 0, s->stream>>>(n, m, d, s->red.partials.data(), s->red.counter.data(), d_out);
+    B2S_CHECK_LAUNCH();
+}
 
 // blocks of the grid-stride reductions and of the preconditioner collect (8
 // per SM; 16 measured slower: the last block's in-order sum of the partials
