@@ -63,6 +63,22 @@ def load_scene_lib() -> C.CDLL:
         for fn in ("b2g_tets", "b2g_triplet_rows", "b2g_triplet_cols", "b2g_adjacency_start", "b2g_adjacency_list"):
             getattr(lib, fn).argtypes = [vp]
             getattr(lib, fn).restype = c_i32_p
+        # Matrix Market I/O (csrc/scene/matrix_market.h)
+        i32, i64, pi32, pi64 = C.c_int32, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64)
+        lib.b2io_write_block_matrix.argtypes = [C.c_char_p, i32, i64, vp, vp, vp, C.c_int]
+        lib.b2io_write_block_matrix.restype = C.c_int
+        lib.b2io_write_vector.argtypes = [C.c_char_p, i64, vp]
+        lib.b2io_write_vector.restype = C.c_int
+        lib.b2io_read_block_matrix.argtypes = [C.c_char_p, C.c_int, C.POINTER(vp)]
+        lib.b2io_read_block_matrix.restype = C.c_int
+        lib.b2io_matrix_size.argtypes = [vp, pi32, pi64, pi64]
+        lib.b2io_matrix_size.restype = C.c_int
+        lib.b2io_matrix_copy.argtypes = [vp, vp, vp, vp]
+        lib.b2io_matrix_copy.restype = C.c_int
+        lib.b2io_matrix_free.argtypes = [vp]
+        lib.b2io_matrix_free.restype = None
+        lib.b2io_read_vector.argtypes = [C.c_char_p, i64, vp, pi64]
+        lib.b2io_read_vector.restype = C.c_int
         _scene = lib
         return lib
 

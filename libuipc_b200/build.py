@@ -97,13 +97,14 @@ def build_solve(force: bool = False, extra_flags: list[str] | None = None) -> st
 def build_scene(force: bool = False) -> str:
     os.makedirs(LIB, exist_ok=True)
     out = os.path.join(LIB, "libb200scene.so")
-    src = os.path.join(CSRC, "scene", "scene_gen.cpp")
+    srcs = [os.path.join(CSRC, "scene", f) for f in ("scene_gen.cpp", "matrix_market.cpp")]
+    hdrs = [os.path.join(CSRC, "scene", f) for f in ("scene_gen.h", "matrix_market.h")]
     flags = ["-O3", "-fopenmp", "-shared", "-fPIC", "-std=c++17"]
     stamp = out + ".stamp"
-    dig = _digest([src, os.path.join(CSRC, "scene", "scene_gen.h")], " ".join(flags))
+    dig = _digest(srcs + hdrs, " ".join(flags))
     if not force and os.path.exists(out) and os.path.exists(stamp) and open(stamp).read() == dig:
         return out
-    _run(["g++", *flags, src, "-o", out])
+    _run(["g++", *flags, *srcs, "-o", out])
     with open(stamp, "w") as f:
         f.write(dig)
     return out

@@ -16,6 +16,7 @@ tensors; PyTorch is only the allocator here.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -453,21 +454,49 @@ class GlobalLinearSystem:
     triplets, build the preconditioner, solve A x = b, dx = -x."""
 
     def __init__(self, solver: Solver, iterative_solver: IterativeSolver,
-                 preconditioner: GlobalPreconditioner | None = None):
+                 preconditioner: GlobalPreconditioner | None = None, dump_folder: str | None = None):
+        """``dump_folder``: when set, every solve writes its assembled A and b
+        before, and x after, as Matrix Market files named like the reference's
+        debug dump (GlobalLinearSystem::_dump_A_b / _dump_x,
+        global_linear_system.cu:44-70, enabled there by the scene setting
+        ``extras/debug/dump_linear_system``; see :func:`dump_folder_from_config`)."""
         self.solver = solver
         self.iterative_solver = iterative_solver
         self.preconditioner = preconditioner or B200Jacobi()
+        self.dump_folder = dump_folder
         self.last_solve_iterations = 0
 
     def build_linear_system(self, n_block_rows, rows, cols, vals):
         self.solver.assemble(n_block_rows, rows, cols, vals)
         self.preconditioner.do_assemble(self)
 
-    def solve(self, n_block_rows, rows, cols, vals, b, history_slot: int = 0):
+    def solve(self, n_block_rows, rows, cols, vals, b, history_slot: int = 0, frame: int = 0,
+              newton_iter: int = 0):
         torch = _torch()
         self.build_linear_system(n_block_rows, rows, cols, vals)
+        names = None
+        if self.dump_folder:
+            from . import matrix_market as mm
+
+            os.makedirs(self.dump_folder, exist_ok=True)
+            names = mm.dump_names(self.dump_folder, frame, newton_iter)
+            mm.export_assembled(self.solver, names[0])
+            mm.export_vector_market(names[1], b.detach().cpu().numpy())
         x = torch.zeros_like(b)
         info = SolvingInfo(x=x, b=b, history_slot=history_slot)
         self.iterative_solver.do_solve(self, info)
         self.last_solve_iterations = info.iter_count
+        if names:
+            from . import matrix_market as mm
+
+            mm.export_vector_market(names[2], x.detach().cpu().numpy())
         return -x  # distribute_solution: dx = -x
+
+
+def dump_folder_from_config(config: dict | None, workspace: str) -> str | None:
+    """The folder of the debug dump when the scene setting
+    ``extras/debug/dump_linear_system`` is non-zero (GlobalLinearSystem::do_build,
+    global_linear_system.cu:34-40), else None."""
+    if int((config or {}).get("extras/debug/dump_linear_system", 0)):
+        return os.path.join(workspace, "debug")
+    return None
