@@ -1,4 +1,5 @@
-/* Matrix Market I/O of block-sparse Newton systems (host side, C ABI).
+/* b200io: Matrix Market I/O of block-sparse Newton systems (host side, C ABI,
+ * exported by libb200scene.so).
  *
  * The format is the one libuipc's debug dump writes and reads
  * (src/backends/cuda/utils/matrix_market.h:35-116 export_matrix_market,

@@ -150,10 +150,10 @@ def declare(lib: C.CDLL) -> None:
         fn.argtypes = args
 
 
-def header_symbols(header_path: str) -> list[str]:
-    """Function names declared in a C header (for the export check)."""
+def header_symbols(header_path: str, prefix: str = "b2s_") -> list[str]:
+    """Function names with `prefix` declared in a C header (for the export check)."""
     import re
 
     text = open(header_path).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(b2s_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(" + prefix + r"[a-z0-9_]+)\s*\(", text)))

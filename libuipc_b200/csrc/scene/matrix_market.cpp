@@ -1,7 +1,7 @@
 // Matrix Market I/O of block-sparse Newton systems; format and semantics in
-// matrix_market.h. The text is formatted by OpenMP threads into per-chunk
+// include/b200io.h. The text is formatted by OpenMP threads into per-chunk
 // buffers written in order, so a 4 M-block matrix (38 M lines) takes seconds.
-#include "matrix_market.h"
+#include "../../../include/b200io.h"
 
 #include <omp.h>
 

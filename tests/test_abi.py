@@ -28,6 +28,18 @@ def test_library_exports_every_header_symbol():
     assert set(declared) <= exported
 
 
+def test_io_library_exports_every_header_symbol():
+    """include/b200io.h (Matrix Market I/O) is exported by libb200scene.so."""
+    from libuipc_b200 import _abi
+
+    declared = _abi.header_symbols(os.path.join(ROOT, "include", "b200io.h"), prefix="b2io_")
+    assert len(declared) == 7
+    lib = os.path.join(ROOT, "libuipc_b200", "_lib", "libb200scene.so")
+    out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l}
+    assert set(declared) <= exported
+
+
 def test_library_is_built_for_sm100a():
     out = subprocess.run(["cuobjdump", "--list-elf", LIB], capture_output=True, text=True).stdout
     assert "sm_100a" in out
