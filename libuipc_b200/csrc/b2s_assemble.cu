@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32
                                                          const int2* __restrict__ bucket,
                                                          int32_t* __restrict__ sorted_col,
                                                          int32_t* __restrict__ sorted_src,
-                                                         int32_t* __restrict__ uniq_count)
+                                                         int32_t* __restrict__ uniq_count, int32_t* long_rows)
 {
     __shared__ int32_t s_col[ASM_BLOCK / 32][ROW_CAP];
     __shared__ int32_t s_src[ASM_BLOCK / 32][ROW_CAP];
@@ -372,30 +372,96 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_sort_rows(int32_t nb, const int32
         }
         else
         {
-            // long row: same ranking straight from global memory
-            for(int k = lane; k < L; k += 32)
-            {
-                const int2    me = bucket[beg + k];
-                const int32_t c = me.x, sr = me.y;
-                int rank = 0, head = 1;
-                for(int q = 0; q < L; ++q)
-                {
-                    const int2    o  = bucket[beg + q];
-                    const int32_t cq = o.x, sq = o.y;
-                    rank += key_less(cq, sq, c, sr) ? 1 : 0;
-                    if(cq == c && sq < sr)
-                        head = 0;
-                }
-                sorted_col[beg + rank] = c;
-                sorted_src[beg + rank] = sr;
-                uniq += head;
-            }
+            // longer than a warp's shared memory: sorted by k_sort_long_rows
+            if(lane == 0)
+                long_rows[1 + atomicAdd(long_rows, 1)] = (int32_t)r;
+            continue;
         }
 #pragma unroll
         for(int o = 16; o > 0; o >>= 1)
             uniq += __shfl_xor_sync(0xffffffffu, uniq, o);
         if(lane == 0)
             uniq_count[r] = uniq;
+    }
+}
+
+// Rows longer than ROW_CAP pairs (e.g. an affine body touched by thousands of
+// cloth vertices), listed by k_sort_rows: one CTA per row (persistent over the
+// list). Every key (column << 32 | source; unique) gets its rank by counting
+// the smaller keys, tile by tile through shared memory; a key is the head of
+// its column's run when no key has its column and a smaller source. O(L^2 / T)
+// work per row with T threads.
+constexpr int LONG_THREADS = 1024;
+constexpr int LONG_TILE    = 4096;
+
+__global__ void __launch_bounds__(LONG_THREADS) k_sort_long_rows(const int32_t* __restrict__ long_rows,
+                                                                 const int32_t* __restrict__ row_start,
+                                                                 const int2* __restrict__ bucket,
+                                                                 int32_t* __restrict__ sorted_col,
+                                                                 int32_t* __restrict__ sorted_src,
+                                                                 int32_t* __restrict__ uniq_count)
+{
+    __shared__ uint64_t s_key[LONG_TILE];
+    __shared__ int      s_heads[LONG_THREADS / 32];
+    const int n_long = long_rows[0];
+    for(int e = blockIdx.x; e < n_long; e += gridDim.x)
+    {
+        const int32_t r = long_rows[1 + e], beg = row_start[r], L = row_start[r + 1] - beg;
+        int           heads = 0;
+        for(int base = 0; base < L; base += LONG_THREADS)
+        {
+            const int      i    = base + (int)threadIdx.x;
+            uint64_t       me   = ~0ull;
+            if(i < L)
+            {
+                const int2 q = bucket[beg + i];
+                me           = ((uint64_t)(uint32_t)q.x << 32) | (uint64_t)(uint32_t)q.y;
+            }
+            const uint32_t col  = (uint32_t)(me >> 32);
+            int            rank = 0;
+            bool           head = true;
+            for(int t0 = 0; t0 < L; t0 += LONG_TILE)
+            {
+                const int n = min(LONG_TILE, L - t0);
+                __syncthreads();  // the previous tile is read
+                for(int k = threadIdx.x; k < n; k += LONG_THREADS)
+                {
+                    const int2 q = bucket[beg + t0 + k];
+                    s_key[k]     = ((uint64_t)(uint32_t)q.x << 32) | (uint64_t)(uint32_t)q.y;
+                }
+                __syncthreads();
+                if(i < L)
+                    for(int k = 0; k < n; ++k)
+                    {
+                        const uint64_t o = s_key[k];
+                        rank += o < me ? 1 : 0;
+                        head = head && !((uint32_t)(o >> 32) == col && o < me);
+                    }
+            }
+            if(i < L)
+            {
+                sorted_col[beg + rank] = (int32_t)col;
+                sorted_src[beg + rank] = (int32_t)(me & 0xFFFFFFFFull);
+                heads += head ? 1 : 0;
+            }
+        }
+        // the row's number of distinct columns
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            heads += __shfl_xor_sync(0xffffffffu, heads, o);
+        if((threadIdx.x & 31) == 0)
+            s_heads[threadIdx.x >> 5] = heads;
+        __syncthreads();
+        if(threadIdx.x < 32)
+        {
+            int h = s_heads[threadIdx.x];
+#pragma unroll
+            for(int o = 16; o > 0; o >>= 1)
+                h += __shfl_xor_sync(0xffffffffu, h, o);
+            if(threadIdx.x == 0)
+                uniq_count[r] = h;
+        }
+        __syncthreads();  // s_heads and s_key are free for the next row
     }
 }
 
@@ -567,9 +633,16 @@ void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const in
     }
     if(nb > 0)
     {
+        w.long_rows.resize((size_t)nb + 1, 1.25);
+        B2S_CUDA(cudaMemsetAsync(w.long_rows.data(), 0, sizeof(int32_t), st));
         k_sort_rows<<<asm_grid((int64_t)nb * 32, ASM_BLOCK), ASM_BLOCK, 0, st>>>(
             nb, w.row_start.data(), w.bucket.data(), w.sorted_col.data(),
-            w.sorted_src.data(), w.uniq_count.data());
+            w.sorted_src.data(), w.uniq_count.data(), w.long_rows.data());
+        B2S_CHECK_LAUNCH();
+        // the long rows (count in long_rows[0], read on the device)
+        k_sort_long_rows<<<NUM_SMS_HINT * 2, LONG_THREADS, 0, st>>>(w.long_rows.data(), w.row_start.data(),
+                                                                    w.bucket.data(), w.sorted_col.data(),
+                                                                    w.sorted_src.data(), w.uniq_count.data());
         B2S_CHECK_LAUNCH();
     }
     exclusive_scan(s, w.uniq_count.data(), M.rowptr.data(), nb, w.scan_tmp);

@@ -139,6 +139,7 @@ struct AssemblyScratch
     DBuf<int2>    bucket;  // (column, source) of the kept triplets, bucketed by row
     DBuf<int32_t> sorted_col, sorted_src;
     DBuf<int32_t> run_start;  // [U+1] sorted position of each unique block's first source
+    DBuf<int32_t> long_rows;  // [1 + nb]: count, then the rows too long for one warp
     DBuf<int32_t> scan_tmp;
     DBuf<int>     err;
 };

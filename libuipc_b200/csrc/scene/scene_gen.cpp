@@ -234,6 +234,11 @@ void b2g_default_config(b2g_config* c)
     c->body_kappa    = 1e8;
     c->bend_k        = 1e-2;
     c->cloth_size    = 2.0;
+    c->wall_gap      = 0.02;
+    c->cloth_n       = 64;
+    c->bodies_x      = 4;
+    c->bodies_z      = 8;
+    c->cloth_k       = 1e3;
 }
 
 const char* b2g_last_error(void) { return g_err.c_str(); }
@@ -258,6 +263,60 @@ namespace
 //    barrier b(d^2) along +y, coupling the vertex with the body's 12 DoF
 //    (rank-1 Hessian over 5 block rows: 15 triplets, 4 vertex-body blocks);
 //  * potentials scaled by dt^2, gravity -y.
+// The 16 blocks of affine body b (block rows 4b .. 4b+3; lower blocks as
+// zero blocks): mass matrix m_b I on p, I_b I on each column of A, plus the
+// orthogonality potential's Hessian 8 kappa V |sym(R^T dA)|^2 at A = R (R a
+// rotation about +y by theta), scaled by dt^2; and its gravity gradient.
+void add_affine_body(Builder& B, std::vector<double>& grad, int64_t b, double theta, double m_b, double I_b,
+                     double V, const b2g_config& C)
+{
+    const double dt2 = C.dt * C.dt;
+    double       H[12][12] = {};
+    for(int a = 0; a < 3; ++a)
+    {
+        H[a][a] = m_b;
+        for(int k = 0; k < 3; ++k)
+            H[3 + 3 * k + a][3 + 3 * k + a] = I_b;
+    }
+    const double cs = std::cos(theta), sn = std::sin(theta);
+    const double R[3][3] = {{cs, 0, sn}, {0, 1, 0}, {-sn, 0, cs}};
+    // q index 3 + 3 k + r <-> A[r][k]; S_m = sym(R^T E_m)
+    double S[9][3][3];
+    for(int m = 0; m < 9; ++m)
+    {
+        const int k = m / 3, r = m % 3;  // E_m has a 1 at (r, k)
+        double RtE[3][3];
+        for(int i = 0; i < 3; ++i)
+            for(int j = 0; j < 3; ++j)
+                RtE[i][j] = (j == k) ? R[r][i] : 0.0;
+        for(int i = 0; i < 3; ++i)
+            for(int j = 0; j < 3; ++j)
+                S[m][i][j] = 0.5 * (RtE[i][j] + RtE[j][i]);
+    }
+    const double ko = dt2 * 8.0 * C.body_kappa * V;
+    for(int m = 0; m < 9; ++m)
+        for(int n = 0; n < 9; ++n)
+        {
+            double d = 0.0;
+            for(int i = 0; i < 3; ++i)
+                for(int j = 0; j < 3; ++j)
+                    d += S[m][i][j] * S[n][i][j];
+            H[3 + m][3 + n] += ko * d;
+        }
+    // kinetic gradient: m (x - x_tilde) with x_tilde = x - dt^2 g on p
+    grad[(4 * b) * 3 + 1] += m_b * dt2 * C.gravity;
+    for(int bi = 0; bi < 4; ++bi)
+        for(int bj = 0; bj < 4; ++bj)
+        {
+            const int32_t r = (int32_t)(4 * b + bi), c = (int32_t)(4 * b + bj);
+            B.rows.push_back(r);
+            B.cols.push_back(c);
+            for(int q = 0; q < 3; ++q)
+                for(int p = 0; p < 3; ++p)
+                    B.vals.push_back(bi > bj ? 0.0 : H[3 * bi + p][3 * bj + q]);
+        }
+}
+
 void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
 {
     const int N = C.cells_x, nbs = C.n_cubes;
@@ -308,52 +367,7 @@ void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
     };
     // ---- affine bodies ----
     for(int64_t b = 0; b < nbod; ++b)
-    {
-        double H[12][12] = {};
-        for(int a = 0; a < 3; ++a)
-        {
-            H[a][a] = m_b;
-            for(int k = 0; k < 3; ++k)
-                H[3 + 3 * k + a][3 + 3 * k + a] = I_b;
-        }
-        const double cs = std::cos(theta[b]), sn = std::sin(theta[b]);
-        const double R[3][3] = {{cs, 0, sn}, {0, 1, 0}, {-sn, 0, cs}};
-        // q index 3 + 3 k + r <-> A[r][k]; S_m = sym(R^T E_m)
-        double S[9][3][3];
-        for(int m = 0; m < 9; ++m)
-        {
-            const int k = m / 3, r = m % 3;  // E_m has a 1 at (r, k)
-            double RtE[3][3];
-            for(int i = 0; i < 3; ++i)
-                for(int j = 0; j < 3; ++j)
-                    RtE[i][j] = (j == k) ? R[r][i] : 0.0;
-            for(int i = 0; i < 3; ++i)
-                for(int j = 0; j < 3; ++j)
-                    S[m][i][j] = 0.5 * (RtE[i][j] + RtE[j][i]);
-        }
-        const double ko = dt2 * 8.0 * C.body_kappa * V;
-        for(int m = 0; m < 9; ++m)
-            for(int n = 0; n < 9; ++n)
-            {
-                double d = 0.0;
-                for(int i = 0; i < 3; ++i)
-                    for(int j = 0; j < 3; ++j)
-                        d += S[m][i][j] * S[n][i][j];
-                H[3 + m][3 + n] += ko * d;
-            }
-        // kinetic gradient: m (x - x_tilde) with x_tilde = x - dt^2 g on p
-        sys->grad[(4 * b) * 3 + 1] += m_b * dt2 * C.gravity;
-        for(int bi = 0; bi < 4; ++bi)
-            for(int bj = 0; bj < 4; ++bj)
-            {
-                const int32_t r = (int32_t)(4 * b + bi), c = (int32_t)(4 * b + bj);
-                B.rows.push_back(r);
-                B.cols.push_back(c);
-                for(int q = 0; q < 3; ++q)
-                    for(int p = 0; p < 3; ++p)
-                        B.vals.push_back(bi > bj ? 0.0 : H[3 * bi + p][3 * bj + q]);
-            }
-    }
+        add_affine_body(B, sys->grad, b, theta[b], m_b, I_b, V, C);
     // ---- cloth ----
     const int32_t c0 = (int32_t)(4 * nbod);
     for(int64_t v = 0; v < ncv; ++v)
@@ -480,36 +494,27 @@ void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
 
 // x_in / xt_in (optional, [n_verts*3]): current positions and kinetic target
 // x_tilde; null = the scene's default first Newton step from rest
-int generate_impl(const b2g_config* cfg, const double* x_in, const double* xt_in, b2g_system** out)
+// Tet cubes (scene 1: stacked along +y; scene 2: one twisted bar; scene 4:
+// a W x W grid in the x-z plane on the ground, W = n_cubes, cubes wall_gap
+// apart so they do not touch each other), the first Newton step from rest or
+// the step at a given state.
+void generate_tets(const b2g_config& C, const double* x_in, const double* xt_in, b2g_system* sys)
 {
-    try
     {
-        if(!cfg || !out)
-            throw std::runtime_error("null argument");
-        const b2g_config C = *cfg;
-        if(C.scene == 3)
-        {
-            if(x_in || xt_in)
-                throw std::runtime_error("scene 3 has no state input");
-            auto sys = std::make_unique<b2g_system>();
-            generate_cloth_abd(C, sys.get());
-            *out = sys.release();
-            return 0;
-        }
         if(C.cells_x < 1 || C.cells_y < 1 || C.cells_z < 1 || C.n_cubes < 1 || C.h <= 0 || C.dt <= 0)
             throw std::runtime_error("invalid configuration sizes");
-        if(C.scene != 1 && C.scene != 2)
+        if(C.scene != 1 && C.scene != 2 && C.scene != 4)
             throw std::runtime_error("unknown scene id");
 #ifdef _OPENMP
         if(C.n_threads > 0)
             omp_set_num_threads(C.n_threads);
 #endif
-        auto sys = std::make_unique<b2g_system>();
+        const bool grid = C.scene == 4;
         const int nx = C.cells_x, ny = C.cells_y, nz = C.cells_z;
         const int64_t vx = nx + 1, vy = ny + 1, vz = nz + 1;
         const int64_t verts_per = vx * vy * vz;
         const int64_t tets_per  = 6ll * nx * ny * nz;
-        const int n_cubes       = (C.scene == 1) ? C.n_cubes : 1;
+        const int n_cubes       = (C.scene == 1) ? C.n_cubes : grid ? C.n_cubes * C.n_cubes : 1;
         const int64_t nv        = verts_per * n_cubes;
         const int64_t nt        = tets_per * n_cubes;
         if(nv > (int64_t)INT32_MAX / 3)
@@ -521,27 +526,35 @@ int generate_impl(const b2g_config* cfg, const double* x_in, const double* xt_in
         // ---- vertices (rest shape = jittered grid) ----
         sys->x_rest.resize(nv * 3);
         const double cube_pitch = ny * C.h + C.gap;
+        const double grid_pitch_x = nx * C.h + C.wall_gap, grid_pitch_z = nz * C.h + C.wall_gap;
 #pragma omp parallel for schedule(static)
         for(int64_t g = 0; g < nv; ++g)
         {
             int64_t c = g / verts_per, l = g % verts_per;
             int64_t i = l % vx, j = (l / vx) % vy, k = l / (vx * vy);
             double  px = i * C.h, py = j * C.h + c * cube_pitch, pz = k * C.h;
+            if(grid)
+            {
+                px += (c % C.n_cubes) * grid_pitch_x;
+                py = j * C.h;
+                pz += (c / C.n_cubes) * grid_pitch_z;
+            }
             double  jx = urand(C.seed, 0, g) * C.jitter * C.h;
             double  jy = urand(C.seed, 1, g) * C.jitter * C.h;
             double  jz = urand(C.seed, 2, g) * C.jitter * C.h;
             bool    x_face = (i == 0 || i == nx), z_face = (k == 0 || k == nz);
             bool    y_face = (j == 0 || j == ny);
-            if(C.scene == 1)
+            if(C.scene == 1 || grid)
             {
                 // keep the outer faces planar in their normal direction; the
-                // contact faces (y) get a bounded normal jitter instead
+                // contact faces (y) get a bounded normal jitter instead (the
+                // grid's top faces, under the cloth, stay planar)
                 if(x_face)
                     jx = 0.0;
                 if(z_face)
                     jz = 0.0;
                 if(y_face)
-                    jy = urand(C.seed, 3, g) * C.normal_jitter;
+                    jy = (grid && j == ny) ? 0.0 : urand(C.seed, 3, g) * C.normal_jitter;
             }
             else
             {
@@ -665,6 +678,22 @@ int generate_impl(const b2g_config* cfg, const double* x_in, const double* xt_in
         std::vector<Pair> pairs;
         std::vector<std::pair<int32_t, double>> ground;  // vertex, distance
         double ground_y = 0.0;
+        if(grid)
+        {
+            // every cube's bottom layer on the ground
+            double miny = 1e300;
+            for(int64_t g = 0; g < nv; ++g)
+                if(((g % verts_per) / vx) % vy == 0)
+                    miny = std::min(miny, sys->x_rest[g * 3 + 1]);
+            ground_y = miny - C.ground_offset;
+            for(int64_t g = 0; g < nv; ++g)
+                if(((g % verts_per) / vx) % vy == 0)
+                {
+                    const double d = sys->x[g * 3 + 1] - ground_y;
+                    if(d < C.dhat)
+                        ground.push_back({(int32_t)g, d});
+                }
+        }
         if(C.scene == 1)
         {
             double miny = 1e300;
@@ -1035,6 +1064,307 @@ int generate_impl(const b2g_config* cfg, const double* x_in, const double* xt_in
                 std::copy(nb[v].begin(), nb[v].end(), sys->adj_list.begin() + sys->adj_start[v]);
         }
 
+    }
+}
+
+// Scene 4 (the full-scale case): a W x W grid of tet cubes on the ground
+// (generate_tets, W = n_cubes), an N x N cloth (N = cloth_n) resting on their
+// top faces, and bodies_x x bodies_z affine bodies resting on the cloth;
+// first Newton step from rest.
+//  * cloth: as scene 3 (lumped mass, membrane and bending springs), covering
+//    the grid, 0.5 dhat above the (planar) top faces;
+//  * cloth-cube contact: each cloth vertex over a top-face triangle at
+//    distance 0 < d < dhat: point-triangle barrier b(d^2), D = (a . x)^2 with
+//    a = (n, -w0 n, -w1 n, -w2 n) over the vertex and the triangle's corners
+//    (10 triplets);
+//  * cloth-body contact: each cloth vertex under a body's bottom face at
+//    0 < d < dhat: barrier along -y coupling the vertex with the body's 12 DoF
+//    (15 triplets);
+//  * DoF order: bodies (4 block rows each), cube vertices, cloth vertices; the
+//    neighbour graph holds the tet edges and the cloth triangle edges.
+void generate_wall(const b2g_config& C, b2g_system* sys)
+{
+    const int W = C.n_cubes, N = C.cloth_n, nbx = C.bodies_x, nbz = C.bodies_z;
+    if(N < 2 || nbx < 0 || nbz < 0 || W < 1)
+        throw std::runtime_error("scene 4 needs n_cubes >= 1, cloth_n >= 2, bodies_x/z >= 0");
+    b2g_config Cc = C;
+    Cc.scene      = 4;
+    b2g_system cubes;
+    generate_tets(Cc, nullptr, nullptr, &cubes);
+    const int     nx = C.cells_x, ny = C.cells_y, nz = C.cells_z;
+    const int64_t vx = nx + 1, vy = ny + 1, vz = nz + 1, verts_per = vx * vy * vz;
+    const int64_t nbod = (int64_t)nbx * nbz, ncube_v = (int64_t)cubes.x.size() / 3, ncv = (int64_t)N * N;
+    const int64_t off_c = 4 * nbod, off_cl = off_c + ncube_v, rows = off_cl + ncv;
+    if(rows > (int64_t)INT32_MAX / 3)
+        throw std::runtime_error("system too large for 32-bit DoF indices");
+    const double px_pitch = nx * C.h + C.wall_gap, pz_pitch = nz * C.h + C.wall_gap;
+    const double Lx = W * px_pitch - C.wall_gap, Lz = W * pz_pitch - C.wall_gap;
+    const double top = ny * C.h, hc = Lx / (N - 1), hcz = Lz / (N - 1);
+    const double y_cloth = top + 0.5 * C.dhat, dt2 = C.dt * C.dt, Dh = C.dhat * C.dhat;
+    const double m_v = C.rho * 1e-3 * hc * hcz;
+    const double bpx = nbx > 0 ? Lx / nbx : 1.0, bpz = nbz > 0 ? Lz / nbz : 1.0;
+    const double s = 0.6 * std::min(bpx, bpz), m_b = C.rho * s * s * s, I_b = m_b * s * s / 12.0, V = s * s * s;
+    sys->n_bodies = nbod;
+    sys->x.assign(rows * 3, 0.0);
+    sys->grad.assign(rows * 3, 0.0);
+    std::vector<double> theta(nbod);
+    for(int64_t b = 0; b < nbod; ++b)
+    {
+        const int64_t i = b % nbx, k = b / nbx;
+        const double  c[3] = {(i + 0.5) * bpx, y_cloth + 0.5 * C.dhat + 0.5 * s, (k + 0.5) * bpz};
+        theta[b]           = urand(C.seed, 4, b) * (M_PI / 4);
+        for(int r = 0; r < 4; ++r)
+            for(int a = 0; a < 3; ++a)
+                sys->x[(4 * b + r) * 3 + a] = c[a];
+    }
+    std::copy(cubes.x.begin(), cubes.x.end(), sys->x.begin() + off_c * 3);
+    std::copy(cubes.grad.begin(), cubes.grad.end(), sys->grad.begin() + off_c * 3);
+    for(int64_t v = 0; v < ncv; ++v)
+    {
+        const int64_t g = off_cl + v;
+        sys->x[g * 3 + 0] = (v % N) * hc;
+        sys->x[g * 3 + 1] = y_cloth;
+        sys->x[g * 3 + 2] = (v / N) * hcz;
+    }
+    sys->x_rest = sys->x;
+
+    Builder B;
+    B.reserve((size_t)nbod * 16 + cubes.rows.size() + (size_t)ncv * 30);
+    auto put = [&](int32_t r, int32_t c, const double* Hrc /*row-major 3x3 of block (r,c)*/)
+    {
+        const bool tp = r > c;
+        B.rows.push_back(tp ? c : r);
+        B.cols.push_back(tp ? r : c);
+        for(int q = 0; q < 3; ++q)
+            for(int p = 0; p < 3; ++p)
+                B.vals.push_back(tp ? Hrc[q * 3 + p] : Hrc[p * 3 + q]);  // column-major
+    };
+    // ---- bodies, cubes ----
+    for(int64_t b = 0; b < nbod; ++b)
+        add_affine_body(B, sys->grad, b, theta[b], m_b, I_b, V, C);
+    for(size_t t = 0; t < cubes.rows.size(); ++t)
+    {
+        B.rows.push_back(cubes.rows[t] + (int32_t)off_c);
+        B.cols.push_back(cubes.cols[t] + (int32_t)off_c);
+    }
+    B.vals.insert(B.vals.end(), cubes.vals.begin(), cubes.vals.end());
+    // ---- cloth ----
+    std::vector<std::vector<int32_t>> nb(ncv);
+    auto cg = [&](int64_t i, int64_t k) { return (int32_t)(off_cl + i + (int64_t)N * k); };
+    for(int64_t v = 0; v < ncv; ++v)
+    {
+        const double Hm[9] = {m_v, 0, 0, 0, m_v, 0, 0, 0, m_v};
+        put((int32_t)(off_cl + v), (int32_t)(off_cl + v), Hm);
+        sys->grad[(off_cl + v) * 3 + 1] += m_v * dt2 * C.gravity;
+    }
+    auto spring = [&](int32_t ga, int32_t gb, double k)
+    {
+        double d[3], l = 0.0;
+        for(int a = 0; a < 3; ++a)
+        {
+            d[a] = sys->x[gb * 3 + a] - sys->x[ga * 3 + a];
+            l += d[a] * d[a];
+        }
+        double H[9], Hn[9];
+        for(int p = 0; p < 3; ++p)
+            for(int q = 0; q < 3; ++q)
+            {
+                H[p * 3 + q]  = dt2 * k * d[p] * d[q] / l;
+                Hn[p * 3 + q] = -H[p * 3 + q];
+            }
+        put(ga, ga, H);
+        put(gb, gb, H);
+        put(ga, gb, Hn);
+    };
+    auto link = [&](int32_t ga, int32_t gb)
+    {
+        nb[ga - off_cl].push_back(gb);
+        nb[gb - off_cl].push_back(ga);
+    };
+    for(int64_t k = 0; k < N; ++k)
+        for(int64_t i = 0; i < N; ++i)
+        {
+            if(i + 1 < N)
+            {
+                spring(cg(i, k), cg(i + 1, k), C.cloth_k);
+                link(cg(i, k), cg(i + 1, k));
+            }
+            if(k + 1 < N)
+            {
+                spring(cg(i, k), cg(i, k + 1), C.cloth_k);
+                link(cg(i, k), cg(i, k + 1));
+            }
+            if(i + 1 < N && k + 1 < N)
+            {
+                spring(cg(i, k), cg(i + 1, k + 1), C.cloth_k);
+                link(cg(i, k), cg(i + 1, k + 1));
+            }
+            if(i + 2 < N)
+                spring(cg(i, k), cg(i + 2, k), C.bend_k / (hc * hc));
+            if(k + 2 < N)
+                spring(cg(i, k), cg(i, k + 2), C.bend_k / (hcz * hcz));
+        }
+    // ---- cloth-cube contacts (point-triangle on the top faces) ----
+    auto pos = [&](int64_t g) -> Vec3 { return {sys->x[g * 3], sys->x[g * 3 + 1], sys->x[g * 3 + 2]}; };
+    auto cube_v = [&](int64_t c, int64_t i, int64_t k) { return off_c + c * verts_per + i + vx * (ny + vy * k); };
+    int64_t n_contacts = (int64_t)cubes.n_contacts;
+    for(int64_t v = 0; v < ncv; ++v)
+    {
+        const int64_t g = off_cl + v;
+        const Vec3    p = pos(g);
+        const int64_t ci = (int64_t)std::floor(p[0] / px_pitch), ck = (int64_t)std::floor(p[2] / pz_pitch);
+        if(ci < 0 || ci >= W || ck < 0 || ck >= W)
+            continue;
+        const double ux = p[0] - ci * px_pitch, uz = p[2] - ck * pz_pitch;
+        if(ux > nx * C.h || uz > nz * C.h)
+            continue;  // over a gap between cubes
+        const int64_t c  = ci + (int64_t)W * ck;
+        const int64_t i0 = std::min<int64_t>((int64_t)(ux / C.h), nx - 1), k0 = std::min<int64_t>((int64_t)(uz / C.h), nz - 1);
+        bool          done = false;
+        for(int64_t i = i0 - 1; i <= i0 + 1 && !done; ++i)
+            for(int64_t k = k0 - 1; k <= k0 + 1 && !done; ++k)
+            {
+                if(i < 0 || k < 0 || i >= nx || k >= nz)
+                    continue;
+                const int64_t v00 = cube_v(c, i, k), v10 = cube_v(c, i + 1, k), v01 = cube_v(c, i, k + 1),
+                              v11 = cube_v(c, i + 1, k + 1);
+                const int64_t tri[2][3] = {{v00, v10, v11}, {v00, v11, v01}};
+                for(int tt = 0; tt < 2 && !done; ++tt)
+                {
+                    const Vec3 t0 = pos(tri[tt][0]), t1 = pos(tri[tt][1]), t2 = pos(tri[tt][2]);
+                    Vec3       n  = cross(sub(t1, t0), sub(t2, t0));
+                    n             = scale(n, (n[1] < 0 ? -1.0 : 1.0) / norm(n));
+                    const double d = dot(sub(p, t0), n);
+                    const Vec3   q = sub(p, scale(n, d));
+                    const Vec3   e0 = sub(t1, t0), e1 = sub(t2, t0), e2 = sub(q, t0);
+                    const double d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1), d20 = dot(e2, e0),
+                                 d21 = dot(e2, e1), den = d00 * d11 - d01 * d01;
+                    const double wb = (d11 * d20 - d01 * d21) / den, wc = (d00 * d21 - d01 * d20) / den,
+                                 wa = 1.0 - wb - wc;
+                    if(wa < 0 || wb < 0 || wc < 0)
+                        continue;
+                    done = true;
+                    if(d <= 0.0 || d >= C.dhat)
+                        continue;
+                    ++n_contacts;
+                    const int32_t vs[4] = {(int32_t)g, (int32_t)tri[tt][0], (int32_t)tri[tt][1], (int32_t)tri[tt][2]};
+                    const double  w[4]  = {1.0, -wa, -wb, -wc};
+                    double        a[4][3];
+                    for(int q2 = 0; q2 < 4; ++q2)
+                        for(int a2 = 0; a2 < 3; ++a2)
+                            a[q2][a2] = w[q2] * n[a2];
+                    double D = d * d, b1, b2;
+                    barrier_d(D, Dh, b1, b2);
+                    const double kc = std::max(0.0, dt2 * C.kappa * (b2 * 4.0 * D + 2.0 * b1));
+                    for(int q2 = 0; q2 < 4; ++q2)
+                        for(int r2 = q2; r2 < 4; ++r2)
+                        {
+                            double Hb[9];
+                            for(int pp = 0; pp < 3; ++pp)
+                                for(int cc = 0; cc < 3; ++cc)
+                                    Hb[pp * 3 + cc] = kc * a[q2][pp] * a[r2][cc];
+                            put(vs[q2], vs[r2], Hb);
+                        }
+                    for(int q2 = 0; q2 < 4; ++q2)
+                        for(int a2 = 0; a2 < 3; ++a2)
+                            sys->grad[vs[q2] * 3 + a2] += dt2 * C.kappa * b1 * 2.0 * d * a[q2][a2];
+                }
+            }
+    }
+    // ---- cloth-body contacts (the bodies' bottom faces) ----
+    for(int64_t v = 0; v < ncv && nbod > 0; ++v)
+    {
+        const int64_t g  = off_cl + v;
+        const double  xv = sys->x[g * 3], yv = sys->x[g * 3 + 1], zv = sys->x[g * 3 + 2];
+        const int64_t bi = (int64_t)std::floor(xv / bpx), bk = (int64_t)std::floor(zv / bpz);
+        if(bi < 0 || bi >= nbx || bk < 0 || bk >= nbz)
+            continue;
+        const int64_t b  = bi + (int64_t)nbx * bk;
+        const double  px = sys->x[(4 * b) * 3], py = sys->x[(4 * b) * 3 + 1], pz = sys->x[(4 * b) * 3 + 2];
+        const double  cs = std::cos(theta[b]), sn = std::sin(theta[b]);
+        const double  ux = cs * (xv - px) - sn * (zv - pz), uz = sn * (xv - px) + cs * (zv - pz);
+        if(std::fabs(ux) > 0.5 * s || std::fabs(uz) > 0.5 * s)
+            continue;
+        const double d = (py - 0.5 * s) - yv;
+        if(d <= 0.0 || d >= C.dhat)
+            continue;
+        ++n_contacts;
+        // d = p_y + (A xbar)_y - y_v with xbar = (ux, -s/2, uz) in the body frame
+        const double xbar[3] = {ux, -0.5 * s, uz};
+        double       avec[5][3] = {};
+        const int32_t rws[5] = {(int32_t)g, (int32_t)(4 * b), (int32_t)(4 * b + 1), (int32_t)(4 * b + 2),
+                                (int32_t)(4 * b + 3)};
+        avec[0][1] = -1.0;
+        avec[1][1] = 1.0;
+        for(int k = 0; k < 3; ++k)
+            avec[2 + k][1] = xbar[k];
+        double D = d * d, b1, b2;
+        barrier_d(D, Dh, b1, b2);
+        const double kc = std::max(0.0, dt2 * C.kappa * (b2 * 4.0 * D + 2.0 * b1));
+        for(int q = 0; q < 5; ++q)
+            for(int r = q; r < 5; ++r)
+            {
+                double Hb[9];
+                for(int pp = 0; pp < 3; ++pp)
+                    for(int cc = 0; cc < 3; ++cc)
+                        Hb[pp * 3 + cc] = kc * avec[q][pp] * avec[r][cc];
+                put(rws[q], rws[r], Hb);
+            }
+        for(int q = 0; q < 5; ++q)
+            for(int a = 0; a < 3; ++a)
+                sys->grad[rws[q] * 3 + a] += dt2 * C.kappa * b1 * 2.0 * d * avec[q][a];
+    }
+    sys->n_contacts = n_contacts;
+    sys->rows       = std::move(B.rows);
+    sys->cols       = std::move(B.cols);
+    sys->vals       = std::move(B.vals);
+    // neighbour graph: bodies none, the cubes' tet edges, the cloth's edges
+    sys->adj_start.assign(rows + 1, 0);
+    for(int64_t r = 0; r < rows; ++r)
+    {
+        int32_t cnt = 0;
+        if(r >= off_c && r < off_cl)
+            cnt = cubes.adj_start[r - off_c + 1] - cubes.adj_start[r - off_c];
+        else if(r >= off_cl)
+        {
+            auto& L = nb[r - off_cl];
+            std::sort(L.begin(), L.end());
+            L.erase(std::unique(L.begin(), L.end()), L.end());
+            cnt = (int32_t)L.size();
+        }
+        sys->adj_start[r + 1] = sys->adj_start[r] + cnt;
+    }
+    sys->adj_list.resize(sys->adj_start[rows]);
+    for(int64_t r = off_c; r < rows; ++r)
+    {
+        int32_t* dst = sys->adj_list.data() + sys->adj_start[r];
+        if(r < off_cl)
+            for(int32_t e = cubes.adj_start[r - off_c]; e < cubes.adj_start[r - off_c + 1]; ++e)
+                *dst++ = cubes.adj_list[e] + (int32_t)off_c;
+        else
+            std::copy(nb[r - off_cl].begin(), nb[r - off_cl].end(), dst);
+    }
+}
+
+int generate_impl(const b2g_config* cfg, const double* x_in, const double* xt_in, b2g_system** out)
+{
+    try
+    {
+        if(!cfg || !out)
+            throw std::runtime_error("null argument");
+        const b2g_config C = *cfg;
+        auto sys = std::make_unique<b2g_system>();
+        if(C.scene == 3 || C.scene == 4)
+        {
+            if(x_in || xt_in)
+                throw std::runtime_error("scenes 3 and 4 have no state input");
+            if(C.scene == 3)
+                generate_cloth_abd(C, sys.get());
+            else
+                generate_wall(C, sys.get());
+        }
+        else
+            generate_tets(C, x_in, xt_in, sys.get());
         *out = sys.release();
         return 0;
     }

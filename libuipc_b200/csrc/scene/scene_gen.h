@@ -23,7 +23,8 @@ extern "C" {
 
 typedef struct b2g_config
 {
-    int    scene;          // 1 = cubes stacked along +y on a ground plane, 2 = twisted bar
+    int    scene;          // 1 = cubes stacked along +y on a ground plane, 2 = twisted bar,
+                           // 3 = cloth over affine bodies, 4 = cube grid + cloth + bodies
     int    cells_x;        // cells per cube edge (x)
     int    cells_y;        // (y)
     int    cells_z;        // (z)
@@ -48,6 +49,13 @@ typedef struct b2g_config
     double body_kappa;     // affine-body orthogonality stiffness [Pa]
     double bend_k;         // cloth bending stiffness [N m]
     double cloth_size;     // cloth side length [m]
+    // scene 4 (cube grid + cloth + bodies): n_cubes = cubes per grid side,
+    // cells_x/y/z = cells per cube edge, E / nu / rho the cubes' material
+    double wall_gap;       // gap between neighbouring cubes of the grid [m]
+    int    cloth_n;        // cloth vertices per side
+    int    bodies_x;       // affine bodies along x
+    int    bodies_z;       // affine bodies along z
+    double cloth_k;        // cloth stretch stiffness [N/m] (scene 4)
 } b2g_config;
 
 typedef struct b2g_system b2g_system;

@@ -40,6 +40,11 @@ class B2GConfig(C.Structure):
         ("body_kappa", C.c_double),
         ("bend_k", C.c_double),
         ("cloth_size", C.c_double),
+        ("wall_gap", C.c_double),
+        ("cloth_n", C.c_int),
+        ("bodies_x", C.c_int),
+        ("bodies_z", C.c_int),
+        ("cloth_k", C.c_double),
     ]
 
 
@@ -172,3 +177,17 @@ def cloth_on_bodies(n: int = 256, bodies_per_side: int = 8, seed: int = 0, **kw)
     The bodies' 4 * n_bodies block rows come first."""
     kw.setdefault("E", 1e3)
     return generate(scene=3, cells_x=n, cells_y=1, cells_z=1, n_cubes=bodies_per_side, seed=seed, **kw)
+
+
+def cube_wall(cells: int = 30, side: int = 10, cloth_n: int = 512, bodies_x: int = 4, bodies_z: int = 8,
+              seed: int = 0, **kw) -> NewtonSystem:
+    """The full-scale case: a side x side grid of jittered tet cubes of
+    cells^3 cells on the ground (2 cm apart), a cloth_n x cloth_n cloth resting
+    on their top faces (point-triangle barrier blocks) and bodies_x x bodies_z
+    affine bodies resting on the cloth (12x3 couplings); dt = 5 ms. The
+    bodies' 4 * n_bodies block rows come first, then the cube vertices, then
+    the cloth; the MAS range is everything after the bodies. The defaults give
+    3.26 M block rows (9.8 M DoF)."""
+    kw.setdefault("dt", 0.005)
+    return generate(scene=4, cells_x=cells, cells_y=cells, cells_z=cells, n_cubes=side, cloth_n=cloth_n,
+                    bodies_x=bodies_x, bodies_z=bodies_z, seed=seed, **kw)

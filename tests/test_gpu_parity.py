@@ -50,6 +50,39 @@ def test_assembly_bit_exact(request, solver, cuda, which):
     assert np.array_equal(val, oval)  # source-order FP64 sums on both sides
 
 
+def test_assembly_values_only_8_byte_aligned(solver, cuda, cube5):
+    """A value array that starts 8 bytes into a 16-byte line (a view one
+    double into a buffer) takes the scalar gathers: same sums bit for bit."""
+    import torch
+
+    s = cube5
+    buf = torch.zeros(s.vals.size + 1, dtype=torch.float64, device=cuda)
+    buf[1:] = torch.from_numpy(np.ascontiguousarray(s.vals).ravel()).to(cuda)
+    vals = buf[1:]
+    assert vals.data_ptr() % 16 == 8
+    solver.assemble(s.n_verts, to_dev(s.rows, cuda), to_dev(s.cols, cuda), vals)
+    rp, col, val = solver.upper_bsr()
+    orp, orow, ocol, oval = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals).bsr()
+    assert np.array_equal(rp, orp) and np.array_equal(col, ocol) and np.array_equal(val, oval)
+
+
+def test_assembly_long_rows(solver, cuda):
+    """Rows of thousands of pairs (an affine body under a large cloth), with
+    duplicates, sorted by the block-per-row kernel: bit-exact."""
+    rng = np.random.default_rng(21)
+    nb = 3000
+    rows = np.concatenate([np.zeros(6000), np.full(300, 7), rng.integers(0, nb, 4000), np.full(5000, 2999)])
+    cols = np.concatenate([rng.integers(0, nb, 6000), rng.integers(7, nb, 300), rng.integers(0, nb, 4000),
+                           np.full(5000, 2999)])
+    rows, cols = rows.astype(np.int32), cols.astype(np.int32)
+    rows[rng.random(rows.size) < 0.01] = -1  # unwritten slots
+    vals = rng.standard_normal((rows.size, 9))
+    solver.assemble(nb, to_dev(rows, cuda), to_dev(cols, cuda), to_dev(vals, cuda))
+    rp, col, val = solver.upper_bsr()
+    orp, _, ocol, oval = O.OracleMatrix(nb, rows, cols, vals).bsr()
+    assert np.array_equal(rp, orp) and np.array_equal(col, ocol) and np.array_equal(val, oval)
+
+
 def test_assembly_edge_cases(solver, cuda):
     import torch
 
