@@ -53,7 +53,8 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clock and clock-event-reason sampling during the timed region
+    (NVML on a host thread, every 5 ms; nvidia-smi as the fallback)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -63,8 +64,47 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.thread = None
+
+    def _nvml_handle(self):
+        """NVML handle of the CUDA device (matched by PCI bus id: NVML numbers
+        every GPU of the machine, CUDA only the visible ones)."""
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.gpu)
+        bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
 
     def start(self):
+        """Samples the SM clock and the clock event reasons every 5 ms through
+        NVML on a host thread (read-only queries); nvidia-smi when NVML is not
+        usable."""
+        try:
+            import threading
+
+            nv, h = self._nvml_handle()
+            self.samples = []
+            self.stop_evt = threading.Event()
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def run():
+                while True:
+                    try:
+                        self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx,
+                                             nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    except Exception:
+                        pass
+                    if self.stop_evt.wait(0.005):
+                        break
+
+            self.nv = nv
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -76,6 +116,19 @@ class ClockSampler:
             self.proc = None
 
     def stop(self) -> dict:
+        if self.thread is not None:
+            self.stop_evt.set()
+            self.thread.join(timeout=5)
+            nv = self.nv
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            sm = [a for a, _, _ in self.samples]
+            reasons = sorted({k for _, _, r in self.samples for k, b in bits.items() if r & b})
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": max(m for _, m, _ in self.samples) if self.samples else None,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         self.proc.terminate()
@@ -100,7 +153,7 @@ class ClockSampler:
                     reasons.add(nm)
         os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def spmv_bytes(U: int, nb: int, s: int = 8) -> int:
