@@ -532,6 +532,179 @@ __global__ void k_ws_infer(int rows, int H, const __nv_bfloat16* __restrict__ w1
     }
 }
 
+// The same inference on the tensor cores for width 128 (the width the bench
+// and tests use): one warp per 16 aggregates, every layer as mma.m16n8k16
+// with BF16 weights (as above) and activations split into BF16 high + low
+// parts (two products into one FP32 accumulator: the activations keep ~16
+// significant bits). Weights are stored transposed in shared memory, rows
+// padded to 8 extra BF16 so the B-fragment loads of a warp hit 32 distinct
+// banks. Layer l's accumulator fragments are layer l+1's A fragments (16 x 8
+// C tiles 2k and 2k+1 form the 16 x 16 A tile k).
+constexpr int MMA_H   = 128;
+constexpr int MMA_K1  = 32;            // WS_F = 22 padded
+constexpr int MMA_LD1 = MMA_K1 + 8;    // W0t row stride (BF16)
+constexpr int MMA_LDH = MMA_H + 8;     // W1t / W2t row stride
+constexpr int MMA_WARPS = 4;
+
+size_t inference_mma_smem()
+{
+    return sizeof(__nv_bfloat16) * ((size_t)MMA_H * MMA_LD1 + (size_t)MMA_H * MMA_LDH + 8 * (size_t)MMA_LDH) +
+           sizeof(float) * (2 * MMA_H + 8);
+}
+
+__device__ __forceinline__ void mma_16816_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// two floats as BF16 pairs: high parts and the remainders
+__device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t& hi, uint32_t& lo)
+{
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+    const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
+    const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
+    hi = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+    lo = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+}
+
+__device__ __forceinline__ uint32_t ld_b32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+__global__ void __launch_bounds__(MMA_WARPS * 32)
+    k_ws_infer_mma(int rows, const __nv_bfloat16* __restrict__ w16, const float* __restrict__ params,
+                   const float* __restrict__ feat, const float* __restrict__ norm, float* __restrict__ Y)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const PLayout  P(MMA_H);
+    __nv_bfloat16* W0t = reinterpret_cast<__nv_bfloat16*>(smem);          // [H][LD1]: W0t[n][k] = W0[k][n]
+    __nv_bfloat16* W1t = W0t + (size_t)MMA_H * MMA_LD1;                      // [H][LDH]
+    __nv_bfloat16* W2t = W1t + (size_t)MMA_H * MMA_LDH;                      // [8][LDH] (rows 4..7 zero)
+    float*         bs  = reinterpret_cast<float*>(W2t + 8 * MMA_LDH);        // b0[H] b1[H] b2[8]
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+    for(int i = threadIdx.x; i < MMA_H * MMA_LD1; i += blockDim.x)
+    {
+        const int n = i / MMA_LD1, k = i % MMA_LD1;
+        W0t[i]      = k < WS_F ? w16[P.W0 + (int64_t)k * MMA_H + n] : zero;
+    }
+    for(int i = threadIdx.x; i < MMA_H * MMA_LDH; i += blockDim.x)
+    {
+        const int n = i / MMA_LDH, k = i % MMA_LDH;
+        W1t[i]      = k < MMA_H ? w16[P.W1 + (int64_t)k * MMA_H + n] : zero;
+    }
+    for(int i = threadIdx.x; i < 8 * MMA_LDH; i += blockDim.x)
+    {
+        const int n = i / MMA_LDH, k = i % MMA_LDH;
+        W2t[i]      = (n < WS_O && k < MMA_H) ? w16[P.W2 + (int64_t)k * WS_O + n] : zero;
+    }
+    for(int i = threadIdx.x; i < 2 * MMA_H + 8; i += blockDim.x)
+        bs[i] = i < MMA_H ? params[P.b0 + i] : i < 2 * MMA_H ? params[P.b1 + i - MMA_H]
+                                             : (i - 2 * MMA_H < WS_O ? params[P.b2 + i - 2 * MMA_H] : 0.f);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int n_tiles = (rows + 15) / 16;
+    for(int tile = blockIdx.x * MMA_WARPS + (threadIdx.x >> 5); tile < n_tiles; tile += gridDim.x * MMA_WARPS)
+    {
+        const int r0 = tile * 16 + g, r1 = r0 + 8;
+        // layer 1 A fragments (16 x 32): standardised features
+        uint32_t ah[2][4], al[2][4];
+#pragma unroll
+        for(int kk = 0; kk < 2; ++kk)
+#pragma unroll
+            for(int q = 0; q < 4; ++q)
+            {
+                const int r = (q & 1) ? r1 : r0, k = 16 * kk + 2 * t + ((q & 2) ? 8 : 0);
+                float     x[2];
+#pragma unroll
+                for(int e = 0; e < 2; ++e)
+                    x[e] = (r < rows && k + e < WS_F) ? (feat[(int64_t)r * WS_F + k + e] - norm[k + e]) * norm[WS_F + k + e]
+                                                      : 0.f;
+                split_bf16x2(x[0], x[1], ah[kk][q], al[kk][q]);
+            }
+        float c[16][4];
+#pragma unroll
+        for(int j = 0; j < 16; ++j)
+        {
+            const float bb0 = bs[8 * j + 2 * t], bb1 = bs[8 * j + 2 * t + 1];
+            c[j][0] = bb0;
+            c[j][1] = bb1;
+            c[j][2] = bb0;
+            c[j][3] = bb1;
+#pragma unroll
+            for(int kk = 0; kk < 2; ++kk)
+            {
+                const __nv_bfloat16* wb = W0t + (size_t)(8 * j + g) * MMA_LD1 + 16 * kk + 2 * t;
+                const uint32_t       b0 = ld_b32(wb), b1 = ld_b32(wb + 8);
+                mma_16816_bf16(c[j], ah[kk], b0, b1);
+                mma_16816_bf16(c[j], al[kk], b0, b1);
+            }
+        }
+        // layers 2 and 3: ReLU of the previous layer as the A operand
+#pragma unroll
+        for(int layer = 0; layer < 2; ++layer)
+        {
+            uint32_t hh[8][4], hl[8][4];
+#pragma unroll
+            for(int kk = 0; kk < 8; ++kk)
+            {
+                split_bf16x2(fmaxf(c[2 * kk][0], 0.f), fmaxf(c[2 * kk][1], 0.f), hh[kk][0], hl[kk][0]);
+                split_bf16x2(fmaxf(c[2 * kk][2], 0.f), fmaxf(c[2 * kk][3], 0.f), hh[kk][1], hl[kk][1]);
+                split_bf16x2(fmaxf(c[2 * kk + 1][0], 0.f), fmaxf(c[2 * kk + 1][1], 0.f), hh[kk][2], hl[kk][2]);
+                split_bf16x2(fmaxf(c[2 * kk + 1][2], 0.f), fmaxf(c[2 * kk + 1][3], 0.f), hh[kk][3], hl[kk][3]);
+            }
+            if(layer == 0)
+            {
+#pragma unroll
+                for(int j = 0; j < 16; ++j)
+                {
+                    const float bb0 = bs[MMA_H + 8 * j + 2 * t], bb1 = bs[MMA_H + 8 * j + 2 * t + 1];
+                    c[j][0] = bb0;
+                    c[j][1] = bb1;
+                    c[j][2] = bb0;
+                    c[j][3] = bb1;
+#pragma unroll
+                    for(int kk = 0; kk < 8; ++kk)
+                    {
+                        const __nv_bfloat16* wb = W1t + (size_t)(8 * j + g) * MMA_LDH + 16 * kk + 2 * t;
+                        const uint32_t       b0 = ld_b32(wb), b1 = ld_b32(wb + 8);
+                        mma_16816_bf16(c[j], hh[kk], b0, b1);
+                        mma_16816_bf16(c[j], hl[kk], b0, b1);
+                    }
+                }
+            }
+            else
+            {
+                float y[4] = {bs[2 * MMA_H + 2 * t], bs[2 * MMA_H + 2 * t + 1], bs[2 * MMA_H + 2 * t],
+                              bs[2 * MMA_H + 2 * t + 1]};
+#pragma unroll
+                for(int kk = 0; kk < 8; ++kk)
+                {
+                    const __nv_bfloat16* wb = W2t + (size_t)g * MMA_LDH + 16 * kk + 2 * t;
+                    const uint32_t       b0 = ld_b32(wb), b1 = ld_b32(wb + 8);
+                    mma_16816_bf16(y, hh[kk], b0, b1);
+                    mma_16816_bf16(y, hl[kk], b0, b1);
+                }
+                // y: rows g / g+8, output columns 2t, 2t+1 (the 4 outputs: t < 2)
+                if(t < 2)
+                {
+                    if(r0 < rows)
+                    {
+                        Y[(int64_t)r0 * WS_O + 2 * t]     = y[0];
+                        Y[(int64_t)r0 * WS_O + 2 * t + 1] = y[1];
+                    }
+                    if(r1 < rows)
+                    {
+                        Y[(int64_t)r1 * WS_O + 2 * t]     = y[2];
+                        Y[(int64_t)r1 * WS_O + 2 * t + 1] = y[3];
+                    }
+                }
+            }
+        }
+    }
+}
+
 // d(v) = sum_i Y[a(v)][i] f_i(v) on the MAS vertices, 0 elsewhere
 __global__ void k_ws_combine(int64_t n, int vn, int off, int L, int level1_begin, int n_agg,
                              const int32_t* __restrict__ ctable, const float* __restrict__ Y,
@@ -1109,11 +1282,23 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
             B2S_CHECK_LAUNCH();
             W.w16_version = W.version;
         }
-        const size_t smem = inference_smem(W.hidden);
-        B2S_CUDA(cudaFuncSetAttribute(k_ws_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        const int tiles = (na + INF_TILE - 1) / INF_TILE;
-        k_ws_infer<<<std::max(1, std::min(tiles, NUM_SMS_HINT * 2)), W.hidden, smem, st>>>(
-            na, W.hidden, W.w16.data(), W.params.data(), W.feat.data(), W.norm_dev.data(), W.Y.data());
+        if(W.hidden == MMA_H)
+        {
+            const size_t smem = inference_mma_smem();
+            B2S_CUDA(cudaFuncSetAttribute(k_ws_infer_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            const int tiles = (na + 15) / 16;
+            const int grid  = std::max(1, std::min((tiles + MMA_WARPS - 1) / MMA_WARPS, NUM_SMS_HINT * 2));
+            k_ws_infer_mma<<<grid, MMA_WARPS * 32, smem, st>>>(na, W.w16.data(), W.params.data(), W.feat.data(),
+                                                               W.norm_dev.data(), W.Y.data());
+        }
+        else
+        {
+            const size_t smem = inference_smem(W.hidden);
+            B2S_CUDA(cudaFuncSetAttribute(k_ws_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            const int tiles = (na + INF_TILE - 1) / INF_TILE;
+            k_ws_infer<<<std::max(1, std::min(tiles, NUM_SMS_HINT * 2)), W.hidden, smem, st>>>(
+                na, W.hidden, W.w16.data(), W.params.data(), W.feat.data(), W.norm_dev.data(), W.Y.data());
+        }
         B2S_CHECK_LAUNCH();
         W.d_mlp.resize(n);
         k_ws_combine<<<ws_grid(n), WS_BLOCK, 0, st>>>(n, g.vn, g.off, g.L, g.level1_begin, na, g.ctable, W.Y.data(),
