@@ -42,6 +42,7 @@ SOLVE_SOURCES = [
     "b2s_mas.cu",
     "b2s_pcg.cu",
     "b2s_learned.cu",
+    "b2s_generate.cu",
     "b2s_abi.cu",
     "b2s_noalloc.cu",
 ]
@@ -66,7 +67,7 @@ def _digest(paths: list[str], extra: str) -> str:
 
 def _headers() -> list[str]:
     hs = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cuh", ".h"))]
-    return hs + [os.path.join(ROOT, "include", "b200solve.h")]
+    return hs + [os.path.join(ROOT, "include", h) for h in ("b200solve.h", "b200gen.h")]
 
 
 def build_solve(force: bool = False, extra_flags: list[str] | None = None) -> str:

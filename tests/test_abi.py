@@ -40,6 +40,17 @@ def test_io_library_exports_every_header_symbol():
     assert set(declared) <= exported
 
 
+def test_generator_symbols_exported():
+    """include/b200gen.h (the GPU Newton-system generator) is exported by libb200solve.so."""
+    from libuipc_b200 import _abi
+
+    declared = _abi.header_symbols(os.path.join(ROOT, "include", "b200gen.h"), prefix="b2gen_")
+    assert len(declared) == 5
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l}
+    assert set(declared) <= exported
+
+
 def test_library_is_built_for_sm100a():
     out = subprocess.run(["cuobjdump", "--list-elf", LIB], capture_output=True, text=True).stdout
     assert "sm_100a" in out
