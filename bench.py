@@ -412,6 +412,10 @@ def main() -> None:
     ap.add_argument("--train-epochs", type=int, default=30)
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed solves with cudaProfilerStart/Stop (ncu --profile-from-start off)")
+    ap.add_argument("--learned-bar", action="store_true",
+                    help="also run the learned warm start at the 200x20x20 twisted bar's scale: 2000 training "
+                         "systems generated and solved on the GPU, then zero / previous-dx / history / learned "
+                         "starts compared on 200 later systems (a few minutes)")
     ap.add_argument("--no-full-scale", action="store_true",
                     help="skip the 9.7 M-DoF cube grid + cloth + bodies case run beside the headline")
     ap.add_argument("--no-bar", action="store_true",
@@ -572,6 +576,15 @@ def main() -> None:
         except Exception as e:  # reported, not fatal
             full = {"error": str(e)}
 
+    learned_bar = None
+    if rank == 0 and args.learned_bar:
+        from libuipc_b200.learned import run_gpu_bar
+
+        try:
+            learned_bar = run_gpu_bar(dev)
+        except Exception as e:  # reported, not fatal
+            learned_bar = {"error": str(e)}
+
     bar = None
     if rank == 0 and not args.no_bar:
         try:
@@ -691,6 +704,7 @@ def main() -> None:
         "generate_s": gen_s,
         "bar_1M": bar,
         "full_scale": full,
+        "learned_bar": learned_bar,
     }
     solver.close()
     if rank == 0:

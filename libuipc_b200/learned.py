@@ -116,3 +116,87 @@ class SequenceRunner:
         for _ in self.seq.run(n_steps, newton_iters, solve):
             pass
         return log
+
+
+def run_gpu_bar(device, cells=(200, 20, 20), E: float = 1e6, nu: float = 0.49, twist: float = 2.0,
+                train_steps: int = 200, eval_steps: int = 20, newton_iters: int = 10, truth_tol: float = 1e-10,
+                tol: float = 1e-4, epochs: int = 5, hidden: int = 128, seed: int = 0,
+                precision=_abi.B2S_PRECISION_FP64, modes=("zero", "prev", "history", "learned")) -> dict:
+    """The learned warm start on the twisted bar at configs[3]'s scale: the bar
+    (cells, E, nu; ends turned +-twist deg per step) is stepped on the GPU
+    (:class:`GpuBarSequence`, every system from the device generator) for
+    ``train_steps`` steps of ``newton_iters`` Newton iterations; every system
+    is solved to ``truth_tol`` (FP64 MAS-PCG from the history start) and is a
+    training sample (train_steps * newton_iters systems); the MLP is trained
+    for ``epochs`` epochs; then ``eval_steps`` more steps are run and each of
+    their systems is also solved to ``tol`` from every start in ``modes``.
+    Returns the mean PCG iterations per mode and the run's timings."""
+    import time
+    from collections import deque
+
+    import torch
+
+    from .sequence import GpuBarSequence
+
+    seq = GpuBarSequence(device, twist_per_step=twist, cells_x=cells[0], cells_y=cells[1], cells_z=cells[2], E=E,
+                         nu=nu)
+    solver = Solver(device.index or 0)
+    stream = torch.cuda.current_stream(device)
+    solver.set_stream(stream.cuda_stream)  # one stream for the solver, the generator and the state updates
+    try:
+        p2r, r2p = partition_maps(partition_rcb(seq.rest))
+        solver.mas_init(0, seq.n_verts, seq.adj_start, seq.adj_list, p2r, r2p)
+        solver.ws_init(hidden, seed=seed)
+        history: dict[int, deque] = {}
+        log = RunLog()
+
+        def newton(collect: bool, eval_modes) -> None:
+            for k in range(newton_iters):
+                rows, cols, vals, b = seq.system()
+                solver.assemble(seq.n_verts, rows, cols, vals)
+                solver.precond_assemble(_abi.B2S_PRECOND_MAS)
+                hist = list(history.get(k, deque()))
+                for mode in eval_modes:
+                    xm = torch.zeros_like(b)
+                    info = solver.ws_predict(b, xm, hist, MODES[mode])
+                    st = solver.pcg(b, xm, tol=tol, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5,
+                                    precision=precision, x0_given=True, replace_every=50)
+                    log.records.append(SolveRecord(seq.step, k, mode, int(st["iterations_exact"]),
+                                                   float(st["rel_res"]), float(info["rel_res0"]),
+                                                   float(info["predict_ms"]), int(info["mode"])))
+                x = torch.zeros_like(b)
+                solver.ws_predict(b, x, hist, MODES["history"])
+                solver.pcg(b, x, tol=truth_tol, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, x0_given=True)
+                if collect:
+                    solver.ws_add_sample(b, x, hist)
+                history.setdefault(k, deque(maxlen=_abi.B2S_WS_HISTORY)).appendleft(x)
+                seq.apply(x)
+
+        t0 = time.time()
+        for _ in range(train_steps):
+            seq.begin_step()
+            newton(True, ())
+            seq.end_step()
+        stream.synchronize()
+        t_run = time.time() - t0
+        n_samples, _ = solver.ws_num_samples()
+        t0 = time.time()
+        solver.ws_fit_normalization()
+        loss = solver.ws_train(epochs, lr=1e-3, seed=seed)
+        t_train = time.time() - t0
+        for _ in range(eval_steps):
+            seq.begin_step()
+            newton(False, modes)
+            seq.end_step()
+        return {
+            "workload": f"twisted bar {cells[0]}x{cells[1]}x{cells[2]} cells ({seq.n_verts:,} vertices, "
+                        f"{3 * seq.n_verts:,} DoF), E={E:g}, nu={nu}, ends +-{twist} deg per step",
+            "training_systems": int(n_samples), "train_steps": train_steps, "newton_iters": newton_iters,
+            "eval_systems": eval_steps * newton_iters, "epochs": epochs, "final_loss": loss,
+            "run_s": t_run, "train_s": t_train,
+            "mean_pcg_iterations": {m: log.mean_iterations(m) for m in modes},
+            "stop": f"rel-res {tol:g}", "precision": "fp64" if precision == _abi.B2S_PRECISION_FP64 else "mixed",
+        }
+    finally:
+        solver.close()
+        seq.close()

@@ -101,3 +101,74 @@ class SceneSequence:
                 yield self.step, k, sysm, sol
                 self.apply(sol)
             self.end_step()
+
+
+class GpuBarSequence:
+    """The twisted bar stepped on the GPU: the state (x, v) stays on the
+    device and every Newton system comes from the device generator
+    (``gpu_scene.GpuTetMesh``), so a run of thousands of systems needs no host
+    work per system. Same stepping as :class:`SceneSequence` (backward Euler,
+    end layers fixed and turned by +-twist_per_step * step degrees).
+    ``cfg``: generator options of the bar (``cells_*``, material, ``dt``)."""
+
+    def __init__(self, device, twist_per_step: float = 2.0, **cfg):
+        import torch
+
+        from .gpu_scene import GpuTetMesh
+
+        self.torch = torch
+        self.dev = device
+        self.cfg = dict(cfg)
+        base = generate(**{**cfg, "scene": 2, "twist_deg": 0.0})
+        c = base.config
+        self.dt = float(c["dt"])
+        self.gravity = float(c["gravity"])
+        self.twist_per_step = float(twist_per_step)
+        self.rest = base.positions.copy()
+        self.n_verts = base.n_verts
+        self.adj_start = base.adj_start
+        self.adj_list = base.adj_list
+        xs = self.rest[:, 0]
+        self.left = np.isclose(xs, xs.min(), atol=1e-12)
+        self.right = np.isclose(xs, xs.max(), atol=1e-12)
+        self.axis_y = 0.5 * (self.rest[:, 1].min() + self.rest[:, 1].max())
+        self.axis_z = 0.5 * (self.rest[:, 2].min() + self.rest[:, 2].max())
+        self.mesh = GpuTetMesh(self.rest, base.tets, c, device, fixed=self.left | self.right)
+        self.x = torch.from_numpy(self.rest.ravel().copy()).to(device)
+        self.v = torch.zeros_like(self.x)
+        self.x_prev = self.x.clone()
+        self.x_tilde = self.x.clone()
+        self.fixed_idx = torch.from_numpy(np.nonzero(self.left | self.right)[0]).to(device)
+        self.step = 0
+
+    def _turned_ends(self) -> np.ndarray:
+        th_deg = self.twist_per_step * self.step
+        out = self.rest.copy()
+        for mask, sign in ((self.left, -1.0), (self.right, 1.0)):
+            th = math.radians(sign * th_deg)
+            cs, sn = math.cos(th), math.sin(th)
+            y, z = self.rest[mask, 1] - self.axis_y, self.rest[mask, 2] - self.axis_z
+            out[mask, 1] = self.axis_y + cs * y - sn * z
+            out[mask, 2] = self.axis_z + sn * y + cs * z
+        return out[self.left | self.right]
+
+    def begin_step(self) -> None:
+        self.step += 1
+        self.x_prev = self.x.clone()
+        self.x_tilde = self.x + self.dt * self.v
+        self.x_tilde.view(-1, 3)[:, 1] -= self.dt * self.dt * self.gravity
+        ends = self.torch.from_numpy(self._turned_ends()).to(self.dev)
+        self.x.view(-1, 3)[self.fixed_idx] = ends
+
+    def system(self):
+        """(rows, cols, vals, b) device tensors of the Newton system at x."""
+        return self.mesh.system(self.x, self.x_tilde)
+
+    def apply(self, sol) -> None:
+        self.x -= sol
+
+    def end_step(self) -> None:
+        self.v = (self.x - self.x_prev) / self.dt
+
+    def close(self) -> None:
+        self.mesh.close()
