@@ -210,6 +210,93 @@ def cpu_baseline(s, budget_s: float = 20.0) -> dict:
             "rel_res": float(info["rel_res_true"]), "assembly_ms": t_asm * 1e3}
 
 
+def config_solve(dev, s, steps: int = 5, warmup: int = 3) -> dict:
+    """One Newton system of a config solved from a zero start, plain FP64 vs
+    mixed precision: ms per solve (assembly + MAS build + PCG, CUDA events),
+    PCG iterations to an FP64-verified rel-res 1e-4 and under the reference's
+    rule |r.z| <= 1e-4 |r0.z0|, SpMV bandwidth; MAS on the FEM range and the
+    12x12 block Jacobi on the affine bodies when the system has any."""
+    import numpy as np
+    import torch
+
+    from libuipc_b200 import _abi
+    from libuipc_b200.linear_system import Solver, partition_maps, partition_rcb
+
+    off = 4 * s.n_bodies
+    a0 = s.adj_start[off]
+    adj_start = (s.adj_start[off:] - a0).astype(np.int32)
+    adj_list = (s.adj_list[a0:] - off).astype(np.int32)
+    p2r, r2p = partition_maps(partition_rcb(s.positions[off:]))
+    stream = torch.cuda.Stream(device=dev)
+    solver = Solver(dev.index or 0)
+    solver.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        rows = torch.from_numpy(s.rows).to(dev)
+        cols = torch.from_numpy(s.cols).to(dev)
+        vals = torch.from_numpy(s.vals).to(dev)
+        b = torch.from_numpy(s.b).to(dev)
+        x = torch.zeros_like(b)
+    stream.synchronize()
+    solver.assemble(s.n_verts, rows, cols, vals)
+    solver.mas_init(off, s.n_verts - off, adj_start, adj_list, p2r, r2p)
+    if s.n_bodies:
+        solver.abd_init(0, s.n_bodies)
+    nb, U = solver.matrix_info()
+    out = {"n_dof": 3 * s.n_verts, "n_triplets": int(len(s.rows)), "upper_blocks": int(U),
+           "n_bodies": int(s.n_bodies), "contacts": int(s.n_contacts)}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    peak, _ = _peaks()
+    for mode, prec in (("plain", _abi.B2S_PRECISION_FP64), ("mixed", _abi.B2S_PRECISION_MIXED)):
+        def solve(rule=_abi.B2S_STOP_RELRES):
+            solver.assemble(s.n_verts, rows, cols, vals)
+            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_SWEEP_F32)
+            return solver.pcg(b, x, tol=1e-4, stop_rule=rule, check_interval=5, precision=prec, replace_every=50)
+
+        for _ in range(warmup):
+            solve()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        st = [solve() for _ in range(steps)]
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        st_rz = solve(_abi.B2S_STOP_RZ)
+        solver.set_timing(True)
+        solve()
+        solver.reset_timers()
+        solve()
+        t = solver.timers()
+        solver.set_timing(False)
+        spmv_ms = t["spmv_ms"] / max(t["spmv_launches"], 1)
+        gbs = spmv_bytes(U, nb, 8 if mode == "plain" else 4) / (spmv_ms * 1e-3) / 1e9 if spmv_ms > 0 else None
+        out[mode] = {"ms_per_solve": ms, "pcg_iterations": int(st[-1]["iterations_exact"]),
+                     "rel_res": float(st[-1]["rel_res"]),
+                     "pcg_iterations_reference_rule": int(st_rz["iterations_exact"]),
+                     "spmv_us": spmv_ms * 1e3, "spmv_gbs": gbs, "spmv_frac": gbs / peak if gbs and peak else None}
+    out["speedup_vs_plain"] = out["plain"]["ms_per_solve"] / out["mixed"]["ms_per_solve"]
+    solver.close()
+    return out
+
+
+def configs_run(dev) -> dict:
+    """The reference-style configs that are not the headline: C1 (one 10^3-cell
+    tet cube on the ground) and C3 (a 256^2 cloth over 64 affine bodies), each
+    with its host-core block-Jacobi CPU baseline."""
+    from libuipc_b200 import scene
+
+    res = {}
+    for name, make in (("C1 cube10", lambda: scene.cube_on_ground(10, seed=0)),
+                       ("C3 cloth256 over 8x8 bodies", lambda: scene.cloth_on_bodies(256, 8, seed=0))):
+        s = make()
+        r = config_solve(dev, s)
+        try:
+            r["cpu_baseline"] = cpu_baseline(s, budget_s=15.0)
+        except Exception as e:  # reported, not fatal
+            r["cpu_baseline"] = {"error": str(e)}
+        res[name] = r
+    return res
+
+
 def bar_run(dev, steps: int, warmup: int, history_steps: int = 6, epochs: int = 30) -> dict:
     """A second run beside the headline: the twisted bar of 400 x 30 x 30 cells
     (385,361 vertices, 1.16 M DoF; E = 1e6, nu = 0.49, ends turned 2 deg per
@@ -412,6 +499,8 @@ def main() -> None:
     ap.add_argument("--train-epochs", type=int, default=30)
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed solves with cudaProfilerStart/Stop (ncu --profile-from-start off)")
+    ap.add_argument("--configs", action="store_true",
+                    help="also run C1 (10^3 cube) and C3 (cloth over affine bodies): plain vs mixed, CPU baseline")
     ap.add_argument("--learned-bar", action="store_true",
                     help="also run the learned warm start at the 200x20x20 twisted bar's scale: 2000 training "
                          "systems generated and solved on the GPU, then zero / previous-dx / history / learned "
@@ -576,6 +665,13 @@ def main() -> None:
         except Exception as e:  # reported, not fatal
             full = {"error": str(e)}
 
+    configs = None
+    if rank == 0 and args.configs:
+        try:
+            configs = configs_run(dev)
+        except Exception as e:  # reported, not fatal
+            configs = {"error": str(e)}
+
     learned_bar = None
     if rank == 0 and args.learned_bar:
         from libuipc_b200.learned import run_gpu_bar
@@ -705,6 +801,7 @@ def main() -> None:
         "bar_1M": bar,
         "full_scale": full,
         "learned_bar": learned_bar,
+        "configs": configs,
     }
     solver.close()
     if rank == 0:

@@ -149,6 +149,12 @@ def run_gpu_bar(device, cells=(200, 20, 20), E: float = 1e6, nu: float = 0.49, t
         solver.ws_init(hidden, seed=seed)
         history: dict[int, deque] = {}
         log = RunLog()
+        # timed evaluation: plain FP64 from zero vs mixed precision from the
+        # learned start (prediction + PCG, CUDA events; assembly and the MAS
+        # build are shared)
+        timed = {"plain": ("zero", _abi.B2S_PRECISION_FP64), "mixed+learned": ("learned", _abi.B2S_PRECISION_MIXED)}
+        tsum = {k: [0.0, 0, 0] for k in timed}
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
         def newton(collect: bool, eval_modes) -> None:
             for k in range(newton_iters):
@@ -156,6 +162,19 @@ def run_gpu_bar(device, cells=(200, 20, 20), E: float = 1e6, nu: float = 0.49, t
                 solver.assemble(seq.n_verts, rows, cols, vals)
                 solver.precond_assemble(_abi.B2S_PRECOND_MAS)
                 hist = list(history.get(k, deque()))
+                if eval_modes:
+                    for label, (mode, prec) in timed.items():
+                        xm = torch.zeros_like(b)
+                        ev0.record(stream)
+                        if mode != "zero":
+                            solver.ws_predict(b, xm, hist, MODES[mode])
+                        st = solver.pcg(b, xm, tol=tol, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5,
+                                        precision=prec, x0_given=mode != "zero", replace_every=50)
+                        ev1.record(stream)
+                        ev1.synchronize()
+                        tsum[label][0] += ev0.elapsed_time(ev1)
+                        tsum[label][1] += int(st["iterations_exact"])
+                        tsum[label][2] += 1
                 for mode in eval_modes:
                     xm = torch.zeros_like(b)
                     info = solver.ws_predict(b, xm, hist, MODES[mode])
@@ -195,6 +214,9 @@ def run_gpu_bar(device, cells=(200, 20, 20), E: float = 1e6, nu: float = 0.49, t
             "eval_systems": eval_steps * newton_iters, "epochs": epochs, "final_loss": loss,
             "run_s": t_run, "train_s": t_train,
             "mean_pcg_iterations": {m: log.mean_iterations(m) for m in modes},
+            "timed_eval": {k: {"ms_per_solve": v[0] / max(v[2], 1), "mean_pcg_iterations": v[1] / max(v[2], 1),
+                               "note": "prediction + PCG; assembly and MAS build shared"}
+                           for k, v in tsum.items()},
             "stop": f"rel-res {tol:g}", "precision": "fp64" if precision == _abi.B2S_PRECISION_FP64 else "mixed",
         }
     finally:
