@@ -62,6 +62,15 @@ int         b2s_version(void);
  * reference's exactly; the sums are deterministic. */
 int b2s_assemble(b2s_solver* s, int32_t n_block_rows, int64_t n_triplets,
                  const int32_t* d_rows, const int32_t* d_cols, const double* d_vals);
+/* Triplet arrays owned by the solver, for producers that write the raw
+ * triplets in place (no staging copy): device pointers to room for
+ * n_triplets (row, col, 9 values column-major), grown by ratio and kept
+ * across calls; b2s_assemble_owned assembles the first n_triplets of them.
+ * Replaces the staging of GlobalLinearSystem::Impl::_assemble_linear_system
+ * (src/backends/cuda/linear_system/global_linear_system.cu:233-268, 407-497):
+ * the subsystems' producers write their triplet sub-ranges here directly. */
+int b2s_triplet_buffers(b2s_solver* s, int64_t n_triplets, int32_t** d_rows, int32_t** d_cols, double** d_vals);
+int b2s_assemble_owned(b2s_solver* s, int32_t n_block_rows, int64_t n_triplets);
 int b2s_matrix_info(const b2s_solver* s, int32_t* n_block_rows, int64_t* n_upper_blocks);
 /* Copy the block-upper BSR out: rowptr [n_block_rows+1], colidx [nnz],
  * vals [nnz*9] column-major. Any pointer may be NULL; "any" memory. */

@@ -110,6 +110,8 @@ SIGNATURES = {
     "b2s_set_stream": (C.c_int, [vp, vp]),
     "b2s_version": (C.c_int, []),
     "b2s_assemble": (C.c_int, [vp, i32, i64, vp, vp, vp]),
+    "b2s_triplet_buffers": (C.c_int, [vp, i64, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+    "b2s_assemble_owned": (C.c_int, [vp, i32, i64]),
     "b2s_matrix_info": (C.c_int, [vp, i32p, i64p]),
     "b2s_get_upper_bsr": (C.c_int, [vp, vp, vp, vp]),
     "b2s_spmv": (C.c_int, [vp, vp, vp, dp]),

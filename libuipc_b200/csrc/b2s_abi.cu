@@ -164,6 +164,36 @@ int b2s_assemble(b2s_solver* s, int32_t nb, int64_t T, const int32_t* rows, cons
                    });
 }
 
+int b2s_triplet_buffers(b2s_solver* s, int64_t T, int32_t** d_rows, int32_t** d_cols, double** d_vals)
+{
+    return guarded(s,
+                   [&]
+                   {
+                       B2S_REQUIRE(T >= 0, B2S_ERR_ARGUMENT, "negative triplet count");
+                       B2S_REQUIRE(d_rows && d_cols && d_vals, B2S_ERR_ARGUMENT, "null output pointer");
+                       B2S_CUDA(cudaSetDevice(s->device));
+                       const size_t n = (size_t)std::max<int64_t>(T, 1);
+                       s->own_rows.resize(n, 1.1);
+                       s->own_cols.resize(n, 1.1);
+                       s->own_vals.resize(9 * n, 1.1);
+                       *d_rows = s->own_rows.data();
+                       *d_cols = s->own_cols.data();
+                       *d_vals = s->own_vals.data();
+                   });
+}
+
+int b2s_assemble_owned(b2s_solver* s, int32_t nb, int64_t T)
+{
+    if(!s)
+        return B2S_ERR_ARGUMENT;
+    if(T > (int64_t)s->own_rows.size() || (T > 0 && s->own_vals.size() < 9 * (size_t)T))
+    {
+        s->last_error = "b2s_assemble_owned: more triplets than b2s_triplet_buffers provided";
+        return B2S_ERR_ARGUMENT;
+    }
+    return b2s_assemble(s, nb, T, s->own_rows.data(), s->own_cols.data(), s->own_vals.data());
+}
+
 int b2s_matrix_info(const b2s_solver* s, int32_t* nb, int64_t* nnz)
 {
     if(!s)

@@ -252,6 +252,10 @@ struct b2s_solver
     cudaEvent_t              ev_begin = nullptr, ev_end = nullptr;
     std::vector<cudaEvent_t> iter_events;  // 4 per iteration of a graph block
     b2s::LearnedState*       ws = nullptr;  // learned warm start, created on first use
+    // triplet arrays owned by the solver (b2s_triplet_buffers): producers
+    // write the raw triplets here, b2s_assemble_owned reads them in place
+    b2s::DBuf<int32_t>       own_rows, own_cols;
+    b2s::DBuf<double>        own_vals;
 };
 
 namespace b2s

@@ -85,6 +85,19 @@ class GpuTetMesh:
             raise RuntimeError("b2gen_system: " + lib.b2gen_last_error().decode())
         return self.rows, self.cols, self.vals, self.grad
 
+    def system_into(self, x, x_tilde, rows_ptr: int, cols_ptr: int, vals_ptr: int, stream=None):
+        """The Newton system written to the given device addresses (e.g. the
+        solver-owned triplet arrays of Solver.triplet_buffers); returns b."""
+        x = x.contiguous()
+        x_tilde = x_tilde.contiguous()
+        st = stream if stream is not None else self.torch.cuda.current_stream(self.dev).cuda_stream
+        lib = _lib()
+        rc = lib.b2gen_system(self.h, x.data_ptr(), x_tilde.data_ptr(), rows_ptr, cols_ptr, vals_ptr,
+                              self.grad.data_ptr(), st)
+        if rc != 0:
+            raise RuntimeError("b2gen_system: " + lib.b2gen_last_error().decode())
+        return self.grad
+
     def close(self):
         if self.h:
             _lib().b2gen_mesh_destroy(self.h)

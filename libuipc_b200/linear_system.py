@@ -75,6 +75,17 @@ class Solver:
         T = int(rows.numel())
         self._check(self.lib.b2s_assemble(self.h, int(n_block_rows), T, _ptr(rows), _ptr(cols), _ptr(vals)))
 
+    def triplet_buffers(self, n_triplets: int):
+        """Device addresses (rows, cols, vals) of solver-owned room for
+        n_triplets raw triplets (b2s_triplet_buffers): producers write there
+        and :meth:`assemble_owned` assembles in place."""
+        r, c, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        self._check(self.lib.b2s_triplet_buffers(self.h, int(n_triplets), C.byref(r), C.byref(c), C.byref(v)))
+        return r.value, c.value, v.value
+
+    def assemble_owned(self, n_block_rows: int, n_triplets: int) -> None:
+        self._check(self.lib.b2s_assemble_owned(self.h, int(n_block_rows), int(n_triplets)))
+
     def matrix_info(self):
         nb = C.c_int32()
         nnz = C.c_int64()

@@ -65,3 +65,29 @@ def test_cube_on_ground(solver, cuda):
         _compare(solver, cuda, s_cpu, mesh.system(x, to_dev(xt.ravel(), cuda)))
     finally:
         mesh.close()
+
+
+def test_generator_writes_into_solver_owned_triplets(solver, cuda):
+    """b2s_triplet_buffers + b2s_assemble_owned: the producer writes in place
+    (no staging copy) and the assembled matrix is the same."""
+    from libuipc_b200.gpu_scene import GpuTetMesh
+    from libuipc_b200.sequence import SceneSequence
+
+    seq = SceneSequence(scene=2, cells_x=12, cells_y=3, cells_z=3, E=1e6, nu=0.49, twist_per_step=2.0)
+    seq.begin_step()
+    s = seq.system()
+    mesh = GpuTetMesh(seq.rest, s.tets, s.config, cuda, fixed=seq.fixed)
+    try:
+        x, xt = to_dev(seq.x.ravel(), cuda), to_dev(seq.x_tilde.ravel(), cuda)
+        rows, cols, vals, _ = mesh.system(x, xt)
+        solver.assemble(s.n_verts, rows, cols, vals)
+        ref = solver.upper_bsr()
+        r_ptr, c_ptr, v_ptr = solver.triplet_buffers(mesh.n_triplets)
+        mesh.system_into(x, xt, r_ptr, c_ptr, v_ptr)
+        solver.assemble_owned(s.n_verts, mesh.n_triplets)
+        got = solver.upper_bsr()
+        assert all(np.array_equal(a, b) for a, b in zip(ref, got))
+        with pytest.raises(RuntimeError):
+            solver.assemble_owned(s.n_verts, mesh.n_triplets * 2)  # more than the buffers hold
+    finally:
+        mesh.close()
