@@ -220,7 +220,8 @@ int b2s_reset_timers(b2s_solver* s);
  * linear_fused_pcg.cu:1782-2005). A small MLP on MAS level-1 aggregates
  * predicts the initial guess of the next Newton solve from the gradient b and
  * the solutions of earlier solves of the same run (history h1 = the latest,
- * h2, h3 older; at most B2S_WS_HISTORY device vectors of 3 n doubles).
+ * h2, h3, ... older; at most B2S_WS_MAX_HISTORY device vectors of 3 n
+ * doubles, of which the newest B2S_WS_HISTORY feed the network's fields).
  * Per aggregate, the network reads 22 features (mean of b, and of each field
  * f = {h1, h1 - h2, h1 - 2 h2 + h3, z = P b}: its mean and log RMS, plus the
  * mean products of consecutive fields) and outputs 4 coefficients c; the
@@ -232,19 +233,20 @@ int b2s_reset_timers(b2s_solver* s);
  * loss sum_v |d_v - x_v|^2 / sum_v |x_v|^2 (fields scaled by RMS(z)), Adam,
  * FP32 weights; inference reads BF16 copies of the weights. Requires an
  * assembled matrix and the MAS preconditioner (b2s_precond_assemble). */
-#define B2S_WS_HISTORY 3
+#define B2S_WS_HISTORY 3     /* history vectors the network's fields read */
+#define B2S_WS_MAX_HISTORY 8 /* history vectors a start may combine */
 #define B2S_WS_FEATURES 22
 #define B2S_WS_OUTPUTS 4
 #define B2S_WS_MODE_ZERO 0    /* x0 = 0 */
 #define B2S_WS_MODE_PREV 1    /* Galerkin on {h1}: the scaled previous solution */
-#define B2S_WS_MODE_HISTORY 2 /* Galerkin on {h1, h2, h3}, no network */
-#define B2S_WS_MODE_LEARNED 3 /* Galerkin on {network field, h1, h2, h3} */
+#define B2S_WS_MODE_HISTORY 2 /* Galerkin on the history {h1, ..., h_n}, no network */
+#define B2S_WS_MODE_LEARNED 3 /* Galerkin on {network field, h1, ..., h_n} */
 
 typedef struct b2s_ws_info
 {
     int    mode;          /* mode used (ZERO when the residual check rejected the start) */
     int    n_candidates;  /* vectors in the Galerkin combination */
-    double coeff[4];      /* their coefficients */
+    double coeff[1 + B2S_WS_MAX_HISTORY]; /* their coefficients */
     double rel_res0;      /* ||b - A x0|| / ||b|| of the returned x0 (FP64) */
     double rel_res_tried; /* the same for the candidate before the check */
     double rz_ratio;      /* (r^T P r) / (b^T P b) of the candidate, r = b - A x0, P the preconditioner:

@@ -29,6 +29,7 @@ B2S_WS_MODE_PREV = 1
 B2S_WS_MODE_HISTORY = 2
 B2S_WS_MODE_LEARNED = 3
 B2S_WS_HISTORY = 3
+B2S_WS_MAX_HISTORY = 8
 B2S_WS_FEATURES = 22
 B2S_WS_OUTPUTS = 4
 
@@ -37,7 +38,7 @@ class WsInfo(C.Structure):
     _fields_ = [
         ("mode", C.c_int32),
         ("n_candidates", C.c_int32),
-        ("coeff", C.c_double * 4),
+        ("coeff", C.c_double * (1 + 8)),
         ("rel_res0", C.c_double),
         ("rel_res_tried", C.c_double),
         ("rz_ratio", C.c_double),

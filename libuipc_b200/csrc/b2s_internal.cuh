@@ -280,7 +280,7 @@ int  reduction_grid();
 void launch_dot(b2s_solver* s, const double* a, const double* b, int64_t n, double* d_out);
 // several dot products in one pass: d_out[k] = a[k] . b[k], k < m (FP64,
 // deterministic)
-constexpr int MAX_DOTS = 6;
+constexpr int MAX_DOTS = 10;
 struct DotPairs
 {
     const double* a[MAX_DOTS];

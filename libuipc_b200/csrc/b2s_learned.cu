@@ -33,6 +33,7 @@
 #include <cstring>
 #include <numeric>
 #include <random>
+#include <type_traits>
 #include <vector>
 
 namespace b2s
@@ -725,20 +726,22 @@ __global__ void k_ws_combine(int64_t n, int vn, int off, int L, int level1_begin
     }
 }
 
-// x = sum_k alpha_k c_k (k < nc, nc <= 4)
-__global__ void k_ws_lincomb(int64_t n, int nc, const double* __restrict__ c0, const double* __restrict__ c1,
-                             const double* __restrict__ c2, const double* __restrict__ c3, double a0, double a1,
-                             double a2, double a3, double* __restrict__ x)
+// the candidate starts of one prediction: the network field and the history
+constexpr int WS_MAXC = 1 + B2S_WS_MAX_HISTORY;
+struct Cands
+{
+    const double* c[WS_MAXC];
+    double        a[WS_MAXC];
+};
+
+// x = sum_k alpha_k c_k (k < nc)
+__global__ void k_ws_lincomb(int64_t n, int nc, Cands cs, double* __restrict__ x)
 {
     for(int64_t i = (int64_t)blockIdx.x * WS_BLOCK + threadIdx.x; i < n; i += (int64_t)gridDim.x * WS_BLOCK)
     {
-        double v = a0 * c0[i];
-        if(nc > 1)
-            v += a1 * c1[i];
-        if(nc > 2)
-            v += a2 * c2[i];
-        if(nc > 3)
-            v += a3 * c3[i];
+        double v = cs.a[0] * cs.c[0][i];
+        for(int k = 1; k < nc; ++k)
+            v += cs.a[k] * cs.c[k][i];
         x[i] = v;
     }
 }
@@ -748,11 +751,6 @@ __global__ void k_ws_lincomb(int64_t n, int nc, const double* __restrict__ c0, c
 // product vectors: with u_k = B c_k(col), a block B at (row, col) adds
 // c_i(row) . u_j and, off the diagonal (the transposed block), u_i . c_j(row).
 // FP64, fixed grid and order: deterministic.
-struct Cands
-{
-    const double* c[4];
-};
-
 template <int K>
 __global__ void __launch_bounds__(RED_BLOCK) k_ws_gram(int64_t U, int64_t S, const int32_t* __restrict__ rows,
                                                        const int32_t* __restrict__ cols,
@@ -855,7 +853,7 @@ int system_aggregates(b2s_solver* s, const double* b, int n_hist, const double* 
     const MasGeom g  = mas_geom(s);
     cudaStream_t  st = s->stream;
     const int64_t n  = 3 * (int64_t)s->A.nb;
-    B2S_REQUIRE(n_hist >= 0 && n_hist <= B2S_WS_HISTORY, B2S_ERR_ARGUMENT, "history length outside [0, 3]");
+    B2S_REQUIRE(n_hist >= 0 && n_hist <= B2S_WS_MAX_HISTORY, B2S_ERR_ARGUMENT, "history length outside [0, 8]");
     for(int i = 0; i < n_hist; ++i)
         B2S_REQUIRE(hist && hist[i], B2S_ERR_ARGUMENT, "null history vector");
     W.fields.resize((size_t)WS_FIELDS * n);
@@ -975,7 +973,7 @@ void forward_backward(b2s_solver* s, const WsSample& smp, bool want_grad)
 // diagonally scaled matrix
 void small_pinv_solve(int k, const double* G, const double* g, double* alpha)
 {
-    double a[16], v[16], d[4];
+    double a[WS_MAXC * WS_MAXC], v[WS_MAXC * WS_MAXC], d[WS_MAXC];
     for(int i = 0; i < k; ++i)
         d[i] = G[i * k + i] > 0 ? 1.0 / std::sqrt(G[i * k + i]) : 0.0;
     for(int i = 0; i < k; ++i)
@@ -1024,7 +1022,7 @@ void small_pinv_solve(int k, const double* G, const double* g, double* alpha)
     double lmax = 0.0;
     for(int i = 0; i < k; ++i)
         lmax = std::max(lmax, a[i * k + i]);
-    double gs[4];
+    double gs[WS_MAXC];
     for(int i = 0; i < k; ++i)
         gs[i] = g[i] * d[i];
     for(int i = 0; i < k; ++i)
@@ -1245,7 +1243,7 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
     B2S_REQUIRE(mode >= B2S_WS_MODE_ZERO && mode <= B2S_WS_MODE_LEARNED, B2S_ERR_ARGUMENT, "unknown warm-start mode");
     B2S_REQUIRE(b && x0, B2S_ERR_ARGUMENT, "null b or x0");
     B2S_REQUIRE(s->A.valid, B2S_ERR_STATE, "no assembled matrix");
-    B2S_REQUIRE(n_hist >= 0 && n_hist <= B2S_WS_HISTORY, B2S_ERR_ARGUMENT, "history length outside [0, 3]");
+    B2S_REQUIRE(n_hist >= 0 && n_hist <= B2S_WS_MAX_HISTORY, B2S_ERR_ARGUMENT, "history length outside [0, 8]");
     for(int i = 0; i < n_hist; ++i)
         B2S_REQUIRE(hist && hist[i], B2S_ERR_ARGUMENT, "null history vector");
     b2s_ws_info out{};
@@ -1316,30 +1314,34 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
     if(k > 0)
     {
         // Galerkin: G alpha = g, G_kl = c_k . A c_l (one pass over the
-        // matrix), g_k = c_k . b and b . b (one pass over the vectors), FP64
+        // matrix), g_k = c_k . b and b . b (one pass over the vectors), FP64.
+        // dots: [0, 45) the Gram's upper triangle, [48, 48 + k] the right-hand
+        // side and b . b, [60, 63) the acceptance check
         W.Ac.resize((size_t)4 * n);
-        W.dots.resize(32);
+        W.dots.resize(64);
         const Matrix& A    = s->A;
         const int     grid = reduction_grid();
-        ensure_reduction(s->red, grid, 10);
+        ensure_reduction(s->red, grid, WS_MAXC * (WS_MAXC + 1) / 2);
         Cands cs{};
-        for(int i = 0; i < 4; ++i)
+        for(int i = 0; i < WS_MAXC; ++i)
             cs.c[i] = cand[i < k ? i : 0];
         double* gram = W.dots.data();
+        auto    gram_launch = [&](auto K) {
+            constexpr int KK = decltype(K)::value;
+            k_ws_gram<KK><<<grid, RED_BLOCK, 0, st>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(), A.vals.data(),
+                                                      cs, s->red.partials.data(), s->red.counter.data(), gram);
+        };
         switch(k)
         {
-        case 1: k_ws_gram<1><<<grid, RED_BLOCK, 0, st>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(),
-                                                          A.vals.data(), cs, s->red.partials.data(),
-                                                          s->red.counter.data(), gram); break;
-        case 2: k_ws_gram<2><<<grid, RED_BLOCK, 0, st>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(),
-                                                          A.vals.data(), cs, s->red.partials.data(),
-                                                          s->red.counter.data(), gram); break;
-        case 3: k_ws_gram<3><<<grid, RED_BLOCK, 0, st>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(),
-                                                          A.vals.data(), cs, s->red.partials.data(),
-                                                          s->red.counter.data(), gram); break;
-        default: k_ws_gram<4><<<grid, RED_BLOCK, 0, st>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(),
-                                                           A.vals.data(), cs, s->red.partials.data(),
-                                                           s->red.counter.data(), gram); break;
+        case 1: gram_launch(std::integral_constant<int, 1>{}); break;
+        case 2: gram_launch(std::integral_constant<int, 2>{}); break;
+        case 3: gram_launch(std::integral_constant<int, 3>{}); break;
+        case 4: gram_launch(std::integral_constant<int, 4>{}); break;
+        case 5: gram_launch(std::integral_constant<int, 5>{}); break;
+        case 6: gram_launch(std::integral_constant<int, 6>{}); break;
+        case 7: gram_launch(std::integral_constant<int, 7>{}); break;
+        case 8: gram_launch(std::integral_constant<int, 8>{}); break;
+        default: gram_launch(std::integral_constant<int, WS_MAXC>{}); break;
         }
         B2S_CHECK_LAUNCH();
         DotPairs dp{};
@@ -1349,27 +1351,27 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
             dp.b[i] = b;
         }
         dp.a[k] = dp.b[k] = b;
-        launch_dots(s, n, dp, k + 1, W.dots.data() + 16);
-        double hd[32];
-        B2S_CUDA(cudaMemcpyAsync(hd, W.dots.data(), sizeof(double) * 32, cudaMemcpyDeviceToHost, st));
+        launch_dots(s, n, dp, k + 1, W.dots.data() + 48);
+        double hd[64];
+        B2S_CUDA(cudaMemcpyAsync(hd, W.dots.data(), sizeof(hd), cudaMemcpyDeviceToHost, st));
         B2S_CUDA(cudaStreamSynchronize(st));
-        double G[16], gv[4], alpha[4] = {0, 0, 0, 0};
+        double G[WS_MAXC * WS_MAXC], gv[WS_MAXC], alpha[WS_MAXC] = {};
         for(int i = 0, q = 0; i < k; ++i)
         {
             for(int j = i; j < k; ++j, ++q)
                 G[i * k + j] = G[j * k + i] = hd[q];
-            gv[i] = hd[16 + i];
+            gv[i] = hd[48 + i];
         }
         small_pinv_solve(k, G, gv, alpha);
-        const double bb = hd[16 + k];
+        const double bb = hd[48 + k];
         bool finite = std::isfinite(bb);
         for(int i = 0; i < k; ++i)
             finite = finite && std::isfinite(alpha[i]);
         if(finite && bb > 0)
         {
-            k_ws_lincomb<<<ws_grid(n), WS_BLOCK, 0, st>>>(n, k, cand[0], k > 1 ? cand[1] : cand[0],
-                                                         k > 2 ? cand[2] : cand[0], k > 3 ? cand[3] : cand[0],
-                                                         alpha[0], alpha[1], alpha[2], alpha[3], x0);
+            for(int i = 0; i < k; ++i)
+                cs.a[i] = alpha[i];
+            k_ws_lincomb<<<ws_grid(n), WS_BLOCK, 0, st>>>(n, k, cs, x0);
             B2S_CHECK_LAUNCH();
             // FP64 residual of the candidate start, r = b - A x0
             double* Ax = W.Ac.data();
@@ -1398,9 +1400,9 @@ void ws_predict(b2s_solver* s, int mode, const double* b, int n_hist, const doub
             dc.b[1] = zr;
             dc.a[2] = b;
             dc.b[2] = zb;
-            launch_dots(s, n, dc, 3, W.dots.data() + 24);
+            launch_dots(s, n, dc, 3, W.dots.data() + 60);
             double h3[3];
-            B2S_CUDA(cudaMemcpyAsync(h3, W.dots.data() + 24, sizeof(h3), cudaMemcpyDeviceToHost, st));
+            B2S_CUDA(cudaMemcpyAsync(h3, W.dots.data() + 60, sizeof(h3), cudaMemcpyDeviceToHost, st));
             B2S_CUDA(cudaStreamSynchronize(st));
             const double rr = h3[0], rz = h3[1], bz = h3[2];
             out.rel_res_tried = std::sqrt(rr / bb);

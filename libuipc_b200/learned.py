@@ -50,9 +50,14 @@ class RunLog:
 class SequenceRunner:
     """Solve the Newton systems of ``seq`` with ``solver`` (MAS-PCG on one
     GPU). ``truth_tol``: FP64 relative residual of the solve that advances the
-    run (and labels the training samples)."""
+    run (and labels the training samples); ``history``: solutions kept per
+    Newton-iteration slot for the starts (at most B2S_WS_MAX_HISTORY; the
+    network's fields read the newest 3). A run whose motion is smooth in time
+    (a driven twist) gains from a long history, one dominated by contacts
+    (a falling stack) from 3 at most."""
 
-    def __init__(self, solver: Solver, seq: SceneSequence, device, truth_tol: float = 1e-10):
+    def __init__(self, solver: Solver, seq: SceneSequence, device, truth_tol: float = 1e-10,
+                 history: int = _abi.B2S_WS_MAX_HISTORY):
         import torch
 
         self.torch = torch
@@ -60,6 +65,7 @@ class SequenceRunner:
         self.seq = seq
         self.dev = device
         self.truth_tol = truth_tol
+        self.keep = max(1, min(int(history), _abi.B2S_WS_MAX_HISTORY))
         self.p2r, self.r2p = partition_maps(partition_rcb(seq.rest))
         self.s.mas_init(0, seq.n_verts, seq.adj_start, seq.adj_list, self.p2r, self.r2p)
         self.history: dict[int, deque] = {}
@@ -109,7 +115,7 @@ class SequenceRunner:
                             x0_given=True)
             if collect:
                 self.s.ws_add_sample(b, x, self.hist(k))
-            d = self.history.setdefault(k, deque(maxlen=_abi.B2S_WS_HISTORY))
+            d = self.history.setdefault(k, deque(maxlen=self.keep))
             d.appendleft(x)
             return x.cpu().numpy()
 
@@ -188,7 +194,7 @@ def run_gpu_bar(device, cells=(200, 20, 20), E: float = 1e6, nu: float = 0.49, t
                 solver.pcg(b, x, tol=truth_tol, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, x0_given=True)
                 if collect:
                     solver.ws_add_sample(b, x, hist)
-                history.setdefault(k, deque(maxlen=_abi.B2S_WS_HISTORY)).appendleft(x)
+                history.setdefault(k, deque(maxlen=_abi.B2S_WS_MAX_HISTORY)).appendleft(x)
                 seq.apply(x)
 
         t0 = time.time()

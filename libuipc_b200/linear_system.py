@@ -198,7 +198,7 @@ class Solver:
     # ---- learned warm start (no counterpart in the reference) ---------------
     @staticmethod
     def _hist(history):
-        history = [h for h in (history or []) if h is not None][: _abi.B2S_WS_HISTORY]
+        history = [h for h in (history or []) if h is not None][: _abi.B2S_WS_MAX_HISTORY]
         arr = (C.c_void_p * max(len(history), 1))(*[h.data_ptr() for h in history])
         return len(history), arr
 
@@ -457,7 +457,7 @@ class B200PCG(IterativeSolver):
         info.iter_count = int(self.last_stats["iterations"])
         if self.warm_start != "zero":
             hist.insert(0, info.x.clone())
-            del hist[_abi.B2S_WS_HISTORY:]
+            del hist[_abi.B2S_WS_MAX_HISTORY:]
 
 
 class GlobalLinearSystem:
