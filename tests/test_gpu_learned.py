@@ -165,3 +165,41 @@ def test_learned_start_beats_plain_starts(solver, cuda):
     assert learned < 0.5 * zero
     assert learned < prev
     assert learned <= hist + 2
+
+
+def test_longer_history_on_a_driven_bar(solver, cuda):
+    """The Galerkin start over up to 8 past solutions (B2S_WS_MAX_HISTORY):
+    on a smoothly driven run it needs no more PCG iterations than over the 3
+    latest (here several times fewer), and a ninth history vector is refused."""
+    import torch
+
+    from libuipc_b200.learned import SequenceRunner
+    from libuipc_b200.sequence import SceneSequence
+
+    means = {}
+    for keep in (3, 8):
+        seq = SceneSequence(scene=2, cells_x=40, cells_y=6, cells_z=6, E=1e6, nu=0.49, twist_per_step=2.0)
+        run = SequenceRunner(solver, seq, cuda, history=keep)
+        run.run(10, newton_iters=1, collect=False)
+        log = run.run(6, newton_iters=1, collect=False, eval_modes=("history",))
+        assert all(r.rel_res <= 1e-4 for r in log.records)
+        means[keep] = log.mean_iterations("history")
+        if keep == 8:
+            assert len(run.hist(0)) == 8
+            import ctypes as C
+
+            from libuipc_b200 import _abi
+
+            b = torch.ones(3 * seq.n_verts, dtype=torch.float64, device=cuda)
+            x = torch.zeros_like(b)
+            nine = run.hist(0) + [b]
+            arr = (C.c_void_p * 9)(*[h.data_ptr() for h in nine])
+            info = _abi.WsInfo()
+            rc = solver.lib.b2s_ws_predict(solver.h, _abi.B2S_WS_MODE_HISTORY, C.c_void_p(b.data_ptr()), 9,
+                                           C.cast(arr, C.c_void_p), C.c_void_p(x.data_ptr()), C.byref(info))
+            assert rc == _abi.B2S_ERR_ARGUMENT
+            assert b"history length" in solver.lib.b2s_last_error(solver.h)
+            # the Python wrapper keeps the newest 8
+            assert solver.ws_predict(b, x, nine, _abi.B2S_WS_MODE_HISTORY)["n_candidates"] <= 8
+    print(f"history start: 3 latest {means[3]:.1f}, 8 latest {means[8]:.1f} PCG iterations")
+    assert means[8] <= means[3]
