@@ -82,6 +82,11 @@ int b2s_get_upper_bsr(b2s_solver* s, int32_t* rowptr, int32_t* colidx, double* v
  * (src/backends/cuda/linear_system/spmv.cu:992-1160) as used by
  * IterativeSolver::spmv / spmv_dot (src/backends/cuda/linear_system/iterative_solver.h:30-40). */
 int b2s_spmv(b2s_solver* s, const double* d_x, double* d_y, double* h_dot /* may be NULL */);
+/* The same y = A x as the mixed-precision PCG computes it: FP32 copy of the
+ * values, FP32 vectors [3 * n_block_rows], FP32 products and sums (y's
+ * reductions in any order), x . y accumulated in FP64 (h_dot, host, may be
+ * NULL). No counterpart in the reference (which runs the SpMV in FP64 only). */
+int b2s_spmv_mixed(b2s_solver* s, const float* d_x, float* d_y, double* h_dot /* may be NULL */);
 
 /* ---- MAS preconditioner ----------------------------------------------------------
  * Initialisation: replaces FEMMASPreconditioner::do_init ->

@@ -247,6 +247,22 @@ int b2s_spmv(b2s_solver* s, const double* x, double* y, double* h_dot)
                    });
 }
 
+int b2s_spmv_mixed(b2s_solver* s, const float* x, float* y, double* h_dot)
+{
+    return guarded(s,
+                   [&]
+                   {
+                       B2S_REQUIRE(s->A.valid, B2S_ERR_STATE, "no assembled matrix");
+                       B2S_REQUIRE(x && y, B2S_ERR_ARGUMENT, "null vector");
+                       s->dot_out.resize(4);
+                       b2s::spmv_mixed(s, x, y, s->dot_out.data());
+                       if(h_dot)
+                           B2S_CUDA(cudaMemcpyAsync(h_dot, s->dot_out.data(), sizeof(double), cudaMemcpyDeviceToHost,
+                                                    s->stream));
+                       B2S_CUDA(cudaStreamSynchronize(s->stream));
+                   });
+}
+
 int b2s_mas_init(b2s_solver* s, int32_t off, int32_t vn, const int32_t* adj_start, const int32_t* adj_list,
                  int32_t N, const int32_t* p2r, const int32_t* r2p)
 {

@@ -295,6 +295,7 @@ void precond_assemble(b2s_solver* s, int kind, int invert_mode);
 void precond_apply(b2s_solver* s, const double* r, double* z);
 void precond_launch(b2s_solver* s, const double* r, double* z);  // queued, no sync
 void precond_apply_mixed(b2s_solver* s, const float* r, float* z);
+void spmv_mixed(b2s_solver* s, const float* x, float* y, double* d_dot);
 void check_device_errors(b2s_solver* s);
 
 // message of the last failed call made without a solver handle (read back

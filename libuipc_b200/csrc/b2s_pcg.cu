@@ -33,7 +33,6 @@ void mas_apply_levels_f32(b2s_solver* s, const float* r, const int* converged, b
 void mas_pack_bf16(b2s_solver* s);
 void spmv_f32_launch(b2s_solver* s, const Matrix& A, const float* x, float* y, Reduction& red, double* d_dot,
                      const int* stop);
-void spmv_prepare_f32(b2s_solver* s);
 void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st_out);
 
 namespace
@@ -597,6 +596,18 @@ struct GraphKey
 };
 }  // namespace
 
+// a stage-timing event: an external event node when the stream is being
+// captured into the PCG graph, a plain stream event otherwise
+static cudaError_t record_timing_event(cudaEvent_t ev, cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t             e  = cudaStreamIsCapturing(st, &cs);
+    if(e != cudaSuccess)
+        return e;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal)
+                                               : cudaEventRecord(ev, st);
+}
+
 // one PCG iteration; with timing on, `slot` selects the 4 events that
 // bracket its SpMV and its preconditioner apply
 static void pcg_iteration(b2s_solver* s, int kind, double* x, int slot)
@@ -607,17 +618,17 @@ static void pcg_iteration(b2s_solver* s, int kind, double* x, int slot)
     const int64_t n  = 3 * (int64_t)A.nb;
     cudaEvent_t*  ev = s->timing ? &s->iter_events[(size_t)slot * 4] : nullptr;
     if(ev)
-        B2S_CUDA(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
+        B2S_CUDA(record_timing_event(ev[0], st));
     spmv_f64_launch(s, A, P.p.data(), P.Ap.data(), P.red, &P.sc.data()->pAp, &P.sc.data()->converged);
     if(ev)
-        B2S_CUDA(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
+        B2S_CUDA(record_timing_event(ev[1], st));
     k_update_xr<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), x, P.p.data(), P.r.data(), P.Ap.data());
     B2S_CHECK_LAUNCH();
     if(ev)
-        B2S_CUDA(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
+        B2S_CUDA(record_timing_event(ev[2], st));
     precond_launch(s, kind, P.r.data(), P.z.data(), P.sc.data(), P.red);
     if(ev)
-        B2S_CUDA(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
+        B2S_CUDA(record_timing_event(ev[3], st));
     k_update_p<<<vec_grid(n), VEC_BLOCK, 0, st>>>(n, P.sc.data(), P.z.data(), P.p.data());
     B2S_CHECK_LAUNCH();
 }
@@ -915,6 +926,39 @@ static void ensure_bf16_inverses(b2s_solver* s)
     }
 }
 
+// the FP32 copy of the value planes the mixed PCG's SpMV reads (once per assembly)
+static void ensure_f32_planes(b2s_solver* s)
+{
+    Matrix& A = s->A;
+    if(A.vals32_generation == A.generation)
+        return;
+    A.vals32.resize((size_t)9 * A.stride, 1.2);
+    k_planes_f32<<<vec_grid(9 * A.stride), VEC_BLOCK, 0, s->stream>>>(9 * A.stride, A.vals.data(), A.vals32.data());
+    B2S_CHECK_LAUNCH();
+    A.vals32_generation = A.generation;
+}
+
+// y = A x as the mixed PCG computes it (FP32 planes and products, x.(A x) in
+// FP64 into d_dot, device); x, y: 3 floats per node, padded around the product
+void spmv_mixed(b2s_solver* s, const float* x, float* y, double* d_dot)
+{
+    Matrix&       A  = s->A;
+    PcgState&     P  = s->pcg;
+    const int32_t nb = A.nb;
+    cudaStream_t  st = s->stream;
+    ensure_f32_planes(s);
+    ensure_reduction(P.red, std::max(spmv_grid(A.nnz), reduction_grid()), 2);
+    P.p32.resize(4 * (size_t)nb, 1.1);
+    P.Ap32.resize(4 * (size_t)nb, 1.1);
+    k_pad4<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(nb, x, P.p32.data());
+    B2S_CHECK_LAUNCH();
+    B2S_CUDA(cudaMemsetAsync(P.Ap32.data(), 0, sizeof(float) * 4 * (size_t)nb, st));
+    B2S_CUDA(cudaMemsetAsync(d_dot, 0, sizeof(double), st));  // stays 0 for an empty matrix
+    spmv_f32_launch(s, A, P.p32.data(), P.Ap32.data(), P.red, d_dot, nullptr);
+    k_unpad4<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(nb, P.Ap32.data(), y);
+    B2S_CHECK_LAUNCH();
+}
+
 // r, z: 3 floats per node (the ABI's layout), padded around the apply
 void precond_apply_mixed(b2s_solver* s, const float* r, float* z)
 {
@@ -941,18 +985,18 @@ static void pcg_iteration_mixed(b2s_solver* s, int kind, double* x, int slot)
     const int32_t nb = A.nb;
     cudaEvent_t*  ev = s->timing ? &s->iter_events[(size_t)slot * 4] : nullptr;
     if(ev)
-        B2S_CUDA(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
+        B2S_CUDA(record_timing_event(ev[0], st));
     spmv_f32_launch(s, A, P.p32.data(), P.Ap32.data(), P.red, &P.sc.data()->pAp, &P.sc.data()->converged);
     if(ev)
-        B2S_CUDA(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
+        B2S_CUDA(record_timing_event(ev[1], st));
     k_update_xr_mixed4<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(nb, P.sc.data(), x, P.p32.data(), P.r32.data(),
                                                            P.Ap32.data());
     B2S_CHECK_LAUNCH();
     if(ev)
-        B2S_CUDA(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
+        B2S_CUDA(record_timing_event(ev[2], st));
     precond_launch_f32(s, kind, P.r32.data(), P.z32.data(), P.sc.data(), P.red);
     if(ev)
-        B2S_CUDA(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
+        B2S_CUDA(record_timing_event(ev[3], st));
     k_update_p_mixed4<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(4 * (int64_t)nb, P.sc.data(), P.z32.data(),
                                                          P.p32.data());
     B2S_CHECK_LAUNCH();
@@ -991,7 +1035,6 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
     ensure_reduction(P.red, std::max(spmv_grid(A.nnz), reduction_grid()), 2);
     ensure_reduction(s->red, reduction_grid(), 2);
     device_error_flag(s);
-    spmv_prepare_f32(s);  // kernel attributes set before any graph capture
     s->dot_out.resize(4);
     B2S_REQUIRE(A.nnz == 0 || A.has_trank, B2S_ERR_STATE, "matrix lacks the SpMV tile ranks");
     const int     ci       = o.check_interval > 0 ? o.check_interval : 1;
@@ -999,13 +1042,7 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
     int           kind     = s->precond_kind;
 
     // FP32 matrix planes, BF16 MAS inverses (once per assembly / build)
-    if(A.vals32_generation != A.generation)
-    {
-        A.vals32.resize((size_t)9 * A.stride, 1.2);
-        k_planes_f32<<<vec_grid(9 * A.stride), VEC_BLOCK, 0, st>>>(9 * A.stride, A.vals.data(), A.vals32.data());
-        B2S_CHECK_LAUNCH();
-        A.vals32_generation = A.generation;
-    }
+    ensure_f32_planes(s);
     ensure_bf16_inverses(s);
 
     // r = b - A x0 (FP64), stored FP32

@@ -6,25 +6,24 @@
 // adds B x_j to y_i and, off the diagonal, B^T x_i to y_j; the dot is
 // sum (2 - delta_ij) x_i^T B x_j.
 //
-// Design: persistent CTAs walk SPMV_TILE-block tiles of the row-sorted block
-// stream. Each thread owns SPMV_BPT consecutive blocks and reads their row and
-// column ids, tile ranks and the 9 value planes with 16-byte vector loads
-// (the planes are padded to a multiple of 16 blocks). The row halves B x_j of
-// a thread's blocks are merged in registers (runs of equal rows) and each run
-// goes to y with one fire-and-forget reduction per component (red.global,
-// resolved in L2). The transposed halves B^T x_i are placed in shared memory
-// at the block's precomputed rank in (column, index) order; after a barrier
-// each thread merges its SPMV_BPT consecutive slots, so runs of equal columns
-// also leave as one reduction each. With FP32 values (mixed precision) the
-// tile's stream is staged in shared memory by bulk asynchronous copies (TMA).
-// Fraction of the HBM roofline reached (B200, 4.28 M blocks): FP64 ~0.60,
-// FP32 ~0.48; the limit is the per-tile chain of L2 gathers of x, shared-
-// memory placement and barriers, not the DRAM stream (doubling the bytes in
-// flight with two TMA stages did not change the time).
+// Design, FP64 values (k_spmv_tile): persistent CTAs walk SPMV_TILE-block
+// tiles of the row-sorted block stream. Each thread owns SPMV_BPT consecutive
+// blocks and reads their row and column ids, tile ranks and the 9 value planes
+// with 16-byte vector loads (the planes are padded to a multiple of 16
+// blocks). The row halves B x_j of a thread's blocks are merged in registers
+// (runs of equal rows) and each run goes to y with one fire-and-forget
+// reduction per component (red.global, resolved in L2). The transposed halves
+// B^T x_i are placed in shared memory at the block's precomputed rank in
+// (column, index) order; after a barrier each thread merges its SPMV_BPT
+// consecutive slots, so runs of equal columns also leave as one reduction
+// each (~0.62 of the measured HBM bandwidth on 4.25 M blocks).
+// FP32 values (k_spmv_direct, mixed precision): the same row runs, but every
+// transposed half leaves as one vector reduction of the padded node and the
+// kernel holds no shared memory and no barrier (~0.77).
 #include "b2s_internal.cuh"
 #include "b2s_reduce.cuh"
-#include "b2s_tma.cuh"
 
+#include <algorithm>
 #include <cstdlib>
 #include <string>
 
@@ -247,126 +246,88 @@ __global__ void __launch_bounds__(SPMV_THREADS)
     }
 }
 
-// FP32 values, TMA-staged: the tile's block stream (row and column ids, tile
-// ranks, the 9 value planes: 46 B per block) is brought into shared memory by
-// bulk asynchronous copies issued by one thread as soon as the previous tile
-// is read out of the stage, so the copy overlaps that tile's reductions and
-// the other CTAs' work, with no registers held for it (one 47 KB stage per
-// CTA: three CTAs per SM; two stages were slower).
-// x and y are the padded FP32 vectors of the mixed PCG (4 floats per node,
-// 16-byte aligned, the 4th zero): a gather is one 16-byte load and a run's
-// reduction one red.global.add.v4.f32. The runs and their order are those of
-// k_spmv_tile.
-constexpr int      TMA_STAGES  = 1;
-constexpr uint32_t STAGE_BYTES = SPMV_TILE * (4 + 4 + 2 + 9 * 4);  // 47,104
-
-size_t spmv_tma_smem()
-{
-    return (size_t)TMA_STAGES * STAGE_BYTES + sizeof(float) * 3 * SPMV_TILE + sizeof(int32_t) * SPMV_TILE +
-           sizeof(uint64_t) * TMA_STAGES;
-}
+// FP32 values (mixed precision), streamed straight into registers: each
+// thread takes SPMV_BPT consecutive blocks (16-byte streaming loads of the row
+// and column ids and of the 9 value planes, marked evict-first so the stream
+// does not push x and y out of L2), merges its row runs in registers as
+// k_spmv_tile does, and sends each off-diagonal block's transposed half
+// B^T x_i to y with its own red.global.add.v4.f32 -- no shared memory, no
+// barriers, no tile ranks. x and y are the padded FP32 vectors of the mixed
+// PCG (4 floats per node, the 4th zero): a gather is one 16-byte load, a
+// reduction one vector red. 128-thread CTAs, six per SM (78 registers): with
+// nothing to wait for but its own loads, each warp keeps 11 stream loads and
+// its gathers in flight. Measured on the 8 x 40^3-cell stack (4.25 M blocks):
+// 37.3 us (0.77 of the measured copy bandwidth) against 53.6 us (0.54) for a
+// TMA-staged tile kernel with shared-memory-merged transposed halves, which
+// saves reductions but serialises every tile behind its copy and two barriers.
+// With FP64 values the per-component f64 reductions (no vector form) tip the
+// balance the other way and k_spmv_tile stays.
+constexpr int DIRECT_THREADS = 128;
+constexpr int DIRECT_CTAS_SM = 6;
 
 template <bool WITH_DOT>
-__global__ void __launch_bounds__(SPMV_THREADS)
-    k_spmv_tma(int64_t U, int64_t S, const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
-               const uint16_t* __restrict__ trank, const float* __restrict__ vals, const float* __restrict__ x,
-               float* y, double* partials, unsigned int* counter, double* dot_out, const int* stop, int* err)
+__global__ void __launch_bounds__(DIRECT_THREADS, DIRECT_CTAS_SM)
+    k_spmv_direct(int64_t S, const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
+                  const float* __restrict__ vals, const float* __restrict__ x, float* y, double* partials,
+                  unsigned int* counter, double* dot_out, const int* stop)
 {
     if(stop && *stop)
         return;
-    extern __shared__ __align__(128) unsigned char sm[];
-    float*        s_t   = reinterpret_cast<float*>(sm + (size_t)TMA_STAGES * STAGE_BYTES);
-    int32_t*      s_col = reinterpret_cast<int32_t*>(s_t + 3 * SPMV_TILE);
-    uint64_t*     bar   = reinterpret_cast<uint64_t*>(s_col + SPMV_TILE);
-    const int     tid     = threadIdx.x;
-    const int64_t n_tiles = (U + SPMV_TILE - 1) / SPMV_TILE;
-    const int64_t G       = gridDim.x;
-    // stage layout: rows[TILE] | cols[TILE] | trank[TILE] | vals[9][TILE]
-    auto st_rows  = [&](int s) { return reinterpret_cast<int32_t*>(sm + (size_t)s * STAGE_BYTES); };
-    auto st_cols  = [&](int s) { return st_rows(s) + SPMV_TILE; };
-    auto st_trank = [&](int s) { return reinterpret_cast<uint16_t*>(st_cols(s) + SPMV_TILE); };
-    auto st_vals  = [&](int s) { return reinterpret_cast<float*>(st_trank(s) + SPMV_TILE); };
-    // blocks of a tile present in the planes: the stride S is a multiple of 16,
-    // so every copy is a multiple of 16 bytes
-    auto tile_count = [&](int64_t tile) -> int {
-        const int64_t left = S - tile * SPMV_TILE;
-        return left < SPMV_TILE ? (int)left : SPMV_TILE;
-    };
-    int issued = 0;  // thread 0: copies issued so far
-    auto issue = [&](int64_t tile) {
-        const int      s   = issued % TMA_STAGES;
-        const int64_t  b   = tile * SPMV_TILE;
-        const uint32_t cnt = (uint32_t)tile_count(tile);
-        mbar_arrive_expect_tx(&bar[s], cnt * (4 + 4 + 2 + 9 * 4));
-        bulk_copy_g2s(st_rows(s), rows + b, cnt * 4, &bar[s]);
-        bulk_copy_g2s(st_cols(s), cols + b, cnt * 4, &bar[s]);
-        bulk_copy_g2s(st_trank(s), trank + b, cnt * 2, &bar[s]);
+    const int64_t n_chunks = S / SPMV_BPT;  // S is a multiple of 16
+    double        dot      = 0.0;
+    for(int64_t c = (int64_t)blockIdx.x * DIRECT_THREADS + threadIdx.x; c < n_chunks;
+        c += (int64_t)gridDim.x * DIRECT_THREADS)
+    {
+        const int64_t e0 = c * SPMV_BPT;
+        const int4    r4 = __ldcs(reinterpret_cast<const int4*>(rows + e0));
+        const int4    c4 = __ldcs(reinterpret_cast<const int4*>(cols + e0));
+        const int32_t r[4] = {r4.x, r4.y, r4.z, r4.w};
+        const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+        float         b[9][4];
+#pragma unroll
         for(int q = 0; q < 9; ++q)
-            bulk_copy_g2s(st_vals(s) + q * SPMV_TILE, vals + (int64_t)q * S + b, cnt * 4, &bar[s]);
-        ++issued;
-    };
-    if(tid == 0)
-    {
-        for(int s = 0; s < TMA_STAGES; ++s)
-            mbar_init(&bar[s], 1);
-        mbar_fence_init();
-        for(int64_t t = blockIdx.x, k = 0; t < n_tiles && k < TMA_STAGES; t += G, ++k)
-            issue(t);
-    }
-    __syncthreads();
-    double dot = 0.0;
-    int    it  = 0;
-    bool   ok  = true;
-    for(int64_t tile = blockIdx.x; tile < n_tiles; tile += G, ++it)
-    {
-        const int  s    = it % TMA_STAGES;
-        const bool good = mbar_wait(&bar[s], (uint32_t)((it / TMA_STAGES) & 1), err, DERR_TMA_TIMEOUT);
-        if(__syncthreads_or(!good))
         {
-            ok = false;
-            break;
+            const float4 v = __ldcs(reinterpret_cast<const float4*>(vals + (int64_t)q * S + e0));
+            b[q][0] = v.x; b[q][1] = v.y; b[q][2] = v.z; b[q][3] = v.w;
         }
-        const int64_t rem = U - tile * SPMV_TILE;
-        const int     n   = rem < SPMV_TILE ? (int)rem : SPMV_TILE;
-        const int     e   = SPMV_BPT * tid;
-        TileLoad<float> t;
-        if(e < tile_count(tile))
-        {
-            const int4  r4 = *reinterpret_cast<const int4*>(st_rows(s) + e);
-            const int4  c4 = *reinterpret_cast<const int4*>(st_cols(s) + e);
-            const uint2 k2 = *reinterpret_cast<const uint2*>(st_trank(s) + e);
-            t.r[0] = r4.x; t.r[1] = r4.y; t.r[2] = r4.z; t.r[3] = r4.w;
-            t.c[0] = c4.x; t.c[1] = c4.y; t.c[2] = c4.z; t.c[3] = c4.w;
-            t.rk[0] = (int)(k2.x & 0xFFFFu); t.rk[1] = (int)(k2.x >> 16);
-            t.rk[2] = (int)(k2.y & 0xFFFFu); t.rk[3] = (int)(k2.y >> 16);
+        int32_t cur = -1;
+        float   a0 = 0.f, a1 = 0.f, a2 = 0.f, xi0 = 0.f, xi1 = 0.f, xi2 = 0.f;
 #pragma unroll
-            for(int q = 0; q < 9; ++q)
+        for(int k = 0; k < SPMV_BPT; ++k)
+        {
+            if(r[k] < 0)
+                break;  // padding: only at the end of the stream
+            const int32_t ck = cc[k];
+            float         xj0, xj1, xj2;
+            load_node<float, true>(x, ck, xj0, xj1, xj2);
+            if(r[k] != cur)
             {
-                const float4 v = *reinterpret_cast<const float4*>(st_vals(s) + q * SPMV_TILE + e);
-                t.b[q][0] = v.x; t.b[q][1] = v.y; t.b[q][2] = v.z; t.b[q][3] = v.w;
+                if(cur >= 0)
+                    red_node<float, true>(y, cur, a0, a1, a2);
+                cur = r[k];
+                a0 = a1 = a2 = 0.f;
+                load_node<float, true>(x, cur, xi0, xi1, xi2);
             }
+            // column-major: B(p,q) = b[q*3 + p]
+            const float y0 = b[0][k] * xj0 + b[3][k] * xj1 + b[6][k] * xj2;
+            const float y1 = b[1][k] * xj0 + b[4][k] * xj1 + b[7][k] * xj2;
+            const float y2 = b[2][k] * xj0 + b[5][k] * xj1 + b[8][k] * xj2;
+            a0 += y0;
+            a1 += y1;
+            a2 += y2;
+            const bool off = cur != ck;
+            if(WITH_DOT)
+            {
+                const double d = (double)xi0 * (double)y0 + (double)xi1 * (double)y1 + (double)xi2 * (double)y2;
+                dot += off ? 2.0 * d : d;
+            }
+            if(off)
+                red_node<float, true>(y, ck, b[0][k] * xi0 + b[1][k] * xi1 + b[2][k] * xi2,
+                                      b[3][k] * xi0 + b[4][k] * xi1 + b[5][k] * xi2,
+                                      b[6][k] * xi0 + b[7][k] * xi1 + b[8][k] * xi2);
         }
-        else
-        {
-#pragma unroll
-            for(int k = 0; k < 4; ++k)
-                t.r[k] = -1;
-        }
-        tile_rows<float, float, WITH_DOT, true>(t, x, y, reinterpret_cast<float(*)[SPMV_TILE]>(s_t), s_col, dot);
-        __syncthreads();  // the stage is read and the transposed halves are placed
-        if(tid == 0 && tile + (int64_t)TMA_STAGES * G < n_tiles)
-        {
-            fence_proxy_async_smem();
-            issue(tile + (int64_t)TMA_STAGES * G);
-        }
-        tile_cols<float, true>(tid, n, reinterpret_cast<const float(*)[SPMV_TILE]>(s_t), s_col, y);
-        __syncthreads();  // s_t is free for the next tile
-    }
-    if(!ok && tid == 0)
-    {
-        // a wait ran out: drain the copies still in flight (bounded)
-        for(int k = it; k < issued; ++k)
-            mbar_wait(&bar[k % TMA_STAGES], (uint32_t)((k / TMA_STAGES) & 1), nullptr, 0);
+        if(cur >= 0)
+            red_node<float, true>(y, cur, a0, a1, a2);
     }
     if(WITH_DOT)
     {
@@ -402,9 +363,10 @@ void launch_stream(cudaStream_t st, int64_t U, int64_t S, const int32_t* rows, c
 }
 }  // namespace
 
+// the largest grid any SpMV kernel launches for U blocks (sizes the dot partials)
 int spmv_grid(int64_t U)
 {
-    const int64_t t = (U + SPMV_TILE - 1) / SPMV_TILE;
+    const int64_t t = (U + SPMV_BPT * DIRECT_THREADS - 1) / (SPMV_BPT * DIRECT_THREADS);
     return (int)std::max<int64_t>(1, std::min<int64_t>(t, (int64_t)NUM_SMS_HINT * 8));
 }
 
@@ -478,34 +440,20 @@ void spmv_f64_launch(b2s_solver* s, const Matrix& A, const double* x, double* y,
 }
 
 // FP32 values and padded FP32 vectors (mixed precision), FP64 dot
-// the TMA SpMV's shared-memory opt-in (once per device; outside graph capture)
-void spmv_prepare_f32(b2s_solver* s)
-{
-    static thread_local int prepared_device = -1;
-    if(prepared_device == s->device)
-        return;
-    B2S_CUDA(cudaFuncSetAttribute(k_spmv_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)spmv_tma_smem()));
-    prepared_device = s->device;
-}
-
 void spmv_f32_launch(b2s_solver* s, const Matrix& A, const float* x, float* y, Reduction& red, double* d_dot,
                      const int* stop)
 {
     if(A.nnz == 0)
         return;
-    int* err = device_error_flag(s);
-    auto k   = k_spmv_tma<true>;
-    const size_t smem = spmv_tma_smem();
-    spmv_prepare_f32(s);
-    int occ = 0;
-    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, SPMV_THREADS, smem) != cudaSuccess || occ < 1)
+    auto k   = k_spmv_direct<true>;
+    int  occ = 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, DIRECT_THREADS, 0) != cudaSuccess || occ < 1)
         occ = 1;
-    const int64_t tiles = (A.nnz + SPMV_TILE - 1) / SPMV_TILE;
-    const int     grid  = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)NUM_SMS_HINT * std::min(occ, 8)));
-    k<<<grid, SPMV_THREADS, smem, s->stream>>>(A.nnz, A.stride, A.rows.data(), A.cols.data(), A.trank.data(),
-                                                A.vals32.data(), x, y, red.partials.data(), red.counter.data(), d_dot,
-                                                stop, err);
+    const int64_t ctas = (A.stride / SPMV_BPT + DIRECT_THREADS - 1) / DIRECT_THREADS;
+    const int     grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>({ctas, (int64_t)NUM_SMS_HINT * std::min(occ, DIRECT_CTAS_SM), (int64_t)spmv_grid(A.nnz)}));
+    k<<<grid, DIRECT_THREADS, 0, s->stream>>>(A.stride, A.rows.data(), A.cols.data(), A.vals32.data(), x, y,
+                                              red.partials.data(), red.counter.data(), d_dot, stop);
     B2S_CHECK_LAUNCH();
 }
 

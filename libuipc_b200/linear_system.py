@@ -106,6 +106,12 @@ class Solver:
         self._check(self.lib.b2s_spmv(self.h, _ptr(x), _ptr(y), C.byref(d) if with_dot else None))
         return d.value if with_dot else None
 
+    def spmv_mixed(self, x32, y32, with_dot: bool = False):
+        """y = A x as the mixed-precision PCG computes it (FP32 vectors)."""
+        d = C.c_double(0.0)
+        self._check(self.lib.b2s_spmv_mixed(self.h, _ptr(x32), _ptr(y32), C.byref(d) if with_dot else None))
+        return d.value if with_dot else None
+
     # ---- MAS ---------------------------------------------------------------------
     def mas_init(self, block_offset: int, vert_num: int, adj_start, adj_list, part_to_real, real_to_part):
         a = [np.ascontiguousarray(v, dtype=np.int32) for v in (adj_start, adj_list, part_to_real, real_to_part)]

@@ -139,6 +139,58 @@ def test_spmv_parity(request, solver, cuda, which):
     assert abs(dot - x @ ref) <= 1e-12 * abs(x @ ref)
 
 
+@pytest.mark.parametrize("which", ["cube10", "cube5", "stack_small"])
+def test_mixed_spmv_parity(request, solver, cuda, which):
+    """The mixed PCG's SpMV (FP32 copy of the values, padded FP32 vectors, one
+    vector reduction per transposed half) against the oracle's FP64 product of
+    the same FP32 x: every entry within 2e-6 of (|A| |x|) -- FP32 rounding of
+    the values and of at most ~30 products and sums -- and x.(A x), summed in
+    FP64 from the FP32 products, within 1e-5 relative."""
+    import torch
+
+    s = request.getfixturevalue(which)
+    _assemble(solver, s, cuda)
+    A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals)
+    absA = abs(A.to_scipy())
+    for seed in (3, 4):
+        x32 = np.random.default_rng(seed).standard_normal(3 * s.n_verts).astype(np.float32)
+        x = x32.astype(np.float64)
+        xd = torch.from_numpy(x32).to(cuda)
+        yd = torch.full_like(xd, np.nan)
+        dot = solver.spmv_mixed(xd, yd, with_dot=True)
+        y = yd.double().cpu().numpy()
+        ref = A.spmv(x)
+        bound = 2e-6 * (absA @ np.abs(x))
+        assert np.all(np.abs(y - ref) <= bound)
+        assert abs(dot - x @ ref) <= 1e-5 * abs(x @ ref)
+    z = torch.zeros(3 * s.n_verts, dtype=torch.float32, device=cuda)
+    yz = torch.full_like(z, np.nan)
+    assert solver.spmv_mixed(z, yz, with_dot=True) == 0.0
+    assert not torch.any(yz != 0)
+
+
+def test_stage_timing_with_and_without_graph(solver, cuda, cube10):
+    """Stage timing brackets every SpMV and preconditioner apply with events,
+    inside the PCG graph (external event nodes) and stream-ordered."""
+    import torch
+
+    b, A, M = _mas_setup(solver, cube10, cuda, partition_rcb(cube10.positions))
+    try:
+        solver.set_timing(True)
+        for graph in (True, False):
+            for prec in (_abi.B2S_PRECISION_FP64, _abi.B2S_PRECISION_MIXED):
+                solver.reset_timers()
+                x = torch.zeros_like(b)
+                st = solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, precision=prec,
+                                use_graph=graph)
+                t = solver.timers()
+                assert st["converged"] == 1
+                assert t["spmv_launches"] >= st["iterations_exact"] > 0
+                assert t["spmv_ms"] > 0 and t["precond_apply_ms"] > 0
+    finally:
+        solver.set_timing(False)
+
+
 # ---------------------------------------------------------------------------
 # MAS
 # ---------------------------------------------------------------------------
