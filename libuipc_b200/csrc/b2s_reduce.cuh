@@ -68,10 +68,21 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double* partials, unsi
     __shared__ double res[NV];
     for(int k = warp; k < NV; k += blockDim.x >> 5)
     {
-        // each lane sums a strided subset in order, then a fixed-shape tree
-        double acc = 0.0;
-        for(unsigned int b = lane; b < gridDim.x; b += 32)
-            acc += ((volatile double*)partials)[(size_t)k * gridDim.x + b];
+        // each lane sums a strided subset in order, then a fixed-shape tree;
+        // the loads go out 8 at a time (independent), the adds keep the order
+        const volatile double* pk  = (const volatile double*)partials + (size_t)k * gridDim.x;
+        double                 acc = 0.0;
+        for(unsigned int b = lane; b < gridDim.x; b += 32 * 8)
+        {
+            double t[8];
+#pragma unroll
+            for(int j = 0; j < 8; ++j)
+                t[j] = b + 32u * j < gridDim.x ? pk[b + 32u * j] : 0.0;
+#pragma unroll
+            for(int j = 0; j < 8; ++j)
+                if(b + 32u * j < gridDim.x)
+                    acc += t[j];
+        }
 #pragma unroll
         for(int o = 16; o > 0; o >>= 1)
             acc += __shfl_xor_sync(0xffffffffu, acc, o);
