@@ -368,7 +368,7 @@ __global__ void k_update_p(int64_t n, const PcgScalars* sc, const double* __rest
 // FP64 solution x holds 3. x += alpha p, r -= alpha Ap, Ap = 0, one node per
 // thread and step.
 __global__ void k_update_xr_mixed4(int32_t nb, PcgScalars* sc, double* __restrict__ x, const float* __restrict__ p,
-                                   float* __restrict__ r, float* __restrict__ Ap)
+                                   float* __restrict__ r, const float* __restrict__ Ap)
 {
     if(frozen(sc))
         return;
@@ -387,21 +387,21 @@ __global__ void k_update_xr_mixed4(int32_t nb, PcgScalars* sc, double* __restric
         rr.x = __fmaf_rn(-af, ap.x, rr.x);
         rr.y = __fmaf_rn(-af, ap.y, rr.y);
         rr.z = __fmaf_rn(-af, ap.z, rr.z);
-        reinterpret_cast<float4*>(r)[i]  = rr;
-        reinterpret_cast<float4*>(Ap)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        reinterpret_cast<float4*>(r)[i] = rr;
     }
 }
 
 // p = z + beta p over the padded vectors (n = 4 nb; pads stay zero)
-__global__ void k_update_p_mixed4(int64_t n, const PcgScalars* sc, const float* __restrict__ z, float* __restrict__ p)
+// p = z + beta p over the padded vectors (nb nodes), and Ap = 0 for the
+// SpMV that follows: zeroed here rather than after its last reader, so the
+// zero lines are still in L2 when the SpMV's reductions reach them
+__global__ void k_update_p_mixed4(int32_t nb, const PcgScalars* sc, const float* __restrict__ z, float* __restrict__ p,
+                                  float* __restrict__ Ap)
 {
     if(frozen(sc))
         return;
-    const float   beta   = (float)sc->beta;
-    const int64_t n4     = n >> 2;
-    const int64_t stride = (int64_t)gridDim.x * VEC_BLOCK;
-    const int64_t t0     = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x;
-    for(int64_t i = t0; i < n4; i += stride)
+    const float beta = (float)sc->beta;
+    for(int64_t i = (int64_t)blockIdx.x * VEC_BLOCK + threadIdx.x; i < nb; i += (int64_t)gridDim.x * VEC_BLOCK)
     {
         const float4 zz = reinterpret_cast<const float4*>(z)[i];
         float4       pp = reinterpret_cast<float4*>(p)[i];
@@ -409,10 +409,9 @@ __global__ void k_update_p_mixed4(int64_t n, const PcgScalars* sc, const float* 
         pp.y = __fmaf_rn(beta, pp.y, zz.y);
         pp.z = __fmaf_rn(beta, pp.z, zz.z);
         pp.w = __fmaf_rn(beta, pp.w, zz.w);
-        reinterpret_cast<float4*>(p)[i] = pp;
+        reinterpret_cast<float4*>(p)[i]  = pp;
+        reinterpret_cast<float4*>(Ap)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    for(int64_t i = 4 * n4 + t0; i < n; i += stride)
-        p[i] = __fmaf_rn(beta, p[i], z[i]);
 }
 
 // r32 = b - Ax computed in FP64, stored FP32 (padded: 4 floats per node)
@@ -997,8 +996,8 @@ static void pcg_iteration_mixed(b2s_solver* s, int kind, double* x, int slot)
     precond_launch_f32(s, kind, P.r32.data(), P.z32.data(), P.sc.data(), P.red);
     if(ev)
         B2S_CUDA(record_timing_event(ev[3], st));
-    k_update_p_mixed4<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(4 * (int64_t)nb, P.sc.data(), P.z32.data(),
-                                                         P.p32.data());
+    k_update_p_mixed4<<<vec_grid(nb), VEC_BLOCK, 0, st>>>(nb, P.sc.data(), P.z32.data(), P.p32.data(),
+                                                         P.Ap32.data());
     B2S_CHECK_LAUNCH();
 }
 
