@@ -135,7 +135,7 @@ __device__ __forceinline__ void load_tile(TileLoad<VT>& t, int64_t e0, int64_t S
 
 // row halves of a thread's blocks to y (runs of equal rows merged), the
 // transposed halves into shared memory at the blocks' ranks, and the dot
-template <typename VT, typename XT, bool WITH_DOT, bool P4>
+template <typename VT, typename XT, bool WITH_DOT>
 __device__ __forceinline__ void tile_rows(const TileLoad<VT>& t, const XT* __restrict__ x, XT* y,
                                           XT (*s_t)[SPMV_TILE], int32_t* s_col, double& dot)
 {
@@ -149,14 +149,14 @@ __device__ __forceinline__ void tile_rows(const TileLoad<VT>& t, const XT* __res
             break;  // padding: only at the end of the stream
         const int32_t ck = t.c[k];
         XT            xj0, xj1, xj2;
-        load_node<XT, P4>(x, ck, xj0, xj1, xj2);
+        load_node<XT, false>(x, ck, xj0, xj1, xj2);
         if(t.r[k] != cur)
         {
             if(cur >= 0)
-                red_node<XT, P4>(y, cur, a0, a1, a2);
+                red_node<XT, false>(y, cur, a0, a1, a2);
             cur = t.r[k];
             a0 = a1 = a2 = 0;
-            load_node<XT, P4>(x, cur, xi0, xi1, xi2);
+            load_node<XT, false>(x, cur, xi0, xi1, xi2);
         }
         // column-major: B(p,q) = b[q*3 + p]
         const XT y0 = (XT)t.b[0][k] * xj0 + (XT)t.b[3][k] * xj1 + (XT)t.b[6][k] * xj2;
@@ -178,12 +178,12 @@ __device__ __forceinline__ void tile_rows(const TileLoad<VT>& t, const XT* __res
         s_col[rk]    = ck;
     }
     if(cur >= 0)
-        red_node<XT, P4>(y, cur, a0, a1, a2);
+        red_node<XT, false>(y, cur, a0, a1, a2);
 }
 
 // transposed halves in (column, index) order: this thread's slots, runs of
 // equal columns merged; n = blocks in the tile
-template <typename XT, bool P4>
+template <typename XT>
 __device__ __forceinline__ void tile_cols(int tid, int n, const XT (*s_t)[SPMV_TILE], const int32_t* s_col, XT* y)
 {
     const int s0  = SPMV_BPT * tid;
@@ -199,7 +199,7 @@ __device__ __forceinline__ void tile_cols(int tid, int n, const XT (*s_t)[SPMV_T
         if(cc != cur)
         {
             if(cur >= 0)
-                red_node<XT, P4>(y, cur, t0, t1, t2);
+                red_node<XT, false>(y, cur, t0, t1, t2);
             cur = cc;
             t0 = t1 = t2 = 0;
         }
@@ -208,7 +208,7 @@ __device__ __forceinline__ void tile_cols(int tid, int n, const XT (*s_t)[SPMV_T
         t2 += s_t[2][sl];
     }
     if(cur >= 0)
-        red_node<XT, P4>(y, cur, t0, t1, t2);
+        red_node<XT, false>(y, cur, t0, t1, t2);
 }
 
 // U: stored blocks; S: plane stride. FP64 values, loaded straight into
@@ -233,9 +233,9 @@ __global__ void __launch_bounds__(SPMV_THREADS)
         const int64_t e0  = tile * SPMV_TILE + SPMV_BPT * tid;
         TileLoad<VT>  cur;
         load_tile(cur, e0, S, e0 < S, rows, cols, trank, vals);
-        tile_rows<VT, XT, WITH_DOT, false>(cur, x, y, s_t, s_col, dot);
+        tile_rows<VT, XT, WITH_DOT>(cur, x, y, s_t, s_col, dot);
         __syncthreads();
-        tile_cols<XT, false>(tid, n, s_t, s_col, y);
+        tile_cols<XT>(tid, n, s_t, s_col, y);
         __syncthreads();
     }
     if(WITH_DOT)
