@@ -528,16 +528,12 @@ def main() -> None:
     from libuipc_b200 import _abi
     from libuipc_b200.linear_system import Solver, partition_maps, partition_rcb
 
+    from libuipc_b200.replicas import Replicas
+
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-        pg = dist
+    # replicas only: one independent solve per rank, collectives only around the timing
+    reps = Replicas("nccl", dev, timeout_s=300)
 
     # ---- the run: step the scene, keep the solutions, train the warm start ----------
     from libuipc_b200.learned import MODES, SequenceRunner
@@ -594,18 +590,8 @@ def main() -> None:
         return solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=check_interval,
                           precision=precision, replace_every=50, x0_given=given, use_graph=use_graph)
 
-    def barrier():
-        torch.cuda.synchronize()
-        if pg is not None:
-            pg.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(v):
-        if pg is None:
-            return v
-        t = torch.tensor([v], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    barrier = reps.barrier
+    max_over_ranks = reps.max
 
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -667,6 +653,7 @@ def main() -> None:
             print(json.dumps({m: {"ms_per_solve": r[0], "iterations": r[1][-1]["iterations_exact"], "timers": r[2]}
                               for m, r in res.items()}), flush=True)
         solver.close()
+        reps.close()
         return
     nb, U = solver.matrix_info()
     head = "mixed+learned"
@@ -821,9 +808,7 @@ def main() -> None:
     solver.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if pg is not None:
-        pg.barrier()
-        pg.destroy_process_group()
+    reps.close()
 
 if __name__ == "__main__":
     main()
