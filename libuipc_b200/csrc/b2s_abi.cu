@@ -130,6 +130,12 @@ int b2s_destroy(b2s_solver* s)
     for(cudaEvent_t e : s->iter_events)
         cudaEventDestroy(e);
     b2s::ws_free(s->ws);
+    if(s->mas_fork)
+        cudaEventDestroy(s->mas_fork);
+    if(s->mas_join)
+        cudaEventDestroy(s->mas_join);
+    if(s->mas_side)
+        cudaStreamDestroy(s->mas_side);
     if(s->own_stream)
         cudaStreamDestroy(s->own_stream);
     delete s;

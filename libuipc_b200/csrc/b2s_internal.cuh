@@ -246,6 +246,10 @@ struct b2s_solver
     b2s::DBuf<double>    dot_out;
     b2s::Reduction       red;
     b2s::DBuf<int>       dev_err;  // DeviceError bits raised by kernels
+    // the MAS apply's second stream: the coarse levels run on it beside the
+    // fine level's products (forked from `stream` and joined back by events)
+    cudaStream_t             mas_side = nullptr;
+    cudaEvent_t              mas_fork = nullptr, mas_join = nullptr;
     // stage timers (CUDA events on `stream`)
     bool                     timing = false;
     b2s_timers               timers{};

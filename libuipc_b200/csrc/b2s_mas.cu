@@ -844,16 +844,85 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
                                    &s_inv[w][0][0], s_r[w], s_bar[w]);
 }
 
-// persistent grid: as many CTAs as fit on the SMs at once, capped by the banks
+// persistent grid: as many CTAs as fit on the SMs at once (less `spare` per
+// SM, at least one), at most `cap` per SM when cap > 0, capped by the banks
 template <typename K>
-int apply_grid(K kernel, int n_banks)
+int apply_grid(K kernel, int n_banks, int spare = 0, int cap = 0)
 {
     int occ = 0;
     if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, APPLY_WARPS * 32, 0) != cudaSuccess || occ < 1)
         occ = 1;
+    occ = occ - spare >= 1 ? occ - spare : 1;
+    if(cap > 0 && occ > cap)
+        occ = cap;
     const int max_warps = NUM_SMS_HINT * occ * APPLY_WARPS;
     const int warps     = n_banks < max_warps ? n_banks : max_warps;
     return (warps + APPLY_WARPS - 1) / APPLY_WARPS;
+}
+
+// The level-1 restriction of the fine residual on its own (the sums the fine
+// level's `push` forms: per connected component of a bank, by its lowest lane,
+// in lane order, so R_1 is bit-identical), one half-warp per bank and one
+// bank per half-warp over the whole grid: the coarse levels need only R_1, so
+// with it in place they run beside the fine level's cluster products.
+template <typename VT>
+__global__ void __launch_bounds__(APPLY_WARPS * 32)
+    k_restrict_fine(int n_banks, const int32_t* __restrict__ p2r, const VT* __restrict__ r, int roff,
+                    const uint16_t* __restrict__ comp_mask, const int32_t* __restrict__ new_local, int next_begin,
+                    float* __restrict__ R, const int* converged)
+{
+    if(converged && *converged)
+        return;
+    __shared__ float s_r[APPLY_WARPS][2][BANK][3];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, half = lane >> 4, sub = lane & 15;
+    const int bank = (blockIdx.x * APPLY_WARPS + w) * 2 + half;
+    float     n0 = 0.f, n1 = 0.f, n2 = 0.f;
+    bool      live = false;
+    uint32_t  cm   = 0;
+    int       nl   = 0;
+    if(bank < n_banks)
+    {
+        const int node = bank * BANK + sub;
+        const int v    = p2r[node];
+        live           = v >= 0;
+        if(live)
+        {
+            if constexpr(sizeof(VT) == 4)
+            {
+                const float4 q = *reinterpret_cast<const float4*>(r + roff + 4 * (int64_t)v);
+                n0 = q.x;
+                n1 = q.y;
+                n2 = q.z;
+            }
+            else
+            {
+                n0 = (float)r[roff + 3 * (int64_t)v];
+                n1 = (float)r[roff + 3 * (int64_t)v + 1];
+                n2 = (float)r[roff + 3 * (int64_t)v + 2];
+            }
+            cm = comp_mask[node];
+            nl = new_local[node];
+        }
+    }
+    s_r[w][half][sub][0] = n0;
+    s_r[w][half][sub][1] = n1;
+    s_r[w][half][sub][2] = n2;
+    __syncwarp();
+    if(live && (cm & ((1u << sub) - 1u)) == 0)
+    {
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+        for(uint32_t m = cm; m; m &= m - 1)
+        {
+            const int l = __ffs(m) - 1;
+            s0 += s_r[w][half][l][0];
+            s1 += s_r[w][half][l][1];
+            s2 += s_r[w][half][l][2];
+        }
+        const int64_t g = (int64_t)next_begin + nl;
+        R[3 * g]     = s0;
+        R[3 * g + 1] = s1;
+        R[3 * g + 2] = s2;
+    }
 }
 
 }  // namespace
@@ -866,6 +935,12 @@ void mas_init(b2s_solver* s, int32_t offset, int32_t vn, const int32_t* adj_star
 {
     B2S_REQUIRE(vn > 0 && N > 0 && offset >= 0, B2S_ERR_ARGUMENT, "MAS range must be non-empty");
     B2S_REQUIRE(N % BANK == 0, B2S_ERR_ARGUMENT, "part_map_size must be a multiple of 16");
+    if(!s->mas_side)
+    {
+        B2S_CUDA(cudaStreamCreateWithFlags(&s->mas_side, cudaStreamNonBlocking));
+        B2S_CUDA(cudaEventCreateWithFlags(&s->mas_fork, cudaEventDisableTiming));
+        B2S_CUDA(cudaEventCreateWithFlags(&s->mas_join, cudaEventDisableTiming));
+    }
     // validate the maps on the host (the reference asserts the same, fem_mas_preconditioner.cu:331-360)
     for(int p = 0; p < N; ++p)
     {
@@ -1087,20 +1162,38 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
     const int    n_banks0 = M.N / BANK;
     const int    tb       = APPLY_WARPS * 32;
     const unsigned char* inv = bf16 ? M.inv16.data() : reinterpret_cast<const unsigned char*>(M.inv.data());
+    // element offset of the range's first vertex in r (FP32: 4 per node)
+    const int off = (sizeof(VT) == 4 ? 4 : 3) * M.offset;
+    // With coarse levels, R_1 is restricted first (whole grid), then the
+    // fine level's products run on `st` with one CTA slot per SM left free
+    // while the coarse levels -- a chain of small, latency-bound launches --
+    // run on the side stream in those slots; `st` waits for them before the
+    // finish. Without coarse levels the fine level runs alone.
+    const bool fork = M.L > 1 && n_banks0 > 0 && s->mas_side != nullptr;
+    if(fork)
+    {
+        const int pairs = (n_banks0 + 1) / 2;
+        k_restrict_fine<VT><<<(pairs + APPLY_WARPS - 1) / APPLY_WARPS, tb, 0, st>>>(
+            n_banks0, M.p2r.data(), r, off, M.comp_mask[0].data(), M.new_local[0].data(), M.level_begin[1],
+            M.R.data(), converged);
+        B2S_CHECK_LAUNCH();
+        B2S_CUDA(cudaEventRecord(s->mas_fork, st));
+        B2S_CUDA(cudaStreamWaitEvent(s->mas_side, s->mas_fork, 0));
+    }
     if(n_banks0 > 0)
     {
         auto k = bf16 ? k_apply_level<true, VT, true, APPLY_STAGES_BF16>
                       : k_apply_level<true, VT, false, APPLY_STAGES_F32>;
-        // element offset of the range's first vertex in r (FP32: 4 per node)
-        const int off = (sizeof(VT) == 4 ? 4 : 3) * M.offset;
-        k<<<apply_grid(k, n_banks0), tb, 0, st>>>(n_banks0, M.N, 0, M.p2r.data(), r, off,
-                                                  M.comp_mask[0].data(), M.new_local[0].data(), M.level_begin[1],
-                                                  M.L > 1 ? 1 : 0, inv, M.R.data(), M.Z.data(), converged, err);
+        k<<<apply_grid(k, n_banks0, fork ? 1 : 0), tb, 0, st>>>(n_banks0, M.N, 0, M.p2r.data(), r, off,
+                                                                  M.comp_mask[0].data(), M.new_local[0].data(),
+                                                                  M.level_begin[1], (M.L > 1 && !fork) ? 1 : 0, inv,
+                                                                  M.R.data(), M.Z.data(), converged, err);
         B2S_CHECK_LAUNCH();
     }
     // coarse levels: one persistent launch each (on the graph's stream the
     // launches follow each other within microseconds; one thread-block cluster
     // running all small levels with cluster barriers between them was slower)
+    cudaStream_t cs = fork ? s->mas_side : st;
     for(int level = 1; level < M.L; ++level)
     {
         const int cnt = M.level_count[level];
@@ -1110,11 +1203,17 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
         const int push    = level + 1 < M.L ? 1 : 0;
         auto k = bf16 ? k_apply_level<false, VT, true, APPLY_STAGES_BF16>
                       : k_apply_level<false, VT, false, APPLY_STAGES_F32>;
-        k<<<apply_grid(k, n_banks), tb, 0, st>>>(n_banks, cnt, M.level_begin[level], nullptr, nullptr, 0,
-                                                 M.comp_mask[level].data(), M.new_local[level].data(),
-                                                 push ? M.level_begin[level + 1] : 0, push, inv, M.R.data(),
-                                                 M.Z.data(), converged, err);
+        k<<<apply_grid(k, n_banks, 0, fork ? 1 : 0), tb, 0, cs>>>(n_banks, cnt, M.level_begin[level], nullptr,
+                                                                    nullptr, 0, M.comp_mask[level].data(),
+                                                                    M.new_local[level].data(),
+                                                                    push ? M.level_begin[level + 1] : 0, push, inv,
+                                                                    M.R.data(), M.Z.data(), converged, err);
         B2S_CHECK_LAUNCH();
+    }
+    if(fork)
+    {
+        B2S_CUDA(cudaEventRecord(s->mas_join, cs));
+        B2S_CUDA(cudaStreamWaitEvent(st, s->mas_join, 0));
     }
 }
 
