@@ -509,6 +509,29 @@ class GlobalLinearSystem:
             mm.export_vector_market(names[2], x.detach().cpu().numpy())
         return -x  # distribute_solution: dx = -x
 
+    def solve_subsystems(self, layout, history_slot: int = 0, frame: int = 0, newton_iter: int = 0):
+        """The solve over linear subsystems (``libuipc_b200.subsystems``), as
+        GlobalLinearSystem::solve runs it (global_linear_system.cu:85-106,
+        321-544): extents and offsets, the -1 / 0 fill, each subsystem's writes
+        into device arrays kept at the layout's reserved capacity, the solve, and
+        dx = -x handed to every diagonal subsystem; returns dx."""
+        torch = _torch()
+        n, T = layout.update()
+        dev = torch.device("cuda", self.solver.device)
+        bufs = getattr(self, "_sub_bufs", None)
+        if bufs is None or bufs[0].numel() < layout.triplet_capacity or bufs[3].numel() < layout.dof_capacity:
+            tc, dc = max(layout.triplet_capacity, 1), max(layout.dof_capacity, 1)
+            bufs = (torch.empty(tc, dtype=torch.int32, device=dev), torch.empty(tc, dtype=torch.int32, device=dev),
+                    torch.empty((tc, 9), dtype=torch.float64, device=dev),
+                    torch.empty(dc, dtype=torch.float64, device=dev))
+            self._sub_bufs = bufs
+        rows, cols, vals, b = bufs
+        layout.assemble(rows, cols, vals, b)
+        dx = self.solve(layout.n_block_rows, rows[:T], cols[:T], vals[:T], b[:n], history_slot=history_slot,
+                        frame=frame, newton_iter=newton_iter)
+        layout.distribute(dx)
+        return dx
+
 
 def dump_folder_from_config(config: dict | None, workspace: str) -> str | None:
     """The folder of the debug dump when the scene setting
