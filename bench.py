@@ -33,9 +33,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    # plain vs mixed precision, 8 stacked 40^3-cell cubes
+    # plain vs mixed precision: 8 stacked 40^3-cell cubes (the headline workload)
     "stack8x40": dict(cells=40, n_cubes=8, seed=0),
-    # the reference's CPU-runnable small case
+    # the reference's CPU-runnable small case: one 10^3-cell cube on the ground
     "cube10": dict(cells=10, n_cubes=1, seed=0),
     # profiling case of the same kernels: 4 cubes (matrix 164 MB > L2)
     "stack4x40": dict(cells=40, n_cubes=4, seed=0),

@@ -128,7 +128,7 @@ def run_gpu_bar(device, cells=(200, 20, 20), E: float = 1e6, nu: float = 0.49, t
                 train_steps: int = 200, eval_steps: int = 20, newton_iters: int = 10, truth_tol: float = 1e-10,
                 tol: float = 1e-4, epochs: int = 5, hidden: int = 128, seed: int = 0,
                 precision=_abi.B2S_PRECISION_FP64, modes=("zero", "prev", "history", "learned")) -> dict:
-    """The learned warm start on the twisted bar at configs[3]'s scale: the bar
+    """The learned warm start on a twisted bar at full scale (200x20x20 cells by default): the bar
     (cells, E, nu; ends turned +-twist deg per step) is stepped on the GPU
     (:class:`GpuBarSequence`, every system from the device generator) for
     ``train_steps`` steps of ``newton_iters`` Newton iterations; every system
