@@ -1,0 +1,31 @@
+"""bench.py's own arithmetic on CPU: the algorithmic bytes of one SpMV (the
+figure the roofline divides by the measured launch time), the peak it divides
+by (the measured copy bandwidth, else the stated fallback), and the workloads
+the line is quoted on."""
+import json
+import os
+
+import bench
+
+
+def test_spmv_algorithmic_bytes():
+    # C2: 4,280,989 stored upper blocks, 551,368 block rows
+    U, nb = 4_280_989, 551_368
+    assert bench.spmv_bytes(U, nb, 4) == U * 40 + 4 * (nb + 1) + 3 * nb * 8 == 186_677_868
+    assert bench.spmv_bytes(U, nb, 8) == U * 76 + 4 * (nb + 1) + 3 * nb * 16
+    assert bench.spmv_bytes(0, 0, 4) == 4
+
+
+def test_peak_is_the_measured_copy_bandwidth_else_the_fallback(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench._peaks() == (6650.0, "fallback")
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6449.1, "bf16_tflops": 1500.0}))
+    assert bench._peaks() == (6449.1, "measured")
+
+
+def test_workloads():
+    w = bench.WORKLOADS
+    assert w["stack8x40"] == dict(cells=40, n_cubes=8, seed=0)
+    assert w["cube10"]["cells"] == 10 and w["cube10"]["n_cubes"] == 1
+    for name, cfg in w.items():
+        assert {"cells", "n_cubes", "seed"} <= set(cfg), name
