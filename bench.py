@@ -3,7 +3,7 @@
 One step = one Newton linear solve of the workload: triplet assembly, MAS
 preconditioner build, warm start, PCG to a relative residual of 1e-4 verified
 in FP64. The workload is 8 jittered Kuhn-split tet cubes of 40^3 cells
-stacked with 1 mm gaps (551,368 vertices, 1.65 M DoF, 31.8 M raw triplets,
+stacked with 1 mm gaps (551,368 vertices, 1.65 M DoF, 31.5 M raw triplets,
 ~4.3 M unique upper blocks incl. point-triangle / edge-edge contact blocks),
 synthetic (seeded) data generated on the host. The stack is stepped under
 gravity (backward Euler, one Newton iteration per step) for --history-steps
