@@ -115,7 +115,7 @@ struct Matrix
 {
     int32_t        nb  = 0;  // block rows
     int64_t        nnz = 0;  // unique upper blocks U
-    int64_t        stride = 0;  // plane stride: U rounded up to 16 (16-byte aligned bulk copies)
+    int64_t        stride = 0;  // plane stride: U rounded up to 16 (16-byte aligned loads of 4 blocks)
     DBuf<int32_t>  rowptr;   // [nb+1]
     DBuf<int32_t>  rows;     // [stride] block row of each block (BCOO row index), -1 in the padding
     DBuf<int32_t>  cols;     // [stride]
