@@ -249,7 +249,7 @@ def config_solve(dev, s, steps: int = 5, warmup: int = 3) -> dict:
     for mode, prec in (("plain", _abi.B2S_PRECISION_FP64), ("mixed", _abi.B2S_PRECISION_MIXED)):
         def solve(rule=_abi.B2S_STOP_RELRES):
             solver.assemble(s.n_verts, rows, cols, vals)
-            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_SWEEP_F32)
+            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_F32)
             return solver.pcg(b, x, tol=1e-4, stop_rule=rule, check_interval=5, precision=prec, replace_every=50)
 
         for _ in range(warmup):
@@ -338,7 +338,7 @@ def bar_run(dev, steps: int, warmup: int, history_steps: int = 6, epochs: int = 
     for mode, (prec, start) in starts.items():
         def solve():
             solver.assemble(s.n_verts, rows, cols, vals)
-            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_SWEEP_F32)
+            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_F32)
             given = start != "zero"
             if given:
                 solver.ws_predict(b, x, hist, MODES[start])
@@ -405,7 +405,7 @@ def full_scale_run(dev, steps: int, warmup: int) -> dict:
     for mode, prec in (("plain", _abi.B2S_PRECISION_FP64), ("mixed", _abi.B2S_PRECISION_MIXED)):
         def solve():
             solver.assemble(s.n_verts, rows, cols, vals)
-            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_SWEEP_F32)
+            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_F32)
             return solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, precision=prec,
                               replace_every=50)
 
@@ -581,7 +581,7 @@ def main() -> None:
     def solve_step(mode, use_graph=True, check_interval=5):
         precision, start = starts[mode]
         solver.assemble(s.n_verts, rows, cols, vals)
-        solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_SWEEP_F32)
+        solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_F32)
         given = start != "zero"
         if given:
             info = solver.ws_predict(b, x, hist, MODES[start])

@@ -111,6 +111,10 @@ int b2s_mas_get_hierarchy(b2s_solver* s, int32_t* h_level_begin, int32_t* h_leve
 /* Cluster matrices after b2s_precond_assemble: Galerkin matrices (FP64) and
  * inverses (FP32), 136 column-major 3x3 blocks per 16-node cluster. */
 int b2s_mas_get_clusters(b2s_solver* s, double* h_hess, float* h_inv);
+/* Stiff clusters of the last build: their count, and per cluster 1 when it
+ * was inverted in FP64 (h_flags: total_nodes / 16 bytes, may be NULL). The
+ * mixed-precision apply uses their FP32 inverse in place of BF16 tiles. */
+int b2s_mas_stiff_info(b2s_solver* s, int32_t* n_stiff, uint8_t* h_flags);
 /* Node buffers of the last MAS apply (FP32, 3 per node slot, total_nodes
  * slots): the restricted residual R of every coarse node and the local
  * solution Z of every node. */
@@ -132,8 +136,13 @@ int b2s_partition_maps(int32_t n, const int32_t* h_part_ids, int32_t max_part,
 #define B2S_PRECOND_JACOBI 1 /* 3x3 block Jacobi (fem_diag_preconditioner.cu:18-58) */
 #define B2S_PRECOND_MAS 2    /* MAS on its range, 3x3 block Jacobi elsewhere */
 
-#define B2S_INVERT_SWEEP_F32 0 /* FP32 symmetric sweep (mas_preconditioner_engine.cu:1077-1175) */
-#define B2S_INVERT_GJ_F64 1    /* FP64 Gauss-Jordan, stored FP32 */
+/* Inversion of the MAS cluster matrices (the reference inverts every cluster
+ * in FP32 without pivoting, mas_preconditioner_engine.cu:1077-1175). Here an
+ * LDL^T factorisation per cluster; a cluster whose FP32 elimination cancels
+ * more than 10 bits of a pivot (stiff contact couplings) is "stiff". */
+#define B2S_INVERT_F32 0      /* FP32; stiff clusters again in FP64 (default) */
+#define B2S_INVERT_F64 1      /* FP64 for every cluster */
+#define B2S_INVERT_F32_ONLY 2 /* FP32 for every cluster, stiff ones too */
 
 /* Affine bodies: block rows [block_offset, block_offset + 4 n_bodies) hold
  * n_bodies affine bodies of 12 DoF (4 block rows each). Every preconditioner
@@ -291,9 +300,13 @@ int b2s_ws_predict(b2s_solver* s, int32_t mode, const double* d_b, int32_t n_his
  * owned by another framework's caching allocator, or a loop that may not
  * touch the allocator after start-up. It takes no solver handle and
  * allocates nothing: the caller owns the block-upper BCOO (d_rows, d_cols,
- * d_vals: 9 doubles per block, column-major, row <= col, no duplicates --
- * the layout b2s_get_upper_bsr returns), d_x, d_y [3 * n_block_rows] and
- * d_dot (one double, may be NULL). Its scratch is a fixed device array in
+ * d_vals: 9 doubles per block, column-major, row <= col, no duplicates, rows
+ * non-decreasing -- the order b2s_get_upper_bsr returns), d_x, d_y
+ * [3 * n_block_rows] and d_dot (one double, may be NULL). The kernel checks
+ * every block: one whose row or column lies outside [0, n_block_rows), whose
+ * row exceeds its column, or whose row is below the previous block's is
+ * skipped (nothing is read or written through its indices) and *d_dot
+ * becomes NaN, so pass d_dot to learn of bad input. Its scratch is a fixed device array in
  * the library (about 256 KB per device that loads it, held until exit), so
  * n_blocks is limited to 8,388,608; larger inputs are rejected with
  * B2S_ERR_ARGUMENT. Work is queued on `stream` (cudaStream_t, NULL = legacy

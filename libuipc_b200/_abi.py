@@ -14,8 +14,9 @@ B2S_PRECOND_NONE = 0
 B2S_PRECOND_JACOBI = 1
 B2S_PRECOND_MAS = 2
 
-B2S_INVERT_SWEEP_F32 = 0
-B2S_INVERT_GJ_F64 = 1
+B2S_INVERT_F32 = 0
+B2S_INVERT_F64 = 1
+B2S_INVERT_F32_ONLY = 2
 
 B2S_STOP_RZ = 0
 B2S_STOP_RELRES = 1
@@ -121,6 +122,7 @@ SIGNATURES = {
     "b2s_mas_info": (C.c_int, [vp, i32p, i32p]),
     "b2s_mas_get_hierarchy": (C.c_int, [vp, vp, vp, vp]),
     "b2s_mas_get_clusters": (C.c_int, [vp, vp, vp]),
+    "b2s_mas_stiff_info": (C.c_int, [vp, i32p, vp]),
     "b2s_mas_get_nodes": (C.c_int, [vp, vp, vp]),
     "b2s_partition_rcb": (C.c_int, [i32, vp, i32, vp]),
     "b2s_partition_maps": (C.c_int, [i32, vp, i32, vp, vp, i32p]),

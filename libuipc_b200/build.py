@@ -40,6 +40,7 @@ SOLVE_SOURCES = [
     "b2s_assemble.cu",
     "b2s_spmv.cu",
     "b2s_mas.cu",
+    "b2s_mas_invert.cu",
     "b2s_pcg.cu",
     "b2s_learned.cu",
     "b2s_generate.cu",

@@ -326,6 +326,23 @@ int b2s_mas_get_clusters(b2s_solver* s, double* hess, float* inv)
                    });
 }
 
+int b2s_mas_stiff_info(b2s_solver* s, int32_t* n_stiff, uint8_t* h_flags)
+{
+    return guarded(s,
+                   [&]
+                   {
+                       const b2s::MasState& M = s->mas;
+                       B2S_REQUIRE(M.initialized, B2S_ERR_STATE, "MAS not initialised");
+                       B2S_REQUIRE(M.stiff_count.size() == 1, B2S_ERR_STATE, "no MAS build yet");
+                       B2S_CUDA(cudaStreamSynchronize(s->stream));
+                       if(n_stiff)
+                           B2S_CUDA(cudaMemcpy(n_stiff, M.stiff_count.data(), sizeof(int32_t),
+                                               cudaMemcpyDeviceToHost));
+                       if(h_flags && M.clusters > 0)
+                           B2S_CUDA(cudaMemcpy(h_flags, M.stiff.data(), (size_t)M.clusters, cudaMemcpyDeviceToHost));
+                   });
+}
+
 int b2s_mas_get_nodes(b2s_solver* s, float* R, float* Z)
 {
     return guarded(s,

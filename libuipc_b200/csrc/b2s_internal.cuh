@@ -167,6 +167,9 @@ struct MasState
     // per assembly
     DBuf<double>  hess;            // [clusters * 136 * 9]
     DBuf<float>   inv;             // [clusters * 136 * 9]
+    DBuf<uint8_t> stiff;           // [clusters] 1: inverted in FP64, applied from the FP32 inverse
+    DBuf<int32_t> stiff_list;      // [clusters] the stiff clusters (first stiff_count entries)
+    DBuf<int32_t> stiff_count;     // [1]
     DBuf<unsigned char> inv16;     // [clusters * 3264]: FP32 factor D (48) + six BF16 16x16 tiles of D^-1 inv D^-1
     long long     inv16_generation = -1;  // assembly generation inv16 was packed from
     // coarse-level Galerkin matrices (upper BCOO per level, in level-local ids)

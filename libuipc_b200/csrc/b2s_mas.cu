@@ -10,8 +10,8 @@
 //  * Galerkin matrices (:530-953): the 48x48 matrix of every bank at every
 //    level is R_l A R_l^T restricted to the bank, R_l summing the fine
 //    vertices of each level-l node.
-//  * inversion (:1077-1175): per-cluster symmetric sweep (Gauss-Jordan without
-//    pivoting, zero diagonal -> 1).
+//  * inversion (:1077-1175): the inverse of every cluster matrix, no pivoting,
+//    zero diagonal -> 1 (b2s_mas_invert.cu).
 //  * apply (:1604-1955, :2887-2960): z = sum_l P_l^T A_l^{-1} P_l r with
 //    summation restriction and injection prolongation, FP32 inside.
 //
@@ -32,6 +32,7 @@
 namespace b2s
 {
 int* device_error_flag(b2s_solver* s);
+void mas_invert_clusters(b2s_solver* s, int mode);
 
 namespace
 {
@@ -341,99 +342,6 @@ __global__ void k_g_extract(int64_t U, const int32_t* rows, const int32_t* cols,
 }
 
 // ---------------------------------------------------------------------------
-// cluster inversion: symmetric sweep, one thread per column, 4 clusters/CTA
-// ---------------------------------------------------------------------------
-constexpr int INV_DIM      = BANK * 3;  // 48
-constexpr int INV_CLUSTERS = 4;
-constexpr int INV_BLOCK    = INV_DIM * INV_CLUSTERS;
-
-template <typename T>
-__device__ __forceinline__ T fma_t(T a, T b, T c);
-template <>
-__device__ __forceinline__ float fma_t<float>(float a, float b, float c)
-{
-    return __fmaf_rn(a, b, c);
-}
-template <>
-__device__ __forceinline__ double fma_t<double>(double a, double b, double c)
-{
-    return __fma_rn(a, b, c);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(INV_BLOCK) k_invert(int clusters, const double* __restrict__ hess,
-                                                      float* __restrict__ inv)
-{
-    __shared__ T s_row[INV_CLUSTERS][2][INV_DIM];
-    const int local = threadIdx.x / INV_DIM;
-    const int col   = threadIdx.x % INV_DIM;
-    const int cl    = blockIdx.x * INV_CLUSTERS + local;
-    const bool live = cl < clusters;
-    const int a = col % 3, nc = col / 3;
-    T c[INV_DIM];
-    const double* H = hess + (size_t)(live ? cl : 0) * SYM * 9;
-#pragma unroll
-    for(int row = 0; row < INV_DIM; ++row)
-    {
-        const int node_row = row / 3;
-        T         v;
-        if(nc >= node_row)
-            v = (T)H[sym_index(node_row, nc) * 9 + a * 3 + (row % 3)];
-        else
-            v = (T)H[sym_index(nc, node_row) * 9 + (row % 3) * 3 + a];
-        if(row == col && v == (T)0)
-            v = (T)1;
-        c[row] = v;
-    }
-#pragma unroll
-    for(int p = 0; p < INV_DIM; ++p)
-    {
-        T* sr   = s_row[local][p & 1];
-        sr[col] = c[p];
-        __syncthreads();
-        const T akk = sr[p];
-        const T f   = c[p];
-        T       nv;
-        if(col == p)
-        {
-            const T iv = (T)1 / akk;
-#pragma unroll
-            for(int i = 0; i < INV_DIM; ++i)
-                c[i] *= iv;
-            nv = -iv;
-        }
-        else
-        {
-            const T sc = f / akk;
-#pragma unroll
-            for(int i = 0; i < INV_DIM; ++i)
-                c[i] = fma_t<T>(-sr[i], sc, c[i]);
-            nv = sc;
-        }
-        c[p] = nv;
-    }
-    if(!live)
-        return;
-    float* O = inv + (size_t)cl * SYM * 9;
-#pragma unroll
-    for(int row = 0; row < INV_DIM; ++row)
-    {
-        const int   node_row = row / 3, b = row % 3;
-        const float v        = (float)(-c[row]);
-        if(node_row < nc)
-            O[sym_index(node_row, nc) * 9 + a * 3 + b] = v;
-        else if(node_row == nc)
-        {
-            const int si = sym_index(nc, nc);
-            if(b <= a)
-                O[si * 9 + a * 3 + b] = v;
-            if(b < a)
-                O[si * 9 + b * 3 + a] = v;
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // apply: one warp per bank, persistent over banks. The bank's inverse is
 // brought into shared memory by bulk asynchronous copies (TMA), NST deep per
 // warp, so later banks' copies are in flight while this one computes. The
@@ -667,6 +575,7 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
                                             const uint16_t* __restrict__ comp_mask,
                                             const int32_t* __restrict__ new_local, int next_begin, int push,
                                             const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
+                                            const uint8_t* __restrict__ stiff, const float* __restrict__ inv32,
                                             int* err, unsigned char* s_inv, float (*s_r)[3], uint64_t* s_bar)
 {
     constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
@@ -743,6 +652,8 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
     {
         const int      bank = gw + j * W;
         const int      slot = (u + j) % NST;
+        // BF16 tiles, except for stiff clusters (inverted in FP64): FP32 from HBM
+        const bool     use32 = BF && stiff != nullptr && stiff[gbank0 + bank] != 0;
         const bool     live = nlive;
         const uint32_t cm   = ncm;
         const int      nl   = nnl;
@@ -781,12 +692,14 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
         if(!__all_sync(0xffffffffu, ok))
             break;
         float* Zb = Z + 3 * ((int64_t)level_begin + (int64_t)bank * BANK);
-        if(BF)
+        if(BF && !use32)
             cluster_product_mma(s_inv + slot * CB, &s_r[0][0], lane, Zb);
         else
         {
-            float out[3];
-            cluster_product(reinterpret_cast<const float*>(s_inv + slot * CB), s_r, lane, out);
+            float        out[3];
+            const float* Mc = use32 ? inv32 + (size_t)(gbank0 + bank) * SYM * 9
+                                    : reinterpret_cast<const float*>(s_inv + slot * CB);
+            cluster_product(Mc, s_r, lane, out);
             if(lane < 16)
             {
                 Zb[3 * sub]     = out[0];
@@ -822,7 +735,7 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
     k_apply_level(int n_banks, int cnt, int level_begin, const int32_t* __restrict__ p2r, const VT* __restrict__ r,
                   int roff, const uint16_t* __restrict__ comp_mask, const int32_t* __restrict__ new_local,
                   int next_begin, int push, const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
-                  const int* converged, int* err)
+                  const uint8_t* __restrict__ stiff, const float* __restrict__ inv32, const int* converged, int* err)
 {
     if(converged && *converged)
         return;
@@ -840,8 +753,8 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
     __syncwarp();
     int u = 0;
     apply_banks<FINE, VT, BF, NST>(blockIdx.x * APPLY_WARPS + w, gridDim.x * APPLY_WARPS, lane, u, n_banks, cnt,
-                                   level_begin, p2r, r, roff, comp_mask, new_local, next_begin, push, inv, R, Z, err,
-                                   &s_inv[w][0][0], s_r[w], s_bar[w]);
+                                   level_begin, p2r, r, roff, comp_mask, new_local, next_begin, push, inv, R, Z, stiff,
+                                   inv32, err, &s_inv[w][0][0], s_r[w], s_bar[w]);
 }
 
 // persistent grid: as many CTAs as fit on the SMs at once (less `spare` per
@@ -1139,15 +1052,7 @@ void mas_assemble(b2s_solver* s, int invert_mode)
         prev_n   = M.level_count[level];
         map      = X.new_local[level].data();
     }
-    if(M.clusters > 0)
-    {
-        const int grid = (M.clusters + INV_CLUSTERS - 1) / INV_CLUSTERS;
-        if(invert_mode == B2S_INVERT_GJ_F64)
-            k_invert<double><<<grid, INV_BLOCK, 0, st>>>(M.clusters, M.hess.data(), M.inv.data());
-        else
-            k_invert<float><<<grid, INV_BLOCK, 0, st>>>(M.clusters, M.hess.data(), M.inv.data());
-        B2S_CHECK_LAUNCH();
-    }
+    mas_invert_clusters(s, invert_mode);
 }
 
 // z[off..off+vn) gets the MAS part of z = P r; Jacobi/identity elsewhere is
@@ -1162,6 +1067,7 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
     const int    n_banks0 = M.N / BANK;
     const int    tb       = APPLY_WARPS * 32;
     const unsigned char* inv = bf16 ? M.inv16.data() : reinterpret_cast<const unsigned char*>(M.inv.data());
+    const uint8_t*       stiff = bf16 ? M.stiff.data() : nullptr;
     // element offset of the range's first vertex in r (FP32: 4 per node)
     const int off = (sizeof(VT) == 4 ? 4 : 3) * M.offset;
     // With coarse levels, R_1 is restricted first (whole grid), then the
@@ -1187,7 +1093,8 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
         k<<<apply_grid(k, n_banks0, fork ? 1 : 0), tb, 0, st>>>(n_banks0, M.N, 0, M.p2r.data(), r, off,
                                                                   M.comp_mask[0].data(), M.new_local[0].data(),
                                                                   M.level_begin[1], (M.L > 1 && !fork) ? 1 : 0, inv,
-                                                                  M.R.data(), M.Z.data(), converged, err);
+                                                                  M.R.data(), M.Z.data(), stiff, M.inv.data(),
+                                                                  converged, err);
         B2S_CHECK_LAUNCH();
     }
     // coarse levels: one persistent launch each (on the graph's stream the
@@ -1207,7 +1114,8 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
                                                                     nullptr, 0, M.comp_mask[level].data(),
                                                                     M.new_local[level].data(),
                                                                     push ? M.level_begin[level + 1] : 0, push, inv,
-                                                                    M.R.data(), M.Z.data(), converged, err);
+                                                                    M.R.data(), M.Z.data(), stiff, M.inv.data(),
+                                                                    converged, err);
         B2S_CHECK_LAUNCH();
     }
     if(fork)

@@ -501,7 +501,8 @@ void precond_assemble(b2s_solver* s, int kind, int invert_mode)
 {
     B2S_REQUIRE(s->A.valid, B2S_ERR_STATE, "precond_assemble before b2s_assemble");
     B2S_REQUIRE(kind >= B2S_PRECOND_NONE && kind <= B2S_PRECOND_MAS, B2S_ERR_ARGUMENT, "unknown preconditioner");
-    B2S_REQUIRE(invert_mode == B2S_INVERT_SWEEP_F32 || invert_mode == B2S_INVERT_GJ_F64, B2S_ERR_ARGUMENT,
+    B2S_REQUIRE(invert_mode == B2S_INVERT_F32 || invert_mode == B2S_INVERT_F64 || invert_mode == B2S_INVERT_F32_ONLY,
+                B2S_ERR_ARGUMENT,
                 "unknown inversion mode");
     cudaStream_t st = s->stream;
     const Matrix& A = s->A;

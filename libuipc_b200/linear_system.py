@@ -143,6 +143,15 @@ class Solver:
         self._check(self.lib.b2s_mas_get_clusters(self.h, hess.ctypes.data, inv.ctypes.data))
         return hess, inv
 
+    def mas_stiff(self):
+        """(count, flags uint8 [clusters]) of the clusters the last build
+        inverted in FP64."""
+        L, tot = self.mas_info()
+        flags = np.zeros(max(tot // 16, 1), np.uint8)
+        n = C.c_int32(0)
+        self._check(self.lib.b2s_mas_stiff_info(self.h, C.byref(n), flags.ctypes.data))
+        return int(n.value), flags[: tot // 16]
+
     def mas_nodes(self):
         """(R, Z) node buffers of the last apply, float32 [total_nodes, 3]."""
         L, tot = self.mas_info()
@@ -157,7 +166,7 @@ class Solver:
         12x12 block-Jacobi there (ABDDiagPreconditioner)."""
         self._check(self.lib.b2s_abd_init(self.h, int(block_offset), int(n_bodies)))
 
-    def precond_assemble(self, kind: int, invert_mode: int = _abi.B2S_INVERT_SWEEP_F32):
+    def precond_assemble(self, kind: int, invert_mode: int = _abi.B2S_INVERT_F32):
         self._check(self.lib.b2s_precond_assemble(self.h, int(kind), int(invert_mode)))
 
     def precond_apply(self, r, z):
@@ -383,7 +392,7 @@ class B200MAS(GlobalPreconditioner):
     (ABDDiagPreconditioner) on their range."""
 
     def __init__(self, block_offset, vert_num, adj_start, adj_list, part_to_real, real_to_part,
-                 invert_mode=_abi.B2S_INVERT_SWEEP_F32, abd=None):
+                 invert_mode=_abi.B2S_INVERT_F32, abd=None):
         self.args = (block_offset, vert_num, adj_start, adj_list, part_to_real, real_to_part)
         self.invert_mode = invert_mode
         self.abd = abd
@@ -514,7 +523,9 @@ class GlobalLinearSystem:
         GlobalLinearSystem::solve runs it (global_linear_system.cu:85-106,
         321-544): extents and offsets, the -1 / 0 fill, each subsystem's writes
         into device arrays kept at the layout's reserved capacity, the solve, and
-        dx = -x handed to every diagonal subsystem; returns dx."""
+        the solution x handed to every diagonal subsystem on its range (each
+        subsystem negates it into its dx, as the reference's do); returns
+        dx = -x."""
         torch = _torch()
         n, T = layout.update()
         dev = torch.device("cuda", self.solver.device)
@@ -529,7 +540,7 @@ class GlobalLinearSystem:
         layout.assemble(rows, cols, vals, b)
         dx = self.solve(layout.n_block_rows, rows[:T], cols[:T], vals[:T], b[:n], history_slot=history_slot,
                         frame=frame, newton_iter=newton_iter)
-        layout.distribute(dx)
+        layout.distribute(-dx)
         return dx
 
 
