@@ -698,6 +698,8 @@ int orc_mas_assemble(orc_mas* s, const orc_matrix* A, int32_t off, int invert_mo
         }
     }
     s->inv.assign((size_t)s->clusters * SYM * 9, 0.0f);
+    // clusters are independent (each inversion uses its own thread's buffers)
+#pragma omp parallel for schedule(dynamic, 64)
     for(int c = 0; c < s->clusters; ++c)
     {
         if(invert_mode == 0)
@@ -767,6 +769,13 @@ void orc_mas_clusters(const orc_mas* s, double* hess, float* inv)
         std::memcpy(inv, s->inv.data(), sizeof(float) * s->inv.size());
 }
 
+// replace the cluster inverses (e.g. by the device's), so an apply can be
+// compared with the same inverse entries
+void orc_mas_set_inverses(orc_mas* s, const float* inv)
+{
+    std::memcpy(s->inv.data(), inv, sizeof(float) * s->inv.size());
+}
+
 // apply (:2887-2960): R_l = sum of float(r) over each level-l node's fine
 // vertices (build_multi_level_R :1205-1321), Z = cluster inverse * R per
 // cluster (schwarz_local_solve :1323-1414), z_v = double(sum_l Z_l[node_l(v)])
@@ -790,6 +799,8 @@ void orc_mas_apply(const orc_mas* s, const double* r, double* z)
                 R[(size_t)node * 3 + a] += rv[a];
         }
     }
+    // local solves: clusters are independent
+#pragma omp parallel for schedule(static)
     for(int c = 0; c < s->clusters; ++c)
     {
         const float* M = &s->inv[(size_t)c * SYM * 9];
@@ -818,6 +829,7 @@ void orc_mas_apply(const orc_mas* s, const double* r, double* z)
                 Z[((size_t)c * BANK + rn) * 3 + a] = acc[a];
         }
     }
+#pragma omp parallel for schedule(static)
     for(int v = 0; v < s->vn; ++v)
     {
         const int p = s->r2p[v];
@@ -849,6 +861,68 @@ struct Precond
     int32_t             off  = 0;
     std::vector<double> dinv;  // 3x3 inverses (row-major) of the diagonal blocks
     std::vector<char>   in_mas;
+    int32_t             abd_off = 0, abd_n = 0;  // affine bodies: 4 block rows each
+    std::vector<double> abd_inv;                 // [abd_n][12][12] row-major
+
+    // ABDDiagPreconditioner (affine_body/abd_diag_preconditioner.cu:15-125):
+    // the inverse of each body's full 12x12 diagonal block (FP64; Eigen's
+    // inverse there, Gauss-Jordan with partial pivoting here)
+    void build_abd(const orc_matrix* A)
+    {
+        abd_inv.assign((size_t)abd_n * 144, 0.0);
+        std::vector<double> H((size_t)abd_n * 144, 0.0);
+        for(size_t u = 0; u < A->rows.size(); ++u)
+        {
+            const int i = A->rows[u] - abd_off, j = A->cols[u] - abd_off;
+            if(i < 0 || j < 0 || i >= 4 * abd_n || j >= 4 * abd_n || i / 4 != j / 4)
+                continue;
+            double*       h  = &H[(size_t)(i / 4) * 144];
+            const int     bi = i % 4, bj = j % 4;
+            const double* B  = &A->vals[u * 9];  // column-major
+            for(int p = 0; p < 3; ++p)
+                for(int q = 0; q < 3; ++q)
+                {
+                    h[(3 * bi + p) * 12 + 3 * bj + q] = B[q * 3 + p];
+                    if(bi != bj)
+                        h[(3 * bj + q) * 12 + 3 * bi + p] = B[q * 3 + p];
+                }
+        }
+        for(int b = 0; b < abd_n; ++b)
+        {
+            double M[12][24];
+            for(int i = 0; i < 12; ++i)
+                for(int j = 0; j < 24; ++j)
+                    M[i][j] = j < 12 ? H[(size_t)b * 144 + i * 12 + j] : (j - 12 == i ? 1.0 : 0.0);
+            bool ok = true;
+            for(int c = 0; c < 12 && ok; ++c)
+            {
+                int piv = c;
+                for(int r = c + 1; r < 12; ++r)
+                    if(std::fabs(M[r][c]) > std::fabs(M[piv][c]))
+                        piv = r;
+                if(!(std::fabs(M[piv][c]) > 0.0))
+                {
+                    ok = false;
+                    break;
+                }
+                for(int j = 0; j < 24; ++j)
+                    std::swap(M[c][j], M[piv][j]);
+                const double d = 1.0 / M[c][c];
+                for(int j = 0; j < 24; ++j)
+                    M[c][j] *= d;
+                for(int r = 0; r < 12; ++r)
+                    if(r != c && M[r][c] != 0.0)
+                    {
+                        const double f = M[r][c];
+                        for(int j = 0; j < 24; ++j)
+                            M[r][j] -= f * M[c][j];
+                    }
+            }
+            for(int i = 0; i < 12; ++i)
+                for(int j = 0; j < 12; ++j)
+                    abd_inv[(size_t)b * 144 + i * 12 + j] = ok ? M[i][12 + j] : (i == j ? 1.0 : 0.0);
+        }
+    }
 
     void build(const orc_matrix* A)
     {
@@ -903,6 +977,21 @@ struct Precond
         }
         if(kind == ORC_PRECOND_MAS && mas)
             orc_mas_apply(mas, r + (size_t)off * 3, z + (size_t)off * 3);
+        // the affine-body range: the 12x12 block inverses (after the others,
+        // global_linear_system.cu:555-576)
+        for(int b = 0; b < abd_n; ++b)
+        {
+            const double* Hi = &abd_inv[(size_t)b * 144];
+            const double* rb = &r[(size_t)(abd_off + 4 * b) * 3];
+            double*       zb = &z[(size_t)(abd_off + 4 * b) * 3];
+            for(int i = 0; i < 12; ++i)
+            {
+                double acc = 0.0;
+                for(int j = 0; j < 12; ++j)
+                    acc += Hi[i * 12 + j] * rb[j];
+                zb[i] = acc;
+            }
+        }
     }
 };
 
@@ -922,6 +1011,14 @@ int orc_pcg(const orc_matrix* A, int precond, const orc_mas* mas, int32_t mas_of
             double* x, double tol, int stop_rule, int check_interval, int64_t max_iter, int n_threads,
             orc_pcg_result* out)
 {
+    return orc_pcg_abd(A, precond, mas, mas_off, 0, 0, b, x, tol, stop_rule, check_interval, max_iter, n_threads,
+                       out);
+}
+
+int orc_pcg_abd(const orc_matrix* A, int precond, const orc_mas* mas, int32_t mas_off, int32_t abd_off,
+                int32_t abd_n, const double* b, double* x, double tol, int stop_rule, int check_interval,
+                int64_t max_iter, int n_threads, orc_pcg_result* out)
+{
 #ifdef _OPENMP
     const int saved = omp_get_max_threads();
     omp_set_num_threads(n_threads > 0 ? n_threads : 1);
@@ -933,6 +1030,12 @@ int orc_pcg(const orc_matrix* A, int precond, const orc_mas* mas, int32_t mas_of
     P.mas  = mas;
     P.off  = mas_off;
     P.build(A);
+    if(precond != ORC_PRECOND_NONE && abd_n > 0)
+    {
+        P.abd_off = abd_off;
+        P.abd_n   = abd_n;
+        P.build_abd(A);
+    }
     auto spmv = [&](const double* in, double* o)
     {
         if(n_threads > 1)

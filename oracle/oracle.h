@@ -57,6 +57,8 @@ int  orc_mas_assemble(orc_mas* s, const orc_matrix* A, int32_t dof_offset_blocks
 void orc_mas_clusters(const orc_mas* s, double* cluster_hess, float* cluster_inv);
 // z = M^{-1} r on the MAS vertex range (r, z point at that range); FP32 inside.
 void orc_mas_apply(const orc_mas* s, const double* r, double* z);
+// overwrite the cluster inverses (clusters * 136 * 9 floats) after assemble
+void orc_mas_set_inverses(orc_mas* s, const float* cluster_inv);
 // Storage precision of the cluster inverses (applied to the current inverses
 // in place): 0 = FP32 (as assembled), 1 = BF16 (round to nearest even),
 // 2 = BF16 of the symmetrically diagonal-scaled inverse S M S with
@@ -88,6 +90,12 @@ typedef struct orc_pcg_result
 int orc_pcg(const orc_matrix* A, int precond, const orc_mas* mas, int32_t mas_offset_blocks,
             const double* b, double* x, double tol, int stop_rule, int check_interval,
             int64_t max_iter, int n_threads, orc_pcg_result* out);
+
+// the same with the 12x12 block Jacobi of abd_n affine bodies on block rows
+// [abd_off, abd_off + 4 abd_n) (applied after the other preconditioners)
+int orc_pcg_abd(const orc_matrix* A, int precond, const orc_mas* mas, int32_t mas_offset_blocks,
+                int32_t abd_off, int32_t abd_n, const double* b, double* x, double tol, int stop_rule,
+                int check_interval, int64_t max_iter, int n_threads, orc_pcg_result* out);
 
 // FP64 truth: block-Jacobi CG to ||r|| <= tol ||b|| (tol ~1e-13).
 int orc_cg_truth(const orc_matrix* A, const double* b, double* x, double tol, int64_t max_iter,

@@ -69,9 +69,13 @@ def lib() -> C.CDLL:
     L.orc_mas_assemble.argtypes = [vp, vp, i32, C.c_int]
     L.orc_mas_clusters.argtypes = [vp, vp, vp]
     L.orc_mas_apply.argtypes = [vp, vp, vp]
+    L.orc_mas_set_inverses.argtypes = [vp, vp]
     L.orc_mas_quantize.argtypes = [vp, C.c_int]
     L.orc_pcg.restype = C.c_int
     L.orc_pcg.argtypes = [vp, C.c_int, vp, i32, vp, vp, d, C.c_int, C.c_int, i64, C.c_int, C.POINTER(OrcPcgResult)]
+    L.orc_pcg_abd.restype = C.c_int
+    L.orc_pcg_abd.argtypes = [vp, C.c_int, vp, i32, i32, i32, vp, vp, d, C.c_int, C.c_int, i64, C.c_int,
+                              C.POINTER(OrcPcgResult)]
     L.orc_cg_truth.restype = C.c_int
     L.orc_cg_truth.argtypes = [vp, vp, vp, d, i64, C.c_int, C.POINTER(C.c_int64)]
     _lib = L
@@ -172,6 +176,13 @@ class OracleMAS:
         lib().orc_mas_clusters(self.h, _p(hess), _p(inv))
         return hess, inv
 
+    def set_inverses(self, inv: np.ndarray):
+        """Use these cluster inverses (float32 [clusters, 136, 9]) instead of
+        the oracle's own, e.g. the device's, to compare applies entry for entry."""
+        inv = np.ascontiguousarray(inv, dtype=np.float32)
+        assert inv.size == self.clusters * 136 * 9
+        lib().orc_mas_set_inverses(self.h, _p(inv))
+
     def quantize(self, mode: int):
         """0 = FP32 inverses, 1 = BF16, 2 = BF16 of the diagonal-scaled inverse."""
         lib().orc_mas_quantize(self.h, int(mode))
@@ -184,13 +195,16 @@ class OracleMAS:
 
 
 def pcg(A: OracleMatrix, b, precond=ORC_PRECOND_JACOBI, mas: OracleMAS | None = None, mas_offset=0, tol=1e-4,
-        stop_rule=ORC_STOP_RZ, check_interval=1, max_iter=0, threads=1):
+        stop_rule=ORC_STOP_RZ, check_interval=1, max_iter=0, threads=1, abd=(0, 0)):
+    """PCG as the reference runs it; ``abd = (block_offset, n_bodies)`` adds
+    the affine bodies' 12x12 block Jacobi on their block rows."""
     b = np.ascontiguousarray(b, dtype=np.float64)
     x = np.zeros_like(b)
     res = OrcPcgResult()
     mi = max_iter if max_iter > 0 else 2 * b.size
-    lib().orc_pcg(A.h, precond, mas.h if mas is not None else None, int(mas_offset), _p(b), _p(x), float(tol),
-                  int(stop_rule), int(check_interval), int(mi), int(threads), C.byref(res))
+    lib().orc_pcg_abd(A.h, precond, mas.h if mas is not None else None, int(mas_offset), int(abd[0]), int(abd[1]),
+                      _p(b), _p(x), float(tol), int(stop_rule), int(check_interval), int(mi), int(threads),
+                      C.byref(res))
     return x, {k: getattr(res, k) for k, _ in OrcPcgResult._fields_}
 
 
