@@ -24,6 +24,7 @@ struct NoallocScratch
 {
     double       partials[NOALLOC_MAX_TILES];  // per-tile partial dots, summed in tile order
     unsigned int counter;                      // CTAs finished (reset by the last one)
+    unsigned int bad_input;                    // a block failed the index / order checks
 };
 
 // Device-resident scratch shared by every call on a device (~256 KB). In host
@@ -61,16 +62,20 @@ __device__ __forceinline__ void red_add(double* p, double v)
 
 // One CTA per tile pass (grid-stride over tiles); thread = block of the
 // caller's BCOO (values 9 doubles, column-major, per block). Row parts are
-// merged over equal rows in-warp, transposed parts scatter as L2 reductions;
-// the tile's dot goes to scratch->partials[tile] and the last CTA adds the
-// partials in tile order (bit-reproducible for a given input).
-__global__ void __launch_bounds__(NOALLOC_TILE) k_spmv_noalloc(int64_t U, const int32_t* __restrict__ rows,
+// merged over equal rows in-warp (rows are non-decreasing, so equal rows are
+// contiguous), transposed parts scatter as L2 reductions; the tile's dot goes
+// to scratch->partials[tile] and the last CTA adds the partials in a fixed
+// order (bit-reproducible for a given input). A block whose row or column is
+// outside [0, nb), whose row exceeds its column, or whose row is below the
+// previous block's is skipped (no access through its indices) and makes the
+// dot NaN.
+__global__ void __launch_bounds__(NOALLOC_TILE) k_spmv_noalloc(int32_t nb, int64_t U, const int32_t* __restrict__ rows,
                                                                const int32_t* __restrict__ cols,
                                                                const double* __restrict__ vals,
                                                                const double* __restrict__ x, double* y,
                                                                double* dot_out, NoallocScratch* scratch)
 {
-    __shared__ double warp_dot[NOALLOC_TILE / 32];
+    __shared__ double red[NOALLOC_TILE];
     __shared__ bool   is_last;
     const int     lane    = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t n_tiles = (U + NOALLOC_TILE - 1) / NOALLOC_TILE;
@@ -81,24 +86,31 @@ __global__ void __launch_bounds__(NOALLOC_TILE) k_spmv_noalloc(int64_t U, const 
         double        a0 = 0, a1 = 0, a2 = 0, d = 0;
         if(k < U)
         {
-            r               = rows[k];
-            const int32_t c = cols[k];
-            double        b[9];
-#pragma unroll
-            for(int q = 0; q < 9; ++q)
-                b[q] = vals[k * 9 + q];
-            const double xj0 = x[3 * (int64_t)c], xj1 = x[3 * (int64_t)c + 1], xj2 = x[3 * (int64_t)c + 2];
-            const double xi0 = x[3 * (int64_t)r], xi1 = x[3 * (int64_t)r + 1], xi2 = x[3 * (int64_t)r + 2];
-            a0 = b[0] * xj0 + b[3] * xj1 + b[6] * xj2;
-            a1 = b[1] * xj0 + b[4] * xj1 + b[7] * xj2;
-            a2 = b[2] * xj0 + b[5] * xj1 + b[8] * xj2;
-            d  = xi0 * a0 + xi1 * a1 + xi2 * a2;
-            if(r != c)
+            const int32_t rk = rows[k];
+            const int32_t c  = cols[k];
+            const bool    ok = rk >= 0 && rk < nb && c >= rk && c < nb && (k == 0 || rows[k - 1] <= rk);
+            if(!ok)
+                atomicOr(&scratch->bad_input, 1u);
+            else
             {
-                red_add(y + 3 * (int64_t)c, b[0] * xi0 + b[1] * xi1 + b[2] * xi2);
-                red_add(y + 3 * (int64_t)c + 1, b[3] * xi0 + b[4] * xi1 + b[5] * xi2);
-                red_add(y + 3 * (int64_t)c + 2, b[6] * xi0 + b[7] * xi1 + b[8] * xi2);
-                d += d;
+                r = rk;
+                double b[9];
+#pragma unroll
+                for(int q = 0; q < 9; ++q)
+                    b[q] = vals[k * 9 + q];
+                const double xj0 = x[3 * (int64_t)c], xj1 = x[3 * (int64_t)c + 1], xj2 = x[3 * (int64_t)c + 2];
+                const double xi0 = x[3 * (int64_t)r], xi1 = x[3 * (int64_t)r + 1], xi2 = x[3 * (int64_t)r + 2];
+                a0 = b[0] * xj0 + b[3] * xj1 + b[6] * xj2;
+                a1 = b[1] * xj0 + b[4] * xj1 + b[7] * xj2;
+                a2 = b[2] * xj0 + b[5] * xj1 + b[8] * xj2;
+                d  = xi0 * a0 + xi1 * a1 + xi2 * a2;
+                if(r != c)
+                {
+                    red_add(y + 3 * (int64_t)c, b[0] * xi0 + b[1] * xi1 + b[2] * xi2);
+                    red_add(y + 3 * (int64_t)c + 1, b[3] * xi0 + b[4] * xi1 + b[5] * xi2);
+                    red_add(y + 3 * (int64_t)c + 2, b[6] * xi0 + b[7] * xi1 + b[8] * xi2);
+                    d += d;
+                }
             }
         }
 #pragma unroll
@@ -127,13 +139,13 @@ __global__ void __launch_bounds__(NOALLOC_TILE) k_spmv_noalloc(int64_t U, const 
         for(int o = 16; o > 0; o >>= 1)
             d += __shfl_xor_sync(0xffffffffu, d, o);
         if(lane == 0)
-            warp_dot[warp] = d;
+            red[warp] = d;
         __syncthreads();
         if(threadIdx.x == 0)
         {
             double t = 0.0;
             for(int w = 0; w < NOALLOC_TILE / 32; ++w)
-                t += warp_dot[w];
+                t += red[w];
             scratch->partials[tile] = t;
         }
         __syncthreads();
@@ -148,14 +160,29 @@ __global__ void __launch_bounds__(NOALLOC_TILE) k_spmv_noalloc(int64_t U, const 
     if(!is_last)
         return;
     __threadfence();
+    // the last CTA: thread t sums its contiguous chunk of the partials in
+    // order, then a fixed pairwise tree over the threads
+    const int64_t chunk = (n_tiles + NOALLOC_TILE - 1) / NOALLOC_TILE;
+    const int64_t q0    = (int64_t)threadIdx.x * chunk;
+    const int64_t q1    = q0 + chunk < n_tiles ? q0 + chunk : n_tiles;
+    double        t     = 0.0;
+    for(int64_t q = q0; q < q1; ++q)
+        t += ((volatile double*)scratch->partials)[q];
+    red[threadIdx.x] = t;
+    __syncthreads();
+    for(int h = NOALLOC_TILE / 2; h > 0; h >>= 1)
+    {
+        if(threadIdx.x < h)
+            red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
     if(threadIdx.x == 0)
     {
-        double t = 0.0;
-        for(int64_t q = 0; q < n_tiles; ++q)
-            t += ((volatile double*)scratch->partials)[q];
+        const bool bad = ((volatile unsigned int*)&scratch->bad_input)[0] != 0u;
         if(dot_out)
-            *dot_out = t;
-        scratch->counter = 0u;
+            *dot_out = bad ? __longlong_as_double(0x7ff8000000000000ll) : red[0];
+        scratch->counter   = 0u;
+        scratch->bad_input = 0u;
     }
 }
 }  // namespace
@@ -176,9 +203,10 @@ extern "C" int b2s_spmv_noalloc(int32_t n_block_rows, int64_t n_blocks, const in
                     "b2s_spmv_noalloc: null array");
         cudaStream_t   st      = static_cast<cudaStream_t>(stream);
         NoallocScratch* scratch = scratch_for_current_device();
-        // y = A x overwrites y; the completion counter must start at zero
+        // y = A x overwrites y; the completion counter and the input-check
+        // word must start at zero (the array keeps the last call's contents)
         B2S_CUDA(cudaMemsetAsync(d_y, 0, sizeof(double) * 3 * (size_t)n_block_rows, st));
-        B2S_CUDA(cudaMemsetAsync(&scratch->counter, 0, sizeof(unsigned int), st));
+        B2S_CUDA(cudaMemsetAsync(&scratch->counter, 0, 2 * sizeof(unsigned int), st));
         if(n_blocks == 0)
         {
             if(d_dot)
@@ -187,7 +215,7 @@ extern "C" int b2s_spmv_noalloc(int32_t n_block_rows, int64_t n_blocks, const in
         }
         const int64_t n_tiles = (n_blocks + NOALLOC_TILE - 1) / NOALLOC_TILE;
         const int     grid    = (int)std::min<int64_t>(n_tiles, (int64_t)NUM_SMS_HINT * 8);
-        k_spmv_noalloc<<<grid, NOALLOC_TILE, 0, st>>>(n_blocks, d_rows, d_cols, d_vals, d_x, d_y, d_dot, scratch);
+        k_spmv_noalloc<<<grid, NOALLOC_TILE, 0, st>>>(n_block_rows, n_blocks, d_rows, d_cols, d_vals, d_x, d_y, d_dot, scratch);
         B2S_CUDA(cudaGetLastError());
         return B2S_OK;
     }
