@@ -17,8 +17,10 @@ Follows src/backends/cuda/linear_system/global_linear_system.cu:
     dof_offset/3); a coupling writes lr blocks at (l_offset, r_offset) and rl
     blocks at (r_offset, l_offset) (TripletMatrixView::subview / submatrix,
     cuda_tool/linear_system/views.h:77-88);
-  * distribute_solution (:531-544): each diagonal subsystem receives
-    dx = -x on its DoF range (do_retrieve_solution).
+  * distribute_solution (:531-544): each diagonal subsystem receives the
+    solution x of A x = b on its DoF range (SolutionInfo::solution) and turns
+    it into its own displacement, dx = -x (FEMLinearSubsystem's
+    retrieve_solution kernel, finite_element/fem_linear_subsystem.cu:119-126).
 
 The arrays are torch tensors (any device) or numpy arrays; a subsystem writes
 with ``write`` (one block) or ``write_many`` (vectorised).
@@ -135,13 +137,15 @@ class OffDiagInfo:
 
 
 class SolutionInfo:
-    """GlobalLinearSystem::SolutionInfo: ``solution()`` = dx on the subsystem's DoF range."""
+    """GlobalLinearSystem::SolutionInfo: ``solution()`` = x, the solution of
+    A x = b, on the subsystem's DoF range; the subsystem negates it into its
+    displacement dx = -x, as the reference's subsystems do."""
 
-    def __init__(self, dx):
-        self._dx = dx
+    def __init__(self, x):
+        self._x = x
 
     def solution(self):
-        return self._dx
+        return self._x
 
 
 class DiagLinearSubsystem:
@@ -249,10 +253,11 @@ class SubsystemLayout:
             o.assemble(OffDiagInfo(TripletView(rows, cols, vals, off, lr, (lb, rb), (ln, rn)),
                                    TripletView(rows, cols, vals, off + lr, rl, (rb, lb), (rn, ln))))
 
-    def distribute(self, dx):
-        """Each diagonal subsystem receives dx on its DoF range."""
+    def distribute(self, x):
+        """Each diagonal subsystem receives the solution x on its DoF range
+        (it negates it into dx itself)."""
         for d, off, cnt in zip(self.diag, self.dof_offsets, self.dof_counts):
-            d.retrieve_solution(SolutionInfo(dx[off:off + cnt]))
+            d.retrieve_solution(SolutionInfo(x[off:off + cnt]))
 
 
 def _exclusive_scan(counts):

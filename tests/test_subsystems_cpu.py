@@ -39,7 +39,8 @@ class Body(DiagLinearSubsystem):
         info.write_gradients(self.g)
 
     def retrieve_solution(self, info):
-        self.dx = info.solution()
+        # as FEMLinearSubsystem / ABDLinearSubsystem: dx = -x
+        self.dx = -info.solution()
 
 
 class Mesh(DiagLinearSubsystem):
@@ -58,7 +59,8 @@ class Mesh(DiagLinearSubsystem):
         info.write_gradients(self.g)
 
     def retrieve_solution(self, info):
-        self.dx = info.solution()
+        # as FEMLinearSubsystem / ABDLinearSubsystem: dx = -x
+        self.dx = -info.solution()
 
 
 class Coupling(OffDiagLinearSubsystem):
@@ -173,6 +175,6 @@ def test_writes_are_range_checked_and_solution_is_distributed():
         v.write(3, 0, 0, np.zeros(9))  # slot outside the range
     with pytest.raises(IndexError):
         v.write_many(1, [0, 1, 2], [0, 0, 0], np.zeros((3, 9)))
-    dx = np.arange(n, dtype=np.float64)
-    lay.distribute(dx)
-    assert np.array_equal(body.dx, dx[:12]) and np.array_equal(mesh.dx, dx[12:])
+    x = np.arange(n, dtype=np.float64)
+    lay.distribute(x)  # the solution of A x = b; each subsystem negates it
+    assert np.array_equal(body.dx, -x[:12]) and np.array_equal(mesh.dx, -x[12:])
