@@ -434,50 +434,119 @@ def full_scale_run(dev, steps: int, warmup: int) -> dict:
     return out
 
 
+TRUTH_TOL = 1e-10  # FP64 rel-res of the solves that advance the run (both arms)
+
+
+def system_checksum(s) -> dict:
+    """Fingerprint of a Newton system, printed by both arms so a reader can
+    see they solve the same one: triplet count, sum and norm of b, and b
+    against a fixed pseudo-random vector."""
+    import numpy as np
+
+    w = np.sin(0.37 * np.arange(s.b.size) + 0.1)
+    return {"n_triplets": int(s.n_triplets), "b_sum": float(s.b.sum()), "b_norm": float(np.linalg.norm(s.b)),
+            "b_dot_w": float(s.b @ w)}
+
+
 def run_reference(args, rank: int) -> None:
-    """The reference's algorithm on the host cores (the oracle port of
-    libuipc's FP64 MAS-PCG; the CUDA reference cannot be built here)."""
+    """The reference's algorithm on the host cores: the oracle port of
+    libuipc's FP64 MAS-PCG (the CUDA reference cannot be built here), on the
+    same Newton system the GPU arm times. The run is stepped exactly as the
+    GPU arm steps it (backward Euler, one Newton iteration per step, each
+    solve to FP64 rel-res 1e-10, here by the oracle's MAS-PCG), so step
+    --history-steps + 1's system is the same up to those solves' residuals
+    (the line's system_checksum). The MAS partition is RCB restated in numpy
+    (the one the GPU arm uses: the reference's METIS takes ~15 min for these
+    551 k vertices). No product library is loaded: the scene generator
+    (input data) and the oracle only.
+
+    Timing: the assembly and the MAS build once, then each of the W + K
+    steps is a bounded sample of the PCG: a 2-iteration and a 12-iteration
+    run (all host threads); per-iteration time = (t12 - t2) / 10 and the
+    per-solve fixed cost = t2 - 2 per-iteration, medians over the K timed
+    steps; ms/solve = assembly + build + fixed + (iterations to rel-res 1e-4,
+    from one full solve) x per-iteration."""
     if rank != 0:
         return
     import numpy as np
 
-    from libuipc_b200.linear_system import partition_maps, partition_rcb
+    from libuipc_b200.sequence import SceneSequence
     from oracle import oracle as O
 
-    s, _ = build_workload(args.workload)
     threads = os.cpu_count() or 1
-    pid = partition_rcb(s.positions)
-    p2r, r2p = partition_maps(pid)
-    M = O.OracleMAS(s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
-    times, iters = [], []
-    # bounded: one untimed solve at most (host code needs no clock warm-up),
-    # and no further timed solve once ~150 s are spent (at least one is timed)
-    warm = min(args.warmup, 1)
-    budget_s, t_start = 150.0, time.time()
-    for k in range(warm + args.steps):
-        if k > warm and time.time() - t_start > budget_s:
-            break
-        t0 = time.time()
-        A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals)
-        M.assemble(A, 0, 0)
-        _, info = O.pcg(A, s.b, precond=O.ORC_PRECOND_MAS, mas=M, tol=1e-4, stop_rule=O.ORC_STOP_RELRES,
-                        check_interval=5, threads=threads)
-        dt = (time.time() - t0) * 1e3
-        if k >= warm:
-            times.append(dt)
-            iters.append(int(info["iterations"]))
-        del A
-    ms = sum(times) / len(times)
+    w = WORKLOADS[args.workload]
+    t_setup = time.time()
+    seq = SceneSequence(scene=1, cells_x=w["cells"], cells_y=w["cells"], cells_z=w["cells"], n_cubes=w["n_cubes"],
+                        seed=w["seed"])
+    p2r, r2p = O.partition_maps(O.rcb_partition(seq.rest))
+    M = O.OracleMAS(seq.n_verts, seq.adj_start, seq.adj_list, p2r, r2p)
+    for _ in range(args.history_steps):
+        seq.begin_step()
+        sh = seq.system()
+        Ah = O.OracleMatrix(sh.n_verts, sh.rows, sh.cols, sh.vals)
+        M.assemble(Ah, 0, 0)
+        xh, _ = O.pcg(Ah, sh.b, precond=O.ORC_PRECOND_MAS, mas=M, tol=TRUTH_TOL, stop_rule=O.ORC_STOP_RELRES,
+                      threads=threads)
+        seq.apply(xh)
+        seq.end_step()
+        del Ah, sh
+    seq.begin_step()
+    s = seq.system()
+    setup_s = time.time() - t_setup
+    t0 = time.time()
+    A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals)
+    t_asm = time.time() - t0
+    t0 = time.time()
+    M.assemble(A, 0, 0)
+    t_build = time.time() - t0
+    t0 = time.time()
+    _, full = O.pcg(A, s.b, precond=O.ORC_PRECOND_MAS, mas=M, tol=1e-4, stop_rule=O.ORC_STOP_RELRES,
+                    threads=threads)
+    t_full = time.time() - t0
+    iters = int(full["iterations"])
+
+    def sample(n_it):
+        # orc_pcg runs max_iter - 1 iterations; tol 0 never stops early
+        t = time.time()
+        O.pcg(A, s.b, precond=O.ORC_PRECOND_MAS, mas=M, tol=0.0, stop_rule=O.ORC_STOP_RELRES,
+              max_iter=n_it + 1, threads=threads)
+        return time.time() - t
+
+    steps_s, per_it, fixed = [], [], []
+    for k in range(args.warmup + args.steps):
+        t2 = sample(2)
+        t12 = sample(12)
+        if k >= args.warmup:
+            steps_s.append(t2 + t12)
+            pi = (t12 - t2) / 10.0
+            per_it.append(pi)
+            fixed.append(t2 - 2.0 * pi)
+    pi = statistics.median(per_it)
+    fx = statistics.median(fixed)
+    ms = (t_asm + t_build + fx + iters * pi) * 1e3
+    step_ms = statistics.mean(steps_s) * 1e3
     line = {
         "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms/solve", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "precision": "fp64", "preconditioner": "mas", "stop": "rel-res 1e-4"},
-        "pcg_iterations": iters[-1] if iters else None,
+        "config": {"workload": args.workload,
+                   "system": f"Newton system of step {seq.step} of the falling stack (1 Newton iteration per step; "
+                             f"steps 1-{seq.step - 1} solved to FP64 rel-res {TRUTH_TOL:g})",
+                   "system_checksum": system_checksum(s), "precision": "fp64", "preconditioner": "mas",
+                   "partition": "rcb (numpy restatement, identical to the GPU arm's)", "stop": "rel-res 1e-4"},
+        "pcg_iterations": iters,
+        "rel_res": float(full["rel_res_true"]),
+        "stages_ms": {"assembly": t_asm * 1e3, "mas_build": t_build * 1e3, "pcg_fixed": fx * 1e3,
+                      "pcg_per_iteration": pi * 1e3, "full_solve_once_pcg": t_full * 1e3},
+        "setup_s": setup_s,
         "cpu_baseline": {"value": ms, "unit": "ms/solve", "cores": threads, "kind": "port",
-                         "sample": f"full solve per step: assembly + MAS build + MAS-PCG to rel-res 1e-4; "
-                                   f"{len(times)} of {args.steps} steps timed within the 150 s budget"},
+                         "sample": f"per step: a 2- and a 12-iteration MAS-PCG run on the step-{seq.step} system; "
+                                   f"ms/solve = assembly + MAS build (timed once) + fixed + {iters} iterations x "
+                                   "the per-iteration time (medians over the timed steps)"},
         "e2e": {"value": ms, "unit": "ms/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_libraries": {"solve": "oracle/_build/liboracle.so (the reference's algorithm restated)",
+                                "inputs": "libuipc_b200/_lib/libb200scene.so (the synthetic Newton-system generator "
+                                          "both arms use)"},
     }
     print(json.dumps(line), flush=True)
 
@@ -501,12 +570,13 @@ def main() -> None:
                     help="solutions the headline run's starts combine (the twisted-bar runs use 8)")
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed solves with cudaProfilerStart/Stop (ncu --profile-from-start off)")
-    ap.add_argument("--configs", action="store_true",
-                    help="also run C1 (10^3 cube) and C3 (cloth over affine bodies): plain vs mixed, CPU baseline")
-    ap.add_argument("--learned-bar", action="store_true",
-                    help="also run the learned warm start at the 200x20x20 twisted bar's scale: 2000 training "
-                         "systems generated and solved on the GPU, then zero / previous-dx / history / learned "
-                         "starts compared on 200 later systems (a few minutes)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the small configs run beside the headline: one 10^3-cell cube and a 256^2 cloth "
+                         "over 64 affine bodies (plain vs mixed, CPU baseline)")
+    ap.add_argument("--no-learned-bar", action="store_true",
+                    help="skip the learned warm start at the 200x20x20 twisted bar's scale (2000 training systems "
+                         "generated and solved on the GPU, then zero / previous-dx / history / learned starts "
+                         "compared on 200 later systems: about three minutes)")
     ap.add_argument("--no-full-scale", action="store_true",
                     help="skip the 9.7 M-DoF cube grid + cloth + bodies case run beside the headline")
     ap.add_argument("--no-bar", action="store_true",
@@ -548,7 +618,7 @@ def main() -> None:
     solver.set_stream(stream.cuda_stream)
     # the falling stack gains nothing from more than the 3 latest solutions
     # (its motion is dominated by the contacts), so its starts combine 3
-    runner = SequenceRunner(solver, seq, dev, history=args.history)
+    runner = SequenceRunner(solver, seq, dev, truth_tol=TRUTH_TOL, history=args.history)
     solver.ws_init(128, seed=0)
     with torch.cuda.stream(stream):
         runner.run(args.history_steps, newton_iters=1, collect=True)
@@ -667,14 +737,14 @@ def main() -> None:
             full = {"error": str(e)}
 
     configs = None
-    if rank == 0 and args.configs:
+    if rank == 0 and not args.no_configs:
         try:
             configs = configs_run(dev)
         except Exception as e:  # reported, not fatal
             configs = {"error": str(e)}
 
     learned_bar = None
-    if rank == 0 and args.learned_bar:
+    if rank == 0 and not args.no_learned_bar:
         from libuipc_b200.learned import run_gpu_bar
 
         try:
@@ -778,6 +848,7 @@ def main() -> None:
         "config": {"workload": args.workload, "system": f"Newton system of step {seq.step} of the falling stack "
                    f"(1 Newton iteration per step; history and training from steps 1-{seq.step - 1})",
                    "n_dof": 3 * s.n_verts, "n_triplets": s.n_triplets, "upper_blocks": U, "contacts": s.n_contacts,
+                   "system_checksum": system_checksum(s),
                    "preconditioner": "mas", "stop": "FP64-verified rel-res 1e-4",
                    "warm_start": f"learned (MLP on MAS level-1 aggregates + Galerkin with the {args.history} latest "
                                  "solutions)",

@@ -127,6 +127,11 @@ struct Matrix
     DBuf<uint16_t> trank;    // [stride]
     bool           has_trank = false;
     DBuf<int32_t>  diag_index;  // [nb] position of block (i,i), -1 if absent
+    // row starts of the FP32 SpMV, per group of 128 blocks: the first block's
+    // row and a 128-bit mask of the blocks that start a row (no row ids read)
+    DBuf<int32_t>  grp_row;
+    DBuf<uint4>    grp_mask;
+    bool           has_groups = false;
     bool           valid = false;
     long long      generation = 0;         // bumped by every assembly
     long long      vals32_generation = -1;  // assembly the FP32 planes were made from
@@ -160,6 +165,8 @@ struct MasState
     // device hierarchy
     DBuf<int32_t> p2r, r2p;        // [N], [vn]
     DBuf<int32_t> ctable;          // [vn * (L-1)] global node at levels 1..L-1
+    DBuf<int32_t> node1;           // [vn] global level-1 node of each vertex (-1: none)
+    DBuf<int32_t> anc;             // [level_count[1] * (L-2)] global slots of each level-1 node's ancestors
     DBuf<int32_t> cst;             // [L * vn] local id of vertex v at level l+1
     DBuf<uint16_t> comp_mask[MAX_LEVELS];  // per level: component lane mask of each node
     DBuf<int32_t>  new_local[MAX_LEVELS];  // per level: local id of each node at the next level
@@ -176,7 +183,8 @@ struct MasState
     Matrix        coarse[MAX_LEVELS];
     DBuf<int32_t> trip_rows, trip_cols;
     DBuf<double>  trip_vals;
-    // apply buffers (FP32, 3 per node slot)
+    // apply buffers (FP32, 3 per node slot); after an apply the level-1 slots
+    // of Z hold the folded prolongation Z_1 + Z_2[parent] + ...
     DBuf<float>   R, Z;
     // host copies for introspection
     std::vector<int32_t> h_ctable;

@@ -228,6 +228,13 @@ __global__ void k_h_ctable(int vn, int L, const int32_t* cst, const int32_t* lev
     }
 }
 
+__global__ void k_h_node1(int vn, int L, const int32_t* ctable, int32_t* node1)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if(v < vn)
+        node1[v] = ctable[(size_t)v * (L - 1)];
+}
+
 // ---------------------------------------------------------------------------
 // Galerkin matrices
 // ---------------------------------------------------------------------------
@@ -534,26 +541,53 @@ __device__ __forceinline__ void cluster_product(const float* M, const float (*r)
     out[2] = acc2;
 }
 
-// The banks of one level handled by one warp (warp gw of W): FINE: level 0,
-// the residual is gathered from r through part_to_real; otherwise R_l is read
-// from the node buffer. With `push`, the restriction sums of the next level
-// (one per connected component of the bank, summed by its lowest lane in lane
-// order) are written to R_{l+1}. Z_l = A_l^{-1} R_l for every node of the
-// bank. BF: BF16 tiles on the tensor cores (INV16_BYTES per cluster),
-// otherwise FP32 (INV_BYTES). VT: type of the fine residual (FP32: 4 values
-// per node, padded; FP64: 3), roff its element offset of the range's first
-// vertex. NST: copies in flight per warp. `u` counts the banks this warp
-// has run through its slots (slot and phase of the next copy), so one warp
-// can go through several levels. Returns false when a copy wait ran out (the error flag is set and
-// the warp's copies in flight are drained).
+// The banks of one level handled by one warp (warp gw of W). Every bank's
+// residual slice R_l (16 nodes x 3 floats, 192 B, contiguous: level 0's slots
+// are written by k_restrict_fine) and its inverse come into shared memory by
+// bulk copies (TMA) on one barrier, NST banks ahead per warp, so a warp never
+// waits on a dependent gather. With `push`, the restriction sums of the next
+// level (one per connected component of the bank, summed by its lowest lane
+// in lane order) are written to R_{l+1}. Z_l = A_l^{-1} R_l for every node of
+// the bank. BF: BF16 tiles on the tensor cores (INV16_BYTES per cluster),
+// otherwise FP32 (INV_BYTES); a stiff cluster (inverted in FP64) is applied
+// from its FP32 inverse in HBM in the BF16 path. `u` counts the banks this
+// warp has run through its slots (slot and phase of the next copy). Returns
+// false when a copy wait ran out (the error flag is set and the warp's copies
+// in flight are drained).
+constexpr uint32_t R_BYTES = BANK * 3 * sizeof(float);  // 192
 
-// the copies of a level's first NST banks of warp gw (lane 0 issues)
-template <bool BF, int NST>
-__device__ __forceinline__ void issue_first_copies(int gw, int W, int lane, int u, int n_banks, int level_begin,
-                                                   const unsigned char* __restrict__ inv, unsigned char* s_inv,
-                                                   uint64_t* s_bar)
+template <bool BF>
+__host__ __device__ constexpr uint32_t stage_bytes()
+{
+    return (BF ? INV16_BYTES : INV_BYTES) + R_BYTES;
+}
+
+// the bank's inverse and (R_TMA) its residual slice, on one barrier
+template <bool BF, bool R_TMA>
+__device__ __forceinline__ void issue_bank_copy(unsigned char* stage, uint64_t* bar, const unsigned char* inv,
+                                                const float* R, int64_t gbank)
 {
     constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
+    mbar_arrive_expect_tx(bar, CB + (R_TMA ? R_BYTES : 0u));
+    bulk_copy_g2s(stage, inv + (size_t)gbank * CB, CB, bar);
+    if(R_TMA)
+        bulk_copy_g2s(stage + CB, R + (size_t)gbank * (BANK * 3), R_BYTES, bar);
+}
+
+// R_TMA: the residual slice comes with the inverse by bulk copy (written by
+// an earlier kernel); otherwise lanes 0-15 load it (written earlier in the
+// same kernel: the single-CTA tail of the small levels)
+template <bool BF, int NST, bool R_TMA>
+__device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int n_banks, int cnt, int level_begin,
+                                            const uint16_t* __restrict__ comp_mask,
+                                            const int32_t* __restrict__ new_local, int next_begin, int push,
+                                            const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
+                                            const uint8_t* __restrict__ stiff, const float* __restrict__ inv32,
+                                            int* err, unsigned char* s_stage, uint64_t* s_bar)
+{
+    constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
+    constexpr uint32_t SB = stage_bytes<BF>();
+    const int     sub    = lane & 15;
     const int     mine   = gw < n_banks ? (n_banks - 1 - gw) / W + 1 : 0;
     const int64_t gbank0 = level_begin / BANK;
     if(lane == 0)
@@ -562,118 +596,49 @@ __device__ __forceinline__ void issue_first_copies(int gw, int W, int lane, int 
         for(int j = 0; j < mine && j < NST; ++j)
         {
             const int slot = (u + j) % NST;
-            mbar_arrive_expect_tx(&s_bar[slot], CB);
-            bulk_copy_g2s(s_inv + slot * CB, inv + (size_t)(gbank0 + gw + (int64_t)j * W) * CB, CB, &s_bar[slot]);
+            issue_bank_copy<BF, R_TMA>(s_stage + slot * SB, &s_bar[slot], inv, R, gbank0 + gw + (int64_t)j * W);
         }
     }
     __syncwarp();
-}
-
-template <bool FINE, typename VT, bool BF, int NST>
-__device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int n_banks, int cnt, int level_begin,
-                                            const int32_t* __restrict__ p2r, const VT* __restrict__ r, int roff,
-                                            const uint16_t* __restrict__ comp_mask,
-                                            const int32_t* __restrict__ new_local, int next_begin, int push,
-                                            const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
-                                            const uint8_t* __restrict__ stiff, const float* __restrict__ inv32,
-                                            int* err, unsigned char* s_inv, float (*s_r)[3], uint64_t* s_bar)
-{
-    constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
-    const int     sub    = lane & 15;
-    const int     mine   = gw < n_banks ? (n_banks - 1 - gw) / W + 1 : 0;
-    const int64_t gbank0 = level_begin / BANK;
-    issue_first_copies<BF, NST>(gw, W, lane, u, n_banks, level_begin, inv, s_inv, s_bar);
-    // registers of the next bank (lanes 0-15): residual, liveness, component
-    // mask and next-level index; at level 0 also part_to_real two banks ahead
-    float    n0 = 0.f, n1 = 0.f, n2 = 0.f;
-    bool     nlive = false;
-    uint32_t ncm   = 0;
-    int      nnl   = 0;
-    int      v_ahead = -1;
-    auto load_index = [&](int jj) -> int {
-        return (FINE && lane < 16 && jj < mine) ? p2r[(gw + jj * W) * BANK + sub] : -1;
-    };
-    auto load_bank = [&](int jj, int v) {
-        n0 = n1 = n2 = 0.f;
-        nlive = false;
-        ncm   = 0;
-        nnl   = 0;
-        if(lane >= 16 || jj >= mine)
+    // component mask and next-level index of the next bank (lanes 0-15)
+    uint32_t ncm = 0;
+    int      nnl = 0;
+    auto load_meta = [&](int jj) {
+        ncm = 0;
+        nnl = 0;
+        if(!push || lane >= 16 || jj >= mine)
             return;
         const int node = (gw + jj * W) * BANK + sub;
-        if(FINE)
-        {
-            nlive = v >= 0;
-            if(nlive)
-            {
-                if constexpr(sizeof(VT) == 4)
-                {
-                    // padded FP32 residual of the mixed PCG: one 16-byte load
-                    const float4 q = *reinterpret_cast<const float4*>(r + roff + 4 * (int64_t)v);
-                    n0 = q.x;
-                    n1 = q.y;
-                    n2 = q.z;
-                }
-                else
-                {
-                    n0 = (float)r[roff + 3 * (int64_t)v];
-                    n1 = (float)r[roff + 3 * (int64_t)v + 1];
-                    n2 = (float)r[roff + 3 * (int64_t)v + 2];
-                }
-            }
-        }
-        else
-        {
-            nlive = node < cnt;
-            if(nlive)
-            {
-                const int64_t g = (int64_t)level_begin + node;
-                n0 = R[3 * g];
-                n1 = R[3 * g + 1];
-                n2 = R[3 * g + 2];
-            }
-        }
-        if(push && nlive)
+        if(node < cnt)
         {
             ncm = comp_mask[node];
             nnl = new_local[node];
         }
     };
-    if(FINE)
-    {
-        const int v0 = load_index(0);
-        v_ahead      = load_index(1);
-        load_bank(0, v0);
-    }
-    else
-        load_bank(0, -1);
+    load_meta(0);
     int j = 0;
     for(; j < mine; ++j)
     {
-        const int      bank = gw + j * W;
-        const int      slot = (u + j) % NST;
-        // BF16 tiles, except for stiff clusters (inverted in FP64): FP32 from HBM
+        const int      bank  = gw + j * W;
+        const int      slot  = (u + j) % NST;
         const bool     use32 = BF && stiff != nullptr && stiff[gbank0 + bank] != 0;
-        const bool     live = nlive;
-        const uint32_t cm   = ncm;
-        const int      nl   = nnl;
-        if(lane < 16)
+        const uint32_t cm    = ncm;
+        const int      nl    = nnl;
+        const bool     live  = bank * BANK + sub < cnt;
+        load_meta(j + 1);
+        unsigned char* stage = s_stage + slot * SB;
+        float(*s_r)[3]       = reinterpret_cast<float(*)[3]>(stage + CB);
+        if(!R_TMA && lane < 16)
         {
-            s_r[sub][0] = n0;
-            s_r[sub][1] = n1;
-            s_r[sub][2] = n2;
+            const int64_t g = (int64_t)level_begin + (int64_t)bank * BANK + sub;
+            s_r[sub][0]     = live ? R[3 * g] : 0.f;
+            s_r[sub][1]     = live ? R[3 * g + 1] : 0.f;
+            s_r[sub][2]     = live ? R[3 * g + 2] : 0.f;
         }
-        // the next bank's loads are issued now and land while this one computes
-        if(FINE)
-        {
-            const int v1 = v_ahead;
-            v_ahead      = load_index(j + 2);
-            load_bank(j + 1, v1);
-        }
-        else
-            load_bank(j + 1, -1);
-        __syncwarp();
-        if(push && live && (cm & ((1u << lane) - 1u)) == 0)
+        const bool ok = mbar_wait(&s_bar[slot], (uint32_t)(((u + j) / NST) & 1), err, DERR_TMA_TIMEOUT);
+        if(!__all_sync(0xffffffffu, ok))
+            break;
+        if(push && lane < 16 && live && (cm & ((1u << lane) - 1u)) == 0)
         {
             float s0 = 0.f, s1 = 0.f, s2 = 0.f;
             for(uint32_t m = cm; m; m &= m - 1)
@@ -688,17 +653,13 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
             R[3 * g + 1] = s1;
             R[3 * g + 2] = s2;
         }
-        const bool ok = mbar_wait(&s_bar[slot], (uint32_t)(((u + j) / NST) & 1), err, DERR_TMA_TIMEOUT);
-        if(!__all_sync(0xffffffffu, ok))
-            break;
         float* Zb = Z + 3 * ((int64_t)level_begin + (int64_t)bank * BANK);
         if(BF && !use32)
-            cluster_product_mma(s_inv + slot * CB, &s_r[0][0], lane, Zb);
+            cluster_product_mma(stage, &s_r[0][0], lane, Zb);
         else
         {
             float        out[3];
-            const float* Mc = use32 ? inv32 + (size_t)(gbank0 + bank) * SYM * 9
-                                    : reinterpret_cast<const float*>(s_inv + slot * CB);
+            const float* Mc = use32 ? inv32 + (size_t)(gbank0 + bank) * SYM * 9 : reinterpret_cast<const float*>(stage);
             cluster_product(Mc, s_r, lane, out);
             if(lane < 16)
             {
@@ -711,9 +672,7 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
         if(lane == 0 && j + NST < mine)
         {
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&s_bar[slot], CB);
-            bulk_copy_g2s(s_inv + slot * CB, inv + (size_t)(gbank0 + bank + (int64_t)NST * W) * CB, CB,
-                          &s_bar[slot]);
+            issue_bank_copy<BF, R_TMA>(stage, &s_bar[slot], inv, R, gbank0 + bank + (int64_t)NST * W);
         }
     }
     if(j < mine)
@@ -730,18 +689,17 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
 }
 
 // one level over a persistent grid of APPLY_WARPS-warp CTAs
-template <bool FINE, typename VT, bool BF, int NST>
+template <bool BF, int NST>
 __global__ void __launch_bounds__(APPLY_WARPS * 32)
-    k_apply_level(int n_banks, int cnt, int level_begin, const int32_t* __restrict__ p2r, const VT* __restrict__ r,
-                  int roff, const uint16_t* __restrict__ comp_mask, const int32_t* __restrict__ new_local,
-                  int next_begin, int push, const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
+    k_apply_level(int n_banks, int cnt, int level_begin, const uint16_t* __restrict__ comp_mask,
+                  const int32_t* __restrict__ new_local, int next_begin, int push,
+                  const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
                   const uint8_t* __restrict__ stiff, const float* __restrict__ inv32, const int* converged, int* err)
 {
     if(converged && *converged)
         return;
-    constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
-    __shared__ __align__(128) unsigned char s_inv[APPLY_WARPS][NST][CB];
-    __shared__ float    s_r[APPLY_WARPS][BANK][3];
+    constexpr uint32_t SB = stage_bytes<BF>();
+    __shared__ __align__(128) unsigned char s_stage[APPLY_WARPS][NST][SB];
     __shared__ uint64_t s_bar[APPLY_WARPS][NST];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if(lane == 0)
@@ -752,9 +710,74 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
     }
     __syncwarp();
     int u = 0;
-    apply_banks<FINE, VT, BF, NST>(blockIdx.x * APPLY_WARPS + w, gridDim.x * APPLY_WARPS, lane, u, n_banks, cnt,
-                                   level_begin, p2r, r, roff, comp_mask, new_local, next_begin, push, inv, R, Z, stiff,
-                                   inv32, err, &s_inv[w][0][0], s_r[w], s_bar[w]);
+    apply_banks<BF, NST, true>(blockIdx.x * APPLY_WARPS + w, gridDim.x * APPLY_WARPS, lane, u, n_banks, cnt,
+                               level_begin, comp_mask, new_local, next_begin, push, inv, R, Z, stiff, inv32, err,
+                               &s_stage[w][0][0], s_bar[w]);
+}
+
+// The small top levels in one CTA: level l0, then l0 + 1, ... up to L - 1,
+// each level's banks over the CTA's warps and a CTA barrier between levels
+// (each level's restriction, written by this CTA, is the next level's R,
+// read by plain loads). A level of a few dozen banks costs one bulk-copy
+// round trip per bank here instead of a launch each.
+constexpr int TAIL_WARPS = 16;
+constexpr int TAIL_BANKS = 4 * TAIL_WARPS;  // levels with at most this many banks go to the tail
+
+struct TailLevels
+{
+    int                  l0, L;
+    int                  cnt[MAX_LEVELS], begin[MAX_LEVELS + 1];
+    const uint16_t*      comp_mask[MAX_LEVELS];
+    const int32_t*       new_local[MAX_LEVELS];
+};
+
+constexpr int TAIL_STAGES = 2;
+
+template <bool BF>
+constexpr size_t tail_smem()
+{
+    return (size_t)TAIL_WARPS * TAIL_STAGES * stage_bytes<BF>();
+}
+
+template <bool BF>
+__global__ void __launch_bounds__(TAIL_WARPS * 32)
+    k_apply_tail(TailLevels tl, const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
+                 const uint8_t* __restrict__ stiff, const float* __restrict__ inv32, const int* converged, int* err)
+{
+    if(converged && *converged)
+        return;
+    constexpr uint32_t SB = stage_bytes<BF>();
+    extern __shared__ __align__(128) unsigned char s_tail[];  // [TAIL_WARPS][TAIL_STAGES][SB]
+    __shared__ uint64_t s_bar[TAIL_WARPS][TAIL_STAGES];
+    __shared__ int      s_fail;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if(threadIdx.x == 0)
+        s_fail = 0;
+    if(lane == 0)
+    {
+        for(int q = 0; q < TAIL_STAGES; ++q)
+            mbar_init(&s_bar[w][q], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int u = 0;
+    for(int l = tl.l0; l < tl.L; ++l)
+    {
+        const int cnt  = tl.cnt[l];
+        const int push = l + 1 < tl.L ? 1 : 0;
+        if(cnt > 0)
+        {
+            const bool ok = apply_banks<BF, TAIL_STAGES, false>(
+                w, TAIL_WARPS, lane, u, (cnt + BANK - 1) / BANK, cnt, tl.begin[l], tl.comp_mask[l], tl.new_local[l],
+                push ? tl.begin[l + 1] : 0, push, inv, R, Z, stiff, inv32, err,
+                s_tail + (size_t)w * TAIL_STAGES * SB, s_bar[w]);
+            if(!ok && lane == 0)
+                s_fail = 1;
+        }
+        __syncthreads();  // R_{l+1} complete and visible to the CTA
+        if(s_fail)
+            return;
+    }
 }
 
 // persistent grid: as many CTAs as fit on the SMs at once (less `spare` per
@@ -773,16 +796,17 @@ int apply_grid(K kernel, int n_banks, int spare = 0, int cap = 0)
     return (warps + APPLY_WARPS - 1) / APPLY_WARPS;
 }
 
-// The level-1 restriction of the fine residual on its own (the sums the fine
-// level's `push` forms: per connected component of a bank, by its lowest lane,
-// in lane order, so R_1 is bit-identical), one half-warp per bank and one
-// bank per half-warp over the whole grid: the coarse levels need only R_1, so
-// with it in place they run beside the fine level's cluster products.
+// The fine residual in partition order and its level-1 restriction, one
+// half-warp per bank over the whole grid: R_0 (the slots of level 0, FP32,
+// zero in padding slots) is the only gather of r through part_to_real, so the
+// fine level streams its banks' residuals with their inverses; with `push`,
+// R_1 = per connected component of a bank the sum of its nodes by its lowest
+// lane, in lane order, so the coarse levels can run beside the fine level.
 template <typename VT>
 __global__ void __launch_bounds__(APPLY_WARPS * 32)
     k_restrict_fine(int n_banks, const int32_t* __restrict__ p2r, const VT* __restrict__ r, int roff,
                     const uint16_t* __restrict__ comp_mask, const int32_t* __restrict__ new_local, int next_begin,
-                    float* __restrict__ R, const int* converged)
+                    int push, float* __restrict__ R, const int* converged)
 {
     if(converged && *converged)
         return;
@@ -813,15 +837,21 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
                 n1 = (float)r[roff + 3 * (int64_t)v + 1];
                 n2 = (float)r[roff + 3 * (int64_t)v + 2];
             }
-            cm = comp_mask[node];
-            nl = new_local[node];
+            if(push)
+            {
+                cm = comp_mask[node];
+                nl = new_local[node];
+            }
         }
+        R[3 * (int64_t)node]     = n0;
+        R[3 * (int64_t)node + 1] = n1;
+        R[3 * (int64_t)node + 2] = n2;
     }
     s_r[w][half][sub][0] = n0;
     s_r[w][half][sub][1] = n1;
     s_r[w][half][sub][2] = n2;
     __syncwarp();
-    if(live && (cm & ((1u << sub) - 1u)) == 0)
+    if(push && live && (cm & ((1u << sub) - 1u)) == 0)
     {
         float s0 = 0.f, s1 = 0.f, s2 = 0.f;
         for(uint32_t m = cm; m; m &= m - 1)
@@ -835,6 +865,60 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
         R[3 * g]     = s0;
         R[3 * g + 1] = s1;
         R[3 * g + 2] = s2;
+    }
+}
+
+// The additive prolongation of the coarse levels folded top-down into the
+// level-1 slots: Z_1[n] += Z_2[parent(n)] + Z_3[grandparent(n)] + ...
+// (left to right from level 2), so the finish adds one coarse value per
+// vertex (Z_0 of its slot + this sum of its level-1 node) instead of one per
+// level. One thread per level-1 node; each reads its own slot and coarser
+// levels only.
+// anc[c * (L - 2) + (l - 2)]: global slot of level-1 node c's ancestor at
+// level l (-1: none), from the hierarchy (mas_init)
+__global__ void k_fold_prolongation(int cnt1, int begin1, int L, const int32_t* __restrict__ anc, float* __restrict__ Z,
+                                    const int* converged)
+{
+    if(converged && *converged)
+        return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= cnt1)
+        return;
+    int32_t a[MAX_LEVELS - 2];
+#pragma unroll
+    for(int l = 0; l < MAX_LEVELS - 2; ++l)
+        a[l] = l < L - 2 ? anc[(int64_t)c * (L - 2) + l] : -1;
+    const int64_t g1 = (int64_t)begin1 + c;
+    float         a0 = Z[3 * g1], a1 = Z[3 * g1 + 1], a2 = Z[3 * g1 + 2];
+#pragma unroll
+    for(int l = 0; l < MAX_LEVELS - 2; ++l)
+        if(a[l] >= 0)
+        {
+            a0 += Z[3 * (int64_t)a[l]];
+            a1 += Z[3 * (int64_t)a[l] + 1];
+            a2 += Z[3 * (int64_t)a[l] + 2];
+        }
+    Z[3 * g1]     = a0;
+    Z[3 * g1 + 1] = a1;
+    Z[3 * g1 + 2] = a2;
+}
+
+// the ancestor table of the level-1 nodes (walks the next-level ids once)
+struct LevelIds
+{
+    const int32_t* new_local[MAX_LEVELS];
+    int32_t        begin[MAX_LEVELS + 1];
+};
+__global__ void k_h_ancestors(int cnt1, int L, LevelIds ids, int32_t* anc)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= cnt1)
+        return;
+    int loc = c;
+    for(int l = 2; l < L; ++l)
+    {
+        loc = loc >= 0 ? ids.new_local[l - 1][loc] : -1;
+        anc[(int64_t)c * (L - 2) + (l - 2)] = loc >= 0 ? ids.begin[l] + loc : -1;
     }
 }
 
@@ -994,6 +1078,26 @@ void mas_init(b2s_solver* s, int32_t offset, int32_t vn, const int32_t* adj_star
     M.Z.resize((size_t)M.total * 3 + 3);
     B2S_CUDA(cudaMemsetAsync(M.R.data(), 0, M.R.bytes(), st));
     B2S_CUDA(cudaMemsetAsync(M.Z.data(), 0, M.Z.bytes(), st));
+    // the coarse ancestors of every level-1 node (the prolongation fold)
+    if(L > 2 && M.level_count[1] > 0)
+    {
+        LevelIds ids{};
+        for(int l = 0; l < L; ++l)
+        {
+            ids.new_local[l] = X.new_local[l].data();
+            ids.begin[l]     = M.level_begin[l];
+        }
+        M.anc.resize((size_t)M.level_count[1] * (L - 2));
+        k_h_ancestors<<<grid_for(M.level_count[1], TB), TB, 0, st>>>(M.level_count[1], L, ids, M.anc.data());
+        B2S_CHECK_LAUNCH();
+    }
+    // level-1 node of every vertex, contiguous (the finish reads it per vertex)
+    M.node1.resize(std::max(vn, 1));
+    if(L > 1)
+    {
+        k_h_node1<<<grid_for(vn, TB), TB, 0, st>>>(vn, L, M.ctable.data(), M.node1.data());
+        B2S_CHECK_LAUNCH();
+    }
     M.h_ctable.resize((size_t)vn * std::max(L - 1, 1));
     if(L > 1)
         B2S_CUDA(cudaMemcpyAsync(M.h_ctable.data(), M.ctable.data(), sizeof(int32_t) * M.h_ctable.size(),
@@ -1070,52 +1174,82 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
     const uint8_t*       stiff = bf16 ? M.stiff.data() : nullptr;
     // element offset of the range's first vertex in r (FP32: 4 per node)
     const int off = (sizeof(VT) == 4 ? 4 : 3) * M.offset;
-    // With coarse levels, R_1 is restricted first (whole grid), then the
-    // fine level's products run on `st` with one CTA slot per SM left free
-    // while the coarse levels -- a chain of small, latency-bound launches --
-    // run on the side stream in those slots; `st` waits for them before the
-    // finish. Without coarse levels the fine level runs alone.
-    const bool fork = M.L > 1 && n_banks0 > 0 && s->mas_side != nullptr;
-    if(fork)
+    auto level_kernel = bf16 ? k_apply_level<true, APPLY_STAGES_BF16> : k_apply_level<false, APPLY_STAGES_F32>;
+    auto launch_level = [&](int level, cudaStream_t cs, int spare, int cap)
+    {
+        const int cnt     = level == 0 ? M.N : M.level_count[level];
+        const int n_banks = (cnt + BANK - 1) / BANK;
+        const int push    = level > 0 && level + 1 < M.L ? 1 : 0;
+        level_kernel<<<apply_grid(level_kernel, n_banks, spare, cap), tb, 0, cs>>>(
+            n_banks, cnt, M.level_begin[level], M.comp_mask[level].data(), M.new_local[level].data(),
+            push ? M.level_begin[level + 1] : 0, push, inv, M.R.data(), M.Z.data(), stiff, M.inv.data(), converged,
+            err);
+        B2S_CHECK_LAUNCH();
+    };
+    // 1. R_0 (the fine residual in partition order) and R_1, whole grid.
+    // 2. Level 1 -- the largest coarse level, a few thousand banks -- on the
+    //    whole GPU (it pushes R_2).
+    // 3. The fine level's products on `st` with one CTA slot per SM left free,
+    //    beside the rest of the coarse chain on the side stream: the middle
+    //    levels one launch each in the free slots, the small top levels in one
+    //    CTA (k_apply_tail), then the prolongation fold; `st` waits for them
+    //    before the finish.
+    if(n_banks0 > 0)
     {
         const int pairs = (n_banks0 + 1) / 2;
         k_restrict_fine<VT><<<(pairs + APPLY_WARPS - 1) / APPLY_WARPS, tb, 0, st>>>(
-            n_banks0, M.p2r.data(), r, off, M.comp_mask[0].data(), M.new_local[0].data(), M.level_begin[1],
-            M.R.data(), converged);
+            n_banks0, M.p2r.data(), r, off, M.comp_mask[0].data(), M.new_local[0].data(),
+            M.L > 1 ? M.level_begin[1] : 0, M.L > 1 ? 1 : 0, M.R.data(), converged);
         B2S_CHECK_LAUNCH();
+    }
+    const bool coarse = M.L > 1 && M.level_count[1] > 0;
+    if(coarse)
+        launch_level(1, st, 0, 0);
+    const bool fork = coarse && M.L > 2 && n_banks0 > 0 && s->mas_side != nullptr;
+    if(fork)
+    {
         B2S_CUDA(cudaEventRecord(s->mas_fork, st));
         B2S_CUDA(cudaStreamWaitEvent(s->mas_side, s->mas_fork, 0));
     }
     if(n_banks0 > 0)
-    {
-        auto k = bf16 ? k_apply_level<true, VT, true, APPLY_STAGES_BF16>
-                      : k_apply_level<true, VT, false, APPLY_STAGES_F32>;
-        k<<<apply_grid(k, n_banks0, fork ? 1 : 0), tb, 0, st>>>(n_banks0, M.N, 0, M.p2r.data(), r, off,
-                                                                  M.comp_mask[0].data(), M.new_local[0].data(),
-                                                                  M.level_begin[1], (M.L > 1 && !fork) ? 1 : 0, inv,
-                                                                  M.R.data(), M.Z.data(), stiff, M.inv.data(),
-                                                                  converged, err);
-        B2S_CHECK_LAUNCH();
-    }
-    // coarse levels: one persistent launch each (on the graph's stream the
-    // launches follow each other within microseconds; one thread-block cluster
-    // running all small levels with cluster barriers between them was slower)
+        launch_level(0, st, fork ? 1 : 0, 0);
     cudaStream_t cs = fork ? s->mas_side : st;
-    for(int level = 1; level < M.L; ++level)
+    int          level = 2;
+    for(; level < M.L; ++level)
     {
         const int cnt = M.level_count[level];
-        if(cnt <= 0)
+        if(cnt <= 0 || (cnt + BANK - 1) / BANK <= TAIL_BANKS)
             break;
-        const int n_banks = (cnt + BANK - 1) / BANK;
-        const int push    = level + 1 < M.L ? 1 : 0;
-        auto k = bf16 ? k_apply_level<false, VT, true, APPLY_STAGES_BF16>
-                      : k_apply_level<false, VT, false, APPLY_STAGES_F32>;
-        k<<<apply_grid(k, n_banks, 0, fork ? 1 : 0), tb, 0, cs>>>(n_banks, cnt, M.level_begin[level], nullptr,
-                                                                    nullptr, 0, M.comp_mask[level].data(),
-                                                                    M.new_local[level].data(),
-                                                                    push ? M.level_begin[level + 1] : 0, push, inv,
-                                                                    M.R.data(), M.Z.data(), stiff, M.inv.data(),
-                                                                    converged, err);
+        launch_level(level, cs, 0, fork ? 1 : 0);
+    }
+    if(level < M.L && M.level_count[level] > 0)
+    {
+        TailLevels tl{};
+        tl.l0 = level;
+        tl.L  = M.L;
+        for(int l = 0; l < M.L; ++l)
+        {
+            tl.cnt[l]       = M.level_count[l];
+            tl.begin[l]     = M.level_begin[l];
+            tl.comp_mask[l] = M.comp_mask[l].data();
+            tl.new_local[l] = M.new_local[l].data();
+        }
+        tl.begin[M.L] = M.level_begin[M.L];
+        auto         tk   = bf16 ? k_apply_tail<true> : k_apply_tail<false>;
+        const size_t smem = bf16 ? tail_smem<true>() : tail_smem<false>();
+        static bool  attr_set[2] = {false, false};
+        if(!attr_set[bf16 ? 1 : 0])
+        {
+            B2S_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_set[bf16 ? 1 : 0] = true;
+        }
+        tk<<<1, TAIL_WARPS * 32, smem, cs>>>(tl, inv, M.R.data(), M.Z.data(), stiff, M.inv.data(), converged, err);
+        B2S_CHECK_LAUNCH();
+    }
+    if(M.L > 2 && M.level_count[1] > 0)
+    {
+        k_fold_prolongation<<<grid_for(M.level_count[1], 256), 256, 0, cs>>>(
+            M.level_count[1], M.level_begin[1], M.L, M.anc.data(), M.Z.data(), converged);
         B2S_CHECK_LAUNCH();
     }
     if(fork)

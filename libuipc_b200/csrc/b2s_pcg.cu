@@ -34,6 +34,7 @@ void mas_pack_bf16(b2s_solver* s);
 void spmv_f32_launch(b2s_solver* s, const Matrix& A, const float* x, float* y, Reduction& red, double* d_dot,
                      const int* stop);
 void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st_out);
+void build_row_groups(b2s_solver* s, Matrix& A);
 
 namespace
 {
@@ -181,9 +182,9 @@ struct MasView
     int            abd_off, abd_n;  // affine-body range: block rows abd_off .. abd_off + 4 abd_n
     const double*  abd_inv;         // [abd_n * 144]
     const int32_t* r2p;
-    const int32_t* ctable;  // [vn * (L-1)] node of each vertex at levels 1..L-1
-    int            T;       // coarse levels to collect (L-1)
-    const float*   Z;
+    const int32_t* node1;  // [vn] level-1 node of each vertex (its Z slot holds the folded coarse sum)
+    int            T;      // coarse levels (L-1)
+    const float*   Z;      // node values by slot
 };
 
 // node i's three entries of r: NS = 3 values per node (FP64 vectors), or 4
@@ -222,20 +223,16 @@ __device__ __forceinline__ void precond_row(int kind, const MasView& mv, const d
             const int p = mv.r2p[v];
             if(p >= 0)
             {
-                float c0 = mv.Z[3 * (int64_t)p], c1 = mv.Z[3 * (int64_t)p + 1], c2 = mv.Z[3 * (int64_t)p + 2];
-                // all coarse node ids first, then the gathers (independent loads)
-                int32_t nodes[MAX_LEVELS - 1];
-#pragma unroll
-                for(int l = 0; l < MAX_LEVELS - 1; ++l)
-                    nodes[l] = l < mv.T ? mv.ctable[(int64_t)v * (mv.L - 1) + l] : 0;
-#pragma unroll
-                for(int l = 0; l < MAX_LEVELS - 1; ++l)
-                    if(l < mv.T)
-                    {
-                        c0 += mv.Z[3 * (int64_t)nodes[l]];
-                        c1 += mv.Z[3 * (int64_t)nodes[l] + 1];
-                        c2 += mv.Z[3 * (int64_t)nodes[l] + 2];
-                    }
+                // the fine level's Z of the vertex's slot plus the coarse
+                // levels' sum folded into its level-1 node
+                const int n1 = mv.T > 0 ? mv.node1[v] : -1;
+                float     c0 = mv.Z[3 * (int64_t)p], c1 = mv.Z[3 * (int64_t)p + 1], c2 = mv.Z[3 * (int64_t)p + 2];
+                if(n1 >= 0)
+                {
+                    c0 += mv.Z[3 * (int64_t)n1];
+                    c1 += mv.Z[3 * (int64_t)n1 + 1];
+                    c2 += mv.Z[3 * (int64_t)n1 + 2];
+                }
                 z[0] = (double)c0;
                 z[1] = (double)c1;
                 z[2] = (double)c2;
@@ -546,7 +543,7 @@ static MasView mas_view(b2s_solver* s)
     mv.vn     = M.vn;
     mv.L      = M.L;
     mv.r2p    = M.r2p.data();
-    mv.ctable = M.ctable.data();
+    mv.node1  = M.node1.data();
     mv.T      = M.L <= 1 ? 0 : M.L - 1;
     mv.Z      = M.Z.data();
     return mv;
@@ -935,6 +932,7 @@ static void ensure_f32_planes(b2s_solver* s)
     A.vals32.resize((size_t)9 * A.stride, 1.2);
     k_planes_f32<<<vec_grid(9 * A.stride), VEC_BLOCK, 0, s->stream>>>(9 * A.stride, A.vals.data(), A.vals32.data());
     B2S_CHECK_LAUNCH();
+    build_row_groups(s, A);
     A.vals32_generation = A.generation;
 }
 

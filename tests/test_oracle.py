@@ -159,3 +159,18 @@ def test_metis_partition_pinned_to_reference(cube10):
         pytest.skip("reference METIS not compiled (reference tree absent)")
     pid = O.metis_mesh_partition(cube10.adj_start, cube10.adj_list)
     assert pid.min() == 0 and np.bincount(pid).max() <= 16 and np.bincount(pid).min() >= 1
+
+
+def test_numpy_rcb_and_maps_equal_the_library(cube10, stack_small):
+    """The host arm's numpy RCB and padded maps give the library's partition."""
+    from libuipc_b200.linear_system import partition_maps, partition_rcb
+
+    for s in (cube10, stack_small):
+        pid = O.rcb_partition(s.positions)
+        assert np.array_equal(pid, partition_rcb(s.positions))
+        p2r, r2p = O.partition_maps(pid)
+        lp2r, lr2p = partition_maps(pid)
+        assert np.array_equal(p2r, lp2r) and np.array_equal(r2p, lr2p)
+    pid = np.array([0, -1, 0, 1, -1], np.int32)
+    p2r, r2p = O.partition_maps(pid)
+    assert list(r2p) == [0, -1, 1, 16, -1] and p2r.size == 32
