@@ -163,7 +163,9 @@ def test_bar_assembly_iterations_and_tight_solution(solver, cuda, bar):
     x = torch.zeros_like(b)
     st = solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=1)
     assert st["converged"] == 1 and info["converged"] == 1
-    assert abs(st["iterations_exact"] - info["iterations"]) <= 2
+    # ~635 iterations: FP64 rounding (the SpMV's atomics, summation orders)
+    # moves the stop by a few
+    assert abs(st["iterations_exact"] - info["iterations"]) <= max(2, 0.01 * info["iterations"])
 
     M64 = O.OracleMAS(s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
     M64.assemble(A, 0, 1)
