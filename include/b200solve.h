@@ -284,6 +284,11 @@ int b2s_ws_loss_grad(b2s_solver* s, int32_t index, double* h_loss, float* h_grad
  * feature mean[F] and std[F]; h_params NULL = size query into *n */
 int b2s_ws_get_params(const b2s_solver* s, float* h_params, int64_t* n);
 int b2s_ws_set_params(b2s_solver* s, const float* h_params, int64_t n);
+/* append a stored sample given as arrays ("any" memory: the layout
+ * b2s_ws_get_sample returns), e.g. a training set read back from a checkpoint;
+ * norm > 0 is the sample's loss normaliser */
+int b2s_ws_put_sample(b2s_solver* s, int32_t rows, const float* feat, const float* H, const float* q,
+                      const float* c0, double norm);
 /* a stored sample for checking: raw features [rows x F], H [rows x 10] (upper
  * triangle of the 4x4 field Gram), q [rows x 4], c0 [rows], loss normaliser;
  * NULL pointers = size query of *rows */

@@ -143,6 +143,7 @@ SIGNATURES = {
     "b2s_ws_loss_grad": (C.c_int, [vp, i32, dp, fp]),
     "b2s_ws_get_params": (C.c_int, [vp, fp, i64p]),
     "b2s_ws_set_params": (C.c_int, [vp, fp, i64]),
+    "b2s_ws_put_sample": (C.c_int, [vp, i32, vp, vp, vp, vp, C.c_double]),
     "b2s_ws_get_sample": (C.c_int, [vp, i32, i32p, fp, fp, fp, fp, dp]),
     "b2s_ws_predict": (C.c_int, [vp, i32, vp, i32, vp, vp, C.POINTER(WsInfo)]),
     "b2s_spmv_noalloc": (C.c_int, [i32, i64, vp, vp, vp, vp, vp, vp, vp]),

@@ -589,6 +589,12 @@ int b2s_ws_add_sample(b2s_solver* s, const double* d_b, int32_t n_hist, const do
     return guarded(s, [&] { b2s::ws_add_sample(s, d_b, n_hist, d_hist, d_x); });
 }
 
+int b2s_ws_put_sample(b2s_solver* s, int32_t rows, const float* feat, const float* H, const float* q,
+                      const float* c0, double norm)
+{
+    return guarded(s, [&] { b2s::ws_put_sample(s, rows, feat, H, q, c0, norm); });
+}
+
 int b2s_ws_num_samples(const b2s_solver* s, int32_t* n_samples, int64_t* n_rows)
 {
     b2s_solver* m = const_cast<b2s_solver*>(s);

@@ -329,6 +329,8 @@ void drop_graphs(b2s_solver* s);
 void    ws_init(b2s_solver* s, int hidden, uint64_t seed);
 void    ws_add_sample(b2s_solver* s, const double* b, int n_hist, const double* const* hist, const double* x);
 void    ws_num_samples(b2s_solver* s, int32_t* n, int64_t* rows);
+void    ws_put_sample(b2s_solver* s, int32_t rows, const float* feat, const float* Hs, const float* q,
+                      const float* c0, double norm);
 void    ws_fit_normalization(b2s_solver* s);
 double  ws_train(b2s_solver* s, int epochs, double lr, uint64_t seed);
 double  ws_loss_grad(b2s_solver* s, int index, float* h_grad);

@@ -1112,6 +1112,35 @@ void ws_add_sample(b2s_solver* s, const double* b, int n_hist, const double* con
     W.store_rows = r1;
 }
 
+// append a stored sample from host arrays (a training set read back from a
+// checkpoint): rows aggregates of features, field Gram, q, |x|^2 and the
+// sample's loss normaliser
+void ws_put_sample(b2s_solver* s, int32_t rows, const float* feat, const float* Hs, const float* q, const float* c0,
+                   double norm)
+{
+    LearnedState& W = ws_of(s);
+    B2S_REQUIRE(rows > 0 && feat && Hs && q && c0, B2S_ERR_ARGUMENT, "empty or null sample");
+    B2S_REQUIRE(std::isfinite(norm) && norm > 0.0, B2S_ERR_ARGUMENT, "sample normaliser must be positive");
+    cudaStream_t  st = s->stream;
+    const int64_t r0 = W.store_rows, r1 = r0 + rows;
+    if(r1 > W.store_cap)
+    {
+        const int64_t cap = std::max<int64_t>(r1, W.store_cap * 2);
+        grow_keep(W.st_feat, (size_t)r0 * WS_F, (size_t)cap * WS_F, st);
+        grow_keep(W.st_H, (size_t)r0 * WS_HSYM, (size_t)cap * WS_HSYM, st);
+        grow_keep(W.st_q, (size_t)r0 * WS_O, (size_t)cap * WS_O, st);
+        grow_keep(W.st_c0, (size_t)r0, (size_t)cap, st);
+        W.store_cap = cap;
+    }
+    B2S_CUDA(cudaMemcpyAsync(W.st_feat.data() + r0 * WS_F, feat, sizeof(float) * rows * WS_F, cudaMemcpyDefault, st));
+    B2S_CUDA(cudaMemcpyAsync(W.st_H.data() + r0 * WS_HSYM, Hs, sizeof(float) * rows * WS_HSYM, cudaMemcpyDefault, st));
+    B2S_CUDA(cudaMemcpyAsync(W.st_q.data() + r0 * WS_O, q, sizeof(float) * rows * WS_O, cudaMemcpyDefault, st));
+    B2S_CUDA(cudaMemcpyAsync(W.st_c0.data() + r0, c0, sizeof(float) * rows, cudaMemcpyDefault, st));
+    B2S_CUDA(cudaStreamSynchronize(st));
+    W.samples.push_back(WsSample{r0, rows, norm});
+    W.store_rows = r1;
+}
+
 void ws_num_samples(b2s_solver* s, int32_t* n, int64_t* rows)
 {
     LearnedState& W = ws_of(s);

@@ -562,22 +562,18 @@ __host__ __device__ constexpr uint32_t stage_bytes()
     return (BF ? INV16_BYTES : INV_BYTES) + R_BYTES;
 }
 
-// the bank's inverse and (R_TMA) its residual slice, on one barrier
-template <bool BF, bool R_TMA>
+// the bank's inverse and its residual slice, on one barrier
+template <bool BF>
 __device__ __forceinline__ void issue_bank_copy(unsigned char* stage, uint64_t* bar, const unsigned char* inv,
                                                 const float* R, int64_t gbank)
 {
     constexpr uint32_t CB = BF ? INV16_BYTES : INV_BYTES;
-    mbar_arrive_expect_tx(bar, CB + (R_TMA ? R_BYTES : 0u));
+    mbar_arrive_expect_tx(bar, CB + R_BYTES);
     bulk_copy_g2s(stage, inv + (size_t)gbank * CB, CB, bar);
-    if(R_TMA)
-        bulk_copy_g2s(stage + CB, R + (size_t)gbank * (BANK * 3), R_BYTES, bar);
+    bulk_copy_g2s(stage + CB, R + (size_t)gbank * (BANK * 3), R_BYTES, bar);
 }
 
-// R_TMA: the residual slice comes with the inverse by bulk copy (written by
-// an earlier kernel); otherwise lanes 0-15 load it (written earlier in the
-// same kernel: the single-CTA tail of the small levels)
-template <bool BF, int NST, bool R_TMA>
+template <bool BF, int NST>
 __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int n_banks, int cnt, int level_begin,
                                             const uint16_t* __restrict__ comp_mask,
                                             const int32_t* __restrict__ new_local, int next_begin, int push,
@@ -596,7 +592,7 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
         for(int j = 0; j < mine && j < NST; ++j)
         {
             const int slot = (u + j) % NST;
-            issue_bank_copy<BF, R_TMA>(s_stage + slot * SB, &s_bar[slot], inv, R, gbank0 + gw + (int64_t)j * W);
+            issue_bank_copy<BF>(s_stage + slot * SB, &s_bar[slot], inv, R, gbank0 + gw + (int64_t)j * W);
         }
     }
     __syncwarp();
@@ -628,13 +624,6 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
         load_meta(j + 1);
         unsigned char* stage = s_stage + slot * SB;
         float(*s_r)[3]       = reinterpret_cast<float(*)[3]>(stage + CB);
-        if(!R_TMA && lane < 16)
-        {
-            const int64_t g = (int64_t)level_begin + (int64_t)bank * BANK + sub;
-            s_r[sub][0]     = live ? R[3 * g] : 0.f;
-            s_r[sub][1]     = live ? R[3 * g + 1] : 0.f;
-            s_r[sub][2]     = live ? R[3 * g + 2] : 0.f;
-        }
         const bool ok = mbar_wait(&s_bar[slot], (uint32_t)(((u + j) / NST) & 1), err, DERR_TMA_TIMEOUT);
         if(!__all_sync(0xffffffffu, ok))
             break;
@@ -672,7 +661,7 @@ __device__ __forceinline__ bool apply_banks(int gw, int W, int lane, int& u, int
         if(lane == 0 && j + NST < mine)
         {
             fence_proxy_async_smem();
-            issue_bank_copy<BF, R_TMA>(stage, &s_bar[slot], inv, R, gbank0 + bank + (int64_t)NST * W);
+            issue_bank_copy<BF>(stage, &s_bar[slot], inv, R, gbank0 + bank + (int64_t)NST * W);
         }
     }
     if(j < mine)
@@ -710,74 +699,9 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32)
     }
     __syncwarp();
     int u = 0;
-    apply_banks<BF, NST, true>(blockIdx.x * APPLY_WARPS + w, gridDim.x * APPLY_WARPS, lane, u, n_banks, cnt,
+    apply_banks<BF, NST>(blockIdx.x * APPLY_WARPS + w, gridDim.x * APPLY_WARPS, lane, u, n_banks, cnt,
                                level_begin, comp_mask, new_local, next_begin, push, inv, R, Z, stiff, inv32, err,
                                &s_stage[w][0][0], s_bar[w]);
-}
-
-// The small top levels in one CTA: level l0, then l0 + 1, ... up to L - 1,
-// each level's banks over the CTA's warps and a CTA barrier between levels
-// (each level's restriction, written by this CTA, is the next level's R,
-// read by plain loads). A level of a few dozen banks costs one bulk-copy
-// round trip per bank here instead of a launch each.
-constexpr int TAIL_WARPS = 16;
-constexpr int TAIL_BANKS = 4 * TAIL_WARPS;  // levels with at most this many banks go to the tail
-
-struct TailLevels
-{
-    int                  l0, L;
-    int                  cnt[MAX_LEVELS], begin[MAX_LEVELS + 1];
-    const uint16_t*      comp_mask[MAX_LEVELS];
-    const int32_t*       new_local[MAX_LEVELS];
-};
-
-constexpr int TAIL_STAGES = 2;
-
-template <bool BF>
-constexpr size_t tail_smem()
-{
-    return (size_t)TAIL_WARPS * TAIL_STAGES * stage_bytes<BF>();
-}
-
-template <bool BF>
-__global__ void __launch_bounds__(TAIL_WARPS * 32)
-    k_apply_tail(TailLevels tl, const unsigned char* __restrict__ inv, float* R, float* __restrict__ Z,
-                 const uint8_t* __restrict__ stiff, const float* __restrict__ inv32, const int* converged, int* err)
-{
-    if(converged && *converged)
-        return;
-    constexpr uint32_t SB = stage_bytes<BF>();
-    extern __shared__ __align__(128) unsigned char s_tail[];  // [TAIL_WARPS][TAIL_STAGES][SB]
-    __shared__ uint64_t s_bar[TAIL_WARPS][TAIL_STAGES];
-    __shared__ int      s_fail;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if(threadIdx.x == 0)
-        s_fail = 0;
-    if(lane == 0)
-    {
-        for(int q = 0; q < TAIL_STAGES; ++q)
-            mbar_init(&s_bar[w][q], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    int u = 0;
-    for(int l = tl.l0; l < tl.L; ++l)
-    {
-        const int cnt  = tl.cnt[l];
-        const int push = l + 1 < tl.L ? 1 : 0;
-        if(cnt > 0)
-        {
-            const bool ok = apply_banks<BF, TAIL_STAGES, false>(
-                w, TAIL_WARPS, lane, u, (cnt + BANK - 1) / BANK, cnt, tl.begin[l], tl.comp_mask[l], tl.new_local[l],
-                push ? tl.begin[l + 1] : 0, push, inv, R, Z, stiff, inv32, err,
-                s_tail + (size_t)w * TAIL_STAGES * SB, s_bar[w]);
-            if(!ok && lane == 0)
-                s_fail = 1;
-        }
-        __syncthreads();  // R_{l+1} complete and visible to the CTA
-        if(s_fail)
-            return;
-    }
 }
 
 // persistent grid: as many CTAs as fit on the SMs at once (less `spare` per
@@ -1190,10 +1114,12 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
     // 2. Level 1 -- the largest coarse level, a few thousand banks -- on the
     //    whole GPU (it pushes R_2).
     // 3. The fine level's products on `st` with one CTA slot per SM left free,
-    //    beside the rest of the coarse chain on the side stream: the middle
-    //    levels one launch each in the free slots, the small top levels in one
-    //    CTA (k_apply_tail), then the prolongation fold; `st` waits for them
-    //    before the finish.
+    //    beside the rest of the coarse chain on the side stream (one launch per
+    //    level in the free slots, then the prolongation fold); `st` waits for
+    //    them before the finish. (One CTA running the small top levels with
+    //    CTA barriers between them needs more shared memory than the fine
+    //    level leaves on an SM, so it waited for the fine level: 1 ms per
+    //    solve slower.)
     if(n_banks0 > 0)
     {
         const int pairs = (n_banks0 + 1) / 2;
@@ -1214,37 +1140,11 @@ static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, boo
     if(n_banks0 > 0)
         launch_level(0, st, fork ? 1 : 0, 0);
     cudaStream_t cs = fork ? s->mas_side : st;
-    int          level = 2;
-    for(; level < M.L; ++level)
+    for(int level = 2; level < M.L; ++level)
     {
-        const int cnt = M.level_count[level];
-        if(cnt <= 0 || (cnt + BANK - 1) / BANK <= TAIL_BANKS)
+        if(M.level_count[level] <= 0)
             break;
         launch_level(level, cs, 0, fork ? 1 : 0);
-    }
-    if(level < M.L && M.level_count[level] > 0)
-    {
-        TailLevels tl{};
-        tl.l0 = level;
-        tl.L  = M.L;
-        for(int l = 0; l < M.L; ++l)
-        {
-            tl.cnt[l]       = M.level_count[l];
-            tl.begin[l]     = M.level_begin[l];
-            tl.comp_mask[l] = M.comp_mask[l].data();
-            tl.new_local[l] = M.new_local[l].data();
-        }
-        tl.begin[M.L] = M.level_begin[M.L];
-        auto         tk   = bf16 ? k_apply_tail<true> : k_apply_tail<false>;
-        const size_t smem = bf16 ? tail_smem<true>() : tail_smem<false>();
-        static bool  attr_set[2] = {false, false};
-        if(!attr_set[bf16 ? 1 : 0])
-        {
-            B2S_CUDA(cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            attr_set[bf16 ? 1 : 0] = true;
-        }
-        tk<<<1, TAIL_WARPS * 32, smem, cs>>>(tl, inv, M.R.data(), M.Z.data(), stiff, M.inv.data(), converged, err);
-        B2S_CHECK_LAUNCH();
     }
     if(M.L > 2 && M.level_count[1] > 0)
     {

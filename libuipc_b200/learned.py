@@ -124,6 +124,55 @@ class SequenceRunner:
         return log
 
 
+CHECKPOINT_VERSION = 1
+
+
+def _hidden_of(n_params: int) -> int:
+    """Hidden width from the parameter count (H^2 + 28 H + 4 weights and biases
+    plus 2 x 22 feature statistics at 22 features and 4 outputs)."""
+    F, O = _abi.B2S_WS_FEATURES, _abi.B2S_WS_OUTPUTS
+    for h in range(32, 1025, 32):
+        if F * h + h + h * h + h + h * O + O + 2 * F == n_params:
+            return h
+    raise ValueError(f"no hidden width has {n_params} parameters")
+
+
+def save_checkpoint(solver: Solver, path: str, with_samples: bool = True) -> None:
+    """The learned warm start to an .npz file: format version, hidden width,
+    the parameters with the feature statistics (b2s_ws_get_params) and, with
+    ``with_samples``, the stored training set (per sample its aggregate rows
+    of features, field Gram, q, |x|^2 and its loss normaliser)."""
+    params = solver.ws_params()
+    out = {"version": np.int32(CHECKPOINT_VERSION), "hidden": np.int32(_hidden_of(params.size)), "params": params}
+    if with_samples:
+        n, _ = solver.ws_num_samples()
+        parts = [solver.ws_sample(i) for i in range(n)]
+        out["rows"] = np.array([p["c0"].size for p in parts], np.int64)
+        out["norms"] = np.array([p["norm"] for p in parts], np.float64)
+        for key in ("feat", "H", "q", "c0"):
+            out[key] = (np.concatenate([p[key] for p in parts]) if parts else np.zeros(0, np.float32))
+    np.savez(path, **out)
+
+
+def load_checkpoint(solver: Solver, path: str, with_samples: bool = True) -> int:
+    """Restore a checkpoint written by save_checkpoint into ``solver`` (its
+    network is created with the stored width); returns the samples appended.
+    The optimiser state is not stored: training resumes with fresh moments."""
+    d = np.load(path)
+    if int(d["version"]) != CHECKPOINT_VERSION:
+        raise ValueError(f"checkpoint format {int(d['version'])}, this library reads {CHECKPOINT_VERSION}")
+    solver.ws_init(int(d["hidden"]))
+    solver.ws_set_params(d["params"])
+    if not with_samples or "rows" not in d:
+        return 0
+    r0 = 0
+    for rows, norm in zip(d["rows"], d["norms"]):
+        r1 = r0 + int(rows)
+        solver.ws_put_sample(d["feat"][r0:r1], d["H"][r0:r1], d["q"][r0:r1], d["c0"][r0:r1], float(norm))
+        r0 = r1
+    return int(d["rows"].size)
+
+
 def run_gpu_bar(device, cells=(200, 20, 20), E: float = 1e6, nu: float = 0.49, twist: float = 2.0,
                 train_steps: int = 200, eval_steps: int = 20, newton_iters: int = 10, truth_tol: float = 1e-10,
                 tol: float = 1e-4, epochs: int = 5, hidden: int = 128, seed: int = 0,

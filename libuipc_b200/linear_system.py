@@ -259,6 +259,12 @@ class Solver:
                                               g.ctypes.data_as(C.POINTER(C.c_float))))
         return float(loss.value), g
 
+    def ws_put_sample(self, feat, H, q, c0, norm: float):
+        """Append a stored sample from host arrays (the layout ws_sample returns)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (feat, H, q, c0)]
+        rows = arrs[3].size
+        self._check(self.lib.b2s_ws_put_sample(self.h, int(rows), *[a.ctypes.data for a in arrs], float(norm)))
+
     def ws_sample(self, index: int) -> dict:
         rows = C.c_int32()
         fp = C.POINTER(C.c_float)

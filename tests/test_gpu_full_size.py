@@ -135,7 +135,17 @@ def test_stack_pcg_matches_the_oracle(solver, cuda, stack8):
     x = torch.zeros_like(b)
     st = solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=1)
     assert st["converged"] == 1
-    assert abs(st["iterations_exact"] - info["iterations"]) <= 2
+    # the reference's inverses (FP32 sweep) against these (FP32 LDL^T): the
+    # two preconditioners differ by FP32 rounding, which moves a ~120-iteration
+    # stop at 1e-4 by a few
+    assert abs(st["iterations_exact"] - info["iterations"]) <= max(2, 0.03 * info["iterations"])
+    # the same preconditioner (the device's inverses in the oracle): within 2
+    _, inv = solver.mas_clusters()
+    M.set_inverses(inv)
+    del inv
+    _, info_d = O.pcg(A, s.b, precond=O.ORC_PRECOND_MAS, mas=M, tol=1e-4, stop_rule=O.ORC_STOP_RELRES,
+                      threads=THREADS)
+    assert abs(st["iterations_exact"] - info_d["iterations"]) <= 2
     # both answers pass the oracle's own FP64 residual
     bn = np.linalg.norm(s.b)
     assert np.linalg.norm(s.b - A.spmv(x.cpu().numpy())) <= 1e-4 * bn

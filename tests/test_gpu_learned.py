@@ -203,3 +203,61 @@ def test_longer_history_on_a_driven_bar(solver, cuda):
             assert solver.ws_predict(b, x, nine, _abi.B2S_WS_MODE_HISTORY)["n_candidates"] <= 8
     print(f"history start: 3 latest {means[3]:.1f}, 8 latest {means[8]:.1f} PCG iterations")
     assert means[8] <= means[3]
+
+
+def test_checkpoint_round_trip(solver, cuda, tmp_path):
+    """save_checkpoint / load_checkpoint: a second solver restored from the
+    file holds the same parameters and training set, so its loss and
+    gradient on every stored sample are the first solver's, and so is its
+    prediction on the same system (up to the order of atomic sums in the
+    feature reductions)."""
+    import torch
+
+    from libuipc_b200.learned import SequenceRunner, load_checkpoint, save_checkpoint
+    from libuipc_b200.linear_system import Solver
+    from libuipc_b200.sequence import SceneSequence
+
+    seq = SceneSequence(scene=2, cells_x=24, cells_y=4, cells_z=4, E=1e6, nu=0.49, twist_per_step=2.0)
+    run = SequenceRunner(solver, seq, cuda)
+    solver.ws_init(64, seed=3)
+    run.run(6, newton_iters=1, collect=True)
+    solver.ws_fit_normalization()
+    solver.ws_train(3, lr=1e-3, seed=0)
+    path = str(tmp_path / "ws.npz")
+    save_checkpoint(solver, path)
+    n, rows = solver.ws_num_samples()
+    assert n >= 3
+
+    other = Solver(0)
+    try:
+        assert load_checkpoint(other, path) == n
+        assert other.ws_num_samples() == (n, rows)
+        assert np.array_equal(other.ws_params(), solver.ws_params())
+        for i in range(n):
+            a, b = solver.ws_sample(i), other.ws_sample(i)
+            for k in ("feat", "H", "q", "c0"):
+                assert np.array_equal(a[k], b[k]), (i, k)
+            assert a["norm"] == b["norm"]
+            la, ga = solver.ws_loss_grad(i)
+            lb, gb = other.ws_loss_grad(i)
+            assert abs(la - lb) <= 1e-6 * abs(la)
+            assert np.abs(ga - gb).max() <= 1e-5 * np.abs(ga).max()
+        # the same prediction on the same system and history
+        sysm = seq.system()
+        hist = run.hist(0)
+        for sv in (solver, other):
+            _setup(sv, sysm, cuda)
+        b = to_dev(sysm.b, cuda)
+        xa, xb = torch.zeros_like(b), torch.zeros_like(b)
+        ia = solver.ws_predict(b, xa, history=hist)
+        ib = other.ws_predict(b, xb, history=hist)
+        assert ia["mode"] == ib["mode"]
+        assert float((xa - xb).norm()) <= 1e-10 * float(xa.norm())
+    finally:
+        other.close()
+    # a file of another format version is refused
+    d = dict(np.load(path))
+    d["version"] = np.int32(99)
+    np.savez(str(tmp_path / "bad.npz"), **d)
+    with pytest.raises(ValueError):
+        load_checkpoint(solver, str(tmp_path / "bad.npz"))

@@ -82,3 +82,17 @@ def test_sequence_twist_moves_only_the_ends_first():
     sysm = seq.system()
     # fixed rows: identity diagonal, zero gradient
     assert np.allclose(sysm.b.reshape(-1, 3)[seq.fixed], 0)
+
+
+def test_checkpoint_width_from_parameter_count():
+    """The hidden width a checkpoint records is recovered from the parameter
+    count b2s_ws_get_params reports (weights, biases and 2 x 22 statistics)."""
+    from libuipc_b200 import _abi
+    from libuipc_b200.learned import _hidden_of
+
+    F, O = _abi.B2S_WS_FEATURES, _abi.B2S_WS_OUTPUTS
+    for h in (64, 128, 256, 512):
+        n = F * h + h + h * h + h + h * O + O + 2 * F
+        assert _hidden_of(n) == h
+    with pytest.raises(ValueError):
+        _hidden_of(1000)
