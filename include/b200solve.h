@@ -128,6 +128,15 @@ int b2s_mas_get_nodes(b2s_solver* s, float* h_R, float* h_Z);
  * in *part_map_size (call it first to size h_part_to_real). */
 int b2s_partition_rcb(int32_t n, const double* h_positions, int32_t max_part,
                       int32_t* h_part_ids);
+/* Graph partition from the vertex adjacency alone (CSR as b2s_mas_init takes
+ * it), the drop-in for geometry::mesh_partition's METIS k-way call
+ * (src/geometry/mesh_partition.cpp:77-231): ceil(n / max_part) parts of at
+ * most max_part vertices, ids 0.. contiguous, no part empty; point clouds (no
+ * edges) take sequential blocks; n <= max_part gives one part per connected
+ * component. Recursive graph bisection, deterministic (no seed): the part
+ * ids follow the bisection tree, so consecutive parts are neighbours. */
+int b2s_partition_graph(int32_t n, const int32_t* h_adj_start, const int32_t* h_adj_list,
+                        int32_t max_part, int32_t* h_part_ids);
 int b2s_partition_maps(int32_t n, const int32_t* h_part_ids, int32_t max_part,
                        int32_t* h_part_to_real, int32_t* h_real_to_part,
                        int32_t* part_map_size);

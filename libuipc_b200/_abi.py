@@ -125,6 +125,7 @@ SIGNATURES = {
     "b2s_mas_stiff_info": (C.c_int, [vp, i32p, vp]),
     "b2s_mas_get_nodes": (C.c_int, [vp, vp, vp]),
     "b2s_partition_rcb": (C.c_int, [i32, vp, i32, vp]),
+    "b2s_partition_graph": (C.c_int, [i32, vp, vp, i32, vp]),
     "b2s_partition_maps": (C.c_int, [i32, vp, i32, vp, vp, i32p]),
     "b2s_abd_init": (C.c_int, [vp, i32, i32]),
     "b2s_precond_assemble": (C.c_int, [vp, C.c_int, C.c_int]),

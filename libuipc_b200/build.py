@@ -46,6 +46,7 @@ SOLVE_SOURCES = [
     "b2s_generate.cu",
     "b2s_abi.cu",
     "b2s_noalloc.cu",
+    "b2s_partition.cu",
 ]
 
 

@@ -534,6 +534,69 @@ int b2s_partition_rcb(int32_t n, const double* pos, int32_t max_part, int32_t* p
     return B2S_OK;
 }
 
+// geometry::mesh_partition (src/geometry/mesh_partition.cpp:77-231) from the
+// vertex adjacency alone: point clouds (no edges) take sequential blocks of
+// max_part; up to max_part vertices take one part per connected component
+// (the reference's n_parts <= 1 branch); otherwise recursive graph bisection
+// into ceil(n / max_part) parts.
+int b2s_partition_graph(int32_t n, const int32_t* adj_start, const int32_t* adj_list, int32_t max_part,
+                        int32_t* part_ids)
+{
+    if(n < 0 || max_part < 1 || (n > 0 && (!adj_start || !part_ids)))
+        return B2S_ERR_ARGUMENT;
+    if(n == 0)
+        return B2S_OK;
+    if(adj_start[0] != 0)
+        return B2S_ERR_ARGUMENT;
+    for(int32_t v = 0; v < n; ++v)
+        if(adj_start[v + 1] < adj_start[v])
+            return B2S_ERR_ARGUMENT;
+    const int32_t E = adj_start[n];
+    if(E > 0 && !adj_list)
+        return B2S_ERR_ARGUMENT;
+    for(int32_t e = 0; e < E; ++e)
+        if(adj_list[e] < 0 || adj_list[e] >= n)
+            return B2S_ERR_ARGUMENT;
+    if(E == 0)
+    {
+        for(int32_t v = 0; v < n; ++v)
+            part_ids[v] = v / max_part;
+        return B2S_OK;
+    }
+    if(n <= max_part)
+    {
+        std::fill(part_ids, part_ids + n, -1);
+        std::vector<int32_t> queue;
+        int32_t              comp = 0;
+        for(int32_t v0 = 0; v0 < n; ++v0)
+        {
+            if(part_ids[v0] >= 0)
+                continue;
+            queue.assign(1, v0);
+            part_ids[v0] = comp;
+            for(size_t h = 0; h < queue.size(); ++h)
+                for(int32_t e = adj_start[queue[h]]; e < adj_start[queue[h] + 1]; ++e)
+                    if(part_ids[adj_list[e]] < 0)
+                    {
+                        part_ids[adj_list[e]] = comp;
+                        queue.push_back(adj_list[e]);
+                    }
+            ++comp;
+        }
+        return B2S_OK;
+    }
+    try
+    {
+        b2s::partition_graph(n, adj_start, adj_list, max_part, part_ids);
+    }
+    catch(const std::exception& e)
+    {
+        b2s::set_handle_free_error(e.what());
+        return B2S_ERR_STATE;
+    }
+    return B2S_OK;
+}
+
 // FEMMASPreconditioner::do_init step 4 (fem_mas_preconditioner.cu:285-330):
 // vertices grouped by part id (parts in id order, vertices ascending), each
 // part padded to a multiple of 16 slots

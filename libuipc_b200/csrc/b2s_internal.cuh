@@ -320,6 +320,8 @@ void mas_init(b2s_solver* s, int32_t offset, int32_t vn, const int32_t* adj_star
               const int32_t* adj_list, int32_t N, const int32_t* p2r, const int32_t* r2p);
 void mas_assemble(b2s_solver* s, int invert_mode);
 void mas_apply(b2s_solver* s, const double* r, double* z);
+// host: recursive graph bisection into parts of at most max_part vertices
+void partition_graph(int32_t n, const int32_t* xadj, const int32_t* adj, int32_t max_part, int32_t* part_ids);
 
 // PCG
 void pcg_solve(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st);

@@ -300,6 +300,20 @@ def partition_rcb(positions: np.ndarray, max_part: int = 16) -> np.ndarray:
     return out
 
 
+def partition_graph(adj_start: np.ndarray, adj_list: np.ndarray, max_part: int = 16) -> np.ndarray:
+    """Part id of every vertex from the vertex adjacency alone (the library's
+    drop-in for geometry::mesh_partition's METIS k-way call)."""
+    lib = load_solve_lib()
+    xs = np.ascontiguousarray(adj_start, dtype=np.int32)
+    xl = np.ascontiguousarray(adj_list, dtype=np.int32)
+    n = xs.size - 1
+    out = np.zeros(max(n, 0), np.int32)
+    rc = lib.b2s_partition_graph(int(n), xs.ctypes.data, xl.ctypes.data, int(max_part), out.ctypes.data)
+    if rc != 0:
+        raise B200SolveError(rc, "b2s_partition_graph failed")
+    return out
+
+
 def partition_maps(part_ids: np.ndarray, max_part: int = 16):
     lib = load_solve_lib()
     pid = np.ascontiguousarray(part_ids, dtype=np.int32)

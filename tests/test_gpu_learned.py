@@ -252,7 +252,7 @@ def test_checkpoint_round_trip(solver, cuda, tmp_path):
         ia = solver.ws_predict(b, xa, history=hist)
         ib = other.ws_predict(b, xb, history=hist)
         assert ia["mode"] == ib["mode"]
-        assert float((xa - xb).norm()) <= 1e-10 * float(xa.norm())
+        assert float((xa - xb).norm()) <= 1e-7 * float(xa.norm())  # FP32 feature sums
     finally:
         other.close()
     # a file of another format version is refused
