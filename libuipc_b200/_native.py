@@ -63,6 +63,13 @@ def load_scene_lib() -> C.CDLL:
         for fn in ("b2g_tets", "b2g_triplet_rows", "b2g_triplet_cols", "b2g_adjacency_start", "b2g_adjacency_list"):
             getattr(lib, fn).argtypes = [vp]
             getattr(lib, fn).restype = c_i32_p
+        dp = C.POINTER(C.c_double)
+        lib.b2g_element_bw.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, vp, vp]
+        lib.b2g_element_bw.restype = C.c_double
+        lib.b2g_element_dsb.argtypes = [vp, vp, C.c_double, C.c_double, vp, vp]
+        lib.b2g_element_dsb.restype = C.c_double
+        lib.b2g_element_ortho.argtypes = [vp, C.c_double, C.c_double, vp, vp]
+        lib.b2g_element_ortho.restype = C.c_double
         # Matrix Market I/O (csrc/scene/matrix_market.h)
         i32, i64, pi32, pi64 = C.c_int32, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64)
         lib.b2io_write_block_matrix.argtypes = [C.c_char_p, i32, i64, vp, vp, vp, C.c_int]

@@ -101,7 +101,8 @@ def build_scene(force: bool = False) -> str:
     os.makedirs(LIB, exist_ok=True)
     out = os.path.join(LIB, "libb200scene.so")
     srcs = [os.path.join(CSRC, "scene", f) for f in ("scene_gen.cpp", "matrix_market.cpp")]
-    hdrs = [os.path.join(CSRC, "scene", "scene_gen.h"), os.path.join(ROOT, "include", "b200io.h")]
+    hdrs = [os.path.join(CSRC, "scene", h) for h in ("scene_gen.h", "elements.h")] + [
+        os.path.join(ROOT, "include", "b200io.h")]
     flags = ["-O3", "-fopenmp", "-shared", "-fPIC", "-std=c++17"]
     stamp = out + ".stamp"
     dig = _digest(srcs + hdrs, " ".join(flags))

@@ -1,0 +1,447 @@
+// Element energies of the cloth / affine-body scenes, shared by the host
+// generator (scene_gen.cpp) and the device generator (b2s_generate.cu).
+// Plain arrays, FP64; matrices row-major unless stated.
+//
+//  * Baraff-Witkin shell, strain-limiting stretch + shear
+//    (libuipc src/backends/cuda/finite_element/constitutions/
+//     strain_limiting_baraff_witkin_shell_2d.h:33-280,
+//     strain_limiting_baraff_witkin_shell_2d.cu:75-150): F = Ds Dm^-1 (3x2)
+//    in the rest triangle's own uv frame, warp a = (1,0), weft b = (0,1);
+//    stretch per direction (r-1)^2 + c s (r-1)^3 (c = 1 when r > 1) of
+//    r = |F a|, shear (a^T F^T F b)^2; the 6x6 d2E/dF2 in the reference's
+//    closed form (exact for the stretch where r > 1, its positive part below;
+//    the shear in its analytic PSD form); weight rest area x dt^2.
+//  * Discrete-shell bending, Gauss-Newton Hessian (the reference's default)
+//    (finite_element/constitutions/discrete_shell_bending_function.h:33-135,
+//     discrete_shell_bending_reference.h:8-28, utils/dihedral_angle.h:14-60):
+//    E = L0 kappa (theta - theta_bar)^2 / h_bar with h_bar = A / (3 L0), over
+//    the hinge (x0, x1, x2, x3), edge x1-x2; H = (2 L0 kappa / h_bar) dt^2
+//    grad(theta) grad(theta)^T.
+//  * Affine-body orthogonality potential
+//    (affine_body/constitutions/ortho_potential.cu:37-70, sym/ortho_potential.inl):
+//    E = kappa sum_ij (a_i . a_j - delta_ij)^2 over the three 3-vectors
+//    a_1..a_3 = q[3..11] of the body's 12 DoF; gradient and Hessian derived
+//    here by hand, the 9x9 Hessian projected to PSD (eigenvalues clamped at 0),
+//    weight volume x dt^2.
+#pragma once
+
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define B2_HD __host__ __device__ inline
+#else
+#define B2_HD inline
+#endif
+
+namespace b2el
+{
+B2_HD double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+B2_HD void   cross3(const double* a, const double* b, double* c)
+{
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+B2_HD void sub3(const double* a, const double* b, double* c)
+{
+    c[0] = a[0] - b[0];
+    c[1] = a[1] - b[1];
+    c[2] = a[2] - b[2];
+}
+
+// cyclic Jacobi eigen-decomposition of a symmetric n x n matrix (n <= 12):
+// a is destroyed (its diagonal ends as the eigenvalues w), v[i*n+k] is
+// component i of eigenvector k
+template <int N>
+B2_HD void jacobi_eigen(double* a, double* w, double* v)
+{
+    for(int i = 0; i < N * N; ++i)
+        v[i] = 0.0;
+    for(int i = 0; i < N; ++i)
+        v[i * N + i] = 1.0;
+    for(int sweep = 0; sweep < 60; ++sweep)
+    {
+        double off = 0.0, diag = 0.0;
+        for(int p = 0; p < N; ++p)
+        {
+            diag += a[p * N + p] * a[p * N + p];
+            for(int q = p + 1; q < N; ++q)
+                off += a[p * N + q] * a[p * N + q];
+        }
+        if(off <= 1e-30 * (diag + 1e-300))
+            break;
+        for(int p = 0; p < N; ++p)
+            for(int q = p + 1; q < N; ++q)
+            {
+                const double apq = a[p * N + q];
+                if(fabs(apq) < 1e-300)
+                    continue;
+                const double app = a[p * N + p], aqq = a[q * N + q];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for(int k = 0; k < N; ++k)
+                {
+                    const double akp = a[k * N + p], akq = a[k * N + q];
+                    a[k * N + p] = c * akp - s * akq;
+                    a[k * N + q] = s * akp + c * akq;
+                }
+                for(int k = 0; k < N; ++k)
+                {
+                    const double apk = a[p * N + k], aqk = a[q * N + k];
+                    a[p * N + k] = c * apk - s * aqk;
+                    a[q * N + k] = s * apk + c * aqk;
+                }
+                for(int k = 0; k < N; ++k)
+                {
+                    const double vkp = v[k * N + p], vkq = v[k * N + q];
+                    v[k * N + p] = c * vkp - s * vkq;
+                    v[k * N + q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    for(int i = 0; i < N; ++i)
+        w[i] = a[i * N + i];
+}
+
+// symmetric H (N x N, row-major) -> its positive part (negative eigenvalues
+// set to zero); returns with H exactly symmetric
+template <int N>
+B2_HD void project_psd(double* H)
+{
+    double a[N * N], w[N], v[N * N];
+    for(int i = 0; i < N * N; ++i)
+        a[i] = H[i];
+    jacobi_eigen<N>(a, w, v);
+    bool neg = false;
+    for(int k = 0; k < N; ++k)
+        neg = neg || w[k] < 0.0;
+    if(!neg)
+        return;
+    for(int i = 0; i < N; ++i)
+        for(int j = i; j < N; ++j)
+        {
+            double s = 0.0;
+            for(int k = 0; k < N; ++k)
+                if(w[k] > 0.0)
+                    s += v[i * N + k] * w[k] * v[j * N + k];
+            H[i * N + j] = s;
+            H[j * N + i] = s;
+        }
+}
+
+// ---- Baraff-Witkin shell --------------------------------------------------------
+// rest frame: the triangle rotated so its normal is +z (Rodrigues form of the
+// rotation taking n to z; n = -z flips x and y), Dm = [uv1 - uv0, uv2 - uv0];
+// IB = Dm^-1 as {IB00, IB10, IB01, IB11} (column-major 2x2)
+B2_HD void bw_rest(const double* x0, const double* x1, const double* x2, double* IB)
+{
+    double e1[3], e2[3], n[3];
+    sub3(x1, x0, e1);
+    sub3(x2, x0, e2);
+    cross3(e1, e2, n);
+    const double nn = sqrt(dot3(n, n));
+    for(int k = 0; k < 3; ++k)
+        n[k] /= nn;
+    const double z[3] = {0.0, 0.0, 1.0};
+    double       vv[3];
+    cross3(n, z, vv);
+    const double c = dot3(n, z);
+    double       R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    if(c + 1.0 == 0.0)
+    {
+        R[0] = -1.0;
+        R[4] = -1.0;
+    }
+    else
+    {
+        const double K[9] = {0.0, -vv[2], vv[1], vv[2], 0.0, -vv[0], -vv[1], vv[0], 0.0};
+        for(int i = 0; i < 3; ++i)
+            for(int j = 0; j < 3; ++j)
+            {
+                double kk = 0.0;
+                for(int m = 0; m < 3; ++m)
+                    kk += K[i * 3 + m] * K[m * 3 + j];
+                R[i * 3 + j] += K[i * 3 + j] + kk / (1.0 + c);
+            }
+    }
+    double uv[3][2];
+    const double* xs[3] = {x0, x1, x2};
+    for(int p = 0; p < 3; ++p)
+        for(int r = 0; r < 2; ++r)
+            uv[p][r] = R[r * 3 + 0] * xs[p][0] + R[r * 3 + 1] * xs[p][1] + R[r * 3 + 2] * xs[p][2];
+    const double m00 = uv[1][0] - uv[0][0], m10 = uv[1][1] - uv[0][1];  // column 0
+    const double m01 = uv[2][0] - uv[0][0], m11 = uv[2][1] - uv[0][1];  // column 1
+    const double det = m00 * m11 - m01 * m10;
+    IB[0] = m11 / det;   // (0,0)
+    IB[1] = -m10 / det;  // (1,0)
+    IB[2] = -m01 / det;  // (0,1)
+    IB[3] = m00 / det;   // (1,1)
+}
+
+B2_HD double tri_area(const double* x0, const double* x1, const double* x2)
+{
+    double e1[3], e2[3], n[3];
+    sub3(x1, x0, e1);
+    sub3(x2, x0, e2);
+    cross3(e1, e2, n);
+    return 0.5 * sqrt(dot3(n, n));
+}
+
+// F columns fu = F a, fv = F b
+B2_HD void bw_F(const double* x0, const double* x1, const double* x2, const double* IB, double* fu, double* fv)
+{
+    for(int k = 0; k < 3; ++k)
+    {
+        const double d1 = x1[k] - x0[k], d2 = x2[k] - x0[k];
+        fu[k]           = d1 * IB[0] + d2 * IB[1];
+        fv[k]           = d1 * IB[2] + d2 * IB[3];
+    }
+}
+
+B2_HD double bw_energy(const double* fu, const double* fv, double stretch, double shear, double rate)
+{
+    const double I6 = dot3(fu, fv);
+    const double ru = sqrt(dot3(fu, fu)), rv = sqrt(dot3(fv, fv));
+    const double cu = ru <= 1.0 ? 0.0 : 1.0, cv = rv <= 1.0 ? 0.0 : 1.0;
+    const double st = (ru - 1) * (ru - 1) + cu * rate * (ru - 1) * (ru - 1) * (ru - 1) + (rv - 1) * (rv - 1)
+                      + cv * rate * (rv - 1) * (rv - 1) * (rv - 1);
+    return stretch * st + shear * I6 * I6;
+}
+
+// dE/dF as P[6] = [dE/dfu, dE/dfv] and the 6x6 d2E/dF2 (row-major) in the
+// reference's closed form
+B2_HD void bw_dF(const double* fu, const double* fv, double stretch, double shear, double rate, double* P, double* HF)
+{
+    const double I6 = dot3(fu, fv);
+    // stretch (the 1/sqrt(I5) singularity guarded as the reference does)
+    double I5u = dot3(fu, fu), I5v = dot3(fv, fv);
+    I5u        = I5u > 1e-12 ? I5u : 1e-12;
+    I5v        = I5v > 1e-12 ? I5v : 1e-12;
+    const double su = sqrt(I5u), sv = sqrt(I5v);
+    double       cu = 1.0 - 1.0 / su, cv = 1.0 - 1.0 / sv;
+    if(I5u > 1.0)
+        cu += 1.5 * rate * (su + 1.0 / su - 2.0);
+    if(I5v > 1.0)
+        cv += 1.5 * rate * (sv + 1.0 / sv - 2.0);
+    for(int k = 0; k < 3; ++k)
+    {
+        P[k]     = stretch * 2.0 * cu * fu[k] + shear * 2.0 * I6 * fv[k];
+        P[3 + k] = stretch * 2.0 * cv * fv[k] + shear * 2.0 * I6 * fu[k];
+    }
+    for(int i = 0; i < 36; ++i)
+        HF[i] = 0.0;
+    // stretch block of each direction: D I + c fhat fhat^T
+    const double* f[2]  = {fu, fv};
+    const double  sq[2] = {su, sv};
+    const double  I5[2] = {I5u, I5v};
+    for(int d = 0; d < 2; ++d)
+    {
+        const double s = sq[d];
+        const double D = s > 1.0 ? (s - 1.0) * (3.0 * s * rate - 3.0 * rate + 2.0) / s : 0.0;
+        const double c = s > 1.0 ? (3.0 * I5[d] * rate - 3.0 * rate + 2.0) / s : 2.0;
+        double       fh[3];
+        const double fn = sqrt(dot3(f[d], f[d]));
+        for(int k = 0; k < 3; ++k)
+            fh[k] = f[d][k] / fn;
+        for(int i = 0; i < 3; ++i)
+            for(int j = 0; j < 3; ++j)
+                HF[(3 * d + i) * 6 + 3 * d + j] = stretch * ((i == j ? D : 0.0) + c * fh[i] * fh[j]);
+    }
+    // shear: 2 (|I6| (T - Tq Tq^T / |Tq|^2) + lambda0 q0 q0^T), T = (I + sign(I6) S) / 2
+    // with S the swap of the two columns, g = [fv, fu], q0 = unit(I6 S g + lambda0 g)
+    double g[6];
+    for(int k = 0; k < 3; ++k)
+    {
+        g[k]     = fv[k];
+        g[3 + k] = fu[k];
+    }
+    const double I2      = dot3(fu, fu) + dot3(fv, fv);
+    const double lambda0 = 0.5 * (I2 + sqrt(I2 * I2 + 12.0 * I6 * I6));
+    const double sgn     = I6 >= 0.0 ? 1.0 : -1.0;
+    double       q0[6];
+    double       qn = 0.0;
+    for(int i = 0; i < 6; ++i)
+    {
+        const double Sg = g[i < 3 ? i + 3 : i - 3];
+        q0[i]           = I6 * Sg + lambda0 * g[i];
+        qn += q0[i] * q0[i];
+    }
+    qn = sqrt(qn);
+    for(int i = 0; i < 6; ++i)
+        q0[i] /= qn;
+    double Tq[6], tn = 0.0;
+    for(int i = 0; i < 6; ++i)
+    {
+        Tq[i] = 0.5 * (q0[i] + sgn * q0[i < 3 ? i + 3 : i - 3]);
+        tn += Tq[i] * Tq[i];
+    }
+    const double aI6 = fabs(I6);
+    for(int i = 0; i < 6; ++i)
+        for(int j = 0; j < 6; ++j)
+        {
+            const double T = 0.5 * ((i == j ? 1.0 : 0.0) + sgn * ((i < 3 ? i + 3 : i - 3) == j ? 1.0 : 0.0));
+            HF[i * 6 + j] += shear * 2.0 * (aI6 * (T - Tq[i] * Tq[j] / tn) + lambda0 * q0[i] * q0[j]);
+        }
+}
+
+// element gradient G[9] and Hessian H[81] (row-major, vertex-major 3-blocks)
+// over (x0, x1, x2), scaled by w (rest area x dt^2)
+B2_HD void bw_grad_hess(const double* x0, const double* x1, const double* x2, const double* IB, double stretch,
+                        double shear, double rate, double w, double* G, double* H)
+{
+    double fu[3], fv[3], P[6], HF[36];
+    bw_F(x0, x1, x2, IB, fu, fv);
+    bw_dF(fu, fv, stretch, shear, rate, P, HF);
+    // dfu/dx_i = cu[i] I, dfv/dx_i = cv[i] I
+    const double cu[3] = {-(IB[0] + IB[1]), IB[0], IB[1]};
+    const double cv[3] = {-(IB[2] + IB[3]), IB[2], IB[3]};
+    for(int i = 0; i < 3; ++i)
+        for(int k = 0; k < 3; ++k)
+            G[3 * i + k] = w * (cu[i] * P[k] + cv[i] * P[3 + k]);
+    for(int i = 0; i < 3; ++i)
+        for(int j = 0; j < 3; ++j)
+            for(int p = 0; p < 3; ++p)
+                for(int q = 0; q < 3; ++q)
+                    H[(3 * i + p) * 9 + 3 * j + q] =
+                        w * (cu[i] * cu[j] * HF[p * 6 + q] + cu[i] * cv[j] * HF[p * 6 + 3 + q]
+                             + cv[i] * cu[j] * HF[(3 + p) * 6 + q] + cv[i] * cv[j] * HF[(3 + p) * 6 + 3 + q]);
+}
+
+// ---- discrete-shell bending -------------------------------------------------------
+// signed dihedral angle of the hinge (x0, x1, x2, x3), edge x1-x2
+B2_HD double dihedral(const double* x0, const double* x1, const double* x2, const double* x3)
+{
+    double a[3], b[3], c[3], d[3], n1[3], n2[3], m[3], e[3];
+    sub3(x1, x0, a);
+    sub3(x2, x0, b);
+    cross3(a, b, n1);
+    sub3(x2, x3, c);
+    sub3(x1, x3, d);
+    cross3(c, d, n2);
+    double cs = dot3(n1, n2) / sqrt(dot3(n1, n1) * dot3(n2, n2));
+    cs        = cs < -1.0 ? -1.0 : (cs > 1.0 ? 1.0 : cs);
+    double th = acos(cs);
+    cross3(n2, n1, m);
+    sub3(x1, x2, e);
+    return dot3(m, e) < 0.0 ? -th : th;
+}
+
+// d theta / d(x0, x1, x2, x3)
+B2_HD void dihedral_grad(const double* x0, const double* x1, const double* x2, const double* x3, double* g)
+{
+    double e0[3], e1[3], e2[3], e3[3], e4[3], n1[3], n2[3];
+    sub3(x2, x1, e0);  // the hinge edge
+    sub3(x0, x1, e1);
+    sub3(x3, x1, e2);
+    sub3(x0, x2, e3);
+    sub3(x3, x2, e4);
+    cross3(e0, e1, n1);
+    cross3(e2, e0, n2);
+    const double n1s = dot3(n1, n1), n2s = dot3(n2, n2), el = sqrt(dot3(e0, e0));
+    for(int k = 0; k < 3; ++k)
+    {
+        g[k]     = -el / n1s * n1[k];
+        g[3 + k] = -dot3(e0, e3) / (el * n1s) * n1[k] - dot3(e0, e4) / (el * n2s) * n2[k];
+        g[6 + k] = dot3(e0, e1) / (el * n1s) * n1[k] + dot3(e0, e2) / (el * n2s) * n2[k];
+        g[9 + k] = -el / n2s * n2[k];
+    }
+}
+
+// rest quantities of a hinge: L0, h_bar, theta_bar
+B2_HD void dsb_rest(const double* x0, const double* x1, const double* x2, const double* x3, double* L0,
+                    double* h_bar, double* theta_bar)
+{
+    double e[3], a[3], b[3], c[3], d[3], n1[3], n2[3];
+    sub3(x2, x1, e);
+    *L0 = sqrt(dot3(e, e));
+    sub3(x1, x0, a);
+    sub3(x2, x0, b);
+    cross3(a, b, n1);
+    sub3(x2, x3, c);
+    sub3(x1, x3, d);
+    cross3(c, d, n2);
+    const double A = (sqrt(dot3(n1, n1)) + sqrt(dot3(n2, n2))) / 2.0;
+    *h_bar         = A / 3.0 / *L0;
+    *theta_bar     = dihedral(x0, x1, x2, x3);
+}
+
+B2_HD double dsb_energy(const double* x0, const double* x1, const double* x2, const double* x3, double L0,
+                        double h_bar, double theta_bar, double kappa)
+{
+    const double d = dihedral(x0, x1, x2, x3) - theta_bar;
+    return L0 * kappa * d * d / h_bar;
+}
+
+// gradient G[12] and Gauss-Newton Hessian H[144] scaled by w (dt^2)
+B2_HD void dsb_grad_hess(const double* x0, const double* x1, const double* x2, const double* x3, double L0,
+                         double h_bar, double theta_bar, double kappa, double w, double* G, double* H)
+{
+    const double th = dihedral(x0, x1, x2, x3);
+    double       g[12];
+    dihedral_grad(x0, x1, x2, x3, g);
+    const double dE  = 2.0 * L0 * kappa * (th - theta_bar) / h_bar;
+    const double ddE = 2.0 * L0 * kappa / h_bar;
+    for(int i = 0; i < 12; ++i)
+        G[i] = w * dE * g[i];
+    const double c = ddE * w;
+    for(int i = 0; i < 12; ++i)
+    {
+        const double ci = c * g[i];
+        H[i * 12 + i]   = ci * g[i];
+        for(int j = i + 1; j < 12; ++j)
+        {
+            const double v = ci * g[j];
+            H[i * 12 + j]  = v;
+            H[j * 12 + i]  = v;
+        }
+    }
+}
+
+// ---- affine-body orthogonality potential -------------------------------------------
+B2_HD double ortho_energy(const double* q, double kappa)
+{
+    double e = 0.0;
+    for(int i = 0; i < 3; ++i)
+        for(int j = 0; j < 3; ++j)
+        {
+            const double d = dot3(q + 3 + 3 * i, q + 3 + 3 * j) - (i == j ? 1.0 : 0.0);
+            e += d * d;
+        }
+    return kappa * e;
+}
+
+// gradient over q[3..11] (G9) and the PSD-projected Hessian H9 (81), scaled by w
+B2_HD void ortho_grad_hess(const double* q, double kappa, double w, double* G9, double* H9)
+{
+    const double* a[3] = {q + 3, q + 6, q + 9};
+    double        Gm[3][3];
+    for(int i = 0; i < 3; ++i)
+        for(int j = 0; j < 3; ++j)
+            Gm[i][j] = dot3(a[i], a[j]) - (i == j ? 1.0 : 0.0);
+    // g_k = 4 kappa sum_j (a_k . a_j - delta_kj) a_j
+    for(int k = 0; k < 3; ++k)
+        for(int c = 0; c < 3; ++c)
+        {
+            double s = 0.0;
+            for(int j = 0; j < 3; ++j)
+                s += Gm[k][j] * a[j][c];
+            G9[3 * k + c] = w * 4.0 * kappa * s;
+        }
+    // H_kl = 4 kappa (delta_kl sum_j a_j a_j^T + a_l a_k^T + (a_k . a_l - delta_kl) I)
+    double S[3][3];
+    for(int r = 0; r < 3; ++r)
+        for(int c = 0; c < 3; ++c)
+            S[r][c] = a[0][r] * a[0][c] + a[1][r] * a[1][c] + a[2][r] * a[2][c];
+    for(int k = 0; k < 3; ++k)
+        for(int l = 0; l < 3; ++l)
+            for(int r = 0; r < 3; ++r)
+                for(int c = 0; c < 3; ++c)
+                    H9[(3 * k + r) * 9 + 3 * l + c] =
+                        4.0 * kappa
+                        * ((k == l ? S[r][c] : 0.0) + a[l][r] * a[k][c] + (r == c ? Gm[k][l] : 0.0));
+    project_psd<9>(H9);
+    for(int i = 0; i < 81; ++i)
+        H9[i] *= w;
+}
+}  // namespace b2el

@@ -8,6 +8,10 @@
 //  * BDF1 kinetic term 1/2 m |x - x_tilde|^2, x_tilde = x + dt v + dt^2 g,
 //    lumped mass rho V / 4 per tet corner
 //    (src/backends/cuda/finite_element/bdf/finite_element_bdf1_kinetic.cu).
+//  * Cloth: Baraff-Witkin strain-limiting stretch + shear and discrete-shell
+//    bending (Gauss-Newton hinge Hessian), elements.h;
+//    affine bodies: the orthogonality potential (elements.h) and the
+//    kinetic term of their 12 DoF.
 //  * IPC log barrier on squared distance D < dhat^2:
 //        b(D) = -(D - Dhat)^2 log(D / Dhat), energy dt^2 kappa b(D).
 //    Contact Hessians use the barrier curvature along the fixed contact
@@ -16,6 +20,7 @@
 //    or I (diagonal) and its gradient is zeroed
 //    (src/backends/cuda/finite_element/fem_linear_subsystem.cu:23-52).
 #include "scene_gen.h"
+#include "elements.h"
 
 #include <algorithm>
 #include <array>
@@ -191,7 +196,110 @@ struct Builder
         cols.reserve(n);
         vals.reserve(n * 9);
     }
+    // block (r, c) of a row-major element matrix, stored block-upper and
+    // column-major (transposed when r > c)
+    void put(int32_t r, int32_t c, const double* Hrc)
+    {
+        const bool tp = r > c;
+        rows.push_back(tp ? c : r);
+        cols.push_back(tp ? r : c);
+        for(int q = 0; q < 3; ++q)
+            for(int p = 0; p < 3; ++p)
+                vals.push_back(tp ? Hrc[q * 3 + p] : Hrc[p * 3 + q]);
+    }
+    // the upper blocks of an n-vertex element Hessian (row-major, 3n x 3n)
+    template <int NV>
+    void put_element(const int32_t* v, const double* H)
+    {
+        for(int i = 0; i < NV; ++i)
+            for(int j = i; j < NV; ++j)
+            {
+                double blk[9];
+                for(int p = 0; p < 3; ++p)
+                    for(int q = 0; q < 3; ++q)
+                        blk[p * 3 + q] = H[(3 * i + p) * (3 * NV) + 3 * j + q];
+                put(v[i], v[j], blk);
+            }
+    }
 };
+
+// Cloth of N x N grid vertices (global block rows off + i + N k), cells
+// split along the (i, k)-(i+1, k+1) diagonal; at state x with rest x_rest:
+//  * Baraff-Witkin stretch (stiffness `stretch`) and shear (0.1 x stretch),
+//    strain rate 100 (the reference's default): 6 triplets per triangle;
+//  * discrete-shell bending (stiffness `bend`) on every interior edge, hinge
+//    (opposite min, edge min, edge max, opposite max) as the reference orders
+//    its stencils: 10 triplets per hinge;
+// energies scaled by rest area x dt^2 (stretch) and dt^2 (bending); the
+// gradient is added to grad. Returns the triangle count.
+int64_t add_cloth_grid(Builder& B, std::vector<double>& grad, const std::vector<double>& x,
+                       const std::vector<double>& x_rest, int64_t off, int N, double stretch, double bend, double dt2,
+                       std::vector<int32_t>* tris_out = nullptr, std::vector<int32_t>* hinges_out = nullptr)
+{
+    auto vid = [&](int64_t i, int64_t k) { return (int32_t)(off + i + (int64_t)N * k); };
+    std::vector<int32_t> tris;
+    tris.reserve((size_t)6 * (N - 1) * (N - 1));
+    for(int64_t k = 0; k + 1 < N; ++k)
+        for(int64_t i = 0; i + 1 < N; ++i)
+        {
+            const int32_t a = vid(i, k), b = vid(i + 1, k), c = vid(i + 1, k + 1), d = vid(i, k + 1);
+            tris.insert(tris.end(), {a, b, c, a, c, d});
+        }
+    const int64_t nt = (int64_t)tris.size() / 3;
+    const double  shear = 0.1 * stretch, rate = 100.0;
+    for(int64_t t = 0; t < nt; ++t)
+    {
+        const int32_t* v = &tris[3 * t];
+        double         IB[4], G[9], H[81];
+        b2el::bw_rest(&x_rest[3 * v[0]], &x_rest[3 * v[1]], &x_rest[3 * v[2]], IB);
+        const double area = b2el::tri_area(&x_rest[3 * v[0]], &x_rest[3 * v[1]], &x_rest[3 * v[2]]);
+        b2el::bw_grad_hess(&x[3 * v[0]], &x[3 * v[1]], &x[3 * v[2]], IB, stretch, shear, rate, area * dt2, G, H);
+        B.put_element<3>(v, H);
+        for(int i = 0; i < 3; ++i)
+            for(int a = 0; a < 3; ++a)
+                grad[3 * (size_t)v[i] + a] += G[3 * i + a];
+    }
+    // hinges: edges with two triangles, in (min, max) edge order
+    std::vector<std::array<int32_t, 4>> opp;  // edge min, edge max, opposite, opposite
+    opp.reserve((size_t)3 * nt);
+    for(int64_t t = 0; t < nt; ++t)
+    {
+        int32_t T[3] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+        std::sort(T, T + 3);
+        opp.push_back({T[0], T[1], T[2], 0});
+        opp.push_back({T[0], T[2], T[1], 0});
+        opp.push_back({T[1], T[2], T[0], 0});
+    }
+    std::sort(opp.begin(), opp.end());
+    std::vector<int32_t> hinges;
+    for(size_t e = 0; e + 1 < opp.size();)
+    {
+        size_t f = e + 1;
+        while(f < opp.size() && opp[f][0] == opp[e][0] && opp[f][1] == opp[e][1])
+            ++f;
+        if(f - e == 2)
+            hinges.insert(hinges.end(), {std::min(opp[e][2], opp[e + 1][2]), opp[e][0], opp[e][1],
+                                         std::max(opp[e][2], opp[e + 1][2])});
+        e = f;
+    }
+    const int64_t nh = (int64_t)hinges.size() / 4;
+    for(int64_t h = 0; h < nh; ++h)
+    {
+        const int32_t* v = &hinges[4 * h];
+        double         L0, hb, thb, G[12], H[144];
+        b2el::dsb_rest(&x_rest[3 * v[0]], &x_rest[3 * v[1]], &x_rest[3 * v[2]], &x_rest[3 * v[3]], &L0, &hb, &thb);
+        b2el::dsb_grad_hess(&x[3 * v[0]], &x[3 * v[1]], &x[3 * v[2]], &x[3 * v[3]], L0, hb, thb, bend, dt2, G, H);
+        B.put_element<4>(v, H);
+        for(int i = 0; i < 4; ++i)
+            for(int a = 0; a < 3; ++a)
+                grad[3 * (size_t)v[i] + a] += G[3 * i + a];
+    }
+    if(tris_out)
+        *tris_out = std::move(tris);
+    if(hinges_out)
+        *hinges_out = std::move(hinges);
+    return nt;
+}
 }  // namespace
 
 struct b2g_system
@@ -252,21 +360,20 @@ namespace
 // angles), first Newton step from rest. Bodies first in the DoF order.
 //  * affine body b: q = (p, A[:,0], A[:,1], A[:,2]), x = p + A xbar; the
 //    kinetic Hessian is the body mass matrix (m I; m s^2/12 I per column, the
-//    cube's second moments), the orthogonality potential kappa V |A A^T - I|^2
-//    at A = R has Hessian 8 kappa V |sym(R^T dA)|^2; 16 triplets per body
-//    (4 x 4 grid of 3x3 blocks), the lower ones written as zero blocks, as the
-//    reference's affine-body subsystem writes them;
-//  * cloth: lumped mass (1 mm sheet), membrane edge springs of stiffness E
-//    (stand-in for the Baraff-Witkin stretch), bending springs between
-//    vertices two apart along both grid axes (stiffness bend_k / h^2);
+//    cube's second moments), plus the orthogonality potential (elements.h)
+//    at A = R, scaled by V dt^2; 16 triplets per body (4 x 4 grid of 3x3
+//    blocks), the lower ones written as zero blocks, as the reference's
+//    affine-body subsystem writes them;
+//  * cloth: lumped mass (1 mm sheet), Baraff-Witkin stretch (stiffness E) and
+//    shear, discrete-shell bending (stiffness bend_k) (add_cloth_grid);
 //  * contact: cloth vertex above a body's top face at distance d < dhat,
 //    barrier b(d^2) along +y, coupling the vertex with the body's 12 DoF
 //    (rank-1 Hessian over 5 block rows: 15 triplets, 4 vertex-body blocks);
 //  * potentials scaled by dt^2, gravity -y.
 // The 16 blocks of affine body b (block rows 4b .. 4b+3; lower blocks as
 // zero blocks): mass matrix m_b I on p, I_b I on each column of A, plus the
-// orthogonality potential's Hessian 8 kappa V |sym(R^T dA)|^2 at A = R (R a
-// rotation about +y by theta), scaled by dt^2; and its gravity gradient.
+// orthogonality potential's PSD Hessian at A = R (R a rotation about +y by
+// theta), scaled by V dt^2; and its gravity gradient.
 void add_affine_body(Builder& B, std::vector<double>& grad, int64_t b, double theta, double m_b, double I_b,
                      double V, const b2g_config& C)
 {
@@ -280,29 +387,17 @@ void add_affine_body(Builder& B, std::vector<double>& grad, int64_t b, double th
     }
     const double cs = std::cos(theta), sn = std::sin(theta);
     const double R[3][3] = {{cs, 0, sn}, {0, 1, 0}, {-sn, 0, cs}};
-    // q index 3 + 3 k + r <-> A[r][k]; S_m = sym(R^T E_m)
-    double S[9][3][3];
-    for(int m = 0; m < 9; ++m)
-    {
-        const int k = m / 3, r = m % 3;  // E_m has a 1 at (r, k)
-        double RtE[3][3];
-        for(int i = 0; i < 3; ++i)
-            for(int j = 0; j < 3; ++j)
-                RtE[i][j] = (j == k) ? R[r][i] : 0.0;
-        for(int i = 0; i < 3; ++i)
-            for(int j = 0; j < 3; ++j)
-                S[m][i][j] = 0.5 * (RtE[i][j] + RtE[j][i]);
-    }
-    const double ko = dt2 * 8.0 * C.body_kappa * V;
+    // orthogonality potential at A = R (q index 3 + 3 k + r <-> A[r][k]):
+    // zero gradient, PSD Hessian
+    double q[12] = {};
+    for(int k = 0; k < 3; ++k)
+        for(int r = 0; r < 3; ++r)
+            q[3 + 3 * k + r] = R[r][k];
+    double G9[9], H9[81];
+    b2el::ortho_grad_hess(q, C.body_kappa, V * dt2, G9, H9);
     for(int m = 0; m < 9; ++m)
         for(int n = 0; n < 9; ++n)
-        {
-            double d = 0.0;
-            for(int i = 0; i < 3; ++i)
-                for(int j = 0; j < 3; ++j)
-                    d += S[m][i][j] * S[n][i][j];
-            H[3 + m][3 + n] += ko * d;
-        }
+            H[3 + m][3 + n] += H9[m * 9 + n];
     // kinetic gradient: m (x - x_tilde) with x_tilde = x - dt^2 g on p
     grad[(4 * b) * 3 + 1] += m_b * dt2 * C.gravity;
     for(int bi = 0; bi < 4; ++bi)
@@ -376,27 +471,7 @@ void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
         put(c0 + (int32_t)v, c0 + (int32_t)v, Hm);
         sys->grad[(c0 + v) * 3 + 1] += m_v * dt2 * C.gravity;
     }
-    auto spring = [&](int64_t va, int64_t vb, double k)
-    {
-        const int32_t ga = c0 + (int32_t)va, gb = c0 + (int32_t)vb;
-        double d[3], l = 0.0;
-        for(int a = 0; a < 3; ++a)
-        {
-            d[a] = sys->x[gb * 3 + a] - sys->x[ga * 3 + a];
-            l += d[a] * d[a];
-        }
-        l = std::sqrt(l);
-        double H[9], Hn[9];
-        for(int p = 0; p < 3; ++p)
-            for(int q = 0; q < 3; ++q)
-            {
-                H[p * 3 + q]  = dt2 * k * d[p] * d[q] / (l * l);
-                Hn[p * 3 + q] = -H[p * 3 + q];
-            }
-        put(ga, ga, H);
-        put(gb, gb, H);
-        put(ga, gb, Hn);
-    };
+    add_cloth_grid(B, sys->grad, sys->x, sys->x_rest, c0, N, C.E, C.bend_k, dt2);
     auto vid = [&](int64_t i, int64_t k) { return i + (int64_t)N * k; };
     std::vector<std::vector<int32_t>> nb(rows);
     auto link = [&](int64_t va, int64_t vb)
@@ -408,24 +483,11 @@ void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
         for(int64_t i = 0; i < N; ++i)
         {
             if(i + 1 < N)
-            {
-                spring(vid(i, k), vid(i + 1, k), C.E);
                 link(vid(i, k), vid(i + 1, k));
-            }
             if(k + 1 < N)
-            {
-                spring(vid(i, k), vid(i, k + 1), C.E);
                 link(vid(i, k), vid(i, k + 1));
-            }
             if(i + 1 < N && k + 1 < N)
-            {
-                spring(vid(i, k), vid(i + 1, k + 1), C.E);
                 link(vid(i, k), vid(i + 1, k + 1));
-            }
-            if(i + 2 < N)
-                spring(vid(i, k), vid(i + 2, k), C.bend_k / (hc * hc));
-            if(k + 2 < N)
-                spring(vid(i, k), vid(i, k + 2), C.bend_k / (hc * hc));
         }
     // ---- cloth-body contacts ----
     int64_t n_contacts = 0;
@@ -1071,7 +1133,7 @@ void generate_tets(const b2g_config& C, const double* x_in, const double* xt_in,
 // (generate_tets, W = n_cubes), an N x N cloth (N = cloth_n) resting on their
 // top faces, and bodies_x x bodies_z affine bodies resting on the cloth;
 // first Newton step from rest.
-//  * cloth: as scene 3 (lumped mass, membrane and bending springs), covering
+//  * cloth: as scene 3 (lumped mass, Baraff-Witkin, bending), covering
 //    the grid, 0.5 dhat above the (planar) top faces;
 //  * cloth-cube contact: each cloth vertex over a top-face triangle at
 //    distance 0 < d < dhat: point-triangle barrier b(d^2), D = (a . x)^2 with
@@ -1157,25 +1219,7 @@ void generate_wall(const b2g_config& C, b2g_system* sys)
         put((int32_t)(off_cl + v), (int32_t)(off_cl + v), Hm);
         sys->grad[(off_cl + v) * 3 + 1] += m_v * dt2 * C.gravity;
     }
-    auto spring = [&](int32_t ga, int32_t gb, double k)
-    {
-        double d[3], l = 0.0;
-        for(int a = 0; a < 3; ++a)
-        {
-            d[a] = sys->x[gb * 3 + a] - sys->x[ga * 3 + a];
-            l += d[a] * d[a];
-        }
-        double H[9], Hn[9];
-        for(int p = 0; p < 3; ++p)
-            for(int q = 0; q < 3; ++q)
-            {
-                H[p * 3 + q]  = dt2 * k * d[p] * d[q] / l;
-                Hn[p * 3 + q] = -H[p * 3 + q];
-            }
-        put(ga, ga, H);
-        put(gb, gb, H);
-        put(ga, gb, Hn);
-    };
+    add_cloth_grid(B, sys->grad, sys->x, sys->x_rest, off_cl, N, C.cloth_k, C.bend_k, dt2);
     auto link = [&](int32_t ga, int32_t gb)
     {
         nb[ga - off_cl].push_back(gb);
@@ -1185,24 +1229,11 @@ void generate_wall(const b2g_config& C, b2g_system* sys)
         for(int64_t i = 0; i < N; ++i)
         {
             if(i + 1 < N)
-            {
-                spring(cg(i, k), cg(i + 1, k), C.cloth_k);
                 link(cg(i, k), cg(i + 1, k));
-            }
             if(k + 1 < N)
-            {
-                spring(cg(i, k), cg(i, k + 1), C.cloth_k);
                 link(cg(i, k), cg(i, k + 1));
-            }
             if(i + 1 < N && k + 1 < N)
-            {
-                spring(cg(i, k), cg(i + 1, k + 1), C.cloth_k);
                 link(cg(i, k), cg(i + 1, k + 1));
-            }
-            if(i + 2 < N)
-                spring(cg(i, k), cg(i + 2, k), C.bend_k / (hc * hc));
-            if(k + 2 < N)
-                spring(cg(i, k), cg(i, k + 2), C.bend_k / (hcz * hcz));
         }
     // ---- cloth-cube contacts (point-triangle on the top faces) ----
     auto pos = [&](int64_t g) -> Vec3 { return {sys->x[g * 3], sys->x[g * 3 + 1], sys->x[g * 3 + 2]}; };
@@ -1407,5 +1438,29 @@ const double* b2g_gradient(const b2g_system* s) { return s->grad.data(); }
 int64_t b2g_num_adjacency(const b2g_system* s) { return (int64_t)s->adj_list.size(); }
 const int32_t* b2g_adjacency_start(const b2g_system* s) { return s->adj_start.data(); }
 const int32_t* b2g_adjacency_list(const b2g_system* s) { return s->adj_list.data(); }
+
+double b2g_element_bw(const double* x, const double* rest, double stretch, double shear, double rate, double w,
+                      double* G9, double* H81)
+{
+    double IB[4], fu[3], fv[3];
+    b2el::bw_rest(rest, rest + 3, rest + 6, IB);
+    b2el::bw_grad_hess(x, x + 3, x + 6, IB, stretch, shear, rate, w, G9, H81);
+    b2el::bw_F(x, x + 3, x + 6, IB, fu, fv);
+    return b2el::bw_energy(fu, fv, stretch, shear, rate);
+}
+
+double b2g_element_dsb(const double* x, const double* rest, double kappa, double w, double* G12, double* H144)
+{
+    double L0, hb, thb;
+    b2el::dsb_rest(rest, rest + 3, rest + 6, rest + 9, &L0, &hb, &thb);
+    b2el::dsb_grad_hess(x, x + 3, x + 6, x + 9, L0, hb, thb, kappa, w, G12, H144);
+    return b2el::dsb_energy(x, x + 3, x + 6, x + 9, L0, hb, thb, kappa);
+}
+
+double b2g_element_ortho(const double* q, double kappa, double w, double* G9, double* H81)
+{
+    b2el::ortho_grad_hess(q, kappa, w, G9, H81);
+    return b2el::ortho_energy(q, kappa);
+}
 
 }  // extern "C"

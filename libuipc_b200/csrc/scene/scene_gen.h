@@ -100,6 +100,19 @@ int64_t        b2g_num_adjacency(const b2g_system* s);
 const int32_t* b2g_adjacency_start(const b2g_system* s);  // [n_verts+1]
 const int32_t* b2g_adjacency_list(const b2g_system* s);   // [num_adjacency]
 
+// Element routines of the cloth / affine-body energies (elements.h), for
+// checks against the formulas: energy, gradient and Hessian (row-major) of
+//  * one Baraff-Witkin triangle: x[9] current and rest[9] rest corners,
+//    weight w (the element scale; the energy is returned unscaled);
+//  * one discrete-shell hinge (x0, x1, x2, x3; edge x1-x2) with its rest
+//    corners, stiffness kappa, weight w (Gauss-Newton Hessian);
+//  * the orthogonality potential of q[12] (gradient/Hessian over q[3..11],
+//    Hessian projected to PSD), weight w.
+double b2g_element_bw(const double* x, const double* rest, double stretch, double shear, double rate, double w,
+                      double* G9, double* H81);
+double b2g_element_dsb(const double* x, const double* rest, double kappa, double w, double* G12, double* H144);
+double b2g_element_ortho(const double* q, double kappa, double w, double* G9, double* H81);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,186 @@
+"""CPU oracle (test infrastructure) of the cloth / affine-body element
+energies the generators produce: a numpy restatement of libuipc's formulas,
+written independently of the library's C++ (csrc/scene/elements.h), used only
+by tests to check it.
+
+* Baraff-Witkin shell: strain_limiting_baraff_witkin_shell_2d.h:33-280 (rest
+  frame Dm2x2 :33-66, E :96-127, dEdF :129-170, ddEddF :172-278) and the
+  element assembly of strain_limiting_baraff_witkin_shell_2d.cu:75-150
+  (G = dFdx^T vec(dEdF), H = dFdx^T ddEddF dFdx, weight rest area dt^2).
+* Discrete-shell bending: discrete_shell_bending_function.h:33-135 (Gauss-
+  Newton Hessian), discrete_shell_bending_reference.h:8-28 (rest L0, h_bar,
+  theta_bar), utils/dihedral_angle.h:14-60 (angle and its gradient).
+* Affine-body orthogonality potential: affine_body/constitutions/
+  sym/ortho_potential.inl (E, dEdq, ddEddq over q[3..11]),
+  ortho_potential.cu:37-70 (make_spd on the 9x9, weight volume dt^2).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+# ---- Baraff-Witkin -------------------------------------------------------------
+def bw_rest(x0, x1, x2):
+    """Dm^-1 of the rest triangle in its own uv frame (normal rotated to +z)."""
+    n = np.cross(x1 - x0, x2 - x0)
+    n = n / np.linalg.norm(n)
+    z = np.array([0.0, 0.0, 1.0])
+    v = np.cross(n, z)
+    c = float(n @ z)
+    R = np.eye(3)
+    if c + 1 == 0:
+        R[0, 0] = R[1, 1] = -1.0
+    else:
+        K = np.array([[0, -v[2], v[1]], [v[2], 0, -v[0]], [-v[1], v[0], 0]])
+        R = R + K + K @ K / (1 + c)
+    uv = [(R @ p)[:2] for p in (x0, x1, x2)]
+    Dm = np.column_stack([uv[1] - uv[0], uv[2] - uv[0]])
+    return np.linalg.inv(Dm)
+
+
+def bw_F(x, IB):
+    Ds = np.column_stack([x[1] - x[0], x[2] - x[0]])
+    return Ds @ IB
+
+
+def bw_energy(F, stretch, shear, rate):
+    a, b = np.array([1.0, 0.0]), np.array([0.0, 1.0])
+    I6 = a @ F.T @ F @ b
+    ru, rv = np.linalg.norm(F @ a), np.linalg.norm(F @ b)
+    cu, cv = (0.0 if ru <= 1 else 1.0), (0.0 if rv <= 1 else 1.0)
+    st = (ru - 1) ** 2 + cu * rate * (ru - 1) ** 3 + (rv - 1) ** 2 + cv * rate * (rv - 1) ** 3
+    return stretch * st + shear * I6 * I6
+
+
+def bw_ddEddF(F, stretch, shear, rate):
+    a, b = np.array([1.0, 0.0]), np.array([0.0, 1.0])
+    Hs = np.zeros((6, 6))
+    I5u = max(float((F @ a) @ (F @ a)), 1e-12)
+    I5v = max(float((F @ b) @ (F @ b)), 1e-12)
+    su, sv = np.sqrt(I5u), np.sqrt(I5v)
+    if su > 1:
+        Hs[0:3, 0:3] += np.eye(3) * 2 * ((su - 1) * (3 * su * rate - 3 * rate + 2) / (2 * su))
+    if sv > 1:
+        Hs[3:6, 3:6] += np.eye(3) * 2 * ((sv - 1) * (3 * sv * rate - 3 * rate + 2) / (2 * sv))
+    fu = F[:, 0] / np.linalg.norm(F[:, 0])
+    fv = F[:, 1] / np.linalg.norm(F[:, 1])
+    uc = (3 * I5u * rate - 3 * rate + 2) / np.sqrt(I5u) if su > 1 else 2.0
+    vc = (3 * I5v * rate - 3 * rate + 2) / np.sqrt(I5v) if sv > 1 else 2.0
+    Hs[0:3, 0:3] += uc * np.outer(fu, fu)
+    Hs[3:6, 3:6] += vc * np.outer(fv, fv)
+    S = np.zeros((6, 6))
+    S[3, 0] = S[4, 1] = S[5, 2] = S[0, 3] = S[1, 4] = S[2, 5] = 1.0
+    I6 = a @ F.T @ F @ b
+    sg = 1.0 if I6 >= 0 else -1.0
+    g = F @ (np.outer(a, b) + np.outer(b, a))
+    vg = np.concatenate([g[:, 0], g[:, 1]])
+    I2 = float((F * F).sum())
+    lam0 = 0.5 * (I2 + np.sqrt(I2 * I2 + 12 * I6 * I6))
+    q0 = I6 * S @ vg + lam0 * vg
+    q0 = q0 / np.linalg.norm(q0)
+    T = 0.5 * (np.eye(6) + sg * S)
+    Tq = T @ q0
+    Hsh = 2 * (abs(I6) * (T - np.outer(Tq, Tq) / (Tq @ Tq)) + lam0 * np.outer(q0, q0))
+    return stretch * Hs + shear * Hsh
+
+
+def bw_dFdx(IB):
+    d0, d1, d2, d3 = IB[0, 0], IB[1, 0], IB[0, 1], IB[1, 1]
+    D = np.zeros((6, 9))
+    for i in range(3):
+        D[i, i] = -(d0 + d1)
+        D[i + 3, i] = -(d2 + d3)
+        D[i, i + 3] = d0
+        D[i + 3, i + 3] = d2
+        D[i, i + 6] = d1
+        D[i + 3, i + 6] = d3
+    return D
+
+
+def bw_element(x, rest, stretch, shear, rate, w):
+    """(E, G[9], H[9x9]) of one triangle: E unscaled, G and H scaled by w.
+    G by central differences of E (an independent check of the closed forms)."""
+    IB = bw_rest(*rest)
+    D = bw_dFdx(IB)
+    H = w * D.T @ bw_ddEddF(bw_F(x, IB), stretch, shear, rate) @ D
+    E = bw_energy(bw_F(x, IB), stretch, shear, rate)
+    def e(k, d):
+        xx = x.copy()
+        xx[k // 3, k % 3] += d
+        return bw_energy(bw_F(xx, IB), stretch, shear, rate)
+
+    h = 1e-6 * np.abs(x).max()
+    # fourth-order central differences
+    G = np.array([w * (8 * (e(k, h) - e(k, -h)) - (e(k, 2 * h) - e(k, -2 * h))) / (12 * h) for k in range(9)])
+    return E, G, H
+
+
+# ---- discrete-shell bending ---------------------------------------------------
+def dihedral(x0, x1, x2, x3):
+    n1 = np.cross(x1 - x0, x2 - x0)
+    n2 = np.cross(x2 - x3, x1 - x3)
+    c = np.clip(n1 @ n2 / np.sqrt((n1 @ n1) * (n2 @ n2)), -1.0, 1.0)
+    th = np.arccos(c)
+    return -th if np.cross(n2, n1) @ (x1 - x2) < 0 else th
+
+
+def dsb_rest(x0, x1, x2, x3):
+    L0 = np.linalg.norm(x2 - x1)
+    A = (np.linalg.norm(np.cross(x1 - x0, x2 - x0)) + np.linalg.norm(np.cross(x2 - x3, x1 - x3))) / 2
+    return L0, A / 3 / L0, dihedral(x0, x1, x2, x3)
+
+
+def dsb_element(x, rest, kappa, w):
+    """(E, G[12], H_GN[12x12]): the angle gradient by central differences."""
+    L0, hb, thb = dsb_rest(*rest)
+    th = dihedral(*x)
+    E = L0 * kappa * (th - thb) ** 2 / hb
+    g = np.zeros(12)
+    h = 1e-7
+    for k in range(12):
+        xp, xm = x.copy(), x.copy()
+        xp[k // 3, k % 3] += h
+        xm[k // 3, k % 3] -= h
+        g[k] = (dihedral(*xp) - dihedral(*xm)) / (2 * h)
+    G = w * 2 * L0 * kappa * (th - thb) / hb * g
+    H = w * 2 * L0 * kappa / hb * np.outer(g, g)
+    return E, G, H
+
+
+# ---- affine-body orthogonality ------------------------------------------------
+def ortho_energy(q, kappa):
+    a = [q[3:6], q[6:9], q[9:12]]
+    return kappa * sum((a[i] @ a[j] - (i == j)) ** 2 for i in range(3) for j in range(3))
+
+
+def ortho_element(q, kappa, w):
+    """(E, G[9], H[9x9]): G and the Hessian by central differences of E, the
+    Hessian then projected to PSD by numpy's eigh."""
+    E = ortho_energy(q, kappa)
+    h = 1e-6
+
+    def grad(qq):
+        g = np.zeros(9)
+        for k in range(9):
+            qp, qm = qq.copy(), qq.copy()
+            qp[3 + k] += h
+            qm[3 + k] -= h
+            g[k] = (ortho_energy(qp, kappa) - ortho_energy(qm, kappa)) / (2 * h)
+        return g
+
+    G = w * grad(q)
+    # second derivatives of E by central differences of E (E is a quartic
+    # polynomial: the differences are exact up to rounding), then the PSD part
+    H = np.zeros((9, 9))
+    hh = 1e-4
+    for k in range(9):
+        for l in range(9):
+            def e(dk, dl):
+                qq = q.copy()
+                qq[3 + k] += dk
+                qq[3 + l] += dl
+                return ortho_energy(qq, kappa)
+            H[k, l] = (e(hh, hh) - e(hh, -hh) - e(-hh, hh) + e(-hh, -hh)) / (4 * hh * hh)
+    wv, V = np.linalg.eigh(0.5 * (H + H.T))
+    H = (V * np.maximum(wv, 0)) @ V.T
+    return E, G, w * H

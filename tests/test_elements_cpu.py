@@ -1,0 +1,102 @@
+"""The cloth / affine-body element routines of the generators
+(csrc/scene/elements.h, through libb200scene.so's b2g_element_* hooks)
+against the oracle's numpy restatement of libuipc's formulas
+(oracle/elements.py): energies equal, gradients equal to central differences
+of the restated energies, the Baraff-Witkin Hessian equal to the reference's
+closed form mapped through dF/dx, the hinge's Gauss-Newton Hessian equal to
+the outer product of the finite-difference angle gradient, and the
+orthogonality Hessian equal to the PSD part of the finite-difference Hessian.
+Random states: stretched, compressed and sheared triangles, bent hinges,
+near-rotation and general affine matrices."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from libuipc_b200._native import load_scene_lib
+from oracle import elements as OE
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _lib_bw(x, rest, stretch, shear, rate, w):
+    lib = load_scene_lib()
+    G, H = np.zeros(9), np.zeros(81)
+    E = lib.b2g_element_bw(_ptr(np.ascontiguousarray(x)), _ptr(np.ascontiguousarray(rest)), stretch, shear, rate,
+                           w, _ptr(G), _ptr(H))
+    return E, G, H.reshape(9, 9)
+
+
+def _lib_dsb(x, rest, kappa, w):
+    lib = load_scene_lib()
+    G, H = np.zeros(12), np.zeros(144)
+    E = lib.b2g_element_dsb(_ptr(np.ascontiguousarray(x)), _ptr(np.ascontiguousarray(rest)), kappa, w, _ptr(G),
+                            _ptr(H))
+    return E, G, H.reshape(12, 12)
+
+
+def _lib_ortho(q, kappa, w):
+    lib = load_scene_lib()
+    G, H = np.zeros(9), np.zeros(81)
+    E = lib.b2g_element_ortho(_ptr(np.ascontiguousarray(q)), kappa, w, _ptr(G), _ptr(H))
+    return E, G, H.reshape(9, 9)
+
+
+def _close(a, b, rtol):
+    return np.abs(a - b).max() <= rtol * max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("stretch_factor", [0.8, 1.0, 1.3])
+def test_baraff_witkin_triangle(seed, stretch_factor):
+    rng = np.random.default_rng(seed)
+    rest = rng.standard_normal((3, 3)) * 0.01
+    # current: rest rotated, stretched along a random in-plane direction, sheared, moved
+    Q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    x = rest @ Q.T
+    d = rng.standard_normal(3)
+    x = x + (stretch_factor - 1.0) * np.outer(x @ d / (d @ d), d) + 0.001 * rng.standard_normal((3, 3))
+    stretch, shear, rate, w = 1e3, 1e2, 100.0, 3.7e-5
+    E, G, H = _lib_bw(x, rest, stretch, shear, rate, w)
+    Eo, Go, Ho = OE.bw_element(x, rest, stretch, shear, rate, w)
+    assert abs(E - Eo) <= 1e-12 * max(abs(Eo), 1e-300) + 1e-300
+    assert _close(G, Go, 1e-6)
+    assert _close(H, Ho, 1e-10)
+    assert np.abs(H - H.T).max() <= 1e-12 * np.abs(H).max()
+    assert np.linalg.eigvalsh(H).min() >= -1e-9 * np.abs(H).max()
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_shell_bending_hinge(seed):
+    rng = np.random.default_rng(100 + seed)
+    rest = np.array([[0.0, 0.0, 1.0], [0.0, -1.0, 0.0], [0.0, 1.0, 0.0], [1.0, 0.0, 0.0]]) * 0.01
+    rest = rest + 0.002 * rng.standard_normal((4, 3))
+    x = rest + 0.003 * rng.standard_normal((4, 3))
+    kappa, w = 1e-2, 1e-4
+    E, G, H = _lib_dsb(x, rest, kappa, w)
+    Eo, Go, Ho = OE.dsb_element(x, rest, kappa, w)
+    assert abs(E - Eo) <= 1e-12 * max(abs(Eo), 1e-30)
+    assert _close(G, Go, 1e-5)
+    assert _close(H, Ho, 1e-5)
+    # at the rest state: zero energy and gradient
+    E0, G0, _ = _lib_dsb(rest, rest, kappa, w)
+    assert E0 == 0.0 and np.abs(G0).max() == 0.0
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("kind", ["rotation", "near", "general"])
+def test_orthogonality_potential(seed, kind):
+    rng = np.random.default_rng(200 + seed)
+    R, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    A = {"rotation": R, "near": R + 0.05 * rng.standard_normal((3, 3)),
+         "general": rng.standard_normal((3, 3))}[kind]
+    q = np.concatenate([rng.standard_normal(3), A.T.reshape(-1)])  # q[3+3k .. ] = column k
+    kappa, w = 1e8, 2.16e-4 * 1e-4
+    E, G, H = _lib_ortho(q, kappa, w)
+    Eo, Go, Ho = OE.ortho_element(q, kappa, w)
+    assert abs(E - Eo) <= 1e-10 * max(abs(Eo), 1e-300) + (1e-300 if kind != "rotation" else kappa * 1e-24)
+    assert np.abs(G - Go).max() <= 1e-6 * np.abs(Go).max() + 1e-10 * w * kappa  # FD noise floor
+    assert _close(H, Ho, 1e-5)
+    assert np.linalg.eigvalsh(H).min() >= -1e-9 * np.abs(H).max()
