@@ -60,6 +60,73 @@ int b2gen_system(b2gen_mesh* m, const double* d_x, const double* d_xtilde, int32
 
 const char* b2gen_last_error(void);
 
+/* ---- cloth (codim-2D) and affine bodies ------------------------------------------
+ * Cloth of n_verts vertices and n_tris triangles (host rest positions
+ * [n_verts*3], triangles [n_tris*3], lumped masses [n_verts], fixed flags or
+ * NULL):
+ *   * kinetic: one diagonal block m I per vertex, gradient m (x - x_tilde);
+ *   * Baraff-Witkin strain-limiting stretch + shear per triangle, in the rest
+ *     triangle's own uv frame, weight rest area x dt^2, 6 upper blocks
+ *     (finite_element/constitutions/strain_limiting_baraff_witkin_shell_2d.cu:75-150,
+ *      strain_limiting_baraff_witkin_shell_2d.h:33-280);
+ *   * discrete-shell bending per interior edge (hinge (opposite min, edge
+ *     min, edge max, opposite max), edges in (min, max) order), Gauss-Newton
+ *     Hessian, weight dt^2, 10 upper blocks
+ *     (finite_element/constitutions/discrete_shell_bending.cu:96-135, 240-300).
+ * Triplet slots [n_verts kinetic][6 n_tris][10 n_hinges]; the cloth's block
+ * rows start at vertex_offset in the global system (d_x, d_xtilde, d_grad are
+ * global vectors). Gradient per vertex: kinetic, triangles by index, hinges
+ * by index. */
+typedef struct b2gen_shell_material
+{
+    double stretch, shear, strain_rate; /* Baraff-Witkin stiffnesses (per area) and strain rate */
+    double bend;                        /* bending stiffness */
+    double dt;                          /* time step [s] */
+} b2gen_shell_material;
+
+typedef struct b2gen_shell b2gen_shell;
+int b2gen_shell_create(int device, int32_t n_verts, int32_t n_tris, const double* rest, const int32_t* tris,
+                       const double* mass, const uint8_t* fixed, const b2gen_shell_material* mat,
+                       b2gen_shell** out);
+int b2gen_shell_destroy(b2gen_shell* s);
+int64_t b2gen_shell_num_triplets(const b2gen_shell* s);
+int32_t b2gen_shell_num_hinges(const b2gen_shell* s);
+int b2gen_shell_system(b2gen_shell* s, const double* d_x, const double* d_xtilde, int32_t vertex_offset,
+                       int32_t* d_rows, int32_t* d_cols, double* d_vals, double* d_grad, void* stream);
+
+/* Affine bodies (12 DoF each: translation, then the three 3-vectors of the
+ * affine matrix), block rows block_offset + 4 b .. + 3: host mass matrices
+ * [n_bodies*144] (row-major 12x12), orthogonality stiffness kappa and volume
+ * per body; 16 triplets per body (the lower blocks written as zero blocks,
+ * as the affine-body subsystem writes them, abd_linear_subsystem.cu:21-31),
+ * Hessian M + the PSD orthogonality Hessian x V dt^2
+ * (affine_body/constitutions/ortho_potential.cu:37-70), gradient
+ * M (q - q_tilde) + the orthogonality gradient. */
+typedef struct b2gen_abd b2gen_abd;
+int b2gen_abd_create(int device, int32_t n_bodies, const double* mass12, const double* kappa,
+                     const double* volume, double dt, b2gen_abd** out);
+int b2gen_abd_destroy(b2gen_abd* a);
+int b2gen_abd_system(b2gen_abd* a, const double* d_q, const double* d_qtilde, int32_t block_offset,
+                     int32_t* d_rows, int32_t* d_cols, double* d_vals, double* d_grad, void* stream);
+/* IPC normal contact of point-triangle (p, t0, t1, t2) and edge-edge
+ * (a0, a1, b0, b1) pairs (host lists in global block rows, is_ee per pair,
+ * mollifier thresholds eps = 1e-3 |ea_rest|^2 |eb_rest|^2 per pair), barrier
+ * kappa dt^2 B(D) with activation distance dhat: the pair's closest-feature
+ * type, the exact Hessian projected to PSD for point-triangle / edge-edge
+ * types and mollified pairs, the closed rank-1 form for point-edge /
+ * point-point types, as the reference's default contact model
+ * (contact_system/contact_models/ipc_simplex_normal_contact.cu:320-680).
+ * 10 triplets per pair from slot 0 of the given arrays; each pair's gradient
+ * is ADDED to d_grad (which holds the other producers' sums), per vertex in
+ * pair order. */
+typedef struct b2gen_contacts b2gen_contacts;
+int b2gen_contacts_create(int device, int32_t n_pairs, const int32_t* pairs, const uint8_t* is_ee,
+                          const double* eps, double dhat, double kappa, double dt, b2gen_contacts** out);
+int b2gen_contacts_destroy(b2gen_contacts* c);
+int b2gen_contacts_system(b2gen_contacts* c, const double* d_x, int32_t* d_rows, int32_t* d_cols,
+                          double* d_vals, double* d_grad, void* stream);
+const char* b2gen_shell_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,7 @@ SOLVE_SOURCES = [
     "b2s_pcg.cu",
     "b2s_learned.cu",
     "b2s_generate.cu",
+    "b2s_generate_shell.cu",
     "b2s_abi.cu",
     "b2s_noalloc.cu",
     "b2s_partition.cu",
@@ -69,6 +70,7 @@ def _digest(paths: list[str], extra: str) -> str:
 
 def _headers() -> list[str]:
     hs = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cuh", ".h"))]
+    hs.append(os.path.join(CSRC, "scene", "elements.h"))
     return hs + [os.path.join(ROOT, "include", h) for h in ("b200solve.h", "b200gen.h")]
 
 

@@ -508,42 +508,43 @@ __global__ void __launch_bounds__(ASM_BLOCK) k_mark_runs(int32_t nb, const int32
     }
 }
 
-// One thread per unique block: the sum of its run's source blocks in source
-// order (the sorted order), written to the value planes. Sources are fetched
-// four at a time, the first included (most runs hold 4 or fewer: one round of
-// 36 independent loads); the additions stay in order starting from the first
-// source, so the sums are those of the sequential loop.
+// One thread per (unique block, column of its 3x3): the column's 3 values
+// summed over the run's sources in source order (the sorted order). The
+// three threads of a block read its sources' 72 contiguous bytes together;
+// four sources are fetched ahead, the additions stay in order from the first.
 __global__ void __launch_bounds__(ASM_BLOCK) k_sum_runs(int64_t U, const int32_t* __restrict__ run_start,
-                                                        const int32_t* __restrict__ sorted_src,
-                                                        const double* __restrict__ src_vals,
-                                                        double* __restrict__ out_vals, int64_t S)
+                                                         const int32_t* __restrict__ sorted_src,
+                                                         const double* __restrict__ src_vals,
+                                                         double* __restrict__ out_vals, int64_t S)
 {
-    for(int64_t o = (int64_t)blockIdx.x * ASM_BLOCK + threadIdx.x; o < U; o += (int64_t)gridDim.x * ASM_BLOCK)
+    for(int64_t t = (int64_t)blockIdx.x * ASM_BLOCK + threadIdx.x; t < 3 * U; t += (int64_t)gridDim.x * ASM_BLOCK)
     {
+        const int64_t o = t / 3;
+        const int     c = (int)(t - 3 * o);
         const int32_t b = run_start[o], e = run_start[o + 1];
-        double        acc[9] = {};
+        double        acc[3] = {};
         for(int32_t k = b; k < e; k += 4)
         {
             int64_t src[4];
 #pragma unroll
-            for(int t = 0; t < 4; ++t)
-                src[t] = k + t < e ? (int64_t)sorted_src[k + t] : -1;
-            double v[4][9];
+            for(int u = 0; u < 4; ++u)
+                src[u] = k + u < e ? (int64_t)sorted_src[k + u] : -1;
+            double v[4][3];
 #pragma unroll
-            for(int t = 0; t < 4; ++t)
+            for(int u = 0; u < 4; ++u)
 #pragma unroll
-                for(int q = 0; q < 9; ++q)
-                    v[t][q] = src[t] >= 0 ? src_vals[src[t] * 9 + q] : 0.0;
+                for(int q = 0; q < 3; ++q)
+                    v[u][q] = src[u] >= 0 ? src_vals[src[u] * 9 + 3 * c + q] : 0.0;
 #pragma unroll
-            for(int t = 0; t < 4; ++t)
-                if(src[t] >= 0)
+            for(int u = 0; u < 4; ++u)
+                if(src[u] >= 0)
 #pragma unroll
-                    for(int q = 0; q < 9; ++q)
-                        acc[q] = k + t == b ? v[t][q] : acc[q] + v[t][q];
+                    for(int q = 0; q < 3; ++q)
+                        acc[q] = k + u == b ? v[u][q] : acc[q] + v[u][q];
         }
 #pragma unroll
-        for(int q = 0; q < 9; ++q)
-            out_vals[(int64_t)q * S + o] = acc[q];
+        for(int q = 0; q < 3; ++q)
+            out_vals[(int64_t)(3 * c + q) * S + o] = acc[q];
     }
 }
 
@@ -675,8 +676,10 @@ void assemble_triplets(b2s_solver* s, Matrix& M, int32_t nb, int64_t T, const in
                                  cudaMemcpyDeviceToDevice, st));
         if(U > 0)
         {
-            k_sum_runs<<<asm_grid(U, ASM_BLOCK), ASM_BLOCK, 0, st>>>(U, w.run_start.data(), w.sorted_src.data(), vals,
-                                                                     M.vals.data(), M.stride);
+            // one pass in block order (no grid-stride loop): the CTAs in
+            // flight cover neighbouring rows, whose sources share cache lines
+            k_sum_runs<<<(unsigned)((3 * U + ASM_BLOCK - 1) / ASM_BLOCK), ASM_BLOCK, 0, st>>>(
+                U, w.run_start.data(), w.sorted_src.data(), vals, M.vals.data(), M.stride);
             B2S_CHECK_LAUNCH();
         }
     }

@@ -23,6 +23,19 @@
 //    a_1..a_3 = q[3..11] of the body's 12 DoF; gradient and Hessian derived
 //    here by hand, the 9x9 Hessian projected to PSD (eigenvalues clamped at 0),
 //    weight volume x dt^2.
+//  * IPC normal contact of a point-triangle or edge-edge pair
+//    (contact_system/contact_models/ipc_simplex_normal_contact.cu:358-680 with
+//    its default Hessian mode, codim_ipc_simplex_normal_contact_function.h,
+//    utils/distance/distance_flagged.h:258-520, edge_edge_mollifier.inl):
+//    barrier B(D) = -kappa dt^2 (D - dhat^2)^2 log(D / dhat^2) of the squared
+//    distance D of the pair's closest-feature type (point-triangle /
+//    point-edge / point-point, edge-edge / point-edge / point-point); edge-edge
+//    energies times the mollifier m(c) = (2 - c/eps) c/eps of c = |ea x eb|^2
+//    below eps = 1e-3 |ea_rest|^2 |eb_rest|^2. PT and EE types (and every
+//    mollified pair): the exact Hessian, projected to PSD; PE and PP types:
+//    the closed form (B'' + B' / (2D)) grad(D) grad(D)^T. The exact second
+//    derivatives come from a second-order forward differentiation of the
+//    distance formulas (Jet12 below), not from hand-expanded expressions.
 #pragma once
 
 #include <cmath>
@@ -443,5 +456,394 @@ B2_HD void ortho_grad_hess(const double* q, double kappa, double w, double* G9, 
     project_psd<9>(H9);
     for(int i = 0; i < 81; ++i)
         H9[i] *= w;
+}
+
+// ---- second-order forward differentiation over 12 variables ------------------------
+// value, gradient and the upper triangle of the Hessian (packed row by row)
+struct Jet12
+{
+    double v;
+    double g[12];
+    double h[78];
+};
+B2_HD int hidx(int i, int j) { return i * 12 - i * (i - 1) / 2 + (j - i); }  // i <= j
+B2_HD void jet_const(Jet12& a, double v)
+{
+    a.v = v;
+    for(int i = 0; i < 12; ++i)
+        a.g[i] = 0.0;
+    for(int i = 0; i < 78; ++i)
+        a.h[i] = 0.0;
+}
+B2_HD void jet_var(Jet12& a, double v, int k)
+{
+    jet_const(a, v);
+    a.g[k] = 1.0;
+}
+B2_HD void jet_add(const Jet12& a, const Jet12& b, Jet12& r, double sb = 1.0)
+{
+    r.v = a.v + sb * b.v;
+    for(int i = 0; i < 12; ++i)
+        r.g[i] = a.g[i] + sb * b.g[i];
+    for(int i = 0; i < 78; ++i)
+        r.h[i] = a.h[i] + sb * b.h[i];
+}
+B2_HD void jet_mul(const Jet12& a, const Jet12& b, Jet12& r)
+{
+    Jet12 t;
+    t.v = a.v * b.v;
+    for(int i = 0; i < 12; ++i)
+        t.g[i] = a.v * b.g[i] + b.v * a.g[i];
+    for(int i = 0; i < 12; ++i)
+        for(int j = i; j < 12; ++j)
+        {
+            const int k = hidx(i, j);
+            t.h[k]      = a.v * b.h[k] + b.v * a.h[k] + a.g[i] * b.g[j] + a.g[j] * b.g[i];
+        }
+    r = t;
+}
+// r = f(a) for a scalar function with f, f', f'' at a.v
+B2_HD void jet_compose(const Jet12& a, double f, double f1, double f2, Jet12& r)
+{
+    Jet12 t;
+    t.v = f;
+    for(int i = 0; i < 12; ++i)
+        t.g[i] = f1 * a.g[i];
+    for(int i = 0; i < 12; ++i)
+        for(int j = i; j < 12; ++j)
+        {
+            const int k = hidx(i, j);
+            t.h[k]      = f1 * a.h[k] + f2 * a.g[i] * a.g[j];
+        }
+    r = t;
+}
+B2_HD void jet_div(const Jet12& a, const Jet12& b, Jet12& r)
+{
+    Jet12        ib;
+    const double iv = 1.0 / b.v;
+    jet_compose(b, iv, -iv * iv, 2.0 * iv * iv * iv, ib);
+    jet_mul(a, ib, r);
+}
+B2_HD void jet_dot3(const Jet12* a, const Jet12* b, Jet12& r)
+{
+    Jet12 t;
+    jet_mul(a[0], b[0], r);
+    jet_mul(a[1], b[1], t);
+    jet_add(r, t, r);
+    jet_mul(a[2], b[2], t);
+    jet_add(r, t, r);
+}
+B2_HD void jet_cross3(const Jet12* a, const Jet12* b, Jet12* r)
+{
+    Jet12 t, u;
+    for(int c = 0; c < 3; ++c)
+    {
+        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+        jet_mul(a[c1], b[c2], t);
+        jet_mul(a[c2], b[c1], u);
+        jet_add(t, u, r[c], -1.0);
+    }
+}
+
+// squared distances as Jets of the 12 pair coordinates X (vertex k at 3k)
+enum PairType
+{
+    PAIR_PP = 0,
+    PAIR_PE = 1,
+    PAIR_PT = 2,
+    PAIR_EE = 3
+};
+// vertex i of the pair as three Jets
+B2_HD void jet_point(const double* X, int i, Jet12* p)
+{
+    for(int c = 0; c < 3; ++c)
+        jet_var(p[c], X[3 * i + c], 3 * i + c);
+}
+B2_HD void jet_d2_pp(const double* X, int a, int b, Jet12& D)
+{
+    Jet12 pa[3], pb[3], d[3];
+    jet_point(X, a, pa);
+    jet_point(X, b, pb);
+    for(int c = 0; c < 3; ++c)
+        jet_add(pa[c], pb[c], d[c], -1.0);
+    jet_dot3(d, d, D);
+}
+// |(p - e0) x (e1 - e0)|^2 / |e1 - e0|^2
+B2_HD void jet_d2_pe(const double* X, int p, int e0, int e1, Jet12& D)
+{
+    Jet12 P[3], A[3], B[3], w[3], e[3], n[3], nn, ee;
+    jet_point(X, p, P);
+    jet_point(X, e0, A);
+    jet_point(X, e1, B);
+    for(int c = 0; c < 3; ++c)
+    {
+        jet_add(P[c], A[c], w[c], -1.0);
+        jet_add(B[c], A[c], e[c], -1.0);
+    }
+    jet_cross3(w, e, n);
+    jet_dot3(n, n, nn);
+    jet_dot3(e, e, ee);
+    jet_div(nn, ee, D);
+}
+// ((q - a0) . n)^2 / |n|^2, n = u x v: point-plane (u, v the triangle edges) and
+// line-line (u, v the two edges)
+B2_HD void jet_d2_plane(const Jet12* q, const Jet12* a0, const Jet12* u, const Jet12* v, Jet12& D)
+{
+    Jet12 n[3], w[3], wn, nn;
+    jet_cross3(u, v, n);
+    for(int c = 0; c < 3; ++c)
+        jet_add(q[c], a0[c], w[c], -1.0);
+    jet_dot3(w, n, wn);
+    jet_dot3(n, n, nn);
+    jet_mul(wn, wn, wn);
+    jet_div(wn, nn, D);
+}
+B2_HD void jet_d2_pt(const double* X, Jet12& D)
+{
+    Jet12 P[3], T0[3], T1[3], T2[3], u[3], v[3];
+    jet_point(X, 0, P);
+    jet_point(X, 1, T0);
+    jet_point(X, 2, T1);
+    jet_point(X, 3, T2);
+    for(int c = 0; c < 3; ++c)
+    {
+        jet_add(T1[c], T0[c], u[c], -1.0);
+        jet_add(T2[c], T0[c], v[c], -1.0);
+    }
+    jet_d2_plane(P, T0, u, v, D);
+}
+B2_HD void jet_d2_ee(const double* X, Jet12& D)
+{
+    Jet12 A0[3], A1[3], B0[3], B1[3], u[3], v[3];
+    jet_point(X, 0, A0);
+    jet_point(X, 1, A1);
+    jet_point(X, 2, B0);
+    jet_point(X, 3, B1);
+    for(int c = 0; c < 3; ++c)
+    {
+        jet_add(A1[c], A0[c], u[c], -1.0);
+        jet_add(B1[c], B0[c], v[c], -1.0);
+    }
+    jet_d2_plane(B0, A0, u, v, D);
+}
+
+// closest-feature type of a point-triangle pair (p, t0, t1, t2): the outside
+// regions of the edges t0t1, t1t2, t2t0 (point-edge), then of the corners
+// (point-point), else the face; returns the type and the participating
+// pair-local vertices in v[]
+B2_HD int pt_type(const double* X, int* v, int* nv)
+{
+    const double *p = X, *t[3] = {X + 3, X + 6, X + 9};
+    double        e1[3], e2[3], n[3];
+    sub3(t[1], t[0], e1);
+    sub3(t[2], t[0], e2);
+    cross3(e1, e2, n);
+    double s[3];  // parameter along each edge (t0t1, t1t2, t2t0)
+    bool   out[3];
+    for(int k = 0; k < 3; ++k)
+    {
+        const double* a = t[k];
+        const double* b = t[(k + 1) % 3];
+        double        e[3], o[3], w[3];
+        sub3(b, a, e);
+        cross3(e, n, o);  // outward normal of the edge in the plane
+        sub3(p, a, w);
+        // coordinates of w in the (e, o) basis (e . o = 0)
+        s[k]   = dot3(w, e) / dot3(e, e);
+        out[k] = dot3(w, o) / dot3(o, o) >= 0.0;
+    }
+    for(int k = 0; k < 3; ++k)
+        if(s[k] > 0.0 && s[k] < 1.0 && out[k])
+        {
+            v[0] = 0;
+            v[1] = 1 + k;
+            v[2] = 1 + (k + 1) % 3;
+            *nv  = 3;
+            return PAIR_PE;
+        }
+    // corners: t_k is closest when p is before edge k and past edge k-1
+    for(int k = 0; k < 3; ++k)
+        if(s[k] <= 0.0 && s[(k + 2) % 3] >= 1.0)
+        {
+            v[0] = 0;
+            v[1] = 1 + k;
+            *nv  = 2;
+            return PAIR_PP;
+        }
+    v[0] = 0;
+    v[1] = 1;
+    v[2] = 2;
+    v[3] = 3;
+    *nv  = 4;
+    return PAIR_PT;
+}
+
+// closest-feature type of an edge-edge pair (a0, a1, b0, b1): the segments'
+// closest points by the clamped line parameters; an interior pair is EE, one
+// clamped end gives point-edge, two give point-point; (near-)parallel edges
+// take the closest of the four endpoint-to-segment candidates
+B2_HD int ee_type(const double* X, int* v, int* nv)
+{
+    const double *a0 = X, *a1 = X + 3, *b0 = X + 6, *b1 = X + 9;
+    double        u[3], w[3], z[3], ux[3];
+    sub3(a1, a0, u);
+    sub3(b1, b0, w);
+    sub3(a0, b0, z);
+    const double a = dot3(u, u), b = dot3(u, w), c = dot3(w, w), d = dot3(u, z), e = dot3(w, z);
+    const double den = a * c - b * b;
+    cross3(u, w, ux);
+    // endpoint-to-segment candidates (point index, segment start, segment end)
+    auto pseg = [&](int pi, int s0, int s1, double* dist, int* vv, int* n)
+    {
+        const double *P = X + 3 * pi, *S0 = X + 3 * s0, *S1 = X + 3 * s1;
+        double        sv[3], pw[3];
+        sub3(S1, S0, sv);
+        sub3(P, S0, pw);
+        const double t = dot3(pw, sv) / dot3(sv, sv);
+        if(t <= 0.0 || t >= 1.0)
+        {
+            const double* Q = t <= 0.0 ? S0 : S1;
+            double        q[3];
+            sub3(P, Q, q);
+            *dist = dot3(q, q);
+            vv[0] = pi;
+            vv[1] = t <= 0.0 ? s0 : s1;
+            *n    = 2;
+        }
+        else
+        {
+            double q[3];
+            for(int k = 0; k < 3; ++k)
+                q[k] = pw[k] - t * sv[k];
+            *dist = dot3(q, q);
+            vv[0] = pi;
+            vv[1] = s0;
+            vv[2] = s1;
+            *n    = 3;
+        }
+    };
+    const bool parallel = dot3(ux, ux) <= 1e-12 * a * c;
+    if(!parallel)
+    {
+        const double sN = b * e - c * d, tN = a * e - b * d;
+        const bool   s_in = sN > 0.0 && sN < den, t_in = tN > 0.0 && tN < den;
+        if(s_in && t_in)
+        {
+            v[0] = 0;
+            v[1] = 1;
+            v[2] = 2;
+            v[3] = 3;
+            *nv  = 4;
+            return PAIR_EE;
+        }
+    }
+    double best = 1e300;
+    int    bv[3], bn = 0;
+    const int cand[4][3] = {{0, 2, 3}, {1, 2, 3}, {2, 0, 1}, {3, 0, 1}};
+    for(int k = 0; k < 4; ++k)
+    {
+        double dist;
+        int    vv[3], n;
+        pseg(cand[k][0], cand[k][1], cand[k][2], &dist, vv, &n);
+        if(dist < best)
+        {
+            best = dist;
+            bn   = n;
+            for(int i = 0; i < n; ++i)
+                bv[i] = vv[i];
+        }
+    }
+    for(int i = 0; i < bn; ++i)
+        v[i] = bv[i];
+    *nv = bn;
+    return bn == 2 ? PAIR_PP : PAIR_PE;
+}
+
+// B(D) = -k (D - Dh)^2 log(D / Dh) and its first two derivatives
+B2_HD void barrier_B(double D, double Dh, double k, double* B0, double* B1, double* B2)
+{
+    const double t = D - Dh, l = log(D / Dh);
+    *B0            = -k * t * t * l;
+    *B1            = -k * (2.0 * t * l + t * t / D);
+    *B2            = -k * (2.0 * l + 4.0 * t / D - t * t / (D * D));
+}
+
+// one contact pair: X[12] its 4 vertices ((p, t0, t1, t2) when is_ee is 0,
+// (a0, a1, b0, b1) otherwise), eps the edge-edge mollifier threshold (unused
+// for point-triangle), k = kappa dt^2; G[12], H[144] over the 4 vertices (zero
+// rows for vertices outside the type's stencil). Returns the type, or -1 when
+// the pair is at or beyond dhat (G, H zero).
+B2_HD int contact_grad_hess(const double* X, int is_ee, double eps, double dhat, double k, double* G, double* H)
+{
+    for(int i = 0; i < 12; ++i)
+        G[i] = 0.0;
+    for(int i = 0; i < 144; ++i)
+        H[i] = 0.0;
+    int       v[4], nv = 0;
+    const int type = is_ee ? ee_type(X, v, &nv) : pt_type(X, v, &nv);
+    Jet12     D;
+    if(type == PAIR_PT)
+        jet_d2_pt(X, D);
+    else if(type == PAIR_EE)
+        jet_d2_ee(X, D);
+    else if(type == PAIR_PE)
+        jet_d2_pe(X, v[0], v[1], v[2], D);
+    else
+        jet_d2_pp(X, v[0], v[1], D);
+    const double Dh = dhat * dhat;
+    if(!(D.v < Dh) || !(D.v > 0.0))
+        return -1;
+    double B0, B1, B2;
+    barrier_B(D.v, Dh, k, &B0, &B1, &B2);
+    // edge-edge mollifier
+    bool  moll = false;
+    Jet12 E;
+    if(is_ee)
+    {
+        double u[3], w[3], ux[3];
+        sub3(X + 3, X, u);
+        sub3(X + 9, X + 6, w);
+        cross3(u, w, ux);
+        moll = dot3(ux, ux) < eps;
+    }
+    if(moll)
+    {
+        Jet12 A0[3], A1[3], B0j[3], B1j[3], u[3], w[3], n[3], c, m, Bj;
+        jet_point(X, 0, A0);
+        jet_point(X, 1, A1);
+        jet_point(X, 2, B0j);
+        jet_point(X, 3, B1j);
+        for(int q = 0; q < 3; ++q)
+        {
+            jet_add(A1[q], A0[q], u[q], -1.0);
+            jet_add(B1j[q], B0j[q], w[q], -1.0);
+        }
+        jet_cross3(u, w, n);
+        jet_dot3(n, n, c);
+        const double x = c.v / eps;
+        jet_compose(c, (2.0 - x) * x, 2.0 / eps * (1.0 - x), -2.0 / (eps * eps), m);
+        jet_compose(D, B0, B1, B2, Bj);
+        jet_mul(m, Bj, E);
+    }
+    if(moll || type == PAIR_PT || type == PAIR_EE)
+    {
+        if(!moll)
+            jet_compose(D, B0, B1, B2, E);
+        for(int i = 0; i < 12; ++i)
+            G[i] = E.g[i];
+        for(int i = 0; i < 12; ++i)
+            for(int j = i; j < 12; ++j)
+                H[i * 12 + j] = H[j * 12 + i] = E.h[hidx(i, j)];
+        project_psd<12>(H);
+        return type;
+    }
+    // point-edge / point-point: the closed rank-1 form
+    const double c = B2 + B1 / (2.0 * D.v);
+    for(int i = 0; i < 12; ++i)
+        G[i] = B1 * D.g[i];
+    for(int i = 0; i < 12; ++i)
+        for(int j = 0; j < 12; ++j)
+            H[i * 12 + j] = c * D.g[i] * D.g[j];
+    return type;
 }
 }  // namespace b2el

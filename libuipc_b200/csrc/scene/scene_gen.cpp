@@ -300,6 +300,71 @@ int64_t add_cloth_grid(Builder& B, std::vector<double>& grad, const std::vector<
         *hinges_out = std::move(hinges);
     return nt;
 }
+
+// Point-triangle contact of vertex g (position xv) with the triangle of an
+// affine body's square face (body frame: y = fy, |x|, |z| <= h, split along
+// (-h,-h)-(h,h)) under its projection (ux, uz): the triangle corners are
+// x_i = p + A xbar_i, so the 12-coordinate contact gradient G and Hessian H
+// (elements.h: contact_grad_hess) map to the vertex and the body's 12 DoF by
+// the constant Jacobian T (x_v -> x_v; x_i -> p + sum_k xbar_i[k] a_k):
+// 15 blocks over the block rows (g, 4b, .., 4b + 3), gradient T^T G.
+// Returns false when the pair is beyond dhat.
+bool add_vertex_body_contact(Builder& B, std::vector<double>& grad, int32_t g, const double* xv, int64_t b,
+                             const double* p, const double A[3][3], double ux, double uz, double fy, double h,
+                             double dhat, double k)
+{
+    const double c[4][3] = {{-h, fy, -h}, {h, fy, -h}, {h, fy, h}, {-h, fy, h}};
+    const int    t0 = 0, t1 = uz <= ux ? 1 : 2, t2 = uz <= ux ? 2 : 3;
+    const int    tri[3] = {t0, t1, t2};
+    double       X[12], G[12], H[144];
+    for(int a = 0; a < 3; ++a)
+        X[a] = xv[a];
+    for(int i = 0; i < 3; ++i)
+        for(int r = 0; r < 3; ++r)
+        {
+            double v = p[r];
+            for(int kk = 0; kk < 3; ++kk)
+                v += A[r][kk] * c[tri[i]][kk];
+            X[3 + 3 * i + r] = v;
+        }
+    if(b2el::contact_grad_hess(X, 0, 0.0, dhat, k, G, H) < 0)
+        return false;
+    // t[I][J]: coefficient of DoF block J (0 vertex, 1 p, 2 + k a_k) in coordinate block I
+    double t[4][5] = {};
+    t[0][0] = 1.0;
+    for(int i = 0; i < 3; ++i)
+    {
+        t[1 + i][1] = 1.0;
+        for(int kk = 0; kk < 3; ++kk)
+            t[1 + i][2 + kk] = c[tri[i]][kk];
+    }
+    const int32_t rws[5] = {g, (int32_t)(4 * b), (int32_t)(4 * b + 1), (int32_t)(4 * b + 2), (int32_t)(4 * b + 3)};
+    for(int J = 0; J < 5; ++J)
+        for(int K = J; K < 5; ++K)
+        {
+            double Hb[9] = {};
+            for(int I = 0; I < 4; ++I)
+                for(int L = 0; L < 4; ++L)
+                {
+                    const double w = t[I][J] * t[L][K];
+                    if(w == 0.0)
+                        continue;
+                    for(int r = 0; r < 3; ++r)
+                        for(int cc = 0; cc < 3; ++cc)
+                            Hb[r * 3 + cc] += w * H[(3 * I + r) * 12 + 3 * L + cc];
+                }
+            B.put(rws[J], rws[K], Hb);
+        }
+    for(int J = 0; J < 5; ++J)
+        for(int r = 0; r < 3; ++r)
+        {
+            double v = 0.0;
+            for(int I = 0; I < 4; ++I)
+                v += t[I][J] * G[3 * I + r];
+            grad[(size_t)rws[J] * 3 + r] += v;
+        }
+    return true;
+}
 }  // namespace
 
 struct b2g_system
@@ -398,6 +463,8 @@ void add_affine_body(Builder& B, std::vector<double>& grad, int64_t b, double th
     for(int m = 0; m < 9; ++m)
         for(int n = 0; n < 9; ++n)
             H[3 + m][3 + n] += H9[m * 9 + n];
+    for(int m = 0; m < 9; ++m)  // zero up to rounding at a rotation
+        grad[(4 * b + 1) * 3 + m] += G9[m];
     // kinetic gradient: m (x - x_tilde) with x_tilde = x - dt^2 g on p
     grad[(4 * b) * 3 + 1] += m_b * dt2 * C.gravity;
     for(int bi = 0; bi < 4; ++bi)
@@ -508,33 +575,11 @@ void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
         const double d = yv - (py + 0.5 * s);
         if(d <= 0.0 || d >= C.dhat)
             continue;
-        ++n_contacts;
-        // a = dd/d(x_v, q_b): +e_y on the vertex; -e_y, -xbar_k e_y on the body
-        const double xbar[3] = {ux, 0.5 * s, uz};
-        double       avec[5][3] = {};
-        int32_t      rws[5]     = {g, (int32_t)(4 * b), (int32_t)(4 * b + 1), (int32_t)(4 * b + 2),
-                                   (int32_t)(4 * b + 3)};
-        avec[0][1] = 1.0;
-        avec[1][1] = -1.0;
-        for(int k = 0; k < 3; ++k)
-            avec[2 + k][1] = -xbar[k];
-        double D = d * d, b1, b2;
-        barrier_d(D, Dh, b1, b2);
-        double kc = dt2 * C.kappa * (b2 * 4.0 * D + 2.0 * b1);
-        if(kc < 0.0)
-            kc = 0.0;
-        for(int q = 0; q < 5; ++q)
-            for(int r = q; r < 5; ++r)
-            {
-                double Hb[9];
-                for(int p = 0; p < 3; ++p)
-                    for(int c = 0; c < 3; ++c)
-                        Hb[p * 3 + c] = kc * avec[q][p] * avec[r][c];
-                put(rws[q], rws[r], Hb);
-            }
-        for(int q = 0; q < 5; ++q)
-            for(int a = 0; a < 3; ++a)
-                sys->grad[rws[q] * 3 + a] += dt2 * C.kappa * b1 * 2.0 * d * avec[q][a];
+        const double R[3][3] = {{cs, 0, sn}, {0, 1, 0}, {-sn, 0, cs}};
+        const double pb[3]   = {px, py, pz}, xvv[3] = {xv, yv, zv};
+        if(add_vertex_body_contact(B, sys->grad, g, xvv, b, pb, R, ux, uz, 0.5 * s, 0.5 * s, C.dhat,
+                                   dt2 * C.kappa))
+            ++n_contacts;
     }
     sys->n_contacts = n_contacts;
     sys->rows       = std::move(B.rows);
@@ -733,9 +778,8 @@ void generate_tets(const b2g_config& C, const double* x_in, const double* xt_in,
         // ---- contacts ----
         struct Pair
         {
-            int32_t v[4];
-            double  a[12];  // D = (a . x)^2
-            int     nverts;
+            int32_t v[4];  // (p, t0, t1, t2) or (a0, a1, b0, b1)
+            int     is_ee;
         };
         std::vector<Pair> pairs;
         std::vector<std::pair<int32_t, double>> ground;  // vertex, distance
@@ -831,12 +875,8 @@ void generate_tets(const b2g_config& C, const double* x_in, const double* xt_in,
                                         if(std::fabs(d) >= C.dhat)
                                             continue;
                                         Pair pr;
-                                        pr.nverts = 4;
+                                        pr.is_ee = 0;
                                         pr.v[0] = pv; pr.v[1] = tri[tt][0]; pr.v[2] = tri[tt][1]; pr.v[3] = tri[tt][2];
-                                        const double w[4] = {1.0, -wa, -wb, -wc};
-                                        for(int q2 = 0; q2 < 4; ++q2)
-                                            for(int a2 = 0; a2 < 3; ++a2)
-                                                pr.a[q2 * 3 + a2] = w[q2] * n[a2];
                                         pairs.push_back(pr);
                                     }
                                 }
@@ -897,14 +937,9 @@ void generate_tets(const b2g_config& C, const double* x_in, const double* xt_in,
                                 double d = norm(dv);
                                 if(d >= C.dhat || d <= 0.0)
                                     continue;
-                                Vec3 n = scale(dv, 1.0 / d);
                                 Pair pr;
-                                pr.nverts = 4;
+                                pr.is_ee = 1;
                                 pr.v[0] = Eu[e][0]; pr.v[1] = Eu[e][1]; pr.v[2] = El[f][0]; pr.v[3] = El[f][1];
-                                const double w[4] = {1.0 - s, s, -(1.0 - t), -t};
-                                for(int q2 = 0; q2 < 4; ++q2)
-                                    for(int a2 = 0; a2 < 3; ++a2)
-                                        pr.a[q2 * 3 + a2] = w[q2] * n[a2];
                                 pairs.push_back(pr);
                             }
                         }
@@ -1037,22 +1072,28 @@ void generate_tets(const b2g_config& C, const double* x_in, const double* xt_in,
             write_block(n_kin + n_snh + gi, g, g, H);
             sys->grad[g * 3 + 1] += dt2 * C.kappa * b1 * 2.0 * d;
         }
-        // pair barriers: D = (a.x)^2, H = dt2 kappa (b'' 4 (a.x)^2 + 2 b') a a^T
+        // pair barriers: the point-triangle / edge-edge contact energy of the
+        // pair's closest-feature type (elements.h: contact_grad_hess)
+        std::vector<double> pair_g(pairs.size() * 12);
 #pragma omp parallel for schedule(static)
         for(int64_t pi = 0; pi < (int64_t)pairs.size(); ++pi)
         {
             const Pair& pr = pairs[pi];
-            double ax = 0.0;
+            double      X[12], H[144], eps = 0.0;
             for(int q = 0; q < 4; ++q)
                 for(int a = 0; a < 3; ++a)
-                    ax += pr.a[q * 3 + a] * sys->x[pr.v[q] * 3 + a];
-            double D = ax * ax, b1, b2;
-            if(D <= 0.0)
-                D = 1e-30;
-            barrier_d(D, Dh, b1, b2);
-            double k = dt2 * C.kappa * (b2 * 4.0 * D + 2.0 * b1);
-            if(k < 0.0)
-                k = 0.0;
+                    X[q * 3 + a] = sys->x[pr.v[q] * 3 + a];
+            if(pr.is_ee)
+            {
+                double ea[3], eb[3];
+                for(int a = 0; a < 3; ++a)
+                {
+                    ea[a] = sys->x_rest[pr.v[1] * 3 + a] - sys->x_rest[pr.v[0] * 3 + a];
+                    eb[a] = sys->x_rest[pr.v[3] * 3 + a] - sys->x_rest[pr.v[2] * 3 + a];
+                }
+                eps = 1e-3 * b2el::dot3(ea, ea) * b2el::dot3(eb, eb);
+            }
+            b2el::contact_grad_hess(X, pr.is_ee, eps, C.dhat, dt2 * C.kappa, &pair_g[pi * 12], H);
             int slot = 0;
             for(int q = 0; q < 4; ++q)
                 for(int r = q; r < 4; ++r, ++slot)
@@ -1060,23 +1101,14 @@ void generate_tets(const b2g_config& C, const double* x_in, const double* xt_in,
                     double Hb[9];
                     for(int a = 0; a < 3; ++a)
                         for(int c = 0; c < 3; ++c)
-                            Hb[a * 3 + c] = k * pr.a[q * 3 + a] * pr.a[r * 3 + c];
+                            Hb[a * 3 + c] = H[(3 * q + a) * 12 + 3 * r + c];
                     write_block(n_kin + n_snh + n_gnd + pi * 10 + slot, pr.v[q], pr.v[r], Hb);
                 }
         }
         for(int64_t pi = 0; pi < (int64_t)pairs.size(); ++pi)
-        {
-            const Pair& pr = pairs[pi];
-            double ax = 0.0;
             for(int q = 0; q < 4; ++q)
                 for(int a = 0; a < 3; ++a)
-                    ax += pr.a[q * 3 + a] * sys->x[pr.v[q] * 3 + a];
-            double D = std::max(ax * ax, 1e-30), b1, b2;
-            barrier_d(D, Dh, b1, b2);
-            for(int q = 0; q < 4; ++q)
-                for(int a = 0; a < 3; ++a)
-                    sys->grad[pr.v[q] * 3 + a] += dt2 * C.kappa * b1 * 2.0 * ax * pr.a[q * 3 + a];
-        }
+                    sys->grad[pairs[pi].v[q] * 3 + a] += pair_g[pi * 12 + q * 3 + a];
 
         // fixed vertices (Dirichlet)
         bool any_fixed = false;
@@ -1279,26 +1311,15 @@ void generate_wall(const b2g_config& C, b2g_system* sys)
                         continue;
                     ++n_contacts;
                     const int32_t vs[4] = {(int32_t)g, (int32_t)tri[tt][0], (int32_t)tri[tt][1], (int32_t)tri[tt][2]};
-                    const double  w[4]  = {1.0, -wa, -wb, -wc};
-                    double        a[4][3];
+                    double        X[12], G[12], H[144];
                     for(int q2 = 0; q2 < 4; ++q2)
                         for(int a2 = 0; a2 < 3; ++a2)
-                            a[q2][a2] = w[q2] * n[a2];
-                    double D = d * d, b1, b2;
-                    barrier_d(D, Dh, b1, b2);
-                    const double kc = std::max(0.0, dt2 * C.kappa * (b2 * 4.0 * D + 2.0 * b1));
-                    for(int q2 = 0; q2 < 4; ++q2)
-                        for(int r2 = q2; r2 < 4; ++r2)
-                        {
-                            double Hb[9];
-                            for(int pp = 0; pp < 3; ++pp)
-                                for(int cc = 0; cc < 3; ++cc)
-                                    Hb[pp * 3 + cc] = kc * a[q2][pp] * a[r2][cc];
-                            put(vs[q2], vs[r2], Hb);
-                        }
+                            X[q2 * 3 + a2] = sys->x[(int64_t)vs[q2] * 3 + a2];
+                    b2el::contact_grad_hess(X, 0, 0.0, C.dhat, dt2 * C.kappa, G, H);
+                    B.put_element<4>(vs, H);
                     for(int q2 = 0; q2 < 4; ++q2)
                         for(int a2 = 0; a2 < 3; ++a2)
-                            sys->grad[vs[q2] * 3 + a2] += dt2 * C.kappa * b1 * 2.0 * d * a[q2][a2];
+                            sys->grad[vs[q2] * 3 + a2] += G[q2 * 3 + a2];
                 }
             }
     }
@@ -1319,31 +1340,11 @@ void generate_wall(const b2g_config& C, b2g_system* sys)
         const double d = (py - 0.5 * s) - yv;
         if(d <= 0.0 || d >= C.dhat)
             continue;
-        ++n_contacts;
-        // d = p_y + (A xbar)_y - y_v with xbar = (ux, -s/2, uz) in the body frame
-        const double xbar[3] = {ux, -0.5 * s, uz};
-        double       avec[5][3] = {};
-        const int32_t rws[5] = {(int32_t)g, (int32_t)(4 * b), (int32_t)(4 * b + 1), (int32_t)(4 * b + 2),
-                                (int32_t)(4 * b + 3)};
-        avec[0][1] = -1.0;
-        avec[1][1] = 1.0;
-        for(int k = 0; k < 3; ++k)
-            avec[2 + k][1] = xbar[k];
-        double D = d * d, b1, b2;
-        barrier_d(D, Dh, b1, b2);
-        const double kc = std::max(0.0, dt2 * C.kappa * (b2 * 4.0 * D + 2.0 * b1));
-        for(int q = 0; q < 5; ++q)
-            for(int r = q; r < 5; ++r)
-            {
-                double Hb[9];
-                for(int pp = 0; pp < 3; ++pp)
-                    for(int cc = 0; cc < 3; ++cc)
-                        Hb[pp * 3 + cc] = kc * avec[q][pp] * avec[r][cc];
-                put(rws[q], rws[r], Hb);
-            }
-        for(int q = 0; q < 5; ++q)
-            for(int a = 0; a < 3; ++a)
-                sys->grad[rws[q] * 3 + a] += dt2 * C.kappa * b1 * 2.0 * d * avec[q][a];
+        const double R[3][3] = {{cs, 0, sn}, {0, 1, 0}, {-sn, 0, cs}};
+        const double pb[3]   = {px, py, pz}, xvv[3] = {xv, yv, zv};
+        if(add_vertex_body_contact(B, sys->grad, (int32_t)g, xvv, b, pb, R, ux, uz, -0.5 * s, 0.5 * s, C.dhat,
+                                   dt2 * C.kappa))
+            ++n_contacts;
     }
     sys->n_contacts = n_contacts;
     sys->rows       = std::move(B.rows);
@@ -1455,6 +1456,11 @@ double b2g_element_dsb(const double* x, const double* rest, double kappa, double
     b2el::dsb_rest(rest, rest + 3, rest + 6, rest + 9, &L0, &hb, &thb);
     b2el::dsb_grad_hess(x, x + 3, x + 6, x + 9, L0, hb, thb, kappa, w, G12, H144);
     return b2el::dsb_energy(x, x + 3, x + 6, x + 9, L0, hb, thb, kappa);
+}
+
+int b2g_element_contact(const double* X, int is_ee, double eps, double dhat, double k, double* G12, double* H144)
+{
+    return b2el::contact_grad_hess(X, is_ee, eps, dhat, k, G12, H144);
 }
 
 double b2g_element_ortho(const double* q, double kappa, double w, double* G9, double* H81)

@@ -112,6 +112,11 @@ double b2g_element_bw(const double* x, const double* rest, double stretch, doubl
                       double* G9, double* H81);
 double b2g_element_dsb(const double* x, const double* rest, double kappa, double w, double* G12, double* H144);
 double b2g_element_ortho(const double* q, double kappa, double w, double* G9, double* H81);
+// one contact pair X[12] ((p, t0, t1, t2) or, with is_ee, (a0, a1, b0, b1)),
+// mollifier threshold eps, dhat, k = kappa dt^2: gradient and Hessian over the
+// 4 vertices; returns the closest-feature type (0 PP, 1 PE, 2 PT, 3 EE) or -1
+// beyond dhat
+int b2g_element_contact(const double* X, int is_ee, double eps, double dhat, double k, double* G12, double* H144);
 
 #ifdef __cplusplus
 }

@@ -1,7 +1,9 @@
-"""Newton systems of tet meshes generated on the GPU (include/b200gen.h,
-csrc/b2s_generate.cu): kinetic + stable Neo-Hookean (PSD-projected) + ground
-barrier + Dirichlet vertices, written straight into device triplet buffers
-that :meth:`Solver.assemble` takes. The mesh (rest shape, tets) comes from the
+"""Newton systems generated on the GPU (include/b200gen.h): tet meshes
+(csrc/b2s_generate.cu: kinetic + stable Neo-Hookean (PSD-projected) + ground
+barrier + Dirichlet vertices), cloth (csrc/b2s_generate_shell.cu: kinetic +
+Baraff-Witkin + discrete-shell bending) and affine bodies (kinetic +
+orthogonality potential), written straight into device triplet buffers that
+:meth:`Solver.assemble` takes. The mesh (rest shape, tets) comes from the
 host generator; only the per-state work runs on the device, so a run of
 thousands of Newton systems (the learned warm start's training runs) needs no
 host round trip per system.
@@ -20,6 +22,11 @@ class GenMaterial(C.Structure):
                 ("kappa", C.c_double), ("dhat", C.c_double), ("ground_y", C.c_double)]
 
 
+class ShellMaterial(C.Structure):
+    _fields_ = [("stretch", C.c_double), ("shear", C.c_double), ("strain_rate", C.c_double), ("bend", C.c_double),
+                ("dt", C.c_double)]
+
+
 def _lib():
     lib = load_solve_lib()
     if not getattr(lib, "_b2gen_declared", False):
@@ -35,6 +42,33 @@ def _lib():
         lib.b2gen_system.restype = C.c_int
         lib.b2gen_last_error.argtypes = []
         lib.b2gen_last_error.restype = C.c_char_p
+        i32 = C.c_int32
+        lib.b2gen_shell_create.argtypes = [C.c_int, i32, i32, vp, vp, vp, vp, C.POINTER(ShellMaterial),
+                                           C.POINTER(vp)]
+        lib.b2gen_shell_create.restype = C.c_int
+        lib.b2gen_shell_destroy.argtypes = [vp]
+        lib.b2gen_shell_destroy.restype = C.c_int
+        lib.b2gen_shell_num_triplets.argtypes = [vp]
+        lib.b2gen_shell_num_triplets.restype = C.c_int64
+        lib.b2gen_shell_num_hinges.argtypes = [vp]
+        lib.b2gen_shell_num_hinges.restype = i32
+        lib.b2gen_shell_system.argtypes = [vp, vp, vp, i32, vp, vp, vp, vp, vp]
+        lib.b2gen_shell_system.restype = C.c_int
+        lib.b2gen_abd_create.argtypes = [C.c_int, i32, vp, vp, vp, C.c_double, C.POINTER(vp)]
+        lib.b2gen_abd_create.restype = C.c_int
+        lib.b2gen_abd_destroy.argtypes = [vp]
+        lib.b2gen_abd_destroy.restype = C.c_int
+        lib.b2gen_abd_system.argtypes = [vp, vp, vp, i32, vp, vp, vp, vp, vp]
+        lib.b2gen_abd_system.restype = C.c_int
+        lib.b2gen_contacts_create.argtypes = [C.c_int, i32, vp, vp, vp, C.c_double, C.c_double, C.c_double,
+                                              C.POINTER(vp)]
+        lib.b2gen_contacts_create.restype = C.c_int
+        lib.b2gen_contacts_destroy.argtypes = [vp]
+        lib.b2gen_contacts_destroy.restype = C.c_int
+        lib.b2gen_contacts_system.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+        lib.b2gen_contacts_system.restype = C.c_int
+        lib.b2gen_shell_last_error.argtypes = []
+        lib.b2gen_shell_last_error.restype = C.c_char_p
         lib._b2gen_declared = True
     return lib
 
@@ -101,6 +135,136 @@ class GpuTetMesh:
     def close(self):
         if self.h:
             _lib().b2gen_mesh_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuShell:
+    """A cloth on the device: rest positions [n, 3], triangles [m, 3], lumped
+    masses [n]; stretch / shear / strain_rate (Baraff-Witkin), bend (discrete-
+    shell bending), dt. Its block rows start at ``vertex_offset`` of the global
+    system; :meth:`system_into` writes its triplet slots
+    ([n kinetic][6 m triangle blocks][10 per hinge]) and its rows of the global
+    gradient."""
+
+    def __init__(self, rest, tris, mass, stretch, shear, bend, dt, device, strain_rate=100.0, fixed=None):
+        rest = np.ascontiguousarray(rest, dtype=np.float64)
+        tris = np.ascontiguousarray(tris, dtype=np.int32)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        fx = None if fixed is None else np.ascontiguousarray(fixed, dtype=np.uint8)
+        mat = ShellMaterial(float(stretch), float(shear), float(strain_rate), float(bend), float(dt))
+        self.n_verts = rest.shape[0]
+        lib = _lib()
+        self.h = C.c_void_p()
+        rc = lib.b2gen_shell_create(device.index or 0, self.n_verts, tris.shape[0], rest.ctypes.data,
+                                    tris.ctypes.data, mass.ctypes.data, None if fx is None else fx.ctypes.data,
+                                    C.byref(mat), C.byref(self.h))
+        if rc != 0:
+            raise RuntimeError("b2gen_shell_create: " + lib.b2gen_shell_last_error().decode())
+        self.n_triplets = int(lib.b2gen_shell_num_triplets(self.h))
+        self.n_hinges = int(lib.b2gen_shell_num_hinges(self.h))
+        self.dev = device
+
+    def system_into(self, x, x_tilde, vertex_offset, rows_ptr, cols_ptr, vals_ptr, grad, stream=None):
+        import torch
+
+        st = stream if stream is not None else torch.cuda.current_stream(self.dev).cuda_stream
+        lib = _lib()
+        rc = lib.b2gen_shell_system(self.h, x.data_ptr(), x_tilde.data_ptr(), int(vertex_offset), rows_ptr, cols_ptr,
+                                    vals_ptr, grad.data_ptr(), st)
+        if rc != 0:
+            raise RuntimeError("b2gen_shell_system: " + lib.b2gen_shell_last_error().decode())
+
+    def close(self):
+        if self.h:
+            _lib().b2gen_shell_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuAffineBodies:
+    """Affine bodies on the device: mass matrices [nb, 12, 12], orthogonality
+    stiffness and volume per body, dt. :meth:`system_into` writes 16 triplets
+    per body and the bodies' rows of the global gradient."""
+
+    def __init__(self, mass12, kappa, volume, dt, device):
+        M = np.ascontiguousarray(mass12, dtype=np.float64).reshape(-1, 144)
+        k = np.ascontiguousarray(kappa, dtype=np.float64)
+        v = np.ascontiguousarray(volume, dtype=np.float64)
+        self.n_bodies = M.shape[0]
+        lib = _lib()
+        self.h = C.c_void_p()
+        rc = lib.b2gen_abd_create(device.index or 0, self.n_bodies, M.ctypes.data, k.ctypes.data, v.ctypes.data,
+                                  float(dt), C.byref(self.h))
+        if rc != 0:
+            raise RuntimeError("b2gen_abd_create: " + lib.b2gen_shell_last_error().decode())
+        self.n_triplets = 16 * self.n_bodies
+        self.dev = device
+
+    def system_into(self, q, q_tilde, block_offset, rows_ptr, cols_ptr, vals_ptr, grad, stream=None):
+        import torch
+
+        st = stream if stream is not None else torch.cuda.current_stream(self.dev).cuda_stream
+        lib = _lib()
+        rc = lib.b2gen_abd_system(self.h, q.data_ptr(), q_tilde.data_ptr(), int(block_offset), rows_ptr, cols_ptr,
+                                  vals_ptr, grad.data_ptr(), st)
+        if rc != 0:
+            raise RuntimeError("b2gen_abd_system: " + lib.b2gen_shell_last_error().decode())
+
+    def close(self):
+        if self.h:
+            _lib().b2gen_abd_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuContacts:
+    """Point-triangle / edge-edge contact pairs on the device: pairs [n, 4]
+    (global block rows), is_ee [n], eps [n] (edge-edge mollifier thresholds),
+    dhat, kappa, dt. :meth:`system_into` writes 10 triplets per pair and adds
+    the pairs' gradients to ``grad``."""
+
+    def __init__(self, pairs, is_ee, eps, dhat, kappa, dt, device):
+        P = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 4)
+        E = np.ascontiguousarray(is_ee, dtype=np.uint8)
+        S = np.ascontiguousarray(eps, dtype=np.float64)
+        self.n_pairs = P.shape[0]
+        lib = _lib()
+        self.h = C.c_void_p()
+        rc = lib.b2gen_contacts_create(device.index or 0, self.n_pairs, P.ctypes.data, E.ctypes.data, S.ctypes.data,
+                                       float(dhat), float(kappa), float(dt), C.byref(self.h))
+        if rc != 0:
+            raise RuntimeError("b2gen_contacts_create: " + lib.b2gen_shell_last_error().decode())
+        self.n_triplets = 10 * self.n_pairs
+        self.dev = device
+
+    def system_into(self, x, rows_ptr, cols_ptr, vals_ptr, grad, stream=None):
+        import torch
+
+        st = stream if stream is not None else torch.cuda.current_stream(self.dev).cuda_stream
+        lib = _lib()
+        rc = lib.b2gen_contacts_system(self.h, x.data_ptr(), rows_ptr, cols_ptr, vals_ptr, grad.data_ptr(), st)
+        if rc != 0:
+            raise RuntimeError("b2gen_contacts_system: " + lib.b2gen_shell_last_error().decode())
+
+    def close(self):
+        if self.h:
+            _lib().b2gen_contacts_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

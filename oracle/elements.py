@@ -13,6 +13,16 @@ by tests to check it.
 * Affine-body orthogonality potential: affine_body/constitutions/
   sym/ortho_potential.inl (E, dEdq, ddEddq over q[3..11]),
   ortho_potential.cu:37-70 (make_spd on the 9x9, weight volume dt^2).
+* IPC normal contact of a point-triangle / edge-edge pair:
+  utils/distance/distance_flagged.h:258-360 (point-triangle closest-feature
+  flags), the squared distances of each type, the barrier
+  sym/codim_ipc_contact.inl:5-110 (thickness 0), the edge-edge mollifier
+  utils/distance/details/edge_edge_mollifier.inl:63-78, 498-507, and the
+  default Hessian mode of ipc_simplex_normal_contact.cu:320-360 (exact
+  Hessian + PSD projection for PT / EE and mollified pairs, the closed form
+  (B'' + B'/(2D)) grad D grad D^T for PE / PP). The distance derivatives
+  here are central differences of the closed-form distances in 50-digit
+  arithmetic (mpmath).
 """
 from __future__ import annotations
 
@@ -184,3 +194,158 @@ def ortho_element(q, kappa, w):
     wv, V = np.linalg.eigh(0.5 * (H + H.T))
     H = (V * np.maximum(wv, 0)) @ V.T
     return E, G, w * H
+
+
+# ---- IPC normal contact ---------------------------------------------------------
+# the squared distances written for any number type (float or mpmath mpf), so
+# that their derivatives can be taken by central differences in 50-digit
+# arithmetic (near-parallel edges make the line-line distance ill-conditioned
+# in double precision)
+def _sub(a, b):
+    return [a[0] - b[0], a[1] - b[1], a[2] - b[2]]
+
+
+def _crs(a, b):
+    return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+
+def _dt(a, b):
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]
+
+
+def _d2_pp(a, b):
+    d = _sub(a, b)
+    return _dt(d, d)
+
+
+def _d2_pe(p, e0, e1):
+    e = _sub(e1, e0)
+    c = _crs(_sub(p, e0), e)
+    return _dt(c, c) / _dt(e, e)
+
+
+def _d2_plane(q, a0, u, v):
+    n = _crs(u, v)
+    return _dt(_sub(q, a0), n) ** 2 / _dt(n, n)
+
+
+def pt_type(X):
+    """(type, local vertices) of a point-triangle pair X[4, 3] = (p, t0, t1, t2)."""
+    p, t = X[0], X[1:]
+    n = np.cross(t[1] - t[0], t[2] - t[0])
+    s, out = [], []
+    for k in range(3):
+        a, b = t[k], t[(k + 1) % 3]
+        e = b - a
+        o = np.cross(e, n)
+        w = p - a
+        s.append(w @ e / (e @ e))
+        out.append(w @ o / (o @ o) >= 0)
+    for k in range(3):
+        if 0 < s[k] < 1 and out[k]:
+            return "PE", [0, 1 + k, 1 + (k + 1) % 3]
+    for k in range(3):
+        if s[k] <= 0 and s[(k + 2) % 3] >= 1:
+            return "PP", [0, 1 + k]
+    return "PT", [0, 1, 2, 3]
+
+
+def ee_type(X):
+    a0, a1, b0, b1 = X
+    u, w, z = a1 - a0, b1 - b0, a0 - b0
+    a, b, c, d, e = u @ u, u @ w, w @ w, u @ z, w @ z
+    den = a * c - b * b
+    ux = np.cross(u, w)
+    if not (ux @ ux <= 1e-12 * a * c):
+        sN, tN = b * e - c * d, a * e - b * d
+        if 0 < sN < den and 0 < tN < den:
+            return "EE", [0, 1, 2, 3]
+    best, bv = np.inf, None
+    for pi, s0, s1 in ((0, 2, 3), (1, 2, 3), (2, 0, 1), (3, 0, 1)):
+        P, S0, S1 = X[pi], X[s0], X[s1]
+        sv = S1 - S0
+        t = (P - S0) @ sv / (sv @ sv)
+        if t <= 0 or t >= 1:
+            Q = S0 if t <= 0 else S1
+            dist, vv = float((P - Q) @ (P - Q)), [pi, s0 if t <= 0 else s1]
+        else:
+            q = P - S0 - t * sv
+            dist, vv = float(q @ q), [pi, s0, s1]
+        if dist < best:
+            best, bv = dist, vv
+    return ("PP" if len(bv) == 2 else "PE"), bv
+
+
+def _dist(X, kind, v):
+    if kind == "PP":
+        return _d2_pp(X[v[0]], X[v[1]])
+    if kind == "PE":
+        return _d2_pe(X[v[0]], X[v[1]], X[v[2]])
+    if kind == "PT":
+        return _d2_plane(X[0], X[1], _sub(X[2], X[1]), _sub(X[3], X[1]))
+    return _d2_plane(X[2], X[0], _sub(X[1], X[0]), _sub(X[3], X[2]))
+
+
+def _fd_grad_hess(f, X):
+    """Gradient and Hessian of f(X[4][3]) by central differences in 50-digit
+    arithmetic."""
+    import mpmath as mp
+
+    with mp.workdps(50):
+        x0 = [mp.mpf(float(c)) for c in np.asarray(X, dtype=np.float64).reshape(-1)]
+        h = mp.mpf(1e-15) * max(abs(c) for c in x0)
+
+        def F(dx):
+            x = [x0[i] + dx.get(i, 0) for i in range(12)]
+            return f([x[0:3], x[3:6], x[6:9], x[9:12]])
+        g = np.zeros(12)
+        H = np.zeros((12, 12))
+        for i in range(12):
+            g[i] = float((F({i: h}) - F({i: -h})) / (2 * h))
+            for j in range(i, 12):
+                def e(di, dj):
+                    d = {i: di}
+                    d[j] = d.get(j, 0) + dj
+                    return F(d)
+                H[i, j] = H[j, i] = float((e(h, h) - e(h, -h) - e(-h, h) + e(-h, -h)) / (4 * h * h))
+    return g, H
+
+
+def barrier(D, Dh, k):
+    t, l = D - Dh, np.log(D / Dh)
+    return -k * t * t * l, -k * (2 * t * l + t * t / D), -k * (2 * l + 4 * t / D - t * t / D ** 2)
+
+
+def contact_element(X, is_ee, eps, dhat, k):
+    """(type, G[12], H[12x12]) of one pair X[4, 3]."""
+    X = np.asarray(X, dtype=np.float64).reshape(4, 3)
+    kind, v = ee_type(X) if is_ee else pt_type(X)
+    D = float(_dist([list(r) for r in X], kind, v))
+    Dh = dhat * dhat
+    if not (0 < D < Dh):
+        return None, np.zeros(12), np.zeros((12, 12))
+    gD, HD = _fd_grad_hess(lambda x: _dist(x, kind, v), X)
+    B0, B1, B2 = barrier(D, Dh, k)
+    moll = False
+    if is_ee:
+        c = np.cross(X[1] - X[0], X[3] - X[2])
+        moll = c @ c < eps
+    if moll:
+        def cfun(x):
+            c = _crs(_sub(x[1], x[0]), _sub(x[3], x[2]))
+            return _dt(c, c)
+        cv = float(cfun([list(r) for r in X]))
+        gc, Hc = _fd_grad_hess(cfun, X)
+        xx = cv / eps
+        m0, m1, m2 = (2 - xx) * xx, 2 / eps * (1 - xx), -2 / eps ** 2
+        gm, Hm = m1 * gc, m1 * Hc + m2 * np.outer(gc, gc)
+        gB, HB = B1 * gD, B2 * np.outer(gD, gD) + B1 * HD
+        G = m0 * gB + B0 * gm
+        H = m0 * HB + np.outer(gm, gB) + np.outer(gB, gm) + B0 * Hm
+    elif kind in ("PT", "EE"):
+        G = B1 * gD
+        H = B2 * np.outer(gD, gD) + B1 * HD
+    else:
+        return kind, B1 * gD, (B2 + B1 / (2 * D)) * np.outer(gD, gD)
+    w, V = np.linalg.eigh(0.5 * (H + H.T))
+    return kind, G, (V * np.maximum(w, 0)) @ V.T

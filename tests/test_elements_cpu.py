@@ -100,3 +100,69 @@ def test_orthogonality_potential(seed, kind):
     assert np.abs(G - Go).max() <= 1e-6 * np.abs(Go).max() + 1e-10 * w * kappa  # FD noise floor
     assert _close(H, Ho, 1e-5)
     assert np.linalg.eigvalsh(H).min() >= -1e-9 * np.abs(H).max()
+
+
+TYPE_NAMES = {0: "PP", 1: "PE", 2: "PT", 3: "EE"}
+
+
+def _lib_contact(X, is_ee, eps, dhat, k):
+    lib = load_scene_lib()
+    G, H = np.zeros(12), np.zeros(144)
+    t = lib.b2g_element_contact(_ptr(np.ascontiguousarray(X, dtype=np.float64)), int(is_ee), eps, dhat, k, _ptr(G),
+                                _ptr(H))
+    return t, G, H.reshape(12, 12)
+
+
+def _contact_case(kind, rng, dhat):
+    """A pair of the given closest-feature type at distance 0.2-0.8 dhat."""
+    d = rng.uniform(0.2, 0.8) * dhat
+    R, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    h = 0.01
+    if kind in ("PT", "PE", "PP"):
+        t = np.array([[0, 0, 0], [h, 0, 0], [0.3 * h, h, 0]]) + 0.1 * h * rng.uniform(-1, 1, (3, 3)) * [1, 1, 0]
+        if kind == "PT":
+            p = t.mean(0) + [0, 0, d]
+        elif kind == "PE":  # beyond the middle of edge t0t1, off the plane
+            p = 0.5 * (t[0] + t[1]) + np.array([0, -d * 0.6, d * 0.8])
+        else:  # beyond corner t0
+            p = t[0] + np.array([-d * 0.5, -d * 0.6, d * 0.62])
+        X = np.vstack([p, t])
+        return (X @ R.T) + rng.standard_normal(3), 0
+    # edge-edge: crossing (EE), or nearly parallel (mollified)
+    a0, a1 = np.array([-h, 0, 0]), np.array([h, 0, 0])
+    if kind == "EE":
+        ang = rng.uniform(0.5, 1.5)
+    else:
+        ang = 1e-3
+    b0 = np.array([-h * np.cos(ang), -h * np.sin(ang), d]) + [0.1 * h, 0, 0]
+    b1 = np.array([h * np.cos(ang), h * np.sin(ang), d]) + [0.1 * h, 0, 0]
+    X = np.vstack([a0, a1, b0, b1])
+    return (X @ R.T) + rng.standard_normal(3), 1
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("kind", ["PT", "PE", "PP", "EE", "EE-parallel"])
+def test_contact_pair(seed, kind):
+    rng = np.random.default_rng(300 + seed)
+    dhat, k = 1e-3, 1e9 * 1e-4
+    X, is_ee = _contact_case(kind, rng, dhat)
+    # mollifier threshold from the rest edges (here: the current ones)
+    ea, eb = X[1] - X[0], X[3] - X[2]
+    eps = 1e-3 * (ea @ ea) * (eb @ eb)
+    t, G, H = _lib_contact(X, is_ee, eps, dhat, k)
+    to, Go, Ho = OE.contact_element(X, is_ee, eps, dhat, k)
+    want = {"EE-parallel": ("PE", "PP", "EE")}.get(kind, (kind,))
+    assert TYPE_NAMES[t] == to and to in want
+    assert np.abs(G - Go).max() <= 1e-5 * np.abs(Go).max()
+    assert np.abs(H - Ho).max() <= 1e-4 * np.abs(Ho).max()
+    assert np.abs(H - H.T).max() <= 1e-12 * np.abs(H).max()
+    assert np.linalg.eigvalsh(H).min() >= -1e-9 * np.abs(H).max()
+    if kind == "EE-parallel":  # the mollifier is active
+        c = np.cross(ea, eb)
+        assert c @ c < eps
+
+
+def test_contact_beyond_dhat_is_zero():
+    X = np.array([[0, 0, 2e-3], [0, 0, 0], [0.01, 0, 0], [0, 0.01, 0]], np.float64)
+    t, G, H = _lib_contact(X, 0, 0.0, 1e-3, 1e5)
+    assert t == -1 and not G.any() and not H.any()
