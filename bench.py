@@ -359,79 +359,99 @@ def bar_run(dev, steps: int, warmup: int, history_steps: int = 6, epochs: int = 
     return out
 
 
-def full_scale_run(dev, steps: int, warmup: int) -> dict:
-    """The full-scale case beside the headline: a 10 x 10 grid of 30^3-cell
-    tet cubes on the ground, a 512 x 512 cloth resting on them and 32 affine
-    bodies on the cloth (3.24 M block rows, 9.72 M DoF, 172 M raw triplets);
-    MAS on the FEM range (cubes + cloth) and 12x12 block Jacobi on the bodies.
-    One Newton system (first step from rest), solved from a zero start to an
-    FP64-verified rel-res 1e-4, plain FP64 vs mixed precision; ms per solve
-    (assembly + preconditioner build + PCG) by CUDA events."""
+FULL_SCALE = dict(cells_x=30, cells_y=30, cells_z=30, n_cubes=10, cloth_n=512, bodies_x=4, bodies_z=8, dt=0.005,
+                  seed=0)
+
+
+def full_scale_run(dev, n_systems: int = 4, scene_kw: dict | None = None) -> dict:
+    """The full-scale case beside the headline, stepped: a 10 x 10 grid of
+    30^3-cell tet cubes on the ground, a 512 x 512 cloth resting on them and
+    32 affine bodies on the cloth (3.24 M block rows, 9.72 M DoF, 172 M raw
+    triplets, dt = 5 ms); MAS on the FEM range (cubes + cloth) and 12x12 block
+    Jacobi on the bodies. The scene falls under gravity for ``n_systems``
+    backward-Euler steps of one Newton iteration each (the host generator
+    writes each step's system at the current state, about 18 s per system,
+    outside the timed region); every system is solved twice to an
+    FP64-verified rel-res 1e-4: plain FP64 from zero, and mixed precision from
+    the history start (the Galerkin combination of the earlier steps'
+    solutions; the network is not trained at this scale). The run advances
+    with the mixed solution. ms per solve (assembly + preconditioner build +
+    warm start + PCG) by CUDA events, per system and averaged."""
     import numpy as np
     import torch
 
-    from libuipc_b200 import _abi, scene
+    from libuipc_b200 import _abi
     from libuipc_b200.linear_system import Solver, partition_maps, partition_rcb
+    from libuipc_b200.sequence import SceneSequence
 
     t0 = time.time()
-    s = scene.cube_wall()
-    gen_s = time.time() - t0
-    off = 4 * s.n_bodies
-    a0 = s.adj_start[off]
-    adj_start = (s.adj_start[off:] - a0).astype(np.int32)
-    adj_list = (s.adj_list[a0:] - off).astype(np.int32)
-    p2r, r2p = partition_maps(partition_rcb(s.positions[off:]))
+    seq = SceneSequence(scene=4, **(scene_kw or FULL_SCALE))
+    off = 4 * seq.n_bodies
+    a0 = seq.adj_start[off]
+    adj_start = (seq.adj_start[off:] - a0).astype(np.int32)
+    adj_list = (seq.adj_list[a0:] - off).astype(np.int32)
+    p2r, r2p = partition_maps(partition_rcb(seq.rest[off:]))
+    gen_s = [time.time() - t0]
     stream = torch.cuda.Stream(device=dev)
     solver = Solver(dev.index or 0)
     solver.set_stream(stream.cuda_stream)
-    with torch.cuda.stream(stream):
-        rows = torch.from_numpy(s.rows).to(dev)
-        cols = torch.from_numpy(s.cols).to(dev)
-        vals = torch.from_numpy(s.vals).to(dev)
-        b = torch.from_numpy(s.b).to(dev)
-        x = torch.zeros_like(b)
-    stream.synchronize()
-    n_trip = len(s.rows)
-    s.vals = None  # 13.8 GB of host memory: the device copy is what is solved
-    solver.assemble(s.n_verts, rows, cols, vals)
-    solver.mas_init(off, s.n_verts - off, adj_start, adj_list, p2r, r2p)
-    solver.abd_init(0, s.n_bodies)
-    nb, U = solver.matrix_info()
-    out = {"workload": f"cube grid 10x10 x 30^3 cells + 512^2 cloth + {s.n_bodies} affine bodies "
-                       f"({s.n_verts:,} block rows, {3 * s.n_verts:,} DoF, {n_trip:,} triplets, "
-                       f"{U:,} upper blocks, {s.n_contacts:,} contacts), first Newton step from rest",
-           "generate_s": gen_s}
+    solver.mas_init(off, seq.n_verts - off, adj_start, adj_list, p2r, r2p)
+    solver.abd_init(0, seq.n_bodies)
+    solver.ws_init(64, seed=0)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for mode, prec in (("plain", _abi.B2S_PRECISION_FP64), ("mixed", _abi.B2S_PRECISION_MIXED)):
-        def solve():
-            solver.assemble(s.n_verts, rows, cols, vals)
-            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_F32)
-            return solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, precision=prec,
-                              replace_every=50)
+    history: list = []
+    per = []
+    info = {}
 
-        for _ in range(warmup):
-            solve()
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        st = [solve() for _ in range(steps)]
-        ev1.record(stream)
-        ev1.synchronize()
-        ms = ev0.elapsed_time(ev1) / steps
-        # stage breakdown: one more solve with the solver's stage events
-        solver.set_timing(True)
-        solve()
-        solver.reset_timers()
-        solve()
-        t = solver.timers()
-        solver.set_timing(False)
-        out[mode] = {"ms_per_solve": ms, "pcg_iterations": int(st[-1]["iterations_exact"]),
-                     "rel_res": float(st[-1]["rel_res"]),
-                     "stages_ms": {"assemble": t["assemble_ms"], "precond_build": t["precond_build_ms"],
-                                   "pcg": t["pcg_ms"], "spmv_avg": t["spmv_ms"] / max(t["spmv_launches"], 1),
-                                   "precond_apply_avg": t["precond_apply_ms"] / max(t["precond_apply_launches"], 1)}}
-    out["speedup_vs_plain"] = out["plain"]["ms_per_solve"] / out["mixed"]["ms_per_solve"]
+    def solve(sysm, step, k):
+        t1 = time.time()
+        with torch.cuda.stream(stream):
+            rows = torch.from_numpy(sysm.rows).to(dev)
+            cols = torch.from_numpy(sysm.cols).to(dev)
+            vals = torch.from_numpy(sysm.vals).to(dev)
+            b = torch.from_numpy(sysm.b).to(dev)
+        stream.synchronize()
+        if not info:
+            info.update(n_triplets=len(sysm.rows), contacts=int(sysm.n_contacts))
+        sysm.vals = None  # 13.8 GB of host memory: the device copy is what is solved
+        rec = {"step": step, "contacts": int(sysm.n_contacts)}
+        for mode, prec in (("plain", _abi.B2S_PRECISION_FP64), ("mixed+history", _abi.B2S_PRECISION_MIXED)):
+            x = torch.zeros_like(b)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            solver.assemble(sysm.n_verts, rows, cols, vals)
+            solver.precond_assemble(_abi.B2S_PRECOND_MAS, _abi.B2S_INVERT_F32)
+            if mode != "plain" and history:
+                solver.ws_predict(b, x, history[:3], _abi.B2S_WS_MODE_HISTORY)
+            st = solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, check_interval=5, precision=prec,
+                            replace_every=50, x0_given=mode != "plain")
+            ev1.record(stream)
+            ev1.synchronize()
+            rec[mode] = {"ms": ev0.elapsed_time(ev1), "pcg_iterations": int(st["iterations_exact"]),
+                         "rel_res": float(st["rel_res"])}
+        if "U" not in info:
+            info["U"] = solver.matrix_info()[1]
+        per.append(rec)
+        history.insert(0, x)
+        del history[3:]
+        gen_s.append(time.time() - t1)
+        return x.cpu().numpy()
+
+    for _ in seq.run(n_systems, 1, solve):
+        pass
     solver.close()
-    return out
+    timed = per[1:] if len(per) > 1 else per  # the history start needs an earlier solution
+    mean = {m: float(np.mean([r[m]["ms"] for r in timed])) for m in ("plain", "mixed+history")}
+    its = {m: float(np.mean([r[m]["pcg_iterations"] for r in timed])) for m in ("plain", "mixed+history")}
+    kw = scene_kw or FULL_SCALE
+    return {"workload": f"cube grid {kw['n_cubes']}x{kw['n_cubes']} x {kw['cells_x']}^3 cells + "
+                        f"{kw['cloth_n']}^2 cloth + {seq.n_bodies} affine bodies "
+                        f"({seq.n_verts:,} block rows, {3 * seq.n_verts:,} DoF, {info['n_triplets']:,} triplets, "
+                        f"{info['U']:,} upper blocks), falling under gravity, dt = 5 ms",
+            "systems": per, "timed_systems": len(timed), "ms_per_solve": mean, "mean_pcg_iterations": its,
+            "speedup_vs_plain": mean["plain"] / mean["mixed+history"],
+            "note": "mean over the systems after the first (whose history is empty); host generation "
+                    f"{np.mean(gen_s):.1f} s per system outside the timed region"}
 
 
 TRUTH_TOL = 1e-10  # FP64 rel-res of the solves that advance the run (both arms)
@@ -579,6 +599,8 @@ def main() -> None:
                          "compared on 200 later systems: about three minutes)")
     ap.add_argument("--no-full-scale", action="store_true",
                     help="skip the 9.7 M-DoF cube grid + cloth + bodies case run beside the headline")
+    ap.add_argument("--full-scale-systems", type=int, default=4,
+                    help="Newton systems of the stepped full-scale run (about 18 s of host generation each)")
     ap.add_argument("--no-bar", action="store_true",
                     help="skip the second run reported beside the headline: a 1.16 M-DoF twisted bar")
     args = ap.parse_args()
@@ -732,7 +754,7 @@ def main() -> None:
     full = None
     if rank == 0 and not args.no_full_scale:
         try:
-            full = full_scale_run(dev, steps=3, warmup=2)
+            full = full_scale_run(dev, n_systems=args.full_scale_systems)
         except Exception as e:  # reported, not fatal
             full = {"error": str(e)}
 

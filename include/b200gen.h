@@ -123,6 +123,9 @@ typedef struct b2gen_contacts b2gen_contacts;
 int b2gen_contacts_create(int device, int32_t n_pairs, const int32_t* pairs, const uint8_t* is_ee,
                           const double* eps, double dhat, double kappa, double dt, b2gen_contacts** out);
 int b2gen_contacts_destroy(b2gen_contacts* c);
+/* closest-feature type of every pair at the last b2gen_contacts_system
+ * (0 point-point, 1 point-edge, 2 point-triangle, 3 edge-edge, -1 beyond dhat) */
+int b2gen_contacts_types(b2gen_contacts* c, int8_t* h_types);
 int b2gen_contacts_system(b2gen_contacts* c, const double* d_x, int32_t* d_rows, int32_t* d_cols,
                           double* d_vals, double* d_grad, void* stream);
 const char* b2gen_shell_last_error(void);

@@ -219,9 +219,12 @@ __global__ void k_abd(int nb, int32_t off, const double* __restrict__ M, const d
 }
 
 // contact pairs: 10 blocks per pair from slot 10 p, the pair's gradient to pair_g
-__global__ void k_contacts(int np, const int32_t* __restrict__ pairs, const uint8_t* __restrict__ is_ee,
-                           const double* __restrict__ eps, const double* __restrict__ x, double dhat, double k,
-                           int32_t* rows, int32_t* cols, double* vals, double* __restrict__ pair_g)
+constexpr int CONTACT_BLOCK = 64;
+
+__global__ void __launch_bounds__(CONTACT_BLOCK)
+    k_contacts(int np, const int32_t* __restrict__ pairs, const uint8_t* __restrict__ is_ee,
+               const double* __restrict__ eps, const double* __restrict__ x, double dhat, double k, int32_t* rows,
+               int32_t* cols, double* vals, double* __restrict__ pair_g, int8_t* __restrict__ pair_type)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if(p >= np)
@@ -231,7 +234,7 @@ __global__ void k_contacts(int np, const int32_t* __restrict__ pairs, const uint
     for(int i = 0; i < 4; ++i)
         for(int a = 0; a < 3; ++a)
             X[3 * i + a] = x[3 * (int64_t)V[i] + a];
-    b2el::contact_grad_hess(X, is_ee[p], eps[p], dhat, k, G, H);
+    pair_type[p] = (int8_t)b2el::contact_grad_hess(X, is_ee[p], eps[p], dhat, k, G, H);
     for(int i = 0; i < 12; ++i)
         pair_g[12ll * p + i] = G[i];
     put_element<4>(10ll * p, V, 0, H, rows, cols, vals);
@@ -300,6 +303,7 @@ struct b2gen_contacts
     int32_t            np = 0, nvert = 0;
     b2s::DBuf<int32_t> pairs, verts, start, list;
     b2s::DBuf<uint8_t> is_ee;
+    b2s::DBuf<int8_t>  pair_type;
     b2s::DBuf<double>  eps, pair_g;
     double             dhat = 0.0, kappa = 0.0, dt = 0.0;
     int                device = 0;
@@ -552,6 +556,7 @@ int b2gen_contacts_create(int device, int32_t n_pairs, const int32_t* pairs, con
             C->is_ee.resize(n_pairs);
             C->eps.resize(n_pairs);
             C->pair_g.resize(12 * (size_t)n_pairs);
+            C->pair_type.resize(n_pairs);
             C->verts.resize(verts.size());
             C->start.resize(start.size());
             C->list.resize(list.size());
@@ -562,6 +567,18 @@ int b2gen_contacts_create(int device, int32_t n_pairs, const int32_t* pairs, con
             B2S_CUDA(cudaMemcpy(C->start.data(), start.data(), C->start.bytes(), cudaMemcpyHostToDevice));
             B2S_CUDA(cudaMemcpy(C->list.data(), list.data(), C->list.bytes(), cudaMemcpyHostToDevice));
             *out = C;
+        });
+}
+
+int b2gen_contacts_types(b2gen_contacts* c, int8_t* h_types)
+{
+    return guarded_gen(
+        [&]
+        {
+            if(!c || !h_types)
+                fail("b2gen_contacts_types: bad arguments");
+            B2S_CUDA(cudaSetDevice(c->device));
+            B2S_CUDA(cudaMemcpy(h_types, c->pair_type.data(), c->pair_type.bytes(), cudaMemcpyDeviceToHost));
         });
 }
 
@@ -581,9 +598,9 @@ int b2gen_contacts_system(b2gen_contacts* c, const double* d_x, int32_t* d_rows,
                 fail("b2gen_contacts_system: bad arguments");
             B2S_CUDA(cudaSetDevice(c->device));
             cudaStream_t st = static_cast<cudaStream_t>(stream);
-            k_contacts<<<grid_of(c->np), 64, 0, st>>>(c->np, c->pairs.data(), c->is_ee.data(), c->eps.data(), d_x,
-                                                      c->dhat, c->kappa * c->dt * c->dt, d_rows, d_cols, d_vals,
-                                                      c->pair_g.data());
+            k_contacts<<<(c->np + CONTACT_BLOCK - 1) / CONTACT_BLOCK, CONTACT_BLOCK, 0, st>>>(
+                c->np, c->pairs.data(), c->is_ee.data(), c->eps.data(), d_x, c->dhat, c->kappa * c->dt * c->dt, d_rows,
+                d_cols, d_vals, c->pair_g.data(), c->pair_type.data());
             B2S_CHECK_LAUNCH();
             k_contacts_gather<<<grid_of(c->nvert), SHELL_BLOCK, 0, st>>>(c->nvert, c->verts.data(), c->start.data(),
                                                                          c->list.data(), c->pair_g.data(), d_grad);

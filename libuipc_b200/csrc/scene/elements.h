@@ -42,8 +42,14 @@
 
 #if defined(__CUDACC__)
 #define B2_HD __host__ __device__ inline
+// contact_grad_hess is compiled as a device function of its own: inlined into
+// the contact kernel (CUDA 12.9, NVVM at -O3), its point-edge, point-point
+// and edge-edge branches came out wrong (correct at NVVM -O1, or not
+// inlined); the GPU test compares every type with the host build
+#define B2_HD_NOINLINE __host__ __device__ __noinline__
 #else
 #define B2_HD inline
+#define B2_HD_NOINLINE inline
 #endif
 
 namespace b2el
@@ -773,7 +779,8 @@ B2_HD void barrier_B(double D, double Dh, double k, double* B0, double* B1, doub
 // for point-triangle), k = kappa dt^2; G[12], H[144] over the 4 vertices (zero
 // rows for vertices outside the type's stencil). Returns the type, or -1 when
 // the pair is at or beyond dhat (G, H zero).
-B2_HD int contact_grad_hess(const double* X, int is_ee, double eps, double dhat, double k, double* G, double* H)
+B2_HD_NOINLINE int contact_grad_hess(const double* X, int is_ee, double eps, double dhat, double k, double* G,
+                                     double* H)
 {
     for(int i = 0; i < 12; ++i)
         G[i] = 0.0;

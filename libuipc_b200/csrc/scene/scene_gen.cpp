@@ -439,8 +439,8 @@ namespace
 // zero blocks): mass matrix m_b I on p, I_b I on each column of A, plus the
 // orthogonality potential's PSD Hessian at A = R (R a rotation about +y by
 // theta), scaled by V dt^2; and its gravity gradient.
-void add_affine_body(Builder& B, std::vector<double>& grad, int64_t b, double theta, double m_b, double I_b,
-                     double V, const b2g_config& C)
+void add_affine_body(Builder& B, std::vector<double>& grad, int64_t b, const double* q, const double* qt,
+                     double m_b, double I_b, double V, const b2g_config& C)
 {
     const double dt2 = C.dt * C.dt;
     double       H[12][12] = {};
@@ -450,33 +450,63 @@ void add_affine_body(Builder& B, std::vector<double>& grad, int64_t b, double th
         for(int k = 0; k < 3; ++k)
             H[3 + 3 * k + a][3 + 3 * k + a] = I_b;
     }
-    const double cs = std::cos(theta), sn = std::sin(theta);
-    const double R[3][3] = {{cs, 0, sn}, {0, 1, 0}, {-sn, 0, cs}};
-    // orthogonality potential at A = R (q index 3 + 3 k + r <-> A[r][k]):
-    // zero gradient, PSD Hessian
-    double q[12] = {};
-    for(int k = 0; k < 3; ++k)
-        for(int r = 0; r < 3; ++r)
-            q[3 + 3 * k + r] = R[r][k];
+    // orthogonality potential at the body's affine matrix (q index 3 + 3 k + r
+    // <-> A[r][k]): PSD Hessian, gradient (zero up to rounding at a rotation)
     double G9[9], H9[81];
     b2el::ortho_grad_hess(q, C.body_kappa, V * dt2, G9, H9);
     for(int m = 0; m < 9; ++m)
         for(int n = 0; n < 9; ++n)
             H[3 + m][3 + n] += H9[m * 9 + n];
-    for(int m = 0; m < 9; ++m)  // zero up to rounding at a rotation
-        grad[(4 * b + 1) * 3 + m] += G9[m];
-    // kinetic gradient: m (x - x_tilde) with x_tilde = x - dt^2 g on p
-    grad[(4 * b) * 3 + 1] += m_b * dt2 * C.gravity;
+    // kinetic gradient M (q - q_tilde), M diagonal
+    for(int i = 0; i < 12; ++i)
+        grad[(4 * b) * 3 + i] += (i < 3 ? m_b : I_b) * (q[i] - qt[i]) + (i >= 3 ? G9[i - 3] : 0.0);
     for(int bi = 0; bi < 4; ++bi)
         for(int bj = 0; bj < 4; ++bj)
         {
             const int32_t r = (int32_t)(4 * b + bi), c = (int32_t)(4 * b + bj);
             B.rows.push_back(r);
             B.cols.push_back(c);
-            for(int q = 0; q < 3; ++q)
+            for(int qq = 0; qq < 3; ++qq)
                 for(int p = 0; p < 3; ++p)
-                    B.vals.push_back(bi > bj ? 0.0 : H[3 * bi + p][3 * bj + q]);
+                    B.vals.push_back(bi > bj ? 0.0 : H[3 * bi + p][3 * bj + qq]);
         }
+}
+
+// q of a body at rest: centre c, the columns of R, a rotation about +y by theta
+void body_rest_q(const double* c, double theta, double* q)
+{
+    const double cs = std::cos(theta), sn = std::sin(theta);
+    const double R[3][3] = {{cs, 0, sn}, {0, 1, 0}, {-sn, 0, cs}};
+    for(int a = 0; a < 3; ++a)
+        q[a] = c[a];
+    for(int k = 0; k < 3; ++k)
+        for(int r = 0; r < 3; ++r)
+            q[3 + 3 * k + r] = R[r][k];
+}
+
+// x = A^-1 (y - p) of a body with q = (p, A[:,0], A[:,1], A[:,2])
+void body_frame(const double* q, const double* y, double* x)
+{
+    double A[3][3];
+    for(int k = 0; k < 3; ++k)
+        for(int r = 0; r < 3; ++r)
+            A[r][k] = q[3 + 3 * k + r];
+    const double d[3] = {y[0] - q[0], y[1] - q[1], y[2] - q[2]};
+    const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                       A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                       A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+    double inv[3][3];
+    inv[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) / det;
+    inv[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) / det;
+    inv[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) / det;
+    inv[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) / det;
+    inv[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) / det;
+    inv[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) / det;
+    inv[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) / det;
+    inv[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) / det;
+    inv[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) / det;
+    for(int r = 0; r < 3; ++r)
+        x[r] = inv[r][0] * d[0] + inv[r][1] * d[1] + inv[r][2] * d[2];
 }
 
 void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
@@ -498,14 +528,10 @@ void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
     for(int64_t b = 0; b < nbod; ++b)
     {
         const int64_t i = b % nbs, k = b / nbs;
-        sys->x[(4 * b) * 3 + 0] = (i + 0.5) * pitch - 0.5 * Lc;
-        sys->x[(4 * b) * 3 + 1] = -0.5 * s;
-        sys->x[(4 * b) * 3 + 2] = (k + 0.5) * pitch - 0.5 * Lc;
-        theta[b] = urand(C.seed, 4, b) * (M_PI / 4);
-        // rows 4b+1..4b+3 carry the body centre too (positions are per block row)
-        for(int r = 1; r < 4; ++r)
-            for(int a = 0; a < 3; ++a)
-                sys->x[(4 * b + r) * 3 + a] = sys->x[(4 * b) * 3 + a];
+        const double c[3] = {(i + 0.5) * pitch - 0.5 * Lc, -0.5 * s, (k + 0.5) * pitch - 0.5 * Lc};
+        theta[b]           = urand(C.seed, 4, b) * (M_PI / 4);
+        // the body's 12 DoF on its 4 block rows: centre, then the columns of A = R
+        body_rest_q(c, theta[b], &sys->x[(4 * b) * 3]);
     }
     for(int64_t v = 0; v < ncv; ++v)
     {
@@ -527,9 +553,15 @@ void generate_cloth_abd(const b2g_config& C, b2g_system* sys)
             for(int p = 0; p < 3; ++p)
                 B.vals.push_back(tp ? Hrc[q * 3 + p] : Hrc[p * 3 + q]);  // column-major
     };
-    // ---- affine bodies ----
+    // ---- affine bodies (first step from rest: q_tilde = q - dt^2 g on p) ----
     for(int64_t b = 0; b < nbod; ++b)
-        add_affine_body(B, sys->grad, b, theta[b], m_b, I_b, V, C);
+    {
+        const double* q = &sys->x[(4 * b) * 3];
+        double        qt[12];
+        std::copy(q, q + 12, qt);
+        qt[1] -= dt2 * C.gravity;
+        add_affine_body(B, sys->grad, b, q, qt, m_b, I_b, V, C);
+    }
     // ---- cloth ----
     const int32_t c0 = (int32_t)(4 * nbod);
     for(int64_t v = 0; v < ncv; ++v)
@@ -1176,19 +1208,22 @@ void generate_tets(const b2g_config& C, const double* x_in, const double* xt_in,
 //    (15 triplets);
 //  * DoF order: bodies (4 block rows each), cube vertices, cloth vertices; the
 //    neighbour graph holds the tet edges and the cloth triangle edges.
-void generate_wall(const b2g_config& C, b2g_system* sys)
+void generate_wall(const b2g_config& C, const double* x_in, const double* xt_in, b2g_system* sys)
 {
     const int W = C.n_cubes, N = C.cloth_n, nbx = C.bodies_x, nbz = C.bodies_z;
     if(N < 2 || nbx < 0 || nbz < 0 || W < 1)
         throw std::runtime_error("scene 4 needs n_cubes >= 1, cloth_n >= 2, bodies_x/z >= 0");
+    if((x_in == nullptr) != (xt_in == nullptr))
+        throw std::runtime_error("scene 4 state input needs both x and x_tilde");
     b2g_config Cc = C;
     Cc.scene      = 4;
-    b2g_system cubes;
-    generate_tets(Cc, nullptr, nullptr, &cubes);
+    b2g_system    cubes;
+    const int64_t nbod = (int64_t)nbx * nbz, off_c = 4 * nbod;
+    generate_tets(Cc, x_in ? x_in + off_c * 3 : nullptr, xt_in ? xt_in + off_c * 3 : nullptr, &cubes);
     const int     nx = C.cells_x, ny = C.cells_y, nz = C.cells_z;
     const int64_t vx = nx + 1, vy = ny + 1, vz = nz + 1, verts_per = vx * vy * vz;
-    const int64_t nbod = (int64_t)nbx * nbz, ncube_v = (int64_t)cubes.x.size() / 3, ncv = (int64_t)N * N;
-    const int64_t off_c = 4 * nbod, off_cl = off_c + ncube_v, rows = off_cl + ncv;
+    const int64_t ncube_v = (int64_t)cubes.x.size() / 3, ncv = (int64_t)N * N;
+    const int64_t off_cl = off_c + ncube_v, rows = off_cl + ncv;
     if(rows > (int64_t)INT32_MAX / 3)
         throw std::runtime_error("system too large for 32-bit DoF indices");
     const double px_pitch = nx * C.h + C.wall_gap, pz_pitch = nz * C.h + C.wall_gap;
@@ -1207,12 +1242,10 @@ void generate_wall(const b2g_config& C, b2g_system* sys)
         const int64_t i = b % nbx, k = b / nbx;
         const double  c[3] = {(i + 0.5) * bpx, y_cloth + 0.5 * C.dhat + 0.5 * s, (k + 0.5) * bpz};
         theta[b]           = urand(C.seed, 4, b) * (M_PI / 4);
-        for(int r = 0; r < 4; ++r)
-            for(int a = 0; a < 3; ++a)
-                sys->x[(4 * b + r) * 3 + a] = c[a];
+        // the body's 12 DoF on its 4 block rows: centre, then the columns of A
+        body_rest_q(c, theta[b], &sys->x[(4 * b) * 3]);
     }
-    std::copy(cubes.x.begin(), cubes.x.end(), sys->x.begin() + off_c * 3);
-    std::copy(cubes.grad.begin(), cubes.grad.end(), sys->grad.begin() + off_c * 3);
+    std::copy(cubes.x_rest.begin(), cubes.x_rest.end(), sys->x.begin() + off_c * 3);
     for(int64_t v = 0; v < ncv; ++v)
     {
         const int64_t g = off_cl + v;
@@ -1221,6 +1254,20 @@ void generate_wall(const b2g_config& C, b2g_system* sys)
         sys->x[g * 3 + 2] = (v / N) * hcz;
     }
     sys->x_rest = sys->x;
+    // the state: given, or the first step from rest (x_tilde = x - dt^2 g on
+    // every translation DoF: cube and cloth vertices and the bodies' centres)
+    std::vector<double> xt(sys->x);
+    if(x_in)
+    {
+        std::copy(x_in, x_in + rows * 3, sys->x.begin());
+        std::copy(xt_in, xt_in + rows * 3, xt.begin());
+    }
+    else
+        for(int64_t r = 0; r < rows; ++r)
+            if(r >= off_c || r % 4 == 0)
+                xt[r * 3 + 1] -= dt2 * C.gravity;
+    std::copy(cubes.x.begin(), cubes.x.end(), sys->x.begin() + off_c * 3);
+    std::copy(cubes.grad.begin(), cubes.grad.end(), sys->grad.begin() + off_c * 3);
 
     Builder B;
     B.reserve((size_t)nbod * 16 + cubes.rows.size() + (size_t)ncv * 30);
@@ -1235,7 +1282,7 @@ void generate_wall(const b2g_config& C, b2g_system* sys)
     };
     // ---- bodies, cubes ----
     for(int64_t b = 0; b < nbod; ++b)
-        add_affine_body(B, sys->grad, b, theta[b], m_b, I_b, V, C);
+        add_affine_body(B, sys->grad, b, &sys->x[(4 * b) * 3], &xt[(4 * b) * 3], m_b, I_b, V, C);
     for(size_t t = 0; t < cubes.rows.size(); ++t)
     {
         B.rows.push_back(cubes.rows[t] + (int32_t)off_c);
@@ -1249,7 +1296,8 @@ void generate_wall(const b2g_config& C, b2g_system* sys)
     {
         const double Hm[9] = {m_v, 0, 0, 0, m_v, 0, 0, 0, m_v};
         put((int32_t)(off_cl + v), (int32_t)(off_cl + v), Hm);
-        sys->grad[(off_cl + v) * 3 + 1] += m_v * dt2 * C.gravity;
+        for(int a = 0; a < 3; ++a)
+            sys->grad[(off_cl + v) * 3 + a] += m_v * (sys->x[(off_cl + v) * 3 + a] - xt[(off_cl + v) * 3 + a]);
     }
     add_cloth_grid(B, sys->grad, sys->x, sys->x_rest, off_cl, N, C.cloth_k, C.bend_k, dt2);
     auto link = [&](int32_t ga, int32_t gb)
@@ -1332,17 +1380,20 @@ void generate_wall(const b2g_config& C, b2g_system* sys)
         if(bi < 0 || bi >= nbx || bk < 0 || bk >= nbz)
             continue;
         const int64_t b  = bi + (int64_t)nbx * bk;
-        const double  px = sys->x[(4 * b) * 3], py = sys->x[(4 * b) * 3 + 1], pz = sys->x[(4 * b) * 3 + 2];
-        const double  cs = std::cos(theta[b]), sn = std::sin(theta[b]);
-        const double  ux = cs * (xv - px) - sn * (zv - pz), uz = sn * (xv - px) + cs * (zv - pz);
-        if(std::fabs(ux) > 0.5 * s || std::fabs(uz) > 0.5 * s)
+        const double* q  = &sys->x[(4 * b) * 3];
+        const double  xvv[3] = {xv, yv, zv};
+        double        u[3];
+        body_frame(q, xvv, u);  // the vertex in the body's frame
+        if(std::fabs(u[0]) > 0.5 * s || std::fabs(u[2]) > 0.5 * s)
             continue;
-        const double d = (py - 0.5 * s) - yv;
+        const double d = -0.5 * s - u[1];  // below the bottom face (A near a rotation)
         if(d <= 0.0 || d >= C.dhat)
             continue;
-        const double R[3][3] = {{cs, 0, sn}, {0, 1, 0}, {-sn, 0, cs}};
-        const double pb[3]   = {px, py, pz}, xvv[3] = {xv, yv, zv};
-        if(add_vertex_body_contact(B, sys->grad, (int32_t)g, xvv, b, pb, R, ux, uz, -0.5 * s, 0.5 * s, C.dhat,
+        double A[3][3];
+        for(int k = 0; k < 3; ++k)
+            for(int r = 0; r < 3; ++r)
+                A[r][k] = q[3 + 3 * k + r];
+        if(add_vertex_body_contact(B, sys->grad, (int32_t)g, xvv, b, q, A, u[0], u[2], -0.5 * s, 0.5 * s, C.dhat,
                                    dt2 * C.kappa))
             ++n_contacts;
     }
@@ -1386,15 +1437,14 @@ int generate_impl(const b2g_config* cfg, const double* x_in, const double* xt_in
             throw std::runtime_error("null argument");
         const b2g_config C = *cfg;
         auto sys = std::make_unique<b2g_system>();
-        if(C.scene == 3 || C.scene == 4)
+        if(C.scene == 3)
         {
             if(x_in || xt_in)
-                throw std::runtime_error("scenes 3 and 4 have no state input");
-            if(C.scene == 3)
-                generate_cloth_abd(C, sys.get());
-            else
-                generate_wall(C, sys.get());
+                throw std::runtime_error("scene 3 has no state input");
+            generate_cloth_abd(C, sys.get());
         }
+        else if(C.scene == 4)
+            generate_wall(C, x_in, xt_in, sys.get());
         else
             generate_tets(C, x_in, xt_in, sys.get());
         *out = sys.release();

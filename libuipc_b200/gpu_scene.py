@@ -65,6 +65,8 @@ def _lib():
         lib.b2gen_contacts_create.restype = C.c_int
         lib.b2gen_contacts_destroy.argtypes = [vp]
         lib.b2gen_contacts_destroy.restype = C.c_int
+        lib.b2gen_contacts_types.argtypes = [vp, vp]
+        lib.b2gen_contacts_types.restype = C.c_int
         lib.b2gen_contacts_system.argtypes = [vp, vp, vp, vp, vp, vp, vp]
         lib.b2gen_contacts_system.restype = C.c_int
         lib.b2gen_shell_last_error.argtypes = []
@@ -261,6 +263,15 @@ class GpuContacts:
         rc = lib.b2gen_contacts_system(self.h, x.data_ptr(), rows_ptr, cols_ptr, vals_ptr, grad.data_ptr(), st)
         if rc != 0:
             raise RuntimeError("b2gen_contacts_system: " + lib.b2gen_shell_last_error().decode())
+
+    def types(self) -> np.ndarray:
+        """Closest-feature type per pair at the last system (0 PP, 1 PE, 2 PT,
+        3 EE, -1 beyond dhat)."""
+        out = np.zeros(self.n_pairs, np.int8)
+        rc = _lib().b2gen_contacts_types(self.h, out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("b2gen_contacts_types: " + _lib().b2gen_shell_last_error().decode())
+        return out
 
     def close(self):
         if self.h:

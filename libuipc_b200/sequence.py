@@ -43,6 +43,11 @@ class SceneSequence:
         self.adj_start = base.adj_start
         self.adj_list = base.adj_list
         self.n_verts = base.n_verts
+        self.n_bodies = int(base.n_bodies)
+        # gravity acts on translations: every vertex row and each affine body's
+        # first block row (its centre), not on the rows of its affine matrix
+        rows = np.arange(self.n_verts)
+        self.gravity_rows = (rows >= 4 * self.n_bodies) | (rows % 4 == 0)
         self.step = 0
         if self.scene == 2:
             xs = self.rest[:, 0]
@@ -71,7 +76,7 @@ class SceneSequence:
         self.step += 1
         self.x_prev = self.x.copy()
         self.x_tilde = self.x + self.dt * self.v
-        self.x_tilde[:, 1] -= self.dt * self.dt * self.gravity
+        self.x_tilde[self.gravity_rows, 1] -= self.dt * self.dt * self.gravity
         if self.scene == 2:
             th = self.twist_per_step * self.step
             self.x[self.left] = self._rotated_rest(self.left, -th)

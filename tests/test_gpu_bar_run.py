@@ -45,3 +45,22 @@ def test_learned_run_on_the_gpu(cuda):
     it = r["mean_pcg_iterations"]
     assert r["training_systems"] == 16 and r["eval_systems"] == 6
     assert it["history"] < it["zero"] and it["learned"] < it["zero"]
+
+
+def test_stepped_full_scale_run_small(cuda):
+    """The stepped cube-grid + cloth + bodies run of the bench on a small
+    instance (2 x 2 cubes of 6^3 cells, 16^2 cloth, 2 x 2 bodies, 3 systems):
+    every solve meets rel-res 1e-4, the systems follow the state (contact
+    counts change), and the history start needs fewer PCG iterations than
+    the plain solve from zero on the later systems."""
+    import bench
+
+    out = bench.full_scale_run(cuda, n_systems=3, scene_kw=dict(cells_x=6, cells_y=6, cells_z=6, n_cubes=2,
+                                                                 cloth_n=16, bodies_x=2, bodies_z=2, dt=0.005,
+                                                                 seed=0))
+    assert len(out["systems"]) == 3 and out["timed_systems"] == 2
+    for r in out["systems"]:
+        for m in ("plain", "mixed+history"):
+            assert r[m]["rel_res"] <= 1e-4
+    for r in out["systems"][1:]:
+        assert r["mixed+history"]["pcg_iterations"] < r["plain"]["pcg_iterations"]

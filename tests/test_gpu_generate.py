@@ -235,10 +235,12 @@ def test_contact_producer_against_the_host_routines(cuda):
     grad = torch.zeros(Xall.size, dtype=torch.float64, device=cuda)
     gc.system_into(to_dev(Xall.reshape(-1), cuda), rows.data_ptr(), cols.data_ptr(), vals.data_ptr(), grad)
     V = vals.cpu().numpy().reshape(n, 10, 3, 3)
+    types = gc.types()
     gref = np.zeros_like(Xall.reshape(-1))
     for p in range(n):
         Xp = Xall[pairs[p]]
-        _, G, H = _lib_contact(Xp, is_ee[p], eps[p], dhat, kappa * dt * dt)
+        t, G, H = _lib_contact(Xp, is_ee[p], eps[p], dhat, kappa * dt * dt)
+        assert types[p] == t, (p, int(types[p]), t)
         scale = max(np.abs(H).max(), 1e-300)
         k = 0
         for i in range(4):
