@@ -474,14 +474,24 @@ __device__ __forceinline__ void cluster_product_mma(const unsigned char* slot, c
 // rounds every entry relative to O(1), and M = D (D^-1 M D^-1) D is recovered
 // in the apply. Entry (a, b) comes from the stored upper 3x3 block of nodes
 // (min, max) and is scaled as stored row times stored column.
-__global__ void k_pack_inverse_bf16(int clusters, const float* __restrict__ inv, unsigned char* __restrict__ out)
+// One CTA per cluster: the FP32 inverse staged in shared memory by 16-byte
+// loads, then each thread writes 8 consecutive BF16 entries of one tile row
+// (one 16-byte store): 6 tiles x 16 rows x 2 halves = 192 threads.
+constexpr int PACK_THREADS = 192;
+__global__ void __launch_bounds__(PACK_THREADS) k_pack_inverse_bf16(int clusters, const float* __restrict__ inv,
+                                                                    unsigned char* __restrict__ out)
 {
     const int c = blockIdx.x;
     if(c >= clusters)
         return;
-    __shared__ float S[BANK * 3];  // 1 / D
-    const float*   M = inv + (size_t)c * SYM * 9;
-    unsigned char* o = out + (size_t)c * INV16_BYTES;
+    __shared__ float4 Ms4[SYM * 9 / 4];
+    __shared__ float  S[BANK * 3];  // 1 / D
+    const float4*  src = reinterpret_cast<const float4*>(inv + (size_t)c * SYM * 9);
+    unsigned char* o   = out + (size_t)c * INV16_BYTES;
+    for(int i = threadIdx.x; i < SYM * 9 / 4; i += PACK_THREADS)
+        Ms4[i] = src[i];
+    __syncthreads();
+    const float* M = reinterpret_cast<const float*>(Ms4);
     if(threadIdx.x < BANK * 3)
     {
         const int   nd = threadIdx.x / 3, a = threadIdx.x % 3;
@@ -491,21 +501,27 @@ __global__ void k_pack_inverse_bf16(int clusters, const float* __restrict__ inv,
         reinterpret_cast<float*>(o)[threadIdx.x] = Dv;
     }
     __syncthreads();
-    for(int e = threadIdx.x; e < 6 * 256; e += blockDim.x)
+    const int t = threadIdx.x >> 5, row = (threadIdx.x >> 1) & 15, half = threadIdx.x & 1;
+    const int I = t < 3 ? 0 : (t < 5 ? 1 : 2);
+    const int J = t - (I * 3 - I * (I + 1) / 2);
+    const int a = I * 16 + row, na = a / 3, pa = a % 3;
+    uint32_t  w[4];
+#pragma unroll
+    for(int k = 0; k < 8; k += 2)
     {
-        const int t = e >> 8, row = (e >> 4) & 15, col = e & 15;
-        const int I = t < 3 ? 0 : (t < 5 ? 1 : 2);
-        const int J = t - (I * 3 - I * (I + 1) / 2);
-        const int a = I * 16 + row, b = J * 16 + col;
-        const int na = a / 3, pa = a % 3, nb = b / 3, pb = b % 3;
-        float     v;
-        if(na <= nb)
-            v = M[sym_index(na, nb) * 9 + pb * 3 + pa] * S[a] * S[b];
-        else
-            v = M[sym_index(nb, na) * 9 + pa * 3 + pb] * S[b] * S[a];
-        *reinterpret_cast<__nv_bfloat16*>(o + INV16_SCALE_BYTES + t * INV16_TILE_BYTES + tile_off(row, col >> 3) +
-                                          (col & 7) * 2) = __float2bfloat16_rn(v);
+        float v2[2];
+#pragma unroll
+        for(int u = 0; u < 2; ++u)
+        {
+            const int b = J * 16 + half * 8 + k + u, nb = b / 3, pb = b % 3;
+            v2[u] = na <= nb ? M[sym_index(na, nb) * 9 + pb * 3 + pa] * S[a] * S[b]
+                             : M[sym_index(nb, na) * 9 + pa * 3 + pb] * S[b] * S[a];
+        }
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v2[0], v2[1]);
+        w[k >> 1]              = *reinterpret_cast<const uint32_t*>(&h);
     }
+    *reinterpret_cast<uint4*>(o + INV16_SCALE_BYTES + t * INV16_TILE_BYTES + tile_off(row, half)) =
+        make_uint4(w[0], w[1], w[2], w[3]);
 }
 
 __device__ __forceinline__ void cluster_product(const float* M, const float (*r)[3], int lane, float out[3])
@@ -1176,7 +1192,7 @@ void mas_pack_bf16(b2s_solver* s)
     M.inv16.resize((size_t)M.clusters * INV16_BYTES);
     if(M.clusters > 0)
     {
-        k_pack_inverse_bf16<<<M.clusters, 128, 0, s->stream>>>(M.clusters, M.inv.data(), M.inv16.data());
+        k_pack_inverse_bf16<<<M.clusters, PACK_THREADS, 0, s->stream>>>(M.clusters, M.inv.data(), M.inv16.data());
         B2S_CHECK_LAUNCH();
     }
 }
