@@ -87,6 +87,10 @@ int b2s_spmv(b2s_solver* s, const double* d_x, double* d_y, double* h_dot /* may
  * reductions in any order), x . y accumulated in FP64 (h_dot, host, may be
  * NULL). No counterpart in the reference (which runs the SpMV in FP64 only). */
 int b2s_spmv_mixed(b2s_solver* s, const float* d_x, float* d_y, double* h_dot /* may be NULL */);
+/* Measurement: the FP32 SpMV kernel (with its fused dot) launched `launches`
+ * times back to back on the assembled matrix, CUDA events on the solver's
+ * stream around the batch; *h_avg_ms = the average launch duration. */
+int b2s_spmv_mixed_timing(b2s_solver* s, int32_t launches, double* h_avg_ms);
 
 /* ---- MAS preconditioner ----------------------------------------------------------
  * Initialisation: replaces FEMMASPreconditioner::do_init ->

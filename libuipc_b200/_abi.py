@@ -118,6 +118,7 @@ SIGNATURES = {
     "b2s_get_upper_bsr": (C.c_int, [vp, vp, vp, vp]),
     "b2s_spmv": (C.c_int, [vp, vp, vp, dp]),
     "b2s_spmv_mixed": (C.c_int, [vp, vp, vp, dp]),
+    "b2s_spmv_mixed_timing": (C.c_int, [vp, i32, C.POINTER(C.c_double)]),
     "b2s_mas_init": (C.c_int, [vp, i32, i32, vp, vp, i32, vp, vp]),
     "b2s_mas_info": (C.c_int, [vp, i32p, i32p]),
     "b2s_mas_get_hierarchy": (C.c_int, [vp, vp, vp, vp]),

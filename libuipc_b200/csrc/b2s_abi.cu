@@ -269,6 +269,17 @@ int b2s_spmv_mixed(b2s_solver* s, const float* x, float* y, double* h_dot)
                    });
 }
 
+int b2s_spmv_mixed_timing(b2s_solver* s, int32_t launches, double* h_avg_ms)
+{
+    return guarded(s,
+                   [&]
+                   {
+                       B2S_REQUIRE(s->A.valid, B2S_ERR_STATE, "no assembled matrix");
+                       B2S_REQUIRE(h_avg_ms, B2S_ERR_ARGUMENT, "null output");
+                       *h_avg_ms = b2s::spmv_mixed_timing(s, launches);
+                   });
+}
+
 int b2s_mas_init(b2s_solver* s, int32_t off, int32_t vn, const int32_t* adj_start, const int32_t* adj_list,
                  int32_t N, const int32_t* p2r, const int32_t* r2p)
 {

@@ -311,6 +311,7 @@ void precond_apply(b2s_solver* s, const double* r, double* z);
 void precond_launch(b2s_solver* s, const double* r, double* z);  // queued, no sync
 void precond_apply_mixed(b2s_solver* s, const float* r, float* z);
 void spmv_mixed(b2s_solver* s, const float* x, float* y, double* d_dot);
+double spmv_mixed_timing(b2s_solver* s, int launches);
 void check_device_errors(b2s_solver* s);
 
 // message of the last failed call made without a solver handle (read back

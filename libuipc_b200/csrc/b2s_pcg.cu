@@ -957,6 +957,39 @@ void spmv_mixed(b2s_solver* s, const float* x, float* y, double* d_dot)
     B2S_CHECK_LAUNCH();
 }
 
+// the FP32 SpMV (with its fused dot) launched back to back on the solver's
+// stream, events around the batch: the kernel's average launch duration on
+// the assembled matrix (the padded vectors' values do not change its work)
+double spmv_mixed_timing(b2s_solver* s, int launches)
+{
+    Matrix&       A  = s->A;
+    PcgState&     P  = s->pcg;
+    const int32_t nb = A.nb;
+    cudaStream_t  st = s->stream;
+    B2S_REQUIRE(launches > 0, B2S_ERR_ARGUMENT, "launch count must be positive");
+    ensure_f32_planes(s);
+    ensure_reduction(P.red, std::max(spmv_grid(A.nnz), reduction_grid()), 2);
+    P.p32.resize(4 * (size_t)nb, 1.1);
+    P.Ap32.resize(4 * (size_t)nb, 1.1);
+    s->dot_out.resize(4);
+    B2S_CUDA(cudaMemsetAsync(P.p32.data(), 0, sizeof(float) * 4 * (size_t)nb, st));
+    B2S_CUDA(cudaMemsetAsync(P.Ap32.data(), 0, sizeof(float) * 4 * (size_t)nb, st));
+    spmv_f32_launch(s, A, P.p32.data(), P.Ap32.data(), P.red, s->dot_out.data(), nullptr);  // warm-up
+    cudaEvent_t e0, e1;
+    B2S_CUDA(cudaEventCreate(&e0));
+    B2S_CUDA(cudaEventCreate(&e1));
+    B2S_CUDA(cudaEventRecord(e0, st));
+    for(int i = 0; i < launches; ++i)
+        spmv_f32_launch(s, A, P.p32.data(), P.Ap32.data(), P.red, s->dot_out.data(), nullptr);
+    B2S_CUDA(cudaEventRecord(e1, st));
+    B2S_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    B2S_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    B2S_CUDA(cudaEventDestroy(e0));
+    B2S_CUDA(cudaEventDestroy(e1));
+    return (double)ms / launches;
+}
+
 // r, z: 3 floats per node (the ABI's layout), padded around the apply
 void precond_apply_mixed(b2s_solver* s, const float* r, float* z)
 {

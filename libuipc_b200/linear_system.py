@@ -106,6 +106,13 @@ class Solver:
         self._check(self.lib.b2s_spmv(self.h, _ptr(x), _ptr(y), C.byref(d) if with_dot else None))
         return d.value if with_dot else None
 
+    def spmv_mixed_timing(self, launches: int = 50) -> float:
+        """Average duration [ms] of the FP32 SpMV kernel launched back to back
+        on the assembled matrix (b2s_spmv_mixed_timing)."""
+        ms = C.c_double()
+        self._check(self.lib.b2s_spmv_mixed_timing(self.h, int(launches), C.byref(ms)))
+        return float(ms.value)
+
     def spmv_mixed(self, x32, y32, with_dot: bool = False):
         """y = A x as the mixed-precision PCG computes it (FP32 vectors)."""
         d = C.c_double(0.0)

@@ -452,3 +452,26 @@ def test_mixed_spmv_bf16_apply_consistent(solver, cuda, cube10):
     x = torch.zeros_like(b)
     st = solver.pcg(b, x, tol=1e-4, stop_rule=_abi.B2S_STOP_RELRES, precision=_abi.B2S_PRECISION_MIXED)
     assert st["converged"] == 1
+
+
+def test_spmv_timing_utility(solver, cuda, cube10):
+    """b2s_spmv_mixed_timing: a positive average launch time, and the solver
+    still solves the assembled system afterwards (the batch writes only its
+    own scratch)."""
+    import torch
+
+    from libuipc_b200 import _abi
+    from libuipc_b200.linear_system import partition_maps, partition_rcb
+
+    s = cube10
+    solver.assemble(s.n_verts, to_dev(s.rows, cuda), to_dev(s.cols, cuda), to_dev(s.vals, cuda))
+    ms = solver.spmv_mixed_timing(20)
+    assert 0.0 < ms < 10.0
+    p2r, r2p = partition_maps(partition_rcb(s.positions))
+    solver.mas_init(0, s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
+    solver.precond_assemble(_abi.B2S_PRECOND_MAS)
+    b = to_dev(s.b, cuda)
+    x = torch.zeros_like(b)
+    st = solver.pcg(b, x, tol=1e-6, stop_rule=_abi.B2S_STOP_RELRES, precision=_abi.B2S_PRECISION_MIXED,
+                    replace_every=20)
+    assert st["converged"] == 1
