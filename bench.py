@@ -421,6 +421,10 @@ def full_scale_run(dev, n_systems: int = 4, scene_kw: dict | None = None) -> dic
             # block count and the history length change between steps) and is
             # not timed
             for timed in (False, True):
+                # the untimed pass runs with the solver's stage events (its
+                # breakdown is reported); the timed one without
+                solver.set_timing(not timed)
+                solver.reset_timers()
                 x = torch.zeros_like(b)
                 torch.cuda.synchronize()
                 ev0.record(stream)
@@ -432,8 +436,12 @@ def full_scale_run(dev, n_systems: int = 4, scene_kw: dict | None = None) -> dic
                                 replace_every=50, x0_given=mode != "plain")
                 ev1.record(stream)
                 ev1.synchronize()
+                if not timed:
+                    tm = solver.timers()
             rec[mode] = {"ms": ev0.elapsed_time(ev1), "pcg_iterations": int(st["iterations_exact"]),
-                         "rel_res": float(st["rel_res"])}
+                         "rel_res": float(st["rel_res"]), "replacements": int(st.get("replacements", 0)),
+                         "stages_ms": {"assemble": tm["assemble_ms"], "precond_build": tm["precond_build_ms"],
+                                       "pcg": tm["pcg_ms"]}}
         if "U" not in info:
             info["U"] = solver.matrix_info()[1]
         per.append(rec)
