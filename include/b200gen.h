@@ -58,6 +58,18 @@ int64_t b2gen_num_triplets(const b2gen_mesh* m);
 int b2gen_system(b2gen_mesh* m, const double* d_x, const double* d_xtilde, int32_t* d_rows, int32_t* d_cols,
                  double* d_vals, double* d_grad, void* stream);
 
+/* The line search after the solve (engine/advance_ipc.cu:487-570), for a tet
+ * mesh: the energy whose gradient and Hessian b2gen_system writes
+ * (1/2 m |x - x_tilde|^2 + dt^2 vol Psi_SNH + dt^2 kappa b(d^2) of the ground
+ * candidates; infinite when a candidate is at or below the plane), summed in a
+ * fixed order, at the device state d_x; and the largest step along d_dx before
+ * a ground candidate reaches the plane, as the vertex / half-plane trajectory
+ * filter computes it (collision_detection/filters/
+ * easy_vertex_half_plane_trajectory_filter.cu:81-145: (1 - 0.1) of the time
+ * of impact, capped at 1). */
+int b2gen_energy(b2gen_mesh* m, const double* d_x, const double* d_xtilde, double* h_energy, void* stream);
+int b2gen_ground_toi(b2gen_mesh* m, const double* d_x, const double* d_dx, double* h_alpha, void* stream);
+
 const char* b2gen_last_error(void);
 
 /* ---- cloth (codim-2D) and affine bodies ------------------------------------------

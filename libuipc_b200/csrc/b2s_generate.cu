@@ -328,10 +328,106 @@ __global__ void k_fixed(int64_t T, int nv, const uint8_t* __restrict__ fixed, co
 }
 
 int grid_of(int64_t n) { return (int)((n + GEN_BLOCK - 1) / GEN_BLOCK); }
+
+// ---- energy and the ground's time of impact (the line search after the solve) ----
+// per-term energies: kinetic 1/2 m |x - x_tilde|^2 per vertex, dt^2 vol Psi(F)
+// per tet with Psi = mu/2 (|F|^2 - 3) - mu (J - 1) + lambda/2 (J - 1)^2 (the
+// potential whose derivatives k_elastic writes), dt^2 kappa b(d^2) per ground
+// candidate (infinite at or below the plane)
+__global__ void k_energy_terms(int nv, int nt, int ng, const int32_t* __restrict__ tets, const double* __restrict__ vol,
+                               const double* __restrict__ G, const double* __restrict__ mass,
+                               const int32_t* __restrict__ ground, const double* __restrict__ x,
+                               const double* __restrict__ xt, double mu, double lambda, double dt2, double ground_y,
+                               double dhat, double kappa, double* __restrict__ e)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < nv)
+    {
+        double d2 = 0.0;
+        for(int a = 0; a < 3; ++a)
+        {
+            const double d = x[i * 3 + a] - xt[i * 3 + a];
+            d2 += d * d;
+        }
+        e[i] = 0.5 * mass[i] * d2;
+    }
+    else if(i < (int64_t)nv + nt)
+    {
+        const int64_t  t  = i - nv;
+        const int32_t* T  = tets + t * 4;
+        const double*  Gs = G + t * 12;
+        double         F[9] = {0};
+        for(int q = 0; q < 4; ++q)
+            for(int a = 0; a < 3; ++a)
+                for(int b = 0; b < 3; ++b)
+                    F[a + 3 * b] += x[T[q] * 3 + a] * Gs[q * 3 + b];
+        const double J = F[0] * (F[4] * F[8] - F[7] * F[5]) - F[3] * (F[1] * F[8] - F[7] * F[2]) +
+                         F[6] * (F[1] * F[5] - F[4] * F[2]);
+        double f2 = 0.0;
+        for(int k = 0; k < 9; ++k)
+            f2 += F[k] * F[k];
+        const double psi = 0.5 * mu * (f2 - 3.0) - mu * (J - 1.0) + 0.5 * lambda * (J - 1.0) * (J - 1.0);
+        e[i]             = dt2 * vol[t] * psi;
+    }
+    else if(i < (int64_t)nv + nt + ng)
+    {
+        const int32_t g = ground[i - nv - nt];
+        const double  d = x[(int64_t)g * 3 + 1] - ground_y;
+        double        v = 0.0;
+        if(!(d > 0.0))
+            v = INFINITY;
+        else if(d < dhat)
+        {
+            const double D = d * d, Dh = dhat * dhat, tt = D - Dh;
+            v              = -dt2 * kappa * tt * tt * log(D / Dh);
+        }
+        e[i] = v;
+    }
+}
+
+// one CTA: each thread sums a fixed strided subset in order, then a fixed
+// shared-memory tree (or the minimum, with take_min)
+constexpr int SUM_THREADS = 1024;
+__global__ void __launch_bounds__(SUM_THREADS) k_fixed_reduce(int64_t n, const double* __restrict__ v, int take_min,
+                                                              double* __restrict__ out)
+{
+    __shared__ double sh[SUM_THREADS];
+    double            acc = take_min ? INFINITY : 0.0;
+    for(int64_t i = threadIdx.x; i < n; i += SUM_THREADS)
+        acc = take_min ? fmin(acc, v[i]) : acc + v[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for(int w = SUM_THREADS / 2; w > 0; w >>= 1)
+    {
+        if(threadIdx.x < w)
+            sh[threadIdx.x] = take_min ? fmin(sh[threadIdx.x], sh[threadIdx.x + w]) : sh[threadIdx.x] + sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if(threadIdx.x == 0)
+        *out = sh[0];
+}
+
+// time of impact with the ground plane (normal +y) of every candidate moving
+// along d: (1 - eta) (y - ground_y) / (-d_y) when it moves down, else 1.1
+__global__ void k_ground_toi(int ng, const int32_t* __restrict__ ground, const double* __restrict__ x,
+                             const double* __restrict__ dx, double ground_y, double eta, double* __restrict__ toi)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= ng)
+        return;
+    const int32_t g = ground[i];
+    const double  t = -dx[(int64_t)g * 3 + 1];  // approach speed along -normal
+    double        v = 1.1;
+    if(t > 0.0)
+        v = (x[(int64_t)g * 3 + 1] - ground_y) / t * (1.0 - eta);
+    toi[i] = v;
+}
 }  // namespace
 
 struct b2gen_mesh : DevMesh
 {
+    b2s::DBuf<double> terms;  // per-term energies / times of impact
+    b2s::DBuf<double> result;
 };
 
 extern "C" {
@@ -461,6 +557,78 @@ int b2gen_system(b2gen_mesh* m, const double* d_x, const double* d_xtilde, int32
             B2S_CHECK_LAUNCH();
         }
         B2S_CUDA(cudaStreamSynchronize(st));
+        return 0;
+    }
+    catch(const b2s::Error& e)
+    {
+        g_gen_err = e.what();
+        return e.code;
+    }
+    catch(const std::exception& e)
+    {
+        g_gen_err = e.what();
+        return B2S_ERR_CUDA;
+    }
+}
+
+int b2gen_energy(b2gen_mesh* m, const double* d_x, const double* d_xtilde, double* h_energy, void* stream)
+{
+    try
+    {
+        if(!m || !d_x || !d_xtilde || !h_energy)
+            throw b2s::Error(B2S_ERR_ARGUMENT, "b2gen_energy: null argument");
+        B2S_CUDA(cudaSetDevice(m->device));
+        cudaStream_t          st = static_cast<cudaStream_t>(stream);
+        const b2gen_material& c  = m->mat;
+        const int64_t         n  = (int64_t)m->nv + m->nt + m->ng;
+        m->terms.resize(n);
+        m->result.resize(1);
+        k_energy_terms<<<grid_of(n), GEN_BLOCK, 0, st>>>(m->nv, m->nt, m->ng, m->tets.data(), m->vol.data(),
+                                                         m->grad.data(), m->mass.data(),
+                                                         m->ng ? m->ground.data() : nullptr, d_x, d_xtilde, c.mu,
+                                                         c.lambda, c.dt * c.dt, c.ground_y, c.dhat, c.kappa,
+                                                         m->terms.data());
+        B2S_CHECK_LAUNCH();
+        k_fixed_reduce<<<1, SUM_THREADS, 0, st>>>(n, m->terms.data(), 0, m->result.data());
+        B2S_CHECK_LAUNCH();
+        B2S_CUDA(cudaMemcpyAsync(h_energy, m->result.data(), sizeof(double), cudaMemcpyDeviceToHost, st));
+        B2S_CUDA(cudaStreamSynchronize(st));
+        return 0;
+    }
+    catch(const b2s::Error& e)
+    {
+        g_gen_err = e.what();
+        return e.code;
+    }
+    catch(const std::exception& e)
+    {
+        g_gen_err = e.what();
+        return B2S_ERR_CUDA;
+    }
+}
+
+int b2gen_ground_toi(b2gen_mesh* m, const double* d_x, const double* d_dx, double* h_alpha, void* stream)
+{
+    try
+    {
+        if(!m || !d_x || !d_dx || !h_alpha)
+            throw b2s::Error(B2S_ERR_ARGUMENT, "b2gen_ground_toi: null argument");
+        *h_alpha = 1.0;
+        if(m->ng == 0)
+            return 0;
+        B2S_CUDA(cudaSetDevice(m->device));
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        m->terms.resize(m->ng);
+        m->result.resize(1);
+        k_ground_toi<<<grid_of(m->ng), GEN_BLOCK, 0, st>>>(m->ng, m->ground.data(), d_x, d_dx, m->mat.ground_y, 0.1,
+                                                           m->terms.data());
+        B2S_CHECK_LAUNCH();
+        k_fixed_reduce<<<1, SUM_THREADS, 0, st>>>(m->ng, m->terms.data(), 1, m->result.data());
+        B2S_CHECK_LAUNCH();
+        double toi = 1.1;
+        B2S_CUDA(cudaMemcpyAsync(&toi, m->result.data(), sizeof(double), cudaMemcpyDeviceToHost, st));
+        B2S_CUDA(cudaStreamSynchronize(st));
+        *h_alpha = toi < 1.0 ? toi : 1.0;
         return 0;
     }
     catch(const b2s::Error& e)

@@ -42,6 +42,10 @@ def _lib():
         lib.b2gen_system.restype = C.c_int
         lib.b2gen_last_error.argtypes = []
         lib.b2gen_last_error.restype = C.c_char_p
+        lib.b2gen_energy.argtypes = [vp, vp, vp, C.POINTER(C.c_double), vp]
+        lib.b2gen_energy.restype = C.c_int
+        lib.b2gen_ground_toi.argtypes = [vp, vp, vp, C.POINTER(C.c_double), vp]
+        lib.b2gen_ground_toi.restype = C.c_int
         i32 = C.c_int32
         lib.b2gen_shell_create.argtypes = [C.c_int, i32, i32, vp, vp, vp, vp, C.POINTER(ShellMaterial),
                                            C.POINTER(vp)]
@@ -133,6 +137,25 @@ class GpuTetMesh:
         if rc != 0:
             raise RuntimeError("b2gen_system: " + lib.b2gen_last_error().decode())
         return self.grad
+
+    def energy(self, x, x_tilde, stream=None) -> float:
+        """The energy b2gen_system differentiates, at device state x."""
+        st = stream if stream is not None else self.torch.cuda.current_stream(self.dev).cuda_stream
+        e = C.c_double()
+        rc = _lib().b2gen_energy(self.h, x.contiguous().data_ptr(), x_tilde.contiguous().data_ptr(), C.byref(e), st)
+        if rc != 0:
+            raise RuntimeError("b2gen_energy: " + _lib().b2gen_last_error().decode())
+        return float(e.value)
+
+    def ground_toi(self, x, dx, stream=None) -> float:
+        """Largest step (<= 1) along dx before a ground candidate reaches the
+        plane, with the trajectory filter's 10 % margin."""
+        st = stream if stream is not None else self.torch.cuda.current_stream(self.dev).cuda_stream
+        a = C.c_double()
+        rc = _lib().b2gen_ground_toi(self.h, x.contiguous().data_ptr(), dx.contiguous().data_ptr(), C.byref(a), st)
+        if rc != 0:
+            raise RuntimeError("b2gen_ground_toi: " + _lib().b2gen_last_error().decode())
+        return float(a.value)
 
     def close(self):
         if self.h:

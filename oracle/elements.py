@@ -349,3 +349,33 @@ def contact_element(X, is_ee, eps, dhat, k):
         return kind, B1 * gD, (B2 + B1 / (2 * D)) * np.outer(gD, gD)
     w, V = np.linalg.eigh(0.5 * (H + H.T))
     return kind, G, (V * np.maximum(w, 0)) @ V.T
+
+
+# ---- tet-mesh energy (the line search's) ------------------------------------------
+def tet_energy(rest, tets, x, x_tilde, mu, lam, rho, dt, ground=None, ground_y=0.0, dhat=1e-3, kappa=1e9):
+    """Kinetic (lumped mass rho V / 4 per corner) + dt^2 V Psi_SNH (Psi = mu/2
+    (|F|^2 - 3) - mu (J - 1) + lambda/2 (J - 1)^2, the simplified stable
+    Neo-Hookean of finite_element/constitutions/sym/simplified_stable_neo_hookean_3d.inl)
+    + dt^2 kappa b(d^2) of the ground candidates (b(D) = -(D - Dh)^2 log(D/Dh)),
+    in numpy (FP64, numpy's summation order)."""
+    rest = np.asarray(rest).reshape(-1, 3)
+    x = np.asarray(x).reshape(-1, 3)
+    xt = np.asarray(x_tilde).reshape(-1, 3)
+    T = np.asarray(tets)
+    Dm = np.stack([rest[T[:, q]] - rest[T[:, 0]] for q in (1, 2, 3)], axis=2)
+    vol = np.linalg.det(Dm) / 6.0
+    Ds = np.stack([x[T[:, q]] - x[T[:, 0]] for q in (1, 2, 3)], axis=2)
+    F = Ds @ np.linalg.inv(Dm)
+    J = np.linalg.det(F)
+    psi = 0.5 * mu * ((F * F).sum(axis=(1, 2)) - 3) - mu * (J - 1) + 0.5 * lam * (J - 1) ** 2
+    mass = np.zeros(len(x))
+    np.add.at(mass, T.reshape(-1), np.repeat(rho * vol / 4.0, 4))
+    e = 0.5 * (mass * ((x - xt) ** 2).sum(1)).sum() + dt * dt * (vol * psi).sum()
+    if ground is not None:
+        d = x[np.asarray(ground), 1] - ground_y
+        if (d <= 0).any():
+            return np.inf
+        a = d < dhat
+        D, Dh = d[a] ** 2, dhat * dhat
+        e += dt * dt * kappa * (-(D - Dh) ** 2 * np.log(D / Dh)).sum()
+    return float(e)
