@@ -475,3 +475,34 @@ def test_spmv_timing_utility(solver, cuda, cube10):
     st = solver.pcg(b, x, tol=1e-6, stop_rule=_abi.B2S_STOP_RELRES, precision=_abi.B2S_PRECISION_MIXED,
                     replace_every=20)
     assert st["converged"] == 1
+
+
+def test_mas_on_the_graph_partition(solver, cuda, cube10):
+    """The MAS built on b2s_partition_graph's parts (connectivity only, the
+    drop-in for mesh_partition's METIS call): the hierarchy equals the
+    oracle's on the same partition and the FP64 MAS-PCG stops within 2
+    iterations of the oracle's."""
+    import torch
+
+    from libuipc_b200 import _abi
+    from libuipc_b200.linear_system import partition_graph, partition_maps
+    from oracle import oracle as O
+
+    s = cube10
+    p2r, r2p = partition_maps(partition_graph(s.adj_start, s.adj_list))
+    solver.assemble(s.n_verts, to_dev(s.rows, cuda), to_dev(s.cols, cuda), to_dev(s.vals, cuda))
+    solver.mas_init(0, s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
+    solver.precond_assemble(_abi.B2S_PRECOND_MAS)
+    A = O.OracleMatrix(s.n_verts, s.rows, s.cols, s.vals)
+    M = O.OracleMAS(s.n_verts, s.adj_start, s.adj_list, p2r, r2p)
+    M.assemble(A, 0, 0)
+    beg, cnt, ct = solver.mas_hierarchy(s.n_verts)
+    obeg, ocnt = M.levels()
+    L, _ = solver.mas_info()
+    assert np.array_equal(beg[: L + 1], obeg[: L + 1]) and np.array_equal(ct, M.coarse_table())
+    _, info = O.pcg(A, s.b, precond=O.ORC_PRECOND_MAS, mas=M, tol=1e-6, stop_rule=O.ORC_STOP_RELRES)
+    b = to_dev(s.b, cuda)
+    x = torch.zeros_like(b)
+    st = solver.pcg(b, x, tol=1e-6, stop_rule=_abi.B2S_STOP_RELRES, check_interval=1)
+    assert st["converged"] == 1 and info["converged"] == 1
+    assert abs(st["iterations_exact"] - info["iterations"]) <= 2
