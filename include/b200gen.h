@@ -140,6 +140,22 @@ int b2gen_contacts_destroy(b2gen_contacts* c);
 int b2gen_contacts_types(b2gen_contacts* c, int8_t* h_types);
 int b2gen_contacts_system(b2gen_contacts* c, const double* d_x, int32_t* d_rows, int32_t* d_cols,
                           double* d_vals, double* d_grad, void* stream);
+/* The line search's contact term at device state d_x: the sum over the
+ * pairs of kappa dt^2 B(D) (times the edge-edge mollifier below eps), the
+ * energy b2gen_contacts_system differentiates, in a fixed order (the
+ * barrier energy of contact_system/contact_models/ipc_simplex_normal_contact.cu
+ * that the line search's compute_energy adds, engine/advance_ipc.cu:515-540). */
+int b2gen_contacts_energy(b2gen_contacts* c, const double* d_x, double* h_energy, void* stream);
+/* The trajectory filter's step bound over the pairs for the move
+ * alpha * d_dx from d_x (the simplex trajectory filter's filter_toi,
+ * collision_detection/filters/lbvh_simplex_trajectory_filter.cu:876-1010 with
+ * utils/distance/details/ccd.inl, reduced as
+ * global_trajectory_filter.cu:111-134): per pair a swept-AABB test expanded
+ * by dhat, then additive CCD (eta 0.1, thickness 0, at most 1000 advances);
+ * *h_toi = min(1, the smallest time of impact), as a fraction of the move.
+ * The candidate pairs are the caller's (no BVH broad phase here). */
+int b2gen_contacts_toi(b2gen_contacts* c, const double* d_x, const double* d_dx, double alpha, double* h_toi,
+                       void* stream);
 const char* b2gen_shell_last_error(void);
 
 #ifdef __cplusplus

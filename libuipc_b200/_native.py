@@ -72,6 +72,11 @@ def load_scene_lib() -> C.CDLL:
         lib.b2g_element_ortho.restype = C.c_double
         lib.b2g_element_contact.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double, vp, vp]
         lib.b2g_element_contact.restype = C.c_int
+        lib.b2g_contact_energy.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double]
+        lib.b2g_contact_energy.restype = C.c_double
+        lib.b2g_accd.argtypes = [vp, vp, C.c_int, C.c_double, C.c_double, C.c_int, C.c_double,
+                                 C.POINTER(C.c_double)]
+        lib.b2g_accd.restype = C.c_int
         # Matrix Market I/O (csrc/scene/matrix_market.h)
         i32, i64, pi32, pi64 = C.c_int32, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64)
         lib.b2io_write_block_matrix.argtypes = [C.c_char_p, i32, i64, vp, vp, vp, C.c_int]

@@ -4,6 +4,7 @@
 // host generator (csrc/scene/scene_gen.cpp: snh_derivatives, jacobi_eigen,
 // the kinetic / elastic / ground / fixed passes) per element; results agree
 // with it to rounding (FMA contraction on the device).
+#include "b2s_fixed_reduce.cuh"
 #include "b2s_internal.cuh"
 
 #include "../../include/b200gen.h"
@@ -385,28 +386,6 @@ __global__ void k_energy_terms(int nv, int nt, int ng, const int32_t* __restrict
     }
 }
 
-// one CTA: each thread sums a fixed strided subset in order, then a fixed
-// shared-memory tree (or the minimum, with take_min)
-constexpr int SUM_THREADS = 1024;
-__global__ void __launch_bounds__(SUM_THREADS) k_fixed_reduce(int64_t n, const double* __restrict__ v, int take_min,
-                                                              double* __restrict__ out)
-{
-    __shared__ double sh[SUM_THREADS];
-    double            acc = take_min ? INFINITY : 0.0;
-    for(int64_t i = threadIdx.x; i < n; i += SUM_THREADS)
-        acc = take_min ? fmin(acc, v[i]) : acc + v[i];
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for(int w = SUM_THREADS / 2; w > 0; w >>= 1)
-    {
-        if(threadIdx.x < w)
-            sh[threadIdx.x] = take_min ? fmin(sh[threadIdx.x], sh[threadIdx.x + w]) : sh[threadIdx.x] + sh[threadIdx.x + w];
-        __syncthreads();
-    }
-    if(threadIdx.x == 0)
-        *out = sh[0];
-}
-
 // time of impact with the ground plane (normal +y) of every candidate moving
 // along d: (1 - eta) (y - ground_y) / (-d_y) when it moves down, else 1.1
 __global__ void k_ground_toi(int ng, const int32_t* __restrict__ ground, const double* __restrict__ x,
@@ -589,7 +568,7 @@ int b2gen_energy(b2gen_mesh* m, const double* d_x, const double* d_xtilde, doubl
                                                          c.lambda, c.dt * c.dt, c.ground_y, c.dhat, c.kappa,
                                                          m->terms.data());
         B2S_CHECK_LAUNCH();
-        k_fixed_reduce<<<1, SUM_THREADS, 0, st>>>(n, m->terms.data(), 0, m->result.data());
+        b2s::k_fixed_reduce<<<1, b2s::SUM_THREADS, 0, st>>>(n, m->terms.data(), 0, m->result.data());
         B2S_CHECK_LAUNCH();
         B2S_CUDA(cudaMemcpyAsync(h_energy, m->result.data(), sizeof(double), cudaMemcpyDeviceToHost, st));
         B2S_CUDA(cudaStreamSynchronize(st));
@@ -623,7 +602,7 @@ int b2gen_ground_toi(b2gen_mesh* m, const double* d_x, const double* d_dx, doubl
         k_ground_toi<<<grid_of(m->ng), GEN_BLOCK, 0, st>>>(m->ng, m->ground.data(), d_x, d_dx, m->mat.ground_y, 0.1,
                                                            m->terms.data());
         B2S_CHECK_LAUNCH();
-        k_fixed_reduce<<<1, SUM_THREADS, 0, st>>>(m->ng, m->terms.data(), 1, m->result.data());
+        b2s::k_fixed_reduce<<<1, b2s::SUM_THREADS, 0, st>>>(m->ng, m->terms.data(), 1, m->result.data());
         B2S_CHECK_LAUNCH();
         double toi = 1.1;
         B2S_CUDA(cudaMemcpyAsync(&toi, m->result.data(), sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -853,4 +853,172 @@ B2_HD_NOINLINE int contact_grad_hess(const double* X, int is_ee, double eps, dou
             H[i * 12 + j] = c * D.g[i] * D.g[j];
     return type;
 }
+// ---- value-only distances, energy and continuous collision detection ------------
+B2_HD double d2_pp(const double* a, const double* b)
+{
+    double d[3];
+    sub3(a, b, d);
+    return dot3(d, d);
+}
+// |(p - e0) x (e1 - e0)|^2 / |e1 - e0|^2
+B2_HD double d2_pe(const double* p, const double* e0, const double* e1)
+{
+    double e[3], w[3], c[3];
+    sub3(e1, e0, e);
+    sub3(p, e0, w);
+    cross3(w, e, c);
+    return dot3(c, c) / dot3(e, e);
+}
+// ((q - a0) . n)^2 / |n|^2, n = u x v
+B2_HD double d2_plane(const double* q, const double* a0, const double* u, const double* v)
+{
+    double n[3], w[3];
+    cross3(u, v, n);
+    sub3(q, a0, w);
+    const double wn = dot3(w, n);
+    return wn * wn / dot3(n, n);
+}
+// squared distance of a pair by its closest-feature type (the value the
+// contact Jets carry)
+B2_HD double pair_d2(const double* X, int is_ee)
+{
+    int       v[4], nv = 0;
+    const int type = is_ee ? ee_type(X, v, &nv) : pt_type(X, v, &nv);
+    if(type == PAIR_PP)
+        return d2_pp(X + 3 * v[0], X + 3 * v[1]);
+    if(type == PAIR_PE)
+        return d2_pe(X + 3 * v[0], X + 3 * v[1], X + 3 * v[2]);
+    double u[3], w[3];
+    if(type == PAIR_PT)
+    {
+        sub3(X + 6, X + 3, u);
+        sub3(X + 9, X + 3, w);
+        return d2_plane(X, X + 3, u, w);
+    }
+    sub3(X + 3, X, u);
+    sub3(X + 9, X + 6, w);
+    return d2_plane(X + 6, X, u, w);
+}
+
+// barrier energy of one pair (k = kappa dt^2): B(D), times the edge-edge
+// mollifier (2 - c/eps) c/eps (c = |ea x eb|^2) below eps; 0 at or beyond dhat
+// (the energy whose gradient and Hessian contact_grad_hess returns)
+B2_HD double contact_energy(const double* X, int is_ee, double eps, double dhat, double k)
+{
+    const double D = pair_d2(X, is_ee), Dh = dhat * dhat;
+    if(!(D < Dh) || !(D > 0.0))
+        return 0.0;
+    double B0, B1, B2;
+    barrier_B(D, Dh, k, &B0, &B1, &B2);
+    if(is_ee)
+    {
+        double u[3], w[3], c[3];
+        sub3(X + 3, X, u);
+        sub3(X + 9, X + 6, w);
+        cross3(u, w, c);
+        const double cc = dot3(c, c);
+        if(cc < eps)
+        {
+            const double x = cc / eps;
+            return (2.0 - x) * x * B0;
+        }
+    }
+    return B0;
+}
+
+// the distance the CCD advances on: an edge-edge pair whose distance is not
+// above the thickness is a (nearly) parallel pair far apart, measured by its
+// closest endpoints instead
+B2_HD double ccd_d2(const double* X, int is_ee, double xi)
+{
+    double d2 = pair_d2(X, is_ee);
+    if(is_ee && d2 - xi * xi <= 0.0)
+    {
+        const double a = d2_pp(X, X + 6), b = d2_pp(X, X + 9), c = d2_pp(X + 3, X + 6), d = d2_pp(X + 3, X + 9);
+        d2 = fmin(fmin(a, b), fmin(c, d));
+    }
+    return d2;
+}
+
+// swept AABBs of the pair's two sides (point | triangle, edge | edge) over the
+// step X -> X + dX: true when they come within dist on every axis
+B2_HD bool ccd_broadphase(const double* X, const double* dX, int is_ee, double dist)
+{
+    const int na = is_ee ? 2 : 1;
+    for(int c = 0; c < 3; ++c)
+    {
+        double amin = 1e300, amax = -1e300, bmin = 1e300, bmax = -1e300;
+        for(int i = 0; i < 4; ++i)
+        {
+            const double p = X[3 * i + c], q = p + dX[3 * i + c];
+            double&      lo = i < na ? amin : bmin;
+            double&      hi = i < na ? amax : bmax;
+            lo              = fmin(lo, fmin(p, q));
+            hi              = fmax(hi, fmax(p, q));
+        }
+        if(amin - bmax > dist || bmin - amax > dist)
+            return false;
+    }
+    return true;
+}
+
+// Additive CCD of one pair (X0 the positions, dX0 its displacement over the
+// step): conservative advancement on the pair's distance (Li et al.,
+// Codimensional Incremental Potential Contact, 2021). The pair's mean
+// displacement is removed; l = the largest displacement of each side,
+// summed; each step advances by (1 - eta) (d^2 - xi^2) / ((d + xi) l), which no
+// motion bounded by l can cross; the loop ends with a hit when the distance
+// function falls below eta times its start (after the first step: the time
+// reached is the time of impact, the last step not taken) and without one
+// when the time passes toi_max. max_iter steps end it with a hit at the time
+// reached.
+B2_HD bool accd_pair(const double* X0, const double* dX0, int is_ee, double eta, double xi, int max_iter,
+                     double toi_max, double* toi)
+{
+    double X[12], dX[12], mov[3], n2[4];
+    for(int c = 0; c < 3; ++c)
+        mov[c] = (((dX0[c] + dX0[3 + c]) + dX0[6 + c]) + dX0[9 + c]) / 4.0;
+    for(int i = 0; i < 4; ++i)
+    {
+        for(int c = 0; c < 3; ++c)
+        {
+            X[3 * i + c]  = X0[3 * i + c];
+            dX[3 * i + c] = dX0[3 * i + c] - mov[c];
+        }
+        n2[i] = dot3(dX + 3 * i, dX + 3 * i);
+    }
+    const double l = is_ee ? sqrt(fmax(n2[0], n2[1])) + sqrt(fmax(n2[2], n2[3]))
+                           : sqrt(n2[0]) + sqrt(fmax(fmax(n2[1], n2[2]), n2[3]));
+    *toi = toi_max;
+    if(!(l > 0.0))
+        return false;
+    const double xi2 = xi * xi;
+    double       d2  = ccd_d2(X, is_ee, xi);
+    double       f   = d2 - xi2;
+    double       d   = sqrt(d2);
+    const double gap = eta * f / (d + xi);
+    double       t   = 0.0;
+    for(;;)
+    {
+        if(max_iter-- <= 0)
+        {
+            *toi = t;
+            return true;
+        }
+        const double tl = (1.0 - eta) * f / ((d + xi) * l);
+        for(int i = 0; i < 12; ++i)
+            X[i] += tl * dX[i];
+        d2 = ccd_d2(X, is_ee, xi);
+        f  = d2 - xi2;
+        d  = sqrt(d2);
+        if(t > 0.0 && f / (d + xi) < gap)
+            break;
+        t += tl;
+        if(t > toi_max)
+            return false;
+    }
+    *toi = t;
+    return true;
+}
+
 }  // namespace b2el

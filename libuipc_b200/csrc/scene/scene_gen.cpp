@@ -1519,4 +1519,15 @@ double b2g_element_ortho(const double* q, double kappa, double w, double* G9, do
     return b2el::ortho_energy(q, kappa);
 }
 
+double b2g_contact_energy(const double* X, int is_ee, double eps, double dhat, double k)
+{
+    return b2el::contact_energy(X, is_ee, eps, dhat, k);
+}
+
+int b2g_accd(const double* X, const double* dX, int is_ee, double eta, double xi, int max_iter, double toi_max,
+             double* toi)
+{
+    return b2el::accd_pair(X, dX, is_ee, eta, xi, max_iter, toi_max, toi) ? 1 : 0;
+}
+
 }  // extern "C"

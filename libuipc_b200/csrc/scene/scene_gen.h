@@ -117,6 +117,13 @@ double b2g_element_ortho(const double* q, double kappa, double w, double* G9, do
 // 4 vertices; returns the closest-feature type (0 PP, 1 PE, 2 PT, 3 EE) or -1
 // beyond dhat
 int b2g_element_contact(const double* X, int is_ee, double eps, double dhat, double k, double* G12, double* H144);
+// the pair's barrier energy (the energy b2g_element_contact differentiates)
+double b2g_contact_energy(const double* X, int is_ee, double eps, double dhat, double k);
+// additive CCD of the pair moving by dX[12] over the step (eta, thickness xi,
+// at most max_iter advances, no hit past toi_max): 1 and *toi on a hit, else 0
+// (*toi = toi_max)
+int b2g_accd(const double* X, const double* dX, int is_ee, double eta, double xi, int max_iter, double toi_max,
+             double* toi);
 
 #ifdef __cplusplus
 }

@@ -73,6 +73,10 @@ def _lib():
         lib.b2gen_contacts_types.restype = C.c_int
         lib.b2gen_contacts_system.argtypes = [vp, vp, vp, vp, vp, vp, vp]
         lib.b2gen_contacts_system.restype = C.c_int
+        lib.b2gen_contacts_energy.argtypes = [vp, vp, C.POINTER(C.c_double), vp]
+        lib.b2gen_contacts_energy.restype = C.c_int
+        lib.b2gen_contacts_toi.argtypes = [vp, vp, vp, C.c_double, C.POINTER(C.c_double), vp]
+        lib.b2gen_contacts_toi.restype = C.c_int
         lib.b2gen_shell_last_error.argtypes = []
         lib.b2gen_shell_last_error.restype = C.c_char_p
         lib._b2gen_declared = True
@@ -286,6 +290,31 @@ class GpuContacts:
         rc = lib.b2gen_contacts_system(self.h, x.data_ptr(), rows_ptr, cols_ptr, vals_ptr, grad.data_ptr(), st)
         if rc != 0:
             raise RuntimeError("b2gen_contacts_system: " + lib.b2gen_shell_last_error().decode())
+
+    def energy(self, x, stream=None) -> float:
+        """The pairs' barrier energy at device state x (the line search's
+        contact term), summed in a fixed order."""
+        import torch
+
+        st = stream if stream is not None else torch.cuda.current_stream(self.dev).cuda_stream
+        e = C.c_double()
+        rc = _lib().b2gen_contacts_energy(self.h, x.contiguous().data_ptr(), C.byref(e), st)
+        if rc != 0:
+            raise RuntimeError("b2gen_contacts_energy: " + _lib().b2gen_shell_last_error().decode())
+        return float(e.value)
+
+    def toi(self, x, dx, alpha: float = 1.0, stream=None) -> float:
+        """Largest fraction (<= 1) of the move alpha dx from x that the pairs
+        allow: additive CCD per pair after a swept-box test."""
+        import torch
+
+        st = stream if stream is not None else torch.cuda.current_stream(self.dev).cuda_stream
+        t = C.c_double()
+        rc = _lib().b2gen_contacts_toi(self.h, x.contiguous().data_ptr(), dx.contiguous().data_ptr(), float(alpha),
+                                       C.byref(t), st)
+        if rc != 0:
+            raise RuntimeError("b2gen_contacts_toi: " + _lib().b2gen_shell_last_error().decode())
+        return float(t.value)
 
     def types(self) -> np.ndarray:
         """Closest-feature type per pair at the last system (0 PP, 1 PE, 2 PT,

@@ -11,9 +11,12 @@ when the largest displacement component of d is at most velocity_tol * dt
 (newton/velocity_tol, 0.05 m/s: newton_tolerance/max_translation_checker.cu:43-62)
 and the time of impact did not cut the step (newton/ccd_tol = 1); a converged
 iteration takes its first trial without the energy test, as the reference does
-against rounding-level energy increases from a tiny d. The contact set of point-triangle /
-edge-edge pairs and their continuous collision detection are not part of this
-(the generator's tet meshes only meet the ground).
+against rounding-level energy increases from a tiny d. With ``contacts`` (a
+`gpu_scene.GpuContacts` set of point-triangle / edge-edge pairs over the same
+vertices) the energy adds the pairs' barrier and the step is also capped by
+the pairs' continuous collision detection (the simplex trajectory filter:
+additive CCD per pair, min(1, the smallest time of impact)); the candidate
+pairs are the caller's.
 """
 from __future__ import annotations
 
@@ -30,13 +33,20 @@ class LineSearchResult:
     converged: bool
 
 
-def line_search(mesh, x, d, x_tilde, dt: float, velocity_tol: float = 0.05, max_iter: int = 8) -> LineSearchResult:
+def line_search(mesh, x, d, x_tilde, dt: float, velocity_tol: float = 0.05, max_iter: int = 8,
+                contacts=None) -> LineSearchResult:
     """Move the device state ``x`` (in place) along ``d`` as the reference's
     line search does; returns the accepted step, the energies and whether the
     Newton iteration had converged."""
+    def energy(state):
+        e = mesh.energy(state, x_tilde)
+        return e + contacts.energy(state) if contacts is not None else e
+
     x0 = x.clone()
-    e0 = mesh.energy(x0, x_tilde)
+    e0 = energy(x0)
     toi = mesh.ground_toi(x0, d)
+    if contacts is not None:
+        toi = min(toi, contacts.toi(x0, d))
     alpha = min(1.0, toi)
     converged = float(d.abs().max()) <= velocity_tol * dt and toi >= 1.0
     e = e0
@@ -44,7 +54,7 @@ def line_search(mesh, x, d, x_tilde, dt: float, velocity_tol: float = 0.05, max_
     for trials in range(1, max_iter + 1):
         x.copy_(x0)
         x.add_(d, alpha=alpha)
-        e = mesh.energy(x, x_tilde)
+        e = energy(x)
         if converged or e <= e0:
             break
         alpha *= 0.5

@@ -351,6 +351,115 @@ def contact_element(X, is_ee, eps, dhat, k):
     return kind, G, (V * np.maximum(w, 0)) @ V.T
 
 
+def _pair_d2(X, is_ee):
+    kind, v = ee_type(X) if is_ee else pt_type(X)
+    return float(_dist([list(r) for r in X], kind, v))
+
+
+def contact_energy(X, is_ee, eps, dhat, k):
+    """Barrier energy of one pair X[4, 3] (k = kappa dt^2): B(D) of its
+    closest-feature squared distance, times the edge-edge mollifier
+    (2 - c/eps) c/eps, c = |ea x eb|^2, below eps; 0 at or beyond dhat."""
+    X = np.asarray(X, dtype=np.float64).reshape(4, 3)
+    D, Dh = _pair_d2(X, is_ee), dhat * dhat
+    if not (0 < D < Dh):
+        return 0.0
+    B0 = barrier(D, Dh, k)[0]
+    if is_ee:
+        c = _crs(_sub(list(X[1]), list(X[0])), _sub(list(X[3]), list(X[2])))
+        cc = _dt(c, c)
+        if cc < eps:
+            xx = cc / eps
+            return (2.0 - xx) * xx * B0
+    return B0
+
+
+def _ccd_d2(X, is_ee, xi):
+    d2 = _pair_d2(X, is_ee)
+    if is_ee and d2 - xi * xi <= 0:
+        # (nearly) parallel edges far apart: the closest endpoint pair
+        d2 = min(_d2_pp(list(X[a]), list(X[b])) for a, b in ((0, 2), (0, 3), (1, 2), (1, 3)))
+    return d2
+
+
+def ccd_broadphase(X, dX, is_ee, dist):
+    """Swept AABBs of the two sides (point | triangle, edge | edge) over the
+    step, apart by more than dist on some axis -> no contact possible
+    (collision_detection/filters/lbvh_simplex_trajectory_filter.cu:905-918,
+    utils/distance/details/ccd.inl point_triangle_ccd_broadphase)."""
+    X = np.asarray(X, dtype=np.float64).reshape(4, 3)
+    Y = X + np.asarray(dX, dtype=np.float64).reshape(4, 3)
+    a = [0, 1] if is_ee else [0]
+    b = [2, 3] if is_ee else [1, 2, 3]
+    pa = np.concatenate([X[a], Y[a]])
+    pb = np.concatenate([X[b], Y[b]])
+    return not (((pa.min(0) - pb.max(0)) > dist).any() or ((pb.min(0) - pa.max(0)) > dist).any())
+
+
+def accd_toi(X, dX, is_ee, eta=0.1, thickness=0.0, max_iter=1000, toi_max=1.1):
+    """(hit, toi) of one pair moving by dX over the step: additive CCD
+    (conservative advancement on the pair's distance, Li et al., Codimensional
+    Incremental Potential Contact, 2021), as the reference's trajectory
+    filter runs it (utils/distance/details/ccd.inl: point_triangle_ccd,
+    edge_edge_ccd; filters/lbvh_simplex_trajectory_filter.cu:876-1010):
+    the pair's mean displacement removed, l = the largest displacement of
+    each side summed, every step advances by (1 - eta) (d^2 - xi^2) /
+    ((d + xi) l), the loop ends when the distance function falls below
+    eta times its start (after the first step) -- hit at the time reached --
+    or when the time passes toi_max (no hit). Written step for step in the
+    library's own order of operations (mean over the pair's four vertices
+    in order)."""
+    X = [list(map(float, r)) for r in np.asarray(X, dtype=np.float64).reshape(4, 3)]
+    dX = [list(map(float, r)) for r in np.asarray(dX, dtype=np.float64).reshape(4, 3)]
+    mov = [(((dX[0][c] + dX[1][c]) + dX[2][c]) + dX[3][c]) / 4.0 for c in range(3)]
+    dX = [[r[c] - mov[c] for c in range(3)] for r in dX]
+    n2 = [_dt(r, r) for r in dX]
+    if is_ee:
+        l = np.sqrt(max(n2[0], n2[1])) + np.sqrt(max(n2[2], n2[3]))
+    else:
+        l = np.sqrt(n2[0]) + np.sqrt(max(n2[1], n2[2], n2[3]))
+    if not (l > 0):
+        return False, toi_max
+    xi2 = thickness * thickness
+    d2 = _ccd_d2(np.array(X), is_ee, thickness)
+    f = d2 - xi2
+    d = np.sqrt(d2)
+    gap = eta * f / (d + thickness)
+    t = 0.0
+    while True:
+        if max_iter <= 0:
+            return True, t
+        max_iter -= 1
+        tl = (1.0 - eta) * f / ((d + thickness) * l)
+        X = [[X[i][c] + tl * dX[i][c] for c in range(3)] for i in range(4)]
+        d2 = _ccd_d2(np.array(X), is_ee, thickness)
+        f = d2 - xi2
+        d = np.sqrt(d2)
+        if t > 0 and f / (d + thickness) < gap:
+            return True, t
+        t += tl
+        if t > toi_max:
+            return False, toi_max
+
+
+def pairs_toi(x, dx, pairs, is_ee, alpha, dhat, thickness=0.0, eta=0.1):
+    """The trajectory filter's step bound over a candidate list: per pair the
+    broadphase (expanded by dhat + thickness) and the additive CCD of
+    alpha dx, 1.1 for pairs without a hit; min(1, the smallest)
+    (collision_detection/global_trajectory_filter.cu:111-134)."""
+    x = np.asarray(x, dtype=np.float64).reshape(-1, 3)
+    dx = alpha * np.asarray(dx, dtype=np.float64).reshape(-1, 3)
+    best = 1.1
+    for p, ee in zip(np.asarray(pairs).reshape(-1, 4), is_ee):
+        X, dX = x[p], dx[p]
+        if not ccd_broadphase(X, dX, ee, dhat + thickness):
+            continue
+        hit, t = accd_toi(X, dX, ee, eta=eta, thickness=thickness)
+        if hit:
+            best = min(best, t)
+    return min(best, 1.0)
+
+
 # ---- tet-mesh energy (the line search's) ------------------------------------------
 def tet_energy(rest, tets, x, x_tilde, mu, lam, rho, dt, ground=None, ground_y=0.0, dhat=1e-3, kappa=1e9):
     """Kinetic (lumped mass rho V / 4 per corner) + dt^2 V Psi_SNH (Psi = mu/2

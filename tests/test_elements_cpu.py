@@ -166,3 +166,76 @@ def test_contact_beyond_dhat_is_zero():
     X = np.array([[0, 0, 2e-3], [0, 0, 0], [0.01, 0, 0], [0, 0.01, 0]], np.float64)
     t, G, H = _lib_contact(X, 0, 0.0, 1e-3, 1e5)
     assert t == -1 and not G.any() and not H.any()
+
+
+def _lib_energy(X, is_ee, eps, dhat, k):
+    return load_scene_lib().b2g_contact_energy(_ptr(np.ascontiguousarray(X, dtype=np.float64)), int(is_ee), eps,
+                                               dhat, k)
+
+
+def _lib_accd(X, dX, is_ee, eta=0.1, xi=0.0, max_iter=1000, toi_max=1.1):
+    t = C.c_double()
+    hit = load_scene_lib().b2g_accd(_ptr(np.ascontiguousarray(X, dtype=np.float64)),
+                                    _ptr(np.ascontiguousarray(dX, dtype=np.float64)), int(is_ee), eta, xi, max_iter,
+                                    toi_max, C.byref(t))
+    return bool(hit), t.value
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("kind", ["PT", "PE", "PP", "EE", "EE-parallel"])
+def test_contact_energy(seed, kind):
+    """The barrier energy (times the mollifier for near-parallel edges) equals
+    the oracle's, and its central difference is the element's gradient."""
+    rng = np.random.default_rng(500 + seed)
+    dhat, k = 1e-3, 1e9 * 1e-4
+    X, is_ee = _contact_case(kind, rng, dhat)
+    ea, eb = X[1] - X[0], X[3] - X[2]
+    eps = 1e-3 * (ea @ ea) * (eb @ eb)
+    e = _lib_energy(X, is_ee, eps, dhat, k)
+    eo = OE.contact_energy(X, is_ee, eps, dhat, k)
+    assert eo > 0 and abs(e - eo) <= 1e-12 * eo
+    _, G, _ = _lib_contact(X, is_ee, eps, dhat, k)
+    h = 1e-4 * dhat
+    fd = np.zeros(12)
+    for i in range(12):
+        Xp, Xm = X.copy().reshape(-1), X.copy().reshape(-1)
+        Xp[i] += h
+        Xm[i] -= h
+        fd[i] = (_lib_energy(Xp.reshape(4, 3), is_ee, eps, dhat, k) - _lib_energy(Xm.reshape(4, 3), is_ee, eps, dhat,
+                                                                                 k)) / (2 * h)
+    assert np.abs(fd - G).max() <= 1e-4 * np.abs(G).max()
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("kind", ["PT", "PE", "PP", "EE", "EE-parallel"])
+def test_additive_ccd(seed, kind):
+    """Additive CCD of a pair under random relative motion of a few times its
+    distance: hit and time of impact equal to the oracle's (to rounding), the
+    pair still apart at the time of impact, and no hit for pure translation."""
+    rng = np.random.default_rng(700 + seed)
+    dhat = 1e-3
+    X, is_ee = _contact_case(kind, rng, dhat)
+    hits = 0
+    for trial in range(8):
+        dX = rng.standard_normal((4, 3)) * dhat * rng.uniform(0.5, 4.0)
+        hit, t = _lib_accd(X, dX, is_ee)
+        ho, to = OE.accd_toi(X, dX, is_ee)
+        assert hit == ho and abs(t - to) <= 1e-13 * to
+        if hit:
+            hits += 1
+            assert 0.0 <= t <= 1.1
+            assert OE._pair_d2(X + t * dX, is_ee) > 0.0
+    assert _lib_accd(X, np.tile(rng.standard_normal(3), (4, 1)), is_ee) == (False, 1.1)
+
+
+def test_additive_ccd_straight_approach():
+    """A point 1 mm above a triangle moving 2 mm down along the normal: the
+    first advance covers (1 - eta) of the distance, the next one ends below
+    eta of it, so the time of impact is (1 - eta) / 2."""
+    X = np.array([[0.2e-2, 1e-3, 0.2e-2], [0.0, 0.0, 0.0], [1e-2, 0.0, 0.0], [0.0, 0.0, 1e-2]])
+    dX = np.zeros((4, 3))
+    dX[0, 1] = -2e-3
+    hit, t = _lib_accd(X, dX, 0)
+    assert hit and abs(t - 0.45) <= 1e-15
+    # moving away: no hit
+    assert _lib_accd(X, -dX, 0) == (False, 1.1)
