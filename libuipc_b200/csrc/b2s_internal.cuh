@@ -14,21 +14,6 @@ namespace b2s
 {
 constexpr int BANK = 16;                    // nodes per MAS cluster
 constexpr int SYM  = BANK * (BANK + 1) / 2;  // 136 upper 3x3 blocks per cluster
-
-// BF16 cluster inverses (mixed precision), per cluster: the FP32 factor
-// D = diag(M)^1/2 (48 floats), then the six upper 16x16 tiles (I <= J) of
-// D^-1 M D^-1 in BF16, rows of 32 B with the two 16-B halves of row R swapped
-// when bit 2 of R is set (conflict-free ldmatrix phases)
-constexpr uint32_t INV16_SCALE_BYTES = BANK * 3 * sizeof(float);                  // 192
-constexpr uint32_t INV16_TILE_BYTES  = 16 * 16 * 2;                               // 512
-constexpr uint32_t INV16_BYTES       = INV16_SCALE_BYTES + 6 * INV16_TILE_BYTES;  // 3264
-// index of the upper tile (I, J), I <= J: (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
-__host__ __device__ __forceinline__ int tile_id(int I, int J) { return I * 3 - I * (I + 1) / 2 + J; }
-// byte offset of 16-B half `half` of row `row` inside a tile
-__host__ __device__ __forceinline__ uint32_t tile_off(int row, int half)
-{
-    return (uint32_t)row * 32u + ((uint32_t)(half ^ ((row >> 2) & 1)) << 4);
-}
 constexpr int MAX_LEVELS = 6;
 constexpr int NUM_SMS_HINT = 148;
 
@@ -193,6 +178,7 @@ struct MasState
     DBuf<int32_t> stiff_list;      // [clusters] the stiff clusters (first stiff_count entries)
     DBuf<int32_t> stiff_count;     // [1]
     DBuf<unsigned char> inv16;     // [clusters * 3264]: FP32 factor D (48) + six BF16 16x16 tiles of D^-1 inv D^-1
+    long long     inv16_generation = -1;  // assembly generation inv16 was packed from
     // coarse-level Galerkin matrices (upper BCOO per level, in level-local ids)
     Matrix        coarse[MAX_LEVELS];
     DBuf<int32_t> trip_rows, trip_cols;

@@ -374,8 +374,19 @@ __global__ void k_g_extract(int64_t U, const int32_t* rows, const int32_t* cols,
 // ---------------------------------------------------------------------------
 constexpr int APPLY_WARPS = 4;
 constexpr uint32_t INV_BYTES = SYM * 9 * sizeof(float);  // 4896, a multiple of 16
+constexpr uint32_t INV16_SCALE_BYTES = BANK * 3 * sizeof(float);                    // 192
+constexpr uint32_t INV16_TILE_BYTES  = 16 * 16 * 2;                                 // 512
+constexpr uint32_t INV16_BYTES       = INV16_SCALE_BYTES + 6 * INV16_TILE_BYTES;  // 3264
 constexpr int APPLY_STAGES_F32  = 2;
 constexpr int APPLY_STAGES_BF16 = 2;
+
+// index of the upper tile (I, J), I <= J: (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+__host__ __device__ __forceinline__ int tile_id(int I, int J) { return I * 3 - I * (I + 1) / 2 + J; }
+// byte offset of 16-B half `half` of row `row` inside a tile
+__host__ __device__ __forceinline__ uint32_t tile_off(int row, int half)
+{
+    return (uint32_t)row * 32u + ((uint32_t)(half ^ ((row >> 2) & 1)) << 4);
+}
 
 __device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t& a3)
 {
@@ -456,6 +467,61 @@ __device__ __forceinline__ void cluster_product_mma(const unsigned char* slot, c
             Zb[k1] = (c2 + c3) * D[k1];
         }
     }
+}
+
+// pack the FP32 inverse M of every cluster as D (FP32) + the BF16 tiles of
+// D^-1 M D^-1, D = diag(M)^1/2: the stored matrix has a unit diagonal, so BF16
+// rounds every entry relative to O(1), and M = D (D^-1 M D^-1) D is recovered
+// in the apply. Entry (a, b) comes from the stored upper 3x3 block of nodes
+// (min, max) and is scaled as stored row times stored column.
+// One CTA per cluster: the FP32 inverse staged in shared memory by 16-byte
+// loads, then each thread writes 8 consecutive BF16 entries of one tile row
+// (one 16-byte store): 6 tiles x 16 rows x 2 halves = 192 threads.
+constexpr int PACK_THREADS = 192;
+__global__ void __launch_bounds__(PACK_THREADS) k_pack_inverse_bf16(int clusters, const float* __restrict__ inv,
+                                                                    unsigned char* __restrict__ out)
+{
+    const int c = blockIdx.x;
+    if(c >= clusters)
+        return;
+    __shared__ float4 Ms4[SYM * 9 / 4];
+    __shared__ float  S[BANK * 3];  // 1 / D
+    const float4*  src = reinterpret_cast<const float4*>(inv + (size_t)c * SYM * 9);
+    unsigned char* o   = out + (size_t)c * INV16_BYTES;
+    for(int i = threadIdx.x; i < SYM * 9 / 4; i += PACK_THREADS)
+        Ms4[i] = src[i];
+    __syncthreads();
+    const float* M = reinterpret_cast<const float*>(Ms4);
+    if(threadIdx.x < BANK * 3)
+    {
+        const int   nd = threadIdx.x / 3, a = threadIdx.x % 3;
+        const float d  = M[sym_index(nd, nd) * 9 + a * 3 + a];
+        const float Dv = d > 0.f ? sqrtf(d) : 1.0f;
+        S[threadIdx.x] = 1.0f / Dv;
+        reinterpret_cast<float*>(o)[threadIdx.x] = Dv;
+    }
+    __syncthreads();
+    const int t = threadIdx.x >> 5, row = (threadIdx.x >> 1) & 15, half = threadIdx.x & 1;
+    const int I = t < 3 ? 0 : (t < 5 ? 1 : 2);
+    const int J = t - (I * 3 - I * (I + 1) / 2);
+    const int a = I * 16 + row, na = a / 3, pa = a % 3;
+    uint32_t  w[4];
+#pragma unroll
+    for(int k = 0; k < 8; k += 2)
+    {
+        float v2[2];
+#pragma unroll
+        for(int u = 0; u < 2; ++u)
+        {
+            const int b = J * 16 + half * 8 + k + u, nb = b / 3, pb = b % 3;
+            v2[u] = na <= nb ? M[sym_index(na, nb) * 9 + pb * 3 + pa] * S[a] * S[b]
+                             : M[sym_index(nb, na) * 9 + pa * 3 + pb] * S[b] * S[a];
+        }
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v2[0], v2[1]);
+        w[k >> 1]              = *reinterpret_cast<const uint32_t*>(&h);
+    }
+    *reinterpret_cast<uint4*>(o + INV16_SCALE_BYTES + t * INV16_TILE_BYTES + tile_off(row, half)) =
+        make_uint4(w[0], w[1], w[2], w[3]);
 }
 
 __device__ __forceinline__ void cluster_product(const float* M, const float (*r)[3], int lane, float out[3])
@@ -1035,7 +1101,7 @@ void mas_assemble(b2s_solver* s, int invert_mode)
 
 // z[off..off+vn) gets the MAS part of z = P r; Jacobi/identity elsewhere is
 // handled by the caller (collect kernel in the PCG, or precond_apply).
-// bf16: use the packed D + BF16 tiles of D^-1 M D^-1 (written by the cluster inverse).
+// bf16: use the packed D + BF16 tiles of D^-1 M D^-1 (mas_pack_bf16 first).
 template <typename VT>
 static void apply_levels_t(b2s_solver* s, const VT* r, const int* converged, bool bf16)
 {
@@ -1119,4 +1185,15 @@ void mas_apply_levels_f32(b2s_solver* s, const float* r, const int* converged, b
     apply_levels_t<float>(s, r, converged, bf16);
 }
 
+// BF16 diagonal-scaled copy of the current FP32 inverses
+void mas_pack_bf16(b2s_solver* s)
+{
+    MasState& M = s->mas;
+    M.inv16.resize((size_t)M.clusters * INV16_BYTES);
+    if(M.clusters > 0)
+    {
+        k_pack_inverse_bf16<<<M.clusters, PACK_THREADS, 0, s->stream>>>(M.clusters, M.inv.data(), M.inv16.data());
+        B2S_CHECK_LAUNCH();
+    }
+}
 }  // namespace b2s

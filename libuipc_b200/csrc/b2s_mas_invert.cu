@@ -35,8 +35,6 @@
 #include "b2s_internal.cuh"
 #include "b2s_tma.cuh"
 
-#include <cuda_bf16.h>
-
 #include <algorithm>
 
 namespace b2s
@@ -270,60 +268,12 @@ __constant__ TileOp c_xops[6] = {
     {8, 1, 1, {{8, 8, 2}}},
 };
 
-// The BF16 copy of the inverse the mixed-precision apply reads (layout of
-// INV16_BYTES): the FP32 factor D = diag(M)^1/2 (1 where the diagonal is not
-// positive), then the six upper tiles of D^-1 M D^-1, entry (a, b) taken as
-// the FP32 value stored for it (upper triangle of X) times 1/D of the stored
-// row, then of the stored column. One 16-byte store per tile half-row
-// (6 tiles x 16 rows x 2 halves over the warp's lanes).
-template <typename T>
-__device__ __forceinline__ void pack_bf16_tiles(const T* S, InvWarpSmem<T>& sm, int lane, unsigned char* __restrict__ o)
-{
-    constexpr int LD   = InvGeom<T>::LD;
-    float*        sinv = reinterpret_cast<float*>(sm.Tt);  // 48 floats; the temporary tile is spent
-    auto          val  = [&](int a, int b) -> float
-    { return a <= b ? (float)S[a * LD + b] : (float)S[b * LD + a]; };
-    for(int a = lane; a < NI; a += 32)
-    {
-        const float d  = val(a, a);
-        const float Dv = d > 0.f ? sqrtf(d) : 1.0f;
-        sinv[a]        = 1.0f / Dv;
-        reinterpret_cast<float*>(o)[a] = Dv;
-    }
-    __syncwarp();
-    for(int idx = lane; idx < 6 * 32; idx += 32)
-    {
-        const int t = idx >> 5, row = (idx >> 1) & 15, half = idx & 1;
-        const int I = t < 3 ? 0 : (t < 5 ? 1 : 2);
-        const int J = t - (I * 3 - I * (I + 1) / 2);
-        const int a = I * 16 + row, na = a / 3;
-        uint32_t  w[4];
-#pragma unroll
-        for(int k = 0; k < 8; k += 2)
-        {
-            float v2[2];
-#pragma unroll
-            for(int u = 0; u < 2; ++u)
-            {
-                const int b = J * 16 + half * 8 + k + u;
-                // stored row first: (v / D_row) / D_col
-                v2[u] = na <= b / 3 ? val(a, b) * sinv[a] * sinv[b] : val(a, b) * sinv[b] * sinv[a];
-            }
-            const __nv_bfloat162 h = __floats2bfloat162_rn(v2[0], v2[1]);
-            w[k >> 1]              = *reinterpret_cast<const uint32_t*>(&h);
-        }
-        *reinterpret_cast<uint4*>(o + INV16_SCALE_BYTES + t * INV16_TILE_BYTES + tile_off(row, half)) =
-            make_uint4(w[0], w[1], w[2], w[3]);
-    }
-    __syncwarp();
-}
-
 // Factorise and invert one cluster (the whole warp). Returns true when the
 // cluster is stiff (a pivot ratio below STIFF_PIVOT_RATIO, or a pivot that
 // is not positive).
 template <typename T, typename AfterScatter>
-__device__ bool invert_cluster(float* __restrict__ out, unsigned char* __restrict__ out16, InvWarpSmem<T>& sm,
-                               const SymPairs& pairs, int lane, AfterScatter after_scatter)
+__device__ bool invert_cluster(float* __restrict__ out, InvWarpSmem<T>& sm, const SymPairs& pairs, int lane,
+                               AfterScatter after_scatter)
 {
     constexpr int LD = InvGeom<T>::LD, TLD = InvGeom<T>::TLD;
     T*            S  = sm.S;
@@ -477,8 +427,6 @@ __device__ bool invert_cluster(float* __restrict__ out, unsigned char* __restric
         }
         out[e] = (float)S[row * LD + col];
     }
-    if(out16)
-        pack_bf16_tiles<T>(S, sm, lane, out16);
     return stiff;
 }
 
@@ -492,7 +440,7 @@ __device__ bool invert_cluster(float* __restrict__ out, unsigned char* __restric
 template <typename T>
 __global__ void __launch_bounds__(InvGeom<T>::WARPS * 32)
     k_cluster_inverse(int clusters, const double* __restrict__ hess, float* __restrict__ inv,
-                      unsigned char* __restrict__ inv16, const int32_t* __restrict__ list, const int32_t* __restrict__ list_count,
+                      const int32_t* __restrict__ list, const int32_t* __restrict__ list_count,
                       uint8_t* __restrict__ stiff, int32_t* __restrict__ stiff_list, int32_t* __restrict__ stiff_count,
                       int queue, int* err)
 {
@@ -536,8 +484,7 @@ __global__ void __launch_bounds__(InvGeom<T>::WARPS * 32)
         }
         // invert_cluster reads the staged blocks first; the next copy goes
         // out once they are in S (ordered by its first __syncwarp)
-        const bool st = invert_cluster<T>(inv + (size_t)cl * SYM * 9, inv16 ? inv16 + (size_t)cl * INV16_BYTES : nullptr,
-                                          sm[w], pairs, lane, [&]
+        const bool st = invert_cluster<T>(inv + (size_t)cl * SYM * 9, sm[w], pairs, lane, [&]
                                           {
                                               if(lane == 0 && i + W < n)
                                               {
@@ -585,21 +532,20 @@ void mas_invert_clusters(b2s_solver* s, int mode)
     M.stiff.resize(std::max(C, 1));
     M.stiff_list.resize(std::max(C, 1));
     M.stiff_count.resize(1);
-    M.inv16.resize((size_t)std::max(C, 1) * INV16_BYTES);  // the BF16 copy, written beside the FP32 inverse
     B2S_CUDA(cudaMemsetAsync(M.stiff_count.data(), 0, sizeof(int32_t), st));
     if(C <= 0)
         return;
     if(mode == B2S_INVERT_F64)
     {
         k_cluster_inverse<double><<<inverse_grid<double>(C), InvGeom<double>::WARPS * 32, 0, st>>>(
-            C, M.hess.data(), M.inv.data(), M.inv16.data(), nullptr, nullptr, M.stiff.data(), M.stiff_list.data(),
+            C, M.hess.data(), M.inv.data(), nullptr, nullptr, M.stiff.data(), M.stiff_list.data(),
             M.stiff_count.data(), 1, err);
         B2S_CHECK_LAUNCH();
         return;
     }
     k_cluster_inverse<float><<<inverse_grid<float>(C), InvGeom<float>::WARPS * 32, 0, st>>>(
-        C, M.hess.data(), M.inv.data(), M.inv16.data(), nullptr, nullptr, M.stiff.data(), M.stiff_list.data(),
-        M.stiff_count.data(), 1, err);
+        C, M.hess.data(), M.inv.data(), nullptr, nullptr, M.stiff.data(), M.stiff_list.data(), M.stiff_count.data(),
+        1, err);
     B2S_CHECK_LAUNCH();
     if(mode == B2S_INVERT_F32_ONLY)
         return;
@@ -607,8 +553,7 @@ void mas_invert_clusters(b2s_solver* s, int mode)
     // a small fixed grid walks the list (it returns at once when it is empty)
     const int grid = std::min(inverse_grid<double>(C), 2 * NUM_SMS_HINT);
     k_cluster_inverse<double><<<grid, InvGeom<double>::WARPS * 32, 0, st>>>(
-        C, M.hess.data(), M.inv.data(), M.inv16.data(), M.stiff_list.data(), M.stiff_count.data(), nullptr, nullptr,
-        nullptr, 0, err);
+        C, M.hess.data(), M.inv.data(), M.stiff_list.data(), M.stiff_count.data(), nullptr, nullptr, nullptr, 0, err);
     B2S_CHECK_LAUNCH();
 }
 }  // namespace b2s

@@ -30,6 +30,7 @@ int  spmv_grid(int64_t U);
 void ensure_reduction(Reduction& red, int grid, int nv);
 void mas_apply_levels(b2s_solver* s, const double* r, const int* converged);
 void mas_apply_levels_f32(b2s_solver* s, const float* r, const int* converged, bool bf16);
+void mas_pack_bf16(b2s_solver* s);
 void spmv_f32_launch(b2s_solver* s, const Matrix& A, const float* x, float* y, Reduction& red, double* d_dot,
                      const int* stop);
 void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_options& o, b2s_pcg_stats& st_out);
@@ -913,6 +914,15 @@ static void precond_launch_f32(b2s_solver* s, int kind, const float* r, float* z
     B2S_CHECK_LAUNCH();
 }
 
+static void ensure_bf16_inverses(b2s_solver* s)
+{
+    if(s->precond_kind == B2S_PRECOND_MAS && s->mas.inv16_generation != s->precond_generation)
+    {
+        mas_pack_bf16(s);
+        s->mas.inv16_generation = s->precond_generation;
+    }
+}
+
 // the FP32 copy of the value planes the mixed PCG's SpMV reads (once per assembly)
 static void ensure_f32_planes(b2s_solver* s)
 {
@@ -984,6 +994,7 @@ double spmv_mixed_timing(b2s_solver* s, int launches)
 void precond_apply_mixed(b2s_solver* s, const float* r, float* z)
 {
     B2S_REQUIRE(s->precond_kind >= 0, B2S_ERR_STATE, "precond_apply before b2s_precond_assemble");
+    ensure_bf16_inverses(s);
     ensure_reduction(s->red, reduction_grid(), 2);
     const int32_t nb = s->A.nb;
     PcgState&     P  = s->pcg;
@@ -1061,8 +1072,9 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
     const int64_t max_iter = o.max_iter > 0 ? o.max_iter : std::max<int64_t>(2 * n, 1);
     int           kind     = s->precond_kind;
 
-    // FP32 matrix planes (once per assembly)
+    // FP32 matrix planes, BF16 MAS inverses (once per assembly / build)
     ensure_f32_planes(s);
+    ensure_bf16_inverses(s);
 
     // r = b - A x0 (FP64), stored FP32
     if(o.x0_given)
@@ -1147,9 +1159,9 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
             ensure_iter_events(s, ci);
         if(use_graph)
         {
-            const void*   ptrs[12] = {x,          A.vals32.data(), A.rows.data(),     P.r32.data(),
+            const void*   ptrs[10] = {x,          A.vals32.data(), A.rows.data(),     P.r32.data(),
                                       s->mas.inv16.data(), s->dinv.data(), P.red.partials.data(), s->mas.Z.data(),
-                                      A.cols.data(), P.p32.data(), P.Ap32.data(), P.z32.data()};
+                                      A.cols.data(), P.p32.data()};
             const int64_t ints[6]  = {A.nnz, A.nb, kind, ci, s->mas.initialized ? s->mas.total : -1,
                                       s->mas.L + (s->timing ? 1000 : 0)};
             size_t hk = 1469598103934665603ull;
