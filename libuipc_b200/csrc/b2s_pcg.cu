@@ -1159,9 +1159,9 @@ void pcg_solve_mixed(b2s_solver* s, const double* b, double* x, const b2s_pcg_op
             ensure_iter_events(s, ci);
         if(use_graph)
         {
-            const void*   ptrs[10] = {x,          A.vals32.data(), A.rows.data(),     P.r32.data(),
+            const void*   ptrs[12] = {x,          A.vals32.data(), A.rows.data(),     P.r32.data(),
                                       s->mas.inv16.data(), s->dinv.data(), P.red.partials.data(), s->mas.Z.data(),
-                                      A.cols.data(), P.p32.data()};
+                                      A.cols.data(), P.p32.data(), P.Ap32.data(), P.z32.data()};
             const int64_t ints[6]  = {A.nnz, A.nb, kind, ci, s->mas.initialized ? s->mas.total : -1,
                                       s->mas.L + (s->timing ? 1000 : 0)};
             size_t hk = 1469598103934665603ull;
