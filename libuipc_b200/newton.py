@@ -51,11 +51,13 @@ def line_search(mesh, x, d, x_tilde, dt: float, velocity_tol: float = 0.05, max_
     converged = float(d.abs().max()) <= velocity_tol * dt and toi >= 1.0
     e = e0
     trials = 0
+    step = alpha  # the step of the state x holds (the last trial's)
     for trials in range(1, max_iter + 1):
+        step = alpha
         x.copy_(x0)
-        x.add_(d, alpha=alpha)
+        x.add_(d, alpha=step)
         e = energy(x)
         if converged or e <= e0:
             break
         alpha *= 0.5
-    return LineSearchResult(alpha=alpha, toi_alpha=toi, energy0=e0, energy=e, trials=trials, converged=converged)
+    return LineSearchResult(alpha=step, toi_alpha=toi, energy0=e0, energy=e, trials=trials, converged=converged)
