@@ -156,6 +156,33 @@ int b2gen_contacts_energy(b2gen_contacts* c, const double* d_x, double* h_energy
  * The candidate pairs are the caller's (no BVH broad phase here). */
 int b2gen_contacts_toi(b2gen_contacts* c, const double* d_x, const double* d_dx, double alpha, double* h_toi,
                        void* stream);
+/* Candidate detection of the line search's trajectory filter: the
+ * point-triangle (surface vertex, surface triangle) and edge-edge (surface
+ * edge pairs) candidates whose swept boxes over the move alpha * d_dx come
+ * within dhat (the far test of utils/distance/details/ccd.inl:
+ * point_triangle_ccd_broadphase / edge_edge_ccd_broadphase), pairs sharing a
+ * vertex excluded -- what the simplex trajectory filter collects with its BVH
+ * (collision_detection/filters/lbvh_simplex_trajectory_filter.cu:1100-1300).
+ * Here a uniform grid of the given cell size (about one surface edge length)
+ * hashed into buckets; the pairs come out in a fixed order (point-triangle by
+ * vertex, then edge-edge by edge, each by cell and primitive id), in the
+ * b2gen_contacts_create layout (p, t0, t1, t2) / (a0, a1, b0, b1).
+ * b2gen_trajectory_toi runs the detection and then the narrow phase of
+ * b2gen_contacts_toi over the candidates: min(1, the smallest time of impact).
+ * Vertex ids index the state vectors (3 doubles per vertex). */
+typedef struct b2gen_trajectory b2gen_trajectory;
+int b2gen_trajectory_create(int device, int32_t n_verts, int32_t n_surf_verts, const int32_t* surf_verts,
+                            int32_t n_surf_edges, const int32_t* surf_edges, int32_t n_surf_tris,
+                            const int32_t* surf_tris, double dhat, double cell, b2gen_trajectory** out);
+int b2gen_trajectory_destroy(b2gen_trajectory* t);
+/* h_counts[2]: point-triangle and edge-edge candidates found */
+int b2gen_trajectory_detect(b2gen_trajectory* t, const double* d_x, const double* d_dx, double alpha,
+                            int64_t* h_counts, void* stream);
+/* the last detection's candidates: h_pairs[4 * n], h_is_ee[n], n = the two counts summed */
+int b2gen_trajectory_pairs(b2gen_trajectory* t, int32_t* h_pairs, uint8_t* h_is_ee);
+int b2gen_trajectory_toi(b2gen_trajectory* t, const double* d_x, const double* d_dx, double alpha, double* h_toi,
+                         void* stream);
+const char* b2gen_trajectory_last_error(void);
 const char* b2gen_shell_last_error(void);
 
 #ifdef __cplusplus

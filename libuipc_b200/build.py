@@ -48,6 +48,7 @@ SOLVE_SOURCES = [
     "b2s_abi.cu",
     "b2s_noalloc.cu",
     "b2s_partition.cu",
+    "b2s_trajectory.cu",
 ]
 
 

@@ -6,6 +6,7 @@
 // add_cloth_grid, add_affine_body), with the same triplet layout and the same
 // per-vertex gradient sum order, so the two agree to rounding (FMA
 // contraction on the device).
+#include "b2s_ccd.cuh"
 #include "b2s_fixed_reduce.cuh"
 #include "b2s_internal.cuh"
 
@@ -273,40 +274,6 @@ __global__ void k_contact_energy(int np, const int32_t* __restrict__ pairs, cons
             X[3 * i + a] = x[3 * (int64_t)V[i] + a];
     e[p] = b2el::contact_energy(X, is_ee[p], eps[p], dhat, k);
 }
-
-// time of impact of every pair over the step alpha dx (TOI_NONE: none): the
-// swept-AABB test expanded by dhat + thickness, then additive CCD
-constexpr double TOI_NONE = 1.1;
-__global__ void k_contact_toi(int np, const int32_t* __restrict__ pairs, const uint8_t* __restrict__ is_ee,
-                              const double* __restrict__ x, const double* __restrict__ dx, double alpha, double dhat,
-                              double xi, double eta, int max_iter, double* __restrict__ toi)
-{
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if(p >= np)
-        return;
-    const int32_t* V = pairs + 4ll * p;
-    double         X[12], dX[12];
-    for(int i = 0; i < 4; ++i)
-        for(int a = 0; a < 3; ++a)
-        {
-            X[3 * i + a]  = x[3 * (int64_t)V[i] + a];
-            dX[3 * i + a] = alpha * dx[3 * (int64_t)V[i] + a];
-        }
-    double    t  = TOI_NONE;
-    const int ee = is_ee[p];
-    if(b2el::ccd_broadphase(X, dX, ee, dhat + xi))
-    {
-        double tt = TOI_NONE;
-        if(b2el::accd_pair(X, dX, ee, eta, xi, max_iter, TOI_NONE, &tt))
-            t = tt;
-    }
-    toi[p] = t;
-}
-
-// the trajectory filter's constants (simplex_trajectory_filter.cu:76, the
-// ipc constitution's toi safety margin; lbvh_simplex_trajectory_filter.cu:18)
-constexpr double CCD_ETA      = 0.1;
-constexpr int    CCD_MAX_ITER = 1000;
 
 void fail(const char* msg) { throw b2s::Error(B2S_ERR_ARGUMENT, msg); }
 
@@ -695,13 +662,13 @@ int b2gen_contacts_toi(b2gen_contacts* c, const double* d_x, const double* d_dx,
             cudaStream_t st = static_cast<cudaStream_t>(stream);
             c->terms.resize(c->np);
             c->result.resize(1);
-            k_contact_toi<<<grid_of(c->np), SHELL_BLOCK, 0, st>>>(c->np, c->pairs.data(), c->is_ee.data(), d_x,
-                                                                   d_dx, alpha, c->dhat, 0.0, CCD_ETA, CCD_MAX_ITER,
+            b2s::k_contact_toi<<<grid_of(c->np), SHELL_BLOCK, 0, st>>>(c->np, c->pairs.data(), c->is_ee.data(), d_x,
+                                                                   d_dx, alpha, c->dhat, 0.0, b2s::CCD_ETA, b2s::CCD_MAX_ITER,
                                                                    c->terms.data());
             B2S_CHECK_LAUNCH();
             b2s::k_fixed_reduce<<<1, b2s::SUM_THREADS, 0, st>>>(c->np, c->terms.data(), 1, c->result.data());
             B2S_CHECK_LAUNCH();
-            double toi = TOI_NONE;
+            double toi = b2s::TOI_NONE;
             B2S_CUDA(cudaMemcpyAsync(&toi, c->result.data(), sizeof(double), cudaMemcpyDeviceToHost, st));
             B2S_CUDA(cudaStreamSynchronize(st));
             *h_toi = toi < 1.0 ? toi : 1.0;

@@ -45,8 +45,9 @@
 // contact_grad_hess is compiled as a device function of its own: inlined into
 // the contact kernel (CUDA 12.9, NVVM at -O3), its point-edge, point-point
 // and edge-edge branches came out wrong (correct at NVVM -O1, or not
-// inlined); the GPU test compares every type with the host build
-#define B2_HD_NOINLINE __host__ __device__ __noinline__
+// inlined); the GPU test compares every type with the host build (static:
+// one copy per translation unit that includes this header)
+#define B2_HD_NOINLINE static __host__ __device__ __noinline__
 #else
 #define B2_HD inline
 #define B2_HD_NOINLINE inline

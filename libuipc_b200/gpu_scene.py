@@ -77,6 +77,19 @@ def _lib():
         lib.b2gen_contacts_energy.restype = C.c_int
         lib.b2gen_contacts_toi.argtypes = [vp, vp, vp, C.c_double, C.POINTER(C.c_double), vp]
         lib.b2gen_contacts_toi.restype = C.c_int
+        lib.b2gen_trajectory_create.argtypes = [C.c_int, i32, i32, vp, i32, vp, i32, vp, C.c_double, C.c_double,
+                                                C.POINTER(vp)]
+        lib.b2gen_trajectory_create.restype = C.c_int
+        lib.b2gen_trajectory_destroy.argtypes = [vp]
+        lib.b2gen_trajectory_destroy.restype = C.c_int
+        lib.b2gen_trajectory_detect.argtypes = [vp, vp, vp, C.c_double, vp, vp]
+        lib.b2gen_trajectory_detect.restype = C.c_int
+        lib.b2gen_trajectory_pairs.argtypes = [vp, vp, vp]
+        lib.b2gen_trajectory_pairs.restype = C.c_int
+        lib.b2gen_trajectory_toi.argtypes = [vp, vp, vp, C.c_double, C.POINTER(C.c_double), vp]
+        lib.b2gen_trajectory_toi.restype = C.c_int
+        lib.b2gen_trajectory_last_error.argtypes = []
+        lib.b2gen_trajectory_last_error.restype = C.c_char_p
         lib.b2gen_shell_last_error.argtypes = []
         lib.b2gen_shell_last_error.restype = C.c_char_p
         lib._b2gen_declared = True
@@ -328,6 +341,85 @@ class GpuContacts:
     def close(self):
         if self.h:
             _lib().b2gen_contacts_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tet_surface(tets):
+    """Boundary of a tet mesh (host): the triangles that belong to one tet
+    only [m, 3], their edges [e, 2] (each once, smaller id first) and their
+    vertices [v], all sorted."""
+    T = np.asarray(tets, dtype=np.int64).reshape(-1, 4)
+    faces = np.concatenate([T[:, [0, 1, 2]], T[:, [0, 1, 3]], T[:, [0, 2, 3]], T[:, [1, 2, 3]]])
+    key = np.sort(faces, axis=1)
+    uniq, idx, cnt = np.unique(key, axis=0, return_index=True, return_counts=True)
+    tris = faces[np.sort(idx[cnt == 1])]
+    e = np.sort(np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [0, 2]]]), axis=1)
+    edges = np.unique(e, axis=0)
+    verts = np.unique(tris)
+    return tris.astype(np.int32), edges.astype(np.int32), verts.astype(np.int32)
+
+
+class GpuTrajectory:
+    """The line search's trajectory filter over a surface on the device:
+    candidate point-triangle / edge-edge pairs of the swept step (a hashed
+    uniform grid of cell size ``cell``, pairs within ``dhat``) and the
+    smallest time of impact over them (additive CCD)."""
+
+    def __init__(self, n_verts, surf_verts, surf_edges, surf_tris, dhat, cell, device):
+        V = np.ascontiguousarray(surf_verts, dtype=np.int32).reshape(-1)
+        E = np.ascontiguousarray(surf_edges, dtype=np.int32).reshape(-1, 2)
+        T = np.ascontiguousarray(surf_tris, dtype=np.int32).reshape(-1, 3)
+        lib = _lib()
+        self.h = C.c_void_p()
+        rc = lib.b2gen_trajectory_create(device.index or 0, int(n_verts), V.size, V.ctypes.data, E.shape[0],
+                                         E.ctypes.data, T.shape[0], T.ctypes.data, float(dhat), float(cell),
+                                         C.byref(self.h))
+        if rc != 0:
+            raise RuntimeError("b2gen_trajectory_create: " + lib.b2gen_trajectory_last_error().decode())
+        self.dev = device
+
+    def _stream(self, stream):
+        import torch
+
+        return stream if stream is not None else torch.cuda.current_stream(self.dev).cuda_stream
+
+    def detect(self, x, dx, alpha: float = 1.0, stream=None):
+        """Candidate pairs [n, 4] and is_ee [n] (point-triangle first) of the
+        move alpha dx from x."""
+        lib = _lib()
+        counts = np.zeros(2, np.int64)
+        rc = lib.b2gen_trajectory_detect(self.h, x.contiguous().data_ptr(), dx.contiguous().data_ptr(), float(alpha),
+                                         counts.ctypes.data, self._stream(stream))
+        if rc != 0:
+            raise RuntimeError("b2gen_trajectory_detect: " + lib.b2gen_trajectory_last_error().decode())
+        n = int(counts.sum())
+        pairs = np.zeros((max(n, 1), 4), np.int32)
+        is_ee = np.zeros(max(n, 1), np.uint8)
+        rc = lib.b2gen_trajectory_pairs(self.h, pairs.ctypes.data, is_ee.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("b2gen_trajectory_pairs: " + lib.b2gen_trajectory_last_error().decode())
+        return pairs[:n], is_ee[:n]
+
+    def toi(self, x, dx, alpha: float = 1.0, stream=None) -> float:
+        """Largest fraction (<= 1) of the move alpha dx from x before a surface
+        pair comes into contact."""
+        lib = _lib()
+        t = C.c_double()
+        rc = lib.b2gen_trajectory_toi(self.h, x.contiguous().data_ptr(), dx.contiguous().data_ptr(), float(alpha),
+                                      C.byref(t), self._stream(stream))
+        if rc != 0:
+            raise RuntimeError("b2gen_trajectory_toi: " + lib.b2gen_trajectory_last_error().decode())
+        return float(t.value)
+
+    def close(self):
+        if self.h:
+            _lib().b2gen_trajectory_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

@@ -16,7 +16,10 @@ against rounding-level energy increases from a tiny d. With ``contacts`` (a
 vertices) the energy adds the pairs' barrier and the step is also capped by
 the pairs' continuous collision detection (the simplex trajectory filter:
 additive CCD per pair, min(1, the smallest time of impact)); the candidate
-pairs are the caller's.
+pairs are the caller's. With ``trajectory`` (a `gpu_scene.GpuTrajectory` over
+the mesh's surface) the candidates of the step are found on the device first
+(a hashed uniform grid in place of the reference's BVH) and their smallest
+time of impact caps the step too.
 """
 from __future__ import annotations
 
@@ -34,7 +37,7 @@ class LineSearchResult:
 
 
 def line_search(mesh, x, d, x_tilde, dt: float, velocity_tol: float = 0.05, max_iter: int = 8,
-                contacts=None) -> LineSearchResult:
+                contacts=None, trajectory=None) -> LineSearchResult:
     """Move the device state ``x`` (in place) along ``d`` as the reference's
     line search does; returns the accepted step, the energies and whether the
     Newton iteration had converged."""
@@ -47,6 +50,8 @@ def line_search(mesh, x, d, x_tilde, dt: float, velocity_tol: float = 0.05, max_
     toi = mesh.ground_toi(x0, d)
     if contacts is not None:
         toi = min(toi, contacts.toi(x0, d))
+    if trajectory is not None:
+        toi = min(toi, trajectory.toi(x0, d))
     alpha = min(1.0, toi)
     converged = float(d.abs().max()) <= velocity_tol * dt and toi >= 1.0
     e = e0

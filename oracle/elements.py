@@ -442,6 +442,47 @@ def accd_toi(X, dX, is_ee, eta=0.1, thickness=0.0, max_iter=1000, toi_max=1.1):
             return False, toi_max
 
 
+def candidate_pairs(x, dx, alpha, surf_verts, surf_edges, surf_tris, dist):
+    """Every candidate pair of the step, by brute force: point-triangle
+    (surface vertex, surface triangle) and edge-edge (surface edges i < j)
+    whose swept boxes over x -> x + alpha dx are not apart by more than dist
+    on any axis (the far test of utils/distance/details/ccd.inl
+    point_triangle_ccd_broadphase / edge_edge_ccd_broadphase), pairs sharing
+    a vertex excluded. Returns the set of (p, t0, t1, t2) and of
+    (a0, a1, b0, b1) tuples."""
+    x = np.asarray(x, dtype=np.float64).reshape(-1, 3)
+    y = x + alpha * np.asarray(dx, dtype=np.float64).reshape(-1, 3)
+    lo, hi = np.minimum(x, y), np.maximum(x, y)
+    V = np.asarray(surf_verts).reshape(-1)
+    E = np.asarray(surf_edges).reshape(-1, 2)
+    T = np.asarray(surf_tris).reshape(-1, 3)
+
+    def boxes(P):
+        return lo[P].min(axis=1), hi[P].max(axis=1)
+
+    def near(alo, ahi, blo, bhi):
+        far = ((alo[:, None, :] - bhi[None, :, :]) > dist) | ((blo[None, :, :] - ahi[:, None, :]) > dist)
+        return ~far.any(axis=2)
+
+    pt = set()
+    if len(V) and len(T):
+        tlo, thi = boxes(T)
+        ok = near(lo[V], hi[V], tlo, thi)
+        for i, j in zip(*np.nonzero(ok)):
+            v, t = int(V[i]), tuple(int(c) for c in T[j])
+            if v not in t:
+                pt.add((v,) + t)
+    ee = set()
+    if len(E) > 1:
+        elo, ehi = boxes(E)
+        ok = near(elo, ehi, elo, ehi)
+        for i, j in zip(*np.nonzero(np.triu(ok, 1))):
+            a, b = tuple(int(c) for c in E[i]), tuple(int(c) for c in E[j])
+            if not set(a) & set(b):
+                ee.add(a + b)
+    return pt, ee
+
+
 def pairs_toi(x, dx, pairs, is_ee, alpha, dhat, thickness=0.0, eta=0.1):
     """The trajectory filter's step bound over a candidate list: per pair the
     broadphase (expanded by dhat + thickness) and the additive CCD of

@@ -45,7 +45,7 @@ def test_generator_symbols_exported():
     from libuipc_b200 import _abi
 
     declared = _abi.header_symbols(os.path.join(ROOT, "include", "b200gen.h"), prefix="b2gen_")
-    assert len(declared) == 22
+    assert len(declared) == 28
     out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True).stdout
     exported = {l.split()[-1] for l in out.splitlines() if " T " in l}
     assert set(declared) <= exported

@@ -186,3 +186,54 @@ def test_line_search_cut_by_contact_pairs(cuda):
     finally:
         C.close()
         mesh.close()
+
+
+def test_trajectory_candidates_against_brute_force(cuda):
+    """The device's candidate detection (hashed uniform grid) on the whole
+    surface of two stacked cubes, the upper one moving down by twice its lift
+    and a little sideways: exactly the oracle's brute-force set of
+    point-triangle and edge-edge pairs within dhat over the swept step (no
+    pair twice, the same order on a second call); the time of impact over
+    them equal to the oracle's narrow phase over the brute-force set; the
+    line search with the filter cut there."""
+    from libuipc_b200.gpu_scene import GpuTrajectory, tet_surface
+    from libuipc_b200.newton import line_search
+    from oracle import elements as OE
+
+    pos, tets, c, ground, ground_y, _, _, n, mesh = _two_cubes(cuda)
+    tris, edges, verts = tet_surface(tets)
+    rng = np.random.default_rng(5)
+    d = np.zeros_like(pos)
+    d[n:, 1] = -2.0 * 2e-3
+    d[n:, [0, 2]] = 1e-3 * rng.standard_normal(2)
+    dist = c["dhat"]
+    cell = float(np.linalg.norm(pos[edges[:, 0]] - pos[edges[:, 1]], axis=1).mean())
+    T = GpuTrajectory(len(pos), verts, edges, tris, dist, cell, cuda)
+    try:
+        x, dd = to_dev(pos.ravel().copy(), cuda), to_dev(d.ravel(), cuda)
+        for alpha in (1.0, 0.5):
+            P, E = T.detect(x, dd, alpha)
+            ref_pt, ref_ee = OE.candidate_pairs(pos, d, alpha, verts, edges, tris, dist)
+            got_pt = [tuple(int(v) for v in p) for p, e in zip(P, E) if not e]
+            got_ee = [tuple(int(v) for v in p) for p, e in zip(P, E) if e]
+            assert len(set(got_pt)) == len(got_pt) and len(set(got_ee)) == len(got_ee)
+            assert set(got_pt) == ref_pt and set(got_ee) == ref_ee
+            assert len(ref_pt) > 50 and len(ref_ee) > 50
+            assert (E[:len(got_pt)] == 0).all()  # point-triangle first
+            P2, E2 = T.detect(x, dd, alpha)
+            assert np.array_equal(P, P2) and np.array_equal(E, E2)
+        ref = sorted(ref_pt) + sorted(ref_ee)  # alpha = 0.5 from the loop above
+        t_ref = OE.pairs_toi(pos, d, ref, [0] * len(ref_pt) + [1] * len(ref_ee), 0.5, dist)
+        t_dev = T.toi(x, dd, alpha=0.5)
+        assert t_ref < 1.0 and abs(t_dev - t_ref) <= 1e-9 * t_ref
+        xt = to_dev((pos + d).ravel().copy(), cuda)
+        r = line_search(mesh, x, dd, xt, c["dt"], trajectory=T)
+        assert r.alpha <= r.toi_alpha < 1.0
+        xa = x.cpu().numpy().reshape(-1, 3)
+        for p in ref_pt:
+            assert OE._pair_d2(xa[list(p)], False) > 0.0
+        for p in ref_ee:
+            assert OE._pair_d2(xa[list(p)], True) > 0.0
+    finally:
+        T.close()
+        mesh.close()

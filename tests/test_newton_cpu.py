@@ -160,3 +160,43 @@ def test_ccd_no_hit_when_the_step_stops_short():
     assert OE.pairs_toi(X, dX, [[0, 1, 2, 3]], [False], 1.0, dhat=1e-3) == 1.0
     # far apart: the swept boxes do not meet, whatever the CCD would say
     assert not OE.ccd_broadphase(X + [0, 5, 0], dX, False, 1e-3)
+
+
+def test_tet_surface_of_a_cube():
+    """The boundary of an n^3-cell tet cube: 2 triangles per face cell, every
+    boundary grid vertex, and every boundary edge shared by two boundary
+    triangles (a closed surface: V - E + F = 2)."""
+    from libuipc_b200 import scene
+    from libuipc_b200.gpu_scene import tet_surface
+
+    n = 3
+    s = scene.cube_on_ground(n, seed=0)
+    tris, edges, verts = tet_surface(s.tets)
+    assert len(tris) == 6 * 2 * n * n
+    assert len(verts) == (n + 1) ** 3 - (n - 1) ** 3
+    assert len(verts) - len(edges) + len(tris) == 2
+    e = np.sort(np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [0, 2]]]), axis=1)
+    _, cnt = np.unique(e, axis=0, return_counts=True)
+    assert (cnt == 2).all()
+
+
+def test_candidate_pairs_brute_force():
+    """The oracle's candidate set on a small case: a vertex over a triangle
+    within dist is a pair, farther is not, a pair sharing a vertex never is,
+    and crossing edges within dist are a pair in one orientation only."""
+    x = np.array([[0.2, 1e-3, 0.2], [0, 0, 0], [1, 0, 0], [0, 0, 1], [0.2, 5e-3, 0.2]], dtype=np.float64)
+    dx = np.zeros_like(x)
+    tris = np.array([[1, 2, 3]])
+    pt, ee = OE.candidate_pairs(x, dx, 1.0, [0, 4], np.zeros((0, 2), int), tris, 2e-3)
+    assert pt == {(0, 1, 2, 3)}
+    # moving the far vertex down brings it in
+    dx[4, 1] = -4e-3
+    pt, _ = OE.candidate_pairs(x, dx, 1.0, [0, 4], np.zeros((0, 2), int), tris, 2e-3)
+    assert pt == {(0, 1, 2, 3), (4, 1, 2, 3)}
+    # edges: (1, 2) and (0, 4) cross near x = 0.2; (1, 3) shares vertex 1 with (1, 2)
+    edges = np.array([[1, 2], [1, 3], [0, 4]])
+    y = x.copy()
+    y[0] = [0.2, 1e-3, -0.5]
+    y[4] = [0.2, 1e-3, 0.5]
+    _, ee = OE.candidate_pairs(y, np.zeros_like(y), 1.0, [], edges, np.zeros((0, 3), int), 2e-3)
+    assert ee == {(1, 2, 0, 4)}
