@@ -122,35 +122,131 @@ __global__ void k_prim_boxes(int32_t n, const int32_t* __restrict__ prim, const 
     cnt[i] = (hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
 }
 
-// exclusive scan of n int64 counts into off[0..n] (off[n] = total), one CTA:
-// each thread a contiguous chunk, then the chunk sums scanned in shared memory
-constexpr int SCAN_THREADS = 1024;
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_one(int64_t n, const int64_t* __restrict__ in,
-                                                           int64_t* __restrict__ off)
+// Exclusive scan of n int64 counts into off[0..n] (off[n] = the total), in
+// three passes: per tile of SCAN_TILE elements its sum (coalesced loads, block
+// reduction), the tile sums scanned by one CTA, each tile scanned in shared
+// memory from its carry.
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_PER     = 8;
+constexpr int SCAN_TILE    = SCAN_THREADS * SCAN_PER;
+
+__device__ __forceinline__ int64_t block_exclusive(int64_t v, int64_t* sh, int64_t* total)
 {
-    __shared__ int64_t part[SCAN_THREADS];
-    const int64_t      chunk = (n + SCAN_THREADS - 1) / SCAN_THREADS;
-    const int64_t      b = threadIdx.x * chunk, e = min(n, b + chunk);
-    int64_t            s = 0;
-    for(int64_t i = b; i < e; ++i)
-        s += in[i];
-    part[threadIdx.x] = s;
+    // inclusive warp scan, then the warps' totals
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int64_t   inc  = v;
+    for(int o = 1; o < 32; o <<= 1)
+    {
+        const int64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if(lane >= o)
+            inc += u;
+    }
+    if(lane == 31)
+        sh[w] = inc;
     __syncthreads();
-    for(int w = 1; w < SCAN_THREADS; w <<= 1)
+    if(threadIdx.x == 0)
     {
-        const int64_t add = threadIdx.x >= w ? part[threadIdx.x - w] : 0;
-        __syncthreads();
-        part[threadIdx.x] += add;
-        __syncthreads();
+        int64_t run = 0;
+        for(int k = 0; k < SCAN_THREADS / 32; ++k)
+        {
+            const int64_t t = sh[k];
+            sh[k]           = run;
+            run += t;
+        }
+        sh[SCAN_THREADS / 32] = run;
     }
-    int64_t run = part[threadIdx.x] - s;
-    for(int64_t i = b; i < e; ++i)
+    __syncthreads();
+    const int64_t ex = sh[w] + inc - v;
+    *total           = sh[SCAN_THREADS / 32];
+    __syncthreads();
+    return ex;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_tile_sums(int64_t n, const int64_t* __restrict__ in,
+                                                            int64_t* __restrict__ sums)
+{
+    __shared__ int64_t sh[SCAN_THREADS / 32 + 1];
+    const int64_t      base = (int64_t)blockIdx.x * SCAN_TILE;
+    int64_t            s    = 0;
+    for(int k = 0; k < SCAN_PER; ++k)
     {
-        off[i] = run;
-        run += in[i];
+        const int64_t i = base + k * SCAN_THREADS + threadIdx.x;
+        if(i < n)
+            s += in[i];
     }
-    if(threadIdx.x == SCAN_THREADS - 1)
-        off[n] = part[SCAN_THREADS - 1];
+    int64_t total = 0;
+    block_exclusive(s, sh, &total);
+    if(threadIdx.x == 0)
+        sums[blockIdx.x] = total;
+}
+
+// one CTA over the (few) tile sums: off[0..nt], off[nt] = total
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int64_t nt, const int64_t* __restrict__ sums,
+                                                            int64_t* __restrict__ off)
+{
+    __shared__ int64_t sh[SCAN_THREADS / 32 + 1];
+    int64_t            carry = 0;
+    for(int64_t b = 0; b < nt; b += SCAN_THREADS)
+    {
+        const int64_t i = b + threadIdx.x;
+        const int64_t v = i < nt ? sums[i] : 0;
+        int64_t       total;
+        const int64_t ex = block_exclusive(v, sh, &total);
+        if(i < nt)
+            off[i] = carry + ex;
+        carry += total;
+    }
+    if(threadIdx.x == 0)
+        off[nt] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_tile_scan(int64_t n, const int64_t* __restrict__ in,
+                                                            const int64_t* __restrict__ tile_off,
+                                                            int64_t* __restrict__ off)
+{
+    __shared__ int64_t tile[SCAN_TILE];
+    __shared__ int64_t sh[SCAN_THREADS / 32 + 1];
+    const int64_t      base = (int64_t)blockIdx.x * SCAN_TILE;
+    for(int k = 0; k < SCAN_PER; ++k)
+    {
+        const int64_t i              = base + k * SCAN_THREADS + threadIdx.x;
+        tile[k * SCAN_THREADS + threadIdx.x] = i < n ? in[i] : 0;
+    }
+    __syncthreads();
+    // each thread its SCAN_PER consecutive elements, then across the threads
+    int64_t s = 0;
+    for(int k = 0; k < SCAN_PER; ++k)
+        s += tile[threadIdx.x * SCAN_PER + k];
+    int64_t       total;
+    int64_t       run = tile_off[blockIdx.x] + block_exclusive(s, sh, &total);
+    for(int k = 0; k < SCAN_PER; ++k)
+    {
+        const int64_t v                  = tile[threadIdx.x * SCAN_PER + k];
+        tile[threadIdx.x * SCAN_PER + k] = run;
+        run += v;
+    }
+    __syncthreads();
+    for(int k = 0; k < SCAN_PER; ++k)
+    {
+        const int64_t i = base + k * SCAN_THREADS + threadIdx.x;
+        if(i < n)
+            off[i] = tile[k * SCAN_THREADS + threadIdx.x];
+    }
+    if(blockIdx.x == 0 && threadIdx.x == 0)
+        off[n] = tile_off[gridDim.x];
+}
+
+// off[0..n] = exclusive scan of in[0..n), off[n] the total (tmp: scratch)
+void scan_counts(int64_t n, const int64_t* in, int64_t* off, b2s::DBuf<int64_t>& tmp, cudaStream_t st)
+{
+    const int64_t nt = std::max<int64_t>((n + SCAN_TILE - 1) / SCAN_TILE, 1);
+    tmp.resize(2 * (size_t)nt + 1);
+    k_tile_sums<<<(unsigned)nt, SCAN_THREADS, 0, st>>>(n, in, tmp.data());
+    B2S_CHECK_LAUNCH();
+    k_scan_sums<<<1, SCAN_THREADS, 0, st>>>(nt, tmp.data(), tmp.data() + nt);
+    B2S_CHECK_LAUNCH();
+    k_tile_scan<<<(unsigned)nt, SCAN_THREADS, 0, st>>>(n, in, tmp.data() + nt, off);
+    B2S_CHECK_LAUNCH();
 }
 
 // every (bucket, primitive) entry of the primitives' cells
@@ -353,7 +449,7 @@ struct b2gen_trajectory
     int                      device = 0;
     // per detection
     b2s::DBuf<Box>           tbox, ebox;
-    b2s::DBuf<int64_t>       cnt, off, off_pt, off_ee, bstart, cursor;
+    b2s::DBuf<int64_t>       cnt, off, off_pt, off_ee, bstart, cursor, scan_tmp;
     b2s::DBuf<uint32_t>      ent_bucket;
     b2s::DBuf<int32_t>       ent_id, tsorted, esorted;
     b2s::DBuf<int64_t>       tstart, estart;
@@ -373,8 +469,7 @@ void build_grid(b2gen_trajectory* T, int32_t n, b2s::DBuf<Box>& box, b2s::DBuf<i
 {
     // cell counts were written by k_prim_boxes into T->cnt
     T->off.resize((size_t)n + 1);
-    k_scan_one<<<1, SCAN_THREADS, 0, st>>>(n, T->cnt.data(), T->off.data());
-    B2S_CHECK_LAUNCH();
+    scan_counts(n, T->cnt.data(), T->off.data(), T->scan_tmp, st);
     int64_t E = 0;
     B2S_CUDA(cudaMemcpyAsync(&E, T->off.data() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     B2S_CUDA(cudaStreamSynchronize(st));
@@ -399,8 +494,7 @@ void build_grid(b2gen_trajectory* T, int32_t n, b2s::DBuf<Box>& box, b2s::DBuf<i
         k_bucket_count<<<grid_of(E), TRAJ_BLOCK, 0, st>>>(E, T->ent_bucket.data(), T->bstart.data());
         B2S_CHECK_LAUNCH();
     }
-    k_scan_one<<<1, SCAN_THREADS, 0, st>>>(H, T->bstart.data(), start.data());
-    B2S_CHECK_LAUNCH();
+    scan_counts(H, T->bstart.data(), start.data(), T->scan_tmp, st);
     B2S_CUDA(cudaMemcpyAsync(T->cursor.data(), start.data(), sizeof(int64_t) * H, cudaMemcpyDeviceToDevice, st));
     if(E > 0)
     {
@@ -437,8 +531,7 @@ void detect(b2gen_trajectory* T, const double* d_x, const double* d_dx, double a
                                                                    T->st.data(), T->cnt.data(), nullptr, nullptr);
         B2S_CHECK_LAUNCH();
         T->off_pt.resize((size_t)T->nsv + 1);
-        k_scan_one<<<1, SCAN_THREADS, 0, st>>>(T->nsv, T->cnt.data(), T->off_pt.data());
-        B2S_CHECK_LAUNCH();
+        scan_counts(T->nsv, T->cnt.data(), T->off_pt.data(), T->scan_tmp, st);
         B2S_CUDA(cudaMemcpyAsync(&tot[0], T->off_pt.data() + T->nsv, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     }
     if(ee)
@@ -454,8 +547,7 @@ void detect(b2gen_trajectory* T, const double* d_x, const double* d_dx, double a
                                                                    nullptr, nullptr);
         B2S_CHECK_LAUNCH();
         T->off_ee.resize((size_t)T->nse + 1);
-        k_scan_one<<<1, SCAN_THREADS, 0, st>>>(T->nse, T->cnt.data(), T->off_ee.data());
-        B2S_CHECK_LAUNCH();
+        scan_counts(T->nse, T->cnt.data(), T->off_ee.data(), T->scan_tmp, st);
         B2S_CUDA(cudaMemcpyAsync(&tot[1], T->off_ee.data() + T->nse, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     }
     int err = 0;
