@@ -363,6 +363,53 @@ FULL_SCALE = dict(cells_x=30, cells_y=30, cells_z=30, n_cubes=10, cloth_n=512, b
                   seed=0)
 
 
+def trajectory_run(dev, cells: int = 40, n_cubes: int = 8, repeats: int = 5) -> dict:
+    """The line search's trajectory filter on the surface of the stacked cubes
+    (the headline's mesh): the stack falling 1 cm in the step (1 m/s over
+    dt = 0.01) with a 10 % spread and 0.1 mm of random relative motion;
+    candidate detection on the device (hashed uniform grid) + additive CCD
+    over every candidate, CUDA events around each call, median of `repeats`
+    after 3 warm-up calls."""
+    import numpy as np
+    import torch
+
+    from libuipc_b200 import scene
+    from libuipc_b200.gpu_scene import GpuTrajectory, tet_surface
+
+    s = scene.stacked_cubes(cells, n_cubes, seed=0)
+    tris, edges, verts = tet_surface(s.tets)
+    pos = s.positions
+    cell = float(np.linalg.norm(pos[edges[:, 0]] - pos[edges[:, 1]], axis=1).mean())
+    rng = np.random.default_rng(0)
+    d = np.zeros_like(pos)
+    d[:, 1] = -1e-2 * (1 + 0.1 * rng.standard_normal(len(pos)))
+    d += 1e-4 * rng.standard_normal(d.shape)
+    x = torch.tensor(pos.ravel(), dtype=torch.float64, device=dev)
+    dd = torch.tensor(d.ravel(), dtype=torch.float64, device=dev)
+    T = GpuTrajectory(len(pos), verts, edges, tris, s.config["dhat"], cell, dev)
+    try:
+        _, is_ee = T.detect(x, dd)
+        for _ in range(3):
+            T.toi(x, dd)
+        torch.cuda.synchronize(dev)
+        times, toi = [], 1.0
+        for _ in range(repeats):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            toi = T.toi(x, dd)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            times.append(e0.elapsed_time(e1))
+    finally:
+        T.close()
+    return {"workload": f"surface of {n_cubes} x {cells}^3-cell tet cubes falling 1 cm in the step",
+            "surface_vertices": int(len(verts)), "surface_edges": int(len(edges)),
+            "surface_triangles": int(len(tris)), "cell": cell,
+            "pt_candidates": int((is_ee == 0).sum()), "ee_candidates": int((is_ee == 1).sum()),
+            "toi": toi, "ms": float(np.median(times)),
+            "timing": "detection + additive CCD per call, CUDA events, median of %d" % repeats}
+
+
 def full_scale_run(dev, n_systems: int = 4, scene_kw: dict | None = None) -> dict:
     """The full-scale case beside the headline, stepped: a 10 x 10 grid of
     30^3-cell tet cubes on the ground, a 512 x 512 cloth resting on them and
@@ -614,6 +661,8 @@ def main() -> None:
                     help="skip the 9.7 M-DoF cube grid + cloth + bodies case run beside the headline")
     ap.add_argument("--full-scale-systems", type=int, default=4,
                     help="Newton systems of the stepped full-scale run (about 8 s of host generation each)")
+    ap.add_argument("--no-trajectory", action="store_true",
+                    help="skip the line search's trajectory filter timing on the stack's surface")
     ap.add_argument("--no-bar", action="store_true",
                     help="skip the second run reported beside the headline: a 1.16 M-DoF twisted bar")
     args = ap.parse_args()
@@ -792,6 +841,13 @@ def main() -> None:
         except Exception as e:  # reported, not fatal
             learned_bar = {"error": str(e)}
 
+    trajectory = None
+    if rank == 0 and not args.no_trajectory:
+        try:
+            trajectory = trajectory_run(dev)
+        except Exception as e:  # reported, not fatal
+            trajectory = {"error": str(e)}
+
     bar = None
     if rank == 0 and not args.no_bar:
         try:
@@ -922,6 +978,7 @@ def main() -> None:
         "full_scale": full,
         "learned_bar": learned_bar,
         "configs": configs,
+        "trajectory_filter": trajectory,
     }
     solver.close()
     if rank == 0:
