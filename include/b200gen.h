@@ -169,6 +169,9 @@ int b2gen_contacts_toi(b2gen_contacts* c, const double* d_x, const double* d_dx,
  * b2gen_contacts_create layout (p, t0, t1, t2) / (a0, a1, b0, b1).
  * b2gen_trajectory_toi runs the detection and then the narrow phase of
  * b2gen_contacts_toi over the candidates: min(1, the smallest time of impact).
+ * A swept box that spans more than 64 cells on an axis (a primitive or a move
+ * far larger than the cell) or is not finite makes the call fail with
+ * B2S_ERR_ARGUMENT: choose the cell from the largest primitives of the surface.
  * Vertex ids index the state vectors (3 doubles per vertex). */
 typedef struct b2gen_trajectory b2gen_trajectory;
 int b2gen_trajectory_create(int device, int32_t n_verts, int32_t n_surf_verts, const int32_t* surf_verts,
