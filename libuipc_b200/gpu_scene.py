@@ -356,11 +356,16 @@ def tet_surface(tets):
     vertices [v], all sorted."""
     T = np.asarray(tets, dtype=np.int64).reshape(-1, 4)
     faces = np.concatenate([T[:, [0, 1, 2]], T[:, [0, 1, 3]], T[:, [0, 2, 3]], T[:, [1, 2, 3]]])
-    key = np.sort(faces, axis=1)
-    uniq, idx, cnt = np.unique(key, axis=0, return_index=True, return_counts=True)
+    f = np.sort(faces, axis=1)
+    n = int(T.max()) + 1 if T.size else 1
+    key = (f[:, 0] * n + f[:, 1]) * n + f[:, 2]  # one int64 per face (n^3 < 2^63 up to 2 M vertices)
+    if n >= (1 << 21):
+        raise ValueError("tet_surface: more than 2^21 vertices")
+    _, idx, cnt = np.unique(key, return_index=True, return_counts=True)
     tris = faces[np.sort(idx[cnt == 1])]
     e = np.sort(np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [0, 2]]]), axis=1)
-    edges = np.unique(e, axis=0)
+    ek = np.unique(e[:, 0] * n + e[:, 1])
+    edges = np.stack([ek // n, ek % n], axis=1)
     verts = np.unique(tris)
     return tris.astype(np.int32), edges.astype(np.int32), verts.astype(np.int32)
 
