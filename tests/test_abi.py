@@ -116,3 +116,37 @@ def test_partition_maps_unpartitioned_vertices():
     p2r, r2p = partition_maps(pid)
     assert p2r.size == 32
     assert list(r2p) == [0, -1, 1, 16, -1]
+
+
+def test_line_search_entry_points_validate_before_the_device():
+    """The contact and trajectory-filter constructors reject bad input (vertex
+    ids out of range, no pairs, a non-positive dhat or cell) with an argument
+    error before touching the device, so they behave the same without a GPU."""
+    from libuipc_b200 import _abi
+    from libuipc_b200.gpu_scene import _lib
+
+    lib = _lib()
+    h = C.c_void_p()
+    sv = np.array([0, 1, 2, 3], np.int32)
+    se = np.array([[0, 1], [2, 3]], np.int32)
+    st = np.array([[0, 1, 2]], np.int32)
+    rc = lib.b2gen_trajectory_create(0, 3, 4, sv.ctypes.data, 2, se.ctypes.data, 1, st.ctypes.data, 1e-3, 1e-2,
+                                     C.byref(h))
+    assert rc == _abi.B2S_ERR_ARGUMENT and b"out of range" in lib.b2gen_trajectory_last_error()
+    for dhat, cell in ((0.0, 1e-2), (1e-3, 0.0), (float("nan"), 1e-2)):
+        rc = lib.b2gen_trajectory_create(0, 4, 4, sv.ctypes.data, 2, se.ctypes.data, 1, st.ctypes.data, dhat, cell,
+                                         C.byref(h))
+        assert rc == _abi.B2S_ERR_ARGUMENT
+    pairs = np.array([[0, 1, 2, -1]], np.int32)
+    ee, eps = np.zeros(1, np.uint8), np.zeros(1)
+    rc = lib.b2gen_contacts_create(0, 1, pairs.ctypes.data, ee.ctypes.data, eps.ctypes.data, 1e-3, 1e6, 1e-2,
+                                   C.byref(h))
+    assert rc == _abi.B2S_ERR_ARGUMENT
+    rc = lib.b2gen_contacts_create(0, 0, pairs.ctypes.data, ee.ctypes.data, eps.ctypes.data, 1e-3, 1e6, 1e-2,
+                                   C.byref(h))
+    assert rc == _abi.B2S_ERR_ARGUMENT
+    for f in (lib.b2gen_contacts_energy, ):
+        assert f(None, None, None, None) == _abi.B2S_ERR_ARGUMENT
+    assert lib.b2gen_contacts_toi(None, None, None, 1.0, None, None) == _abi.B2S_ERR_ARGUMENT
+    assert lib.b2gen_trajectory_toi(None, None, None, 1.0, None, None) == _abi.B2S_ERR_ARGUMENT
+    assert lib.b2gen_trajectory_detect(None, None, None, 1.0, None, None) == _abi.B2S_ERR_ARGUMENT
