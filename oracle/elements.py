@@ -23,6 +23,13 @@ by tests to check it.
   (B'' + B'/(2D)) grad D grad D^T for PE / PP). The distance derivatives
   here are central differences of the closed-form distances in 50-digit
   arithmetic (mpmath).
+* The line search's contact term: the pairs' barrier energy, the trajectory
+  filter's far test of swept boxes (utils/distance/details/ccd.inl
+  *_ccd_broadphase), a brute-force candidate enumeration, and additive CCD
+  (ccd.inl point_triangle_ccd / edge_edge_ccd, the published conservative
+  advancement of Li et al. 2021) with the filter's constants
+  (collision_detection/filters/lbvh_simplex_trajectory_filter.cu:18-21,
+  876-1010; global_trajectory_filter.cu:111-134).
 """
 from __future__ import annotations
 
