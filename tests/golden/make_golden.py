@@ -14,9 +14,11 @@
   oracle/build_oracle.py) through the oracle's restatement of
   geometry::mesh_partition (seed 0, parts of at most 16 vertices). Needs the
   reference sources (the oracle build), so it is generated here and committed.
-* ``metis_cube10.npy``, ``metis_bar60.npy``: the same for the 10^3-cell
-  jittered cube (seed 0) and the 60x8x8-cell twisted bar (the reference
-  partitions of the graph partitioner's quality checks).
+* ``metis_cube10.npy``, ``metis_bar60.npy``, ``metis_stack3x8.npy``: the same
+  for the 10^3-cell jittered cube (seed 0), the 60x8x8-cell twisted bar and
+  three stacked 8^3-cell cubes (seed 0, the stack's first Newton system: a
+  mesh of several bodies joined by contact pairs) -- the reference partitions
+  of the graph partitioner's quality checks.
 """
 from __future__ import annotations
 
@@ -80,7 +82,8 @@ def main() -> None:
     pid = O.metis_mesh_partition(cube.adj_start, cube.adj_list)
     np.save(os.path.join(HERE, "metis_cube5.npy"), pid.astype(np.int32))
     for name, mesh in (("metis_cube10.npy", scene.cube_on_ground(10, seed=0)),
-                       ("metis_bar60.npy", scene.twisted_bar(60, 8, 8))):
+                       ("metis_bar60.npy", scene.twisted_bar(60, 8, 8)),
+                       ("metis_stack3x8.npy", scene.stacked_cubes(8, 3, seed=0))):
         pid = O.metis_mesh_partition(mesh.adj_start, mesh.adj_list)
         np.save(os.path.join(HERE, name), pid.astype(np.int16))
 

@@ -3,8 +3,9 @@ geometry::mesh_partition's METIS k-way call (src/geometry/mesh_partition.cpp:
 77-231), on the CPU: the reference's contract (ceil(n / 16) parts of at most
 16 vertices, contiguous non-empty ids, sequential blocks for point clouds,
 connected components for n <= 16), determinism, and quality against the
-reference's own METIS partitions (tests/golden/metis_*.npy): edge cut and the
-oracle's MAS-PCG iteration count within 15 % of METIS's."""
+reference's own METIS partitions (tests/golden/metis_*.npy: a cube, a bar, and
+three stacked cubes joined by contact pairs): edge cut and the oracle's MAS-PCG
+iteration count within 15 % of METIS's."""
 import os
 
 import numpy as np
@@ -64,6 +65,7 @@ def test_contract_and_determinism(request, mesh):
 @pytest.mark.parametrize("name, make", [
     ("metis_cube10.npy", lambda: scene.cube_on_ground(10, seed=0)),
     ("metis_bar60.npy", lambda: scene.twisted_bar(60, 8, 8)),
+    ("metis_stack3x8.npy", lambda: scene.stacked_cubes(8, 3, seed=0)),
 ])
 def test_quality_against_the_reference_metis(name, make):
     s = make()
