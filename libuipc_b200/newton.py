@@ -19,7 +19,9 @@ additive CCD per pair, min(1, the smallest time of impact)); the candidate
 pairs are the caller's. With ``trajectory`` (a `gpu_scene.GpuTrajectory` over
 the mesh's surface) the candidates of the step are found on the device first
 (a hashed uniform grid in place of the reference's BVH) and their smallest
-time of impact caps the step too.
+time of impact caps the step too. With ``cfl_dhat`` (the reference's
+cfl/enable, off by default there too) a step the time of impact cut is
+further capped to 0.5 dhat over the largest surface-vertex displacement.
 """
 from __future__ import annotations
 
@@ -36,8 +38,22 @@ class LineSearchResult:
     converged: bool
 
 
+def cfl_bound(d, dhat: float, verts=None) -> float:
+    """The contact CFL step bound: min(1, 0.5 dhat / max |d_v|) over the
+    surface vertices ``verts`` (every vertex when None), 1 when nothing moves
+    (contact_system/global_contact_manager.cu:500-541, config cfl/enable).
+    ``d`` is a torch tensor or a numpy array of 3 values per vertex."""
+    v = d.reshape(-1, 3)
+    if verts is not None:
+        v = v[verts]
+    if v.shape[0] == 0:
+        return 1.0
+    m = float((v * v).sum(1).max()) ** 0.5
+    return 1.0 if m == 0.0 else min(0.5 * dhat / m, 1.0)
+
+
 def line_search(mesh, x, d, x_tilde, dt: float, velocity_tol: float = 0.05, max_iter: int = 8,
-                contacts=None, trajectory=None) -> LineSearchResult:
+                contacts=None, trajectory=None, cfl_dhat=None, cfl_verts=None) -> LineSearchResult:
     """Move the device state ``x`` (in place) along ``d`` as the reference's
     line search does; returns the accepted step, the energies and whether the
     Newton iteration had converged."""
@@ -53,6 +69,10 @@ def line_search(mesh, x, d, x_tilde, dt: float, velocity_tol: float = 0.05, max_
     if trajectory is not None:
         toi = min(toi, trajectory.toi(x0, d))
     alpha = min(1.0, toi)
+    if cfl_dhat is not None and toi < 1.0:
+        # the reference's experimental CFL filter, only when a time of impact
+        # cut the step (engine/advance_ipc.cu:523-527)
+        alpha = min(alpha, cfl_bound(d, cfl_dhat, cfl_verts))
     converged = float(d.abs().max()) <= velocity_tol * dt and toi >= 1.0
     e = e0
     trials = 0

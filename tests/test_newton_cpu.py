@@ -40,6 +40,9 @@ class _Vec:
     def max(self):
         return float(self.a.max())
 
+    def reshape(self, *shape):
+        return self.a.reshape(*shape)
+
 
 class _Mesh:
     """E(x) = 1/2 |x - target|^2; the ground cuts at `ground_toi`."""
@@ -200,3 +203,23 @@ def test_candidate_pairs_brute_force():
     y[4] = [0.2, 1e-3, 0.5]
     _, ee = OE.candidate_pairs(y, np.zeros_like(y), 1.0, [], edges, np.zeros((0, 3), int), 2e-3)
     assert ee == {(1, 2, 0, 4)}
+
+
+def test_cfl_bound_and_its_use():
+    """0.5 dhat over the largest (surface) vertex displacement, capped at 1;
+    the line search applies it only when a time of impact cut the step."""
+    from libuipc_b200.newton import cfl_bound
+
+    d = np.array([[0.0, -2e-3, 0.0], [0.0, 0.0, 1e-3], [0.0, 0.0, 0.0]])
+    assert cfl_bound(d, 1e-3) == pytest.approx(0.25)
+    assert cfl_bound(d, 1e-3, verts=[1, 2]) == pytest.approx(0.5)
+    assert cfl_bound(d, 1e-2) == 1.0 and cfl_bound(np.zeros((2, 3)), 1e-3) == 1.0
+    x = _Vec(np.zeros(9))
+    dv = _Vec(d.ravel())
+    mesh = _Mesh(d.ravel())  # the energy falls all the way along d
+    r = line_search(mesh, x, dv, None, dt=1.0, velocity_tol=0.0, contacts=_Contacts(0.8, lambda a: 0.0),
+                    cfl_dhat=1e-3)
+    assert r.toi_alpha == 0.8 and r.alpha == pytest.approx(0.25)
+    r = line_search(mesh, _Vec(np.zeros(9)), dv, None, dt=1.0, velocity_tol=0.0,
+                    contacts=_Contacts(1.0, lambda a: 0.0), cfl_dhat=1e-3)
+    assert r.alpha == 1.0  # no cut by a time of impact: no CFL cap
