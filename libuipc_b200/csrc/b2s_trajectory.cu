@@ -29,7 +29,6 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
-#include <vector>
 
 namespace
 {
